@@ -1,0 +1,225 @@
+/*
+ * pcb200.h -- C ABI of libpcb200.so, the sm_100a kernels behind pyjuice_b200.
+ *
+ * Every entry point takes device pointers, sizes and a cudaStream_t (passed as
+ * void*), launches asynchronously on that stream and returns 0 on success or a
+ * negative PCB_E* code; pcb_last_error() then describes the failure. No entry point
+ * allocates device memory: every buffer, including workspaces, is owned by the
+ * caller. Index tables are int32 unless stated otherwise.
+ *
+ * Matrices of per-node values ("rows x batch") are row-major with leading
+ * dimension `ld` (>= B): value (row r, sample b) lives at base[r * ld + b].
+ *
+ * The reference (SimonHaepers/pyjuice) is Python + Triton. Each entry point below
+ * replaces the Triton launch(es) cited in its comment; paths are relative to the
+ * reference project root.
+ */
+#ifndef PCB200_H
+#define PCB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCB_OK 0
+#define PCB_E_ARG -1       /* bad size / pointer / unsupported configuration */
+#define PCB_E_LAUNCH -2    /* CUDA launch error */
+#define PCB_E_CUDA -3      /* other CUDA runtime error */
+
+/* One tile of an LSE contraction (sum forward / element flows). */
+typedef struct {
+    int32_t out_row;  /* first output row of the tile */
+    int32_t n_rows;   /* rows in the tile (<= tile height of the launch) */
+    int32_t k_off;    /* offset into krow[] / kw[] */
+    int32_t k_cnt;    /* number of contraction terms */
+    int32_t w_add;    /* added to kw[k] for tile row 0 */
+    int32_t aux_row;  /* element-flow epilogue: first element_mars row of the tile */
+} PcbLseTile;
+
+/* One tile of the sum-parameter-flow contraction (contraction over the batch). */
+typedef struct {
+    int32_t nid;      /* first node row of the tile */
+    int32_t n_rows;   /* nodes in the tile */
+    int32_t k_off;    /* offset into cids[] / pids[] / pfids[] of the tile's first child */
+    int32_t k_cnt;    /* children in the tile */
+    int32_t p_add;    /* index of the tile's first node within its block (added to pids / pfids) */
+} PcbPflowTile;
+
+/* Version of the library ABI (currently 1). */
+int pcb_version(void);
+
+/* Last error message of the calling host thread ("" if none). */
+const char* pcb_last_error(void);
+
+/* Number of SMs of the current device (for grid sizing on the host). */
+int pcb_num_sms(void);
+
+/*
+ * Fill rows [row0, row1) of a rows x ld matrix with `value` (all ld columns).
+ * Replaces the buffer initialisations of TensorCircuit.forward / backward
+ * (src/pyjuice/model/tensorcircuit.py:240-241, 394-395) for the rows that are read
+ * before being written (dummy rows).
+ */
+int pcb_fill_rows(float* mat, int64_t ld, int64_t row0, int64_t row1, float value, void* stream);
+
+/*
+ * Categorical input layer forward: node_mars[node_offset + n, b] =
+ *   log(params[s_pids[n] + data[vids[n] * data_ld + b]]) for n < num_nodes, b < B
+ * (NaN where the category is outside [0, ncats[n])). data is int64 [num_vars, data_ld].
+ * Replaces InputLayer._mars_kernel_template + Categorical.fw_mar_fn
+ * (src/pyjuice/layer/input_layer.py:1016-1054, src/pyjuice/nodes/distributions/categorical.py:83-91).
+ */
+int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params,
+                      const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, int32_t num_nodes,
+                      int32_t node_offset, float* node_mars, int64_t ld, int32_t B, void* stream);
+
+/*
+ * Categorical input layer backward (parameter flows), deterministic:
+ * param_flows[s_pfids[n] + k] += sum_{b : data[v, b] == k} node_flows[node_offset + n, b]
+ * for every node n of every variable group. Groups are runs of nodes over the same
+ * variable: group g covers nodes [grp_node0[g], grp_node0[g] + grp_count[g]) of
+ * variable grp_var[g], with grp_ncats[g] categories; samples whose category is outside
+ * [0, ncats) are skipped. logspace_flows: node flows hold log flows.
+ * Replaces InputLayer._flows_kernel_template + Categorical.bk_flow_fn
+ * (src/pyjuice/layer/input_layer.py:1098-1155, categorical.py:94-100), whose atomic
+ * scatter this replaces with a per-variable counting sort of the batch.
+ */
+int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,
+                      const int32_t* grp_var, const int32_t* grp_node0, const int32_t* grp_count,
+                      const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
+                      const int32_t* s_pfids, int32_t node_offset, float* param_flows,
+                      int32_t logspace_flows, void* stream);
+
+/*
+ * Categorical EM update of the source nodes (in FP64):
+ *   theta' = (1 - s) * theta + s * (f + pc / K) / (sum_k f + pc)
+ * (keep_zero_params: zero parameters stay zero and the normaliser excludes them).
+ * Replaces InputLayer._em_kernel_template + Categorical.{small,large}_ncats_em_fn
+ * (src/pyjuice/layer/input_layer.py:1275-1296, categorical.py:164-244).
+ */
+int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_pids, const int32_t* s_pfids,
+                     const int32_t* ncats, const int32_t* source_nids, int32_t num_source_nodes,
+                     double step_size, double pseudocount, int32_t keep_zero_params, void* stream);
+
+/*
+ * Sum of tied input-node flow slots into the source slot:
+ * param_flows[dst + i] = sum_j param_flows[srcs[j] + i], i < n.
+ * Replaces InputLayer._pflow_accum_kernel (src/pyjuice/layer/input_layer.py:1254-1272)
+ * and cum_par_flows_kernel (src/pyjuice/model/backend/parflow_fusing.py:81-99).
+ */
+int pcb_pflow_accum(float* param_flows, int64_t dst, int64_t n, const int64_t* srcs, int32_t nsrc, void* stream);
+
+/*
+ * Product layer, forward (accum=0): out[r0 + i, b] = sum_j in[c_j + i, b], or
+ * backward (accum=1): out[r0 + i, b] += sum_j in[c_j + i, b], where the block list
+ * gives for block g: r0 = blk_row[g], its children c_j = chs[blk_off[g] + j],
+ * j < blk_cnt[g] (zero entries are padding and skipped), and blk_size rows.
+ * logsumexp=1 combines in log space (logspace flows).
+ * Replaces ProdLayer._forward_backward_kernel_2d / _large
+ * (src/pyjuice/layer/prod_layer.py:398-555).
+ */
+int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int32_t B,
+                        const int32_t* blk_row, const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs,
+                        int32_t num_blocks, int32_t blk_size, int32_t accum, int32_t logsumexp, void* stream);
+
+/*
+ * Log-sum-exp contraction over tiles, FP32 FMA (plain) or BF16 tensor-core (prec=1):
+ *   acc[r, b] = sum_k W(k, r) * exp(src[krow[k], b] - m_b),  m_b = max_k src[krow[k], b]
+ *   W(k, r)   = params[kw[k] + w_add + r * w_stride]
+ * mode 0 (sum forward):    out[out_row + r, b] = log(acc) + m_b
+ * mode 1 (element flows):  out[out_row + r, b] = acc * exp(aux[aux_row + r, b] + m_b)
+ * mode 2 (element flows, unmodified node flows): as mode 1 with src = log(src) - src2.
+ * Replaces SumLayer._fw_triton_block_sparse_*_kernel, _fw_triton_sparse_kernel,
+ * _fw_triton_large_sparse_kernel (src/pyjuice/layer/sum_layer.py:454-1104) and
+ * _bk_triton_block_sparse_ele_kernel / _csmm2 / sparse element-flow kernels
+ * (sum_layer.py:1572-1889, 2466-2666).
+ */
+int pcb_lse_contract(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
+                     const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t tile_rows,
+                     const int32_t* krow, const int32_t* kw, int32_t w_stride, int32_t mode, int32_t prec,
+                     void* stream);
+
+/*
+ * In place on rows [row0, row1) of node_flows: f <- (m == -inf) ? -inf : log(f) - m.
+ * Replaces SumLayer._bk_triton_modify_flow_kernel (src/pyjuice/layer/sum_layer.py:1355-1515).
+ */
+int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int32_t B,
+                     int64_t row0, int64_t row1, void* stream);
+
+/*
+ * Sum-layer parameter flows, contraction over the batch:
+ *   pf[pfids[k] + p_add + i] += params[pids[k] + p_add + i] * sum_b exp(lf[nid + i, b] - M_b) * exp(em[cids[k], b] + M_b)
+ * with lf = node_flows already in "log f - log m" form (modified=1) or computed as
+ * log(node_flows) - node_mars (modified=0), M_b the max over the tile's nodes.
+ * atomic=1 when flow slots are shared by tied nodes.
+ * Replaces SumLayer._bk_triton_block_sparse_par_kernel / _csmm2 / sparse par kernel
+ * (src/pyjuice/layer/sum_layer.py:2052-2282, 2795-2902).
+ */
+int pcb_sum_pflows(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld, int32_t B,
+                   const float* params, float* param_flows, const PcbPflowTile* tiles, int32_t num_tiles,
+                   const int32_t* cids, const int32_t* pids, const int32_t* pfids, int32_t modified, int32_t atomic,
+                   void* stream);
+
+/*
+ * Sum-parameter EM update, per node block (FP64 normalisation):
+ *   for node i < bs, child k < nch:   p = params[pbase + k * bs + i], f = pflows[pfbase + k * bs + i]
+ *   theta' = (1 - s) * p + s * (f + pc / nch) / (sum_k f + pc)
+ * keep_zero_params: zero parameters stay zero; the normaliser then counts pc / nch
+ * only for non-zero parameters and adds no extra pc.
+ * Replaces cum_pflow_kernel + em_par_update_kernel
+ * (src/pyjuice/model/backend/par_update.py:174-256).
+ */
+int pcb_sum_em(float* params, const float* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
+               const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks,
+               double step_size, double pseudocount, int32_t keep_zero_params, void* stream);
+
+/*
+ * Sum-parameter normalisation (FP64), same block table as pcb_sum_em:
+ *   theta' = (p + pc / nch) / (sum_k p + pc)
+ * Replaces cum_par_kernel + par_update_kernel (src/pyjuice/model/backend/normalize.py:13-68).
+ */
+int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const int32_t* blk_nch, const int32_t* blk_bs,
+                      int32_t num_blocks, double pseudocount, void* stream);
+
+/*
+ * Log-likelihood reduction in FP64: out[0] += sum_b lls[row * ld + b] for b < B.
+ * Dataset-level LL accumulation.
+ */
+int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double* out, void* stream);
+
+/*
+ * Ancestral sampling (replaces queries.sample: sample_sum_layer_kernel, count_prod_nch_kernel,
+ * sample_prod_layer_kernel and the Categorical sample kernel; src/pyjuice/queries/sample.py:38-474,
+ * src/pyjuice/layer/input_layer.py:1222-1249, categorical.py:137-161).
+ * Per sample s, nlist[s * cap_n + j] (j < ncnt[s]) are its active node ids and
+ * elist[s * cap_e + j] (j < ecnt[s]) its active element ids. Uniform draws are
+ * u(seed, id, s) = top 24 bits of SplitMix64(seed + ((id << 32) | s + 1) * 0x9E3779B97F4A7C15) / 2^24.
+ * *err is set to 1 on list overflow, 2 on an element outside the product group.
+ *
+ * pcb_sample_sum: nodes of the sum layer [lo, hi) (block size bs) choose the first child
+ * k with u < cumsum_k(params[kw[k] + i]) (the last non-zero child if rounding leaves none);
+ * the node's block is node2blk[(id - lo) / bs] in the forward tables (blk_nid, blk_koff,
+ * blk_kcnt, krow = child element ids, kw = parameter bases).
+ * pcb_sample_prod: active elements in [elo, ehi) append their children (chs[blk_off[g] + c] + i);
+ * elements of other product layers stay in the element list.
+ * pcb_sample_input: active input nodes in [lo, hi) draw category k = first k with
+ * u <= cumsum_k (0 if none) into samples[s * sld + vids[id - lo]].
+ */
+int pcb_sample_sum(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt, int32_t S, int32_t cap_n,
+                   int32_t cap_e, int32_t lo, int32_t hi, int32_t bs, const int32_t* node2blk, const int32_t* blk_nid,
+                   const int32_t* blk_koff, const int32_t* blk_kcnt, const int32_t* krow, const int32_t* kw,
+                   const float* params, uint64_t seed, int32_t* err, void* stream);
+int pcb_sample_prod(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt, int32_t S, int32_t cap_n,
+                    int32_t cap_e, int32_t elo, int32_t ehi, const int32_t* elem2blk, const int32_t* blk_row,
+                    const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs, int32_t* err, void* stream);
+int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
+                     const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, const float* params,
+                     int64_t* samples, int64_t sld, uint64_t seed, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCB200_H */

@@ -1,0 +1,15 @@
+"""pyjuice_b200: PyJuice's compiled-circuit hot path on hand-written sm_100a kernels.
+
+Same public API as the reference package for the circuit passes:
+``compile`` / ``TensorCircuit``, ``inputs`` / ``multiply`` / ``summate`` /
+``set_block_size``, ``distributions.Categorical``, ``structures.HCLT`` and
+``queries.sample``.
+"""
+
+from . import nodes, layer, model, structures, queries
+from .nodes import inputs, multiply, summate, set_block_size, distributions
+from .model import TensorCircuit, compile
+from .layer import InputLayer, ProdLayer, SumLayer
+
+__all__ = ["compile", "TensorCircuit", "inputs", "multiply", "summate", "set_block_size", "distributions",
+           "structures", "queries", "InputLayer", "ProdLayer", "SumLayer"]

@@ -1,0 +1,131 @@
+"""Loader and thin Python binding of ``libpcb200.so`` (the C ABI in ``include/pcb200.h``).
+
+The shared library is built in-tree by :func:`build` (nvcc, sm_100a) and loaded with
+``ctypes``. Every call passes raw device pointers, sizes and the current CUDA stream;
+a non-zero return status raises ``RuntimeError`` with the library's error message.
+There is no fallback: if the library is missing or a tensor is not on a CUDA device,
+the call fails.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import c_double, c_float, c_int32, c_int64, c_uint64, c_void_p
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpcb200.so")
+CSRC = os.path.join(_HERE, "csrc")
+SOURCES = ["capi_common.cu", "lse_contract.cu", "lse_contract_tc.cu", "prod_kernels.cu", "sum_pflows.cu",
+           "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-shared",
+              "-Xcompiler", "-fPIC"]
+
+_lib = None
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.sep not in cand or os.path.exists(cand)):
+            return cand
+    return "nvcc"
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile ``libpcb200.so`` for sm_100a if it is missing or older than its sources."""
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(_HERE, "..", "include", "pcb200.h")]
+    if not force and os.path.exists(LIB_PATH):
+        lib_m = os.path.getmtime(LIB_PATH)
+        if all(os.path.getmtime(d) <= lib_m for d in deps if os.path.exists(d)):
+            return LIB_PATH
+    tmp = LIB_PATH + ".tmp"
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + srcs
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("building libpcb200.so failed:\n" + res.stdout + res.stderr)
+    if verbose:
+        print(res.stdout + res.stderr)
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+class _LseTile(ctypes.Structure):
+    _fields_ = [("out_row", c_int32), ("n_rows", c_int32), ("k_off", c_int32), ("k_cnt", c_int32),
+                ("w_add", c_int32), ("aux_row", c_int32)]
+
+
+_SIGS = {
+    "pcb_version": ([], c_int32),
+    "pcb_last_error": ([], ctypes.c_char_p),
+    "pcb_num_sms": ([], c_int32),
+    "pcb_fill_rows": ([c_void_p, c_int64, c_int64, c_int64, c_float, c_void_p], c_int32),
+    "pcb_input_cat_fwd": ([c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
+                           c_int64, c_int32, c_void_p], c_int32),
+    "pcb_input_cat_bwd": ([c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                           c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_void_p], c_int32),
+    "pcb_input_cat_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double,
+                          c_int32, c_void_p], c_int32),
+    "pcb_pflow_accum": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),
+    "pcb_prod_gather_sum": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+                             c_int32, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_lse_contract": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
+                          c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_modify_flows": ([c_void_p, c_void_p, c_int64, c_int32, c_int64, c_int64, c_void_p], c_int32),
+    "pcb_sum_pflows": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
+                        c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_sum_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double, c_int32,
+                    c_void_p], c_int32),
+    "pcb_sum_normalize": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_void_p], c_int32),
+    "pcb_ll_sum_f64": ([c_void_p, c_int64, c_int32, c_int64, c_void_p, c_void_p], c_int32),
+    "pcb_sample_sum": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
+                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p,
+                        c_void_p], c_int32),
+    "pcb_sample_prod": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32,
+                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
+    "pcb_sample_input": ([c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
+                          c_void_p, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
+}
+
+EXPORTED_SYMBOLS = sorted(_SIGS.keys())
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run pyjuice_b200._native.build() (or __graft_entry__.build()) first")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args):
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        msg = lib.pcb_last_error().decode(errors="replace")
+        raise RuntimeError(f"{name} failed ({rc}): {msg}")
+    return rc
+
+
+def ptr(t) -> c_void_p:
+    """Device pointer of a CUDA tensor (None -> NULL)."""
+    if t is None:
+        return c_void_p(0)
+    if not t.is_cuda:
+        raise RuntimeError("pyjuice_b200 kernels need CUDA tensors (no CPU path)")
+    return c_void_p(t.data_ptr())
+
+
+def stream() -> c_void_p:
+    return c_void_p(torch.cuda.current_stream().cuda_stream)

@@ -1,0 +1,99 @@
+// Library-level entry points and error reporting.
+#include <cstdarg>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace pcb {
+
+static thread_local char g_last_error[512] = {0};
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        return set_error(PCB_E_LAUNCH, "%s: launch failed: %s", what, cudaGetErrorString(e));
+    }
+    return PCB_OK;
+}
+
+}  // namespace pcb
+
+namespace {
+
+__global__ void fill_rows_kernel(float* __restrict__ mat, int64_t n, float value) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) mat[i] = value;
+}
+
+__global__ void ll_sum_kernel(const float* __restrict__ lls, int B, double* __restrict__ out) {
+    __shared__ double part[8];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) s += (double)lls[b];
+    s = pcb::warp_sum(s);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < (blockDim.x >> 5)) ? part[threadIdx.x] : 0.0;
+        t = pcb::warp_sum(t);
+        if (threadIdx.x == 0) out[0] += t;
+    }
+}
+
+__global__ void pflow_accum_kernel(float* __restrict__ pf, int64_t dst, int64_t n, const int64_t* __restrict__ srcs,
+                                   int nsrc) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.f;
+    for (int j = 0; j < nsrc; ++j) s += pf[srcs[j] + i];
+    pf[dst + i] = s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pcb_version(void) { return 1; }
+
+const char* pcb_last_error(void) { return pcb::g_last_error; }
+
+int pcb_num_sms(void) {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "cudaGetDevice failed");
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return pcb::set_error(PCB_E_CUDA, "cudaDeviceGetAttribute failed");
+    return n;
+}
+
+int pcb_fill_rows(float* mat, int64_t ld, int64_t row0, int64_t row1, float value, void* stream) {
+    if (!mat || ld <= 0 || row0 < 0 || row1 < row0) return pcb::set_error(PCB_E_ARG, "pcb_fill_rows: bad arguments");
+    int64_t n = (row1 - row0) * ld;
+    if (n == 0) return PCB_OK;
+    int64_t blocks = pcb::cdiv(n, 256);
+    if (blocks > 4 * 148 * 8) blocks = 4 * 148 * 8;
+    fill_rows_kernel<<<(unsigned)blocks, 256, 0, pcb::as_stream(stream)>>>(mat + row0 * ld, n, value);
+    return pcb::check_launch("pcb_fill_rows");
+}
+
+int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double* out, void* stream) {
+    if (!lls || !out || B <= 0 || row < 0) return pcb::set_error(PCB_E_ARG, "pcb_ll_sum_f64: bad arguments");
+    ll_sum_kernel<<<1, 256, 0, pcb::as_stream(stream)>>>(lls + row * ld, B, out);
+    return pcb::check_launch("pcb_ll_sum_f64");
+}
+
+int pcb_pflow_accum(float* param_flows, int64_t dst, int64_t n, const int64_t* srcs, int32_t nsrc, void* stream) {
+    if (!param_flows || !srcs || n < 0 || nsrc <= 0) return pcb::set_error(PCB_E_ARG, "pcb_pflow_accum: bad arguments");
+    if (n == 0) return PCB_OK;
+    pflow_accum_kernel<<<(unsigned)pcb::cdiv(n, 256), 256, 0, pcb::as_stream(stream)>>>(param_flows, dst, n, srcs, nsrc);
+    return pcb::check_launch("pcb_pflow_accum");
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Shared helpers of the libpcb200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cmath>
+
+#include "../../include/pcb200.h"
+
+namespace pcb {
+
+// Records a message as the calling thread's last error and returns `code`.
+int set_error(int code, const char* fmt, ...);
+
+// Checks the launch that was just issued; returns PCB_OK or PCB_E_LAUNCH.
+int check_launch(const char* what);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+__device__ __forceinline__ float neg_inf() { return -INFINITY; }
+
+// 4 consecutive samples of row `row`: vectorised when the row start is 16-byte aligned
+// and all 4 samples are in range, scalar (with `fill` beyond B) otherwise.
+__device__ __forceinline__ float4 load4(const float* __restrict__ base, int64_t row, int64_t ld, int b, int B,
+                                        bool vec, float fill) {
+    const float* p = base + row * ld + b;
+    if (vec && b + 3 < B) {
+        return __ldg(reinterpret_cast<const float4*>(p));
+    }
+    float4 v;
+    v.x = (b + 0 < B) ? __ldg(p + 0) : fill;
+    v.y = (b + 1 < B) ? __ldg(p + 1) : fill;
+    v.z = (b + 2 < B) ? __ldg(p + 2) : fill;
+    v.w = (b + 3 < B) ? __ldg(p + 3) : fill;
+    return v;
+}
+
+__device__ __forceinline__ void store4(float* __restrict__ base, int64_t row, int64_t ld, int b, int B, bool vec,
+                                       float4 v) {
+    float* p = base + row * ld + b;
+    if (vec && b + 3 < B) {
+        *reinterpret_cast<float4*>(p) = v;
+        return;
+    }
+    if (b + 0 < B) p[0] = v.x;
+    if (b + 1 < B) p[1] = v.y;
+    if (b + 2 < B) p[2] = v.z;
+    if (b + 3 < B) p[3] = v.w;
+}
+
+__device__ __forceinline__ float get(const float4& v, int j) {
+    return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void set(float4& v, int j, float x) {
+    if (j == 0) v.x = x; else if (j == 1) v.y = x; else if (j == 2) v.z = x; else v.w = x;
+}
+
+// log(a) + log(b) combined in log space: log(exp(a) + exp(b)).
+__device__ __forceinline__ float logaddexp(float a, float b) {
+    if (a == -INFINITY) return b;
+    if (b == -INFINITY) return a;
+    float m = fmaxf(a, b);
+    return m + log1pf(expf(-fabsf(a - b)));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Vectorised access needs ld % 4 == 0 and a 16-byte aligned base.
+inline bool vec_ok(const void* p, int64_t ld) {
+    return (ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
+}
+
+}  // namespace pcb

@@ -1,0 +1,148 @@
+// EM parameter updates and sum-to-one normalisation, accumulated in FP64.
+//
+// A sum node block's parameters form a contiguous [nch x bs] slab (child-major, node
+// index fastest), and so do its parameter flows. One CTA owns one node block: it reads
+// the slab with coalesced row loads, reduces each column (node) in FP64 and rewrites
+// the slab. No atomics, no second pass over a per-node scratch buffer.
+#include "common.cuh"
+
+namespace {
+
+// Column sums of a [nch x bs] slab for columns [c0, c0 + 256/ROWS...]: thread layout
+// (row group rg, column c); partial sums in shared memory.
+template <bool EM, bool KEEP_ZERO>
+__global__ void __launch_bounds__(256)
+sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int64_t* __restrict__ pbase,
+              const int64_t* __restrict__ pfbase, const int* __restrict__ nchs, const int* __restrict__ bss,
+              double step, double pc) {
+    __shared__ double part[256];
+    const int g = blockIdx.x;
+    const int64_t pb = pbase[g];
+    const int64_t fb = EM ? pfbase[g] : 0;
+    const int nch = nchs[g];
+    const int bs = bss[g];
+    const int cols = bs < 256 ? bs : 256;       // columns handled per pass
+    const int rgs = 256 / cols;                 // row groups
+    const int c = threadIdx.x % cols;
+    const int rg = threadIdx.x / cols;
+    const double pcn = pc / (double)nch;
+
+    for (int c0 = 0; c0 < bs; c0 += cols) {
+        const int col = c0 + c;
+        double s = 0.0;
+        if (rg < rgs) {
+            for (int k = rg; k < nch; k += rgs) {
+                const int64_t off = (int64_t)k * bs + col;
+                if (EM) {
+                    const double f = (double)pflows[fb + off];
+                    if (KEEP_ZERO) {
+                        const float p = params[pb + off];
+                        s += (p < 1e-12f) ? 0.0 : (f + pcn);
+                    } else {
+                        s += f;
+                    }
+                } else {
+                    s += (double)params[pb + off];
+                }
+            }
+        }
+        part[threadIdx.x] = s;
+        __syncthreads();
+        double tot = 0.0;
+        for (int r = 0; r < rgs; ++r) tot += part[r * cols + c];
+        __syncthreads();
+        if (rg < rgs) {
+            for (int k = rg; k < nch; k += rgs) {
+                const int64_t off = (int64_t)k * bs + col;
+                const double p = (double)params[pb + off];
+                double np;
+                if (EM) {
+                    const double f = (double)pflows[fb + off];
+                    if (KEEP_ZERO) {
+                        np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / tot;
+                    } else {
+                        np = (1.0 - step) * p + step * (f + pcn) / (tot + pc);
+                    }
+                } else {
+                    np = (p + pcn) / (tot + pc);
+                }
+                params[pb + off] = (float)np;
+            }
+        }
+    }
+}
+
+// One warp per source input node, categories strided over the lanes.
+template <bool KEEP_ZERO>
+__global__ void __launch_bounds__(256)
+input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int* __restrict__ s_pids,
+                const int* __restrict__ s_pfids, const int* __restrict__ ncats, const int* __restrict__ source_nids,
+                int num_src, double step, double pc) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= num_src) return;
+    const int n = source_nids[w];
+    const int K = ncats[n];
+    const int64_t sp = s_pids[n];
+    const int64_t sf = s_pfids[n];
+    const double pcn = pc / (double)K;
+    double s = 0.0;
+    for (int k = lane; k < K; k += 32) {
+        const double f = (double)pflows[sf + k];
+        if (KEEP_ZERO) s += (params[sp + k] < 1e-12f) ? 0.0 : f + pcn;
+        else s += f;
+    }
+    s = pcb::warp_sum(s);
+    for (int k = lane; k < K; k += 32) {
+        const double p = (double)params[sp + k];
+        const double f = (double)pflows[sf + k];
+        double np;
+        if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / s;
+        else np = (1.0 - step) * p + step * (f + pcn) / (s + pc);
+        params[sp + k] = (float)np;
+    }
+}
+
+}  // namespace
+
+extern "C" int pcb_sum_em(float* params, const float* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
+                          const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks, double step_size,
+                          double pseudocount, int32_t keep_zero_params, void* stream) {
+    if (!params || !param_flows || !blk_pbase || !blk_pfbase || !blk_nch || !blk_bs || num_blocks < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_sum_em: bad arguments");
+    if (!(step_size > 0.0 && step_size <= 1.0)) return pcb::set_error(PCB_E_ARG, "pcb_sum_em: step_size must be in (0, 1]");
+    if (num_blocks == 0) return PCB_OK;
+    cudaStream_t s = pcb::as_stream(stream);
+    if (keep_zero_params)
+        sum_em_kernel<true, true><<<num_blocks, 256, 0, s>>>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, step_size, pseudocount);
+    else
+        sum_em_kernel<true, false><<<num_blocks, 256, 0, s>>>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, step_size, pseudocount);
+    return pcb::check_launch("pcb_sum_em");
+}
+
+extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const int32_t* blk_nch, const int32_t* blk_bs,
+                                 int32_t num_blocks, double pseudocount, void* stream) {
+    if (!params || !blk_pbase || !blk_nch || !blk_bs || num_blocks < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_sum_normalize: bad arguments");
+    if (num_blocks == 0) return PCB_OK;
+    sum_em_kernel<false, false><<<num_blocks, 256, 0, pcb::as_stream(stream)>>>(params, nullptr, blk_pbase, nullptr, blk_nch,
+                                                                                 blk_bs, 1.0, pseudocount);
+    return pcb::check_launch("pcb_sum_normalize");
+}
+
+extern "C" int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_pids, const int32_t* s_pfids,
+                                const int32_t* ncats, const int32_t* source_nids, int32_t num_source_nodes,
+                                double step_size, double pseudocount, int32_t keep_zero_params, void* stream) {
+    if (!params || !param_flows || !s_pids || !s_pfids || !ncats || !source_nids || num_source_nodes < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_em: bad arguments");
+    if (!(step_size > 0.0 && step_size <= 1.0))
+        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_em: step_size must be in (0, 1]");
+    if (num_source_nodes == 0) return PCB_OK;
+    const unsigned grid = (unsigned)pcb::cdiv((int64_t)num_source_nodes * 32, 256);
+    cudaStream_t s = pcb::as_stream(stream);
+    if (keep_zero_params)
+        input_em_kernel<true><<<grid, 256, 0, s>>>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes, step_size, pseudocount);
+    else
+        input_em_kernel<false><<<grid, 256, 0, s>>>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes, step_size, pseudocount);
+    return pcb::check_launch("pcb_input_cat_em");
+}

@@ -1,0 +1,145 @@
+// Categorical input layer: forward lookup and deterministic parameter-flow histogram.
+#include "common.cuh"
+
+namespace {
+
+// node_mars[node_offset + n, b] = log(params[s_pids[n] + x]) with x = data[vids[n], b].
+// A category outside [0, ncats) yields NaN (no out-of-range read).
+__global__ void __launch_bounds__(256)
+input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
+                     const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
+                     int node_offset, float* __restrict__ nm, int64_t ld, int B, int ngrp, int64_t total, bool vec) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int b = (int)(idx % ngrp) * 4;
+    const int n = (int)(idx / ngrp);
+    const int64_t v = __ldg(vids + n);
+    const int64_t sp = __ldg(s_pids + n);
+    const int K = __ldg(ncats + n);
+    float4 o;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float r = 0.f;
+        if (b + q < B) {
+            const int64_t x = __ldg(data + v * data_ld + b + q);
+            r = (x >= 0 && x < K) ? logf(__ldg(params + sp + x)) : NAN;
+        }
+        pcb::set(o, q, r);
+    }
+    pcb::store4(nm, (int64_t)node_offset + n, ld, b, B, vec, o);
+}
+
+// One CTA per variable group: stable counting sort of the batch by category (chunks of
+// up to CB samples), then one warp per node sums its flows per category in sample order
+// and adds the sums to the node's flow slots. Deterministic: no float atomics.
+__global__ void __launch_bounds__(256)
+input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ nf, int64_t ld,
+                     int B, const int* __restrict__ grp_var, const int* __restrict__ grp_node0,
+                     const int* __restrict__ grp_count, const int* __restrict__ grp_ncats,
+                     const int* __restrict__ s_pfids, int node_offset, float* __restrict__ pf, bool logspace, int CB) {
+    extern __shared__ int smem[];
+    const int g = blockIdx.x;
+    const int K = grp_ncats[g];
+    const int64_t v = grp_var[g];
+    const int node0 = grp_node0[g];
+    const int cnt = grp_count[g];
+    int* keys = smem;              // [CB]
+    int* perm = keys + CB;         // [CB]
+    int* seg = perm + CB;          // [K + 2]
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+
+    for (int c0 = 0; c0 < B; c0 += CB) {
+        const int nb = min(CB, B - c0);
+        for (int i = tid; i < K + 2; i += blockDim.x) seg[i] = 0;
+        __syncthreads();
+        for (int i = tid; i < nb; i += blockDim.x) {
+            const int64_t x = data[v * data_ld + c0 + i];
+            const int key = (x >= 0 && x < K) ? (int)x : K;  // out-of-range samples are dropped
+            keys[i] = key;
+            atomicAdd(&seg[key + 1], 1);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < K + 2; ++k) seg[k] += seg[k - 1];
+        }
+        __syncthreads();
+        // Stable scatter by warp 0: 32 samples at a time, ranks from lane matching.
+        if (warp == 0) {
+            for (int i0 = 0; i0 < nb; i0 += 32) {
+                const int i = i0 + lane;
+                const bool act = i < nb;
+                const int key = act ? keys[i] : -1;
+                const unsigned same = __match_any_sync(0xffffffffu, key);
+                const int rank = __popc(same & ((1u << lane) - 1u));
+                int pos = 0;
+                if (act) pos = seg[key] + rank;
+                __syncwarp();
+                if (act) perm[pos] = i;
+                // The highest lane of each key group advances the cursor.
+                const bool leader = act && ((same >> lane) == 1u);
+                __syncwarp();
+                if (leader) seg[key] += __popc(same);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // seg[k] now holds the end of category k; its start is the end of category k-1.
+        for (int n = warp; n < cnt; n += (blockDim.x >> 5)) {
+            const int64_t row = (int64_t)node_offset + node0 + n;
+            const float* frow = nf + row * ld + c0;
+            const int64_t sf = s_pfids[node0 + n];
+            for (int k = lane; k < K; k += 32) {
+                const int s = (k == 0) ? 0 : seg[k - 1];
+                const int e = seg[k];
+                if (e == s) continue;
+                float acc = 0.f;
+                for (int p = s; p < e; ++p) {
+                    const float f = __ldg(frow + perm[p]);
+                    acc += logspace ? __expf(f) : f;
+                }
+                pf[sf + k] += acc;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params, const int32_t* vids,
+                                 const int32_t* s_pids, const int32_t* ncats, int32_t num_nodes, int32_t node_offset,
+                                 float* node_mars, int64_t ld, int32_t B, void* stream) {
+    if (!data || !params || !vids || !s_pids || !ncats || !node_mars || B <= 0 || ld < B || data_ld < B || num_nodes < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: bad arguments");
+    if (num_nodes == 0) return PCB_OK;
+    const int ngrp = (int)pcb::cdiv(B, 4);
+    const int64_t total = (int64_t)num_nodes * ngrp;
+    const bool vec = pcb::vec_ok(node_mars, ld);
+    input_cat_fwd_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
+        data, data_ld, params, vids, s_pids, ncats, node_offset, node_mars, ld, B, ngrp, total, vec);
+    return pcb::check_launch("pcb_input_cat_fwd");
+}
+
+extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,
+                                 const int32_t* grp_var, const int32_t* grp_node0, const int32_t* grp_count,
+                                 const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
+                                 const int32_t* s_pfids, int32_t node_offset, float* param_flows,
+                                 int32_t logspace_flows, void* stream) {
+    if (!data || !node_flows || !grp_var || !grp_node0 || !grp_count || !grp_ncats || !s_pfids || !param_flows ||
+        B <= 0 || ld < B || data_ld < B || num_groups < 0 || max_ncats <= 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: bad arguments");
+    if (num_groups == 0) return PCB_OK;
+    const int CB = B < 8192 ? B : 8192;
+    const size_t smem = (size_t)(2 * CB + max_ncats + 2) * sizeof(int);
+    if (smem > 200 * 1024) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: too many categories (%d)", max_ncats);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(input_cat_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_input_cat_bwd: %s", cudaGetErrorString(e));
+    }
+    input_cat_bwd_kernel<<<num_groups, 256, smem, pcb::as_stream(stream)>>>(
+        data, data_ld, node_flows, ld, B, grp_var, grp_node0, grp_count, grp_ncats, s_pfids, node_offset, param_flows,
+        logspace_flows != 0, CB);
+    return pcb::check_launch("pcb_input_cat_bwd");
+}

@@ -1,0 +1,196 @@
+// BF16 tensor-core form of the log-sum-exp contraction (see lse_contract.cu).
+//
+// Same tiling and online-max scheme as the FP32 kernel; the contraction of each staged
+// chunk runs on the tensor cores: A = W (rows x K, rounded to bf16), B = exp(src - m)
+// (K x samples, rounded to bf16), FP32 accumulators. max / exp / log stay in FP32.
+// Tile: TM (16 or 32) rows x 128 samples, 8 warps, warp w owns samples [16w, 16w + 16).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int TB = 128;
+constexpr int KC = 64;
+constexpr int ES = TB + 4;  // padded shared-memory row strides (conflict-free fragment loads)
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int TM, int MODE>
+__global__ void __launch_bounds__(kThreads)
+lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
+                float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
+                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
+                int w_stride, bool vec) {
+    constexpr int MT = TM / 16;  // m16 tiles per warp
+    constexpr int WS = TM + 4;
+    __shared__ __align__(16) float sE[KC][ES];
+    __shared__ __align__(16) float sW[KC][WS];
+    __shared__ float sMax[TB];
+    __shared__ float sScale[TB];
+
+    const PcbLseTile t = tiles[blockIdx.x];
+    const int b0 = blockIdx.y * TB;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int g = lane >> 2;
+    const int q = lane & 3;
+    const int n0 = warp * 16;
+
+    for (int i = tid; i < TB; i += kThreads) sMax[i] = -INFINITY;
+
+    float acc[MT][2][4];
+#pragma unroll
+    for (int a = 0; a < MT; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+
+    for (int kc = 0; kc < t.k_cnt; kc += KC) {
+        const int n = min(KC, t.k_cnt - kc);
+        for (int idx = tid; idx < KC * (TB / 4); idx += kThreads) {
+            const int k = idx / (TB / 4);
+            const int c4 = idx % (TB / 4);
+            float4 v = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+            if (k < n) {
+                const int row = krow[t.k_off + kc + k];
+                v = pcb::load4(src, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
+                if (MODE == 2) {
+                    const float4 m = pcb::load4(src2, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float mm = pcb::get(m, j);
+                        pcb::set(v, j, (mm == -INFINITY) ? -INFINITY : logf(pcb::get(v, j)) - mm);
+                    }
+                }
+            }
+            *reinterpret_cast<float4*>(&sE[k][c4 * 4]) = v;
+        }
+        for (int idx = tid; idx < KC * TM; idx += kThreads) {
+            const int k = idx / TM;
+            const int r = idx % TM;
+            float w = 0.f;
+            if (k < n && r < t.n_rows) w = __ldg(params + (int64_t)kw[t.k_off + kc + k] + t.w_add + (int64_t)r * w_stride);
+            sW[k][r] = w;
+        }
+        __syncthreads();
+        for (int b = tid; b < TB; b += kThreads) {
+            float cm = -INFINITY;
+            for (int k = 0; k < n; ++k) cm = fmaxf(cm, sE[k][b]);
+            const float old = sMax[b];
+            const float nm = fmaxf(old, cm);
+            sScale[b] = (nm == -INFINITY) ? 1.f : __expf(old - nm);
+            sMax[b] = nm;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < KC * TB; idx += kThreads) {
+            const int k = idx / TB;
+            const int b = idx % TB;
+            const float m = sMax[b];
+            sE[k][b] = (m == -INFINITY || k >= n) ? 0.f : __expf(sE[k][b] - m);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            const float s0 = sScale[n0 + nt * 8 + 2 * q];
+            const float s1 = sScale[n0 + nt * 8 + 2 * q + 1];
+#pragma unroll
+            for (int a = 0; a < MT; ++a) {
+                acc[a][nt][0] *= s0;
+                acc[a][nt][1] *= s1;
+                acc[a][nt][2] *= s0;
+                acc[a][nt][3] *= s1;
+            }
+        }
+        const int kend = (n + 15) & ~15;
+        for (int k0 = 0; k0 < kend; k0 += 16) {
+            uint32_t bf[2][2];
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                const int col = n0 + nt * 8 + g;
+                bf[nt][0] = pack_bf16(sE[k0 + 2 * q][col], sE[k0 + 2 * q + 1][col]);
+                bf[nt][1] = pack_bf16(sE[k0 + 2 * q + 8][col], sE[k0 + 2 * q + 9][col]);
+            }
+#pragma unroll
+            for (int a = 0; a < MT; ++a) {
+                const int r0 = a * 16 + g;
+                const uint32_t a0 = pack_bf16(sW[k0 + 2 * q][r0], sW[k0 + 2 * q + 1][r0]);
+                const uint32_t a1 = pack_bf16(sW[k0 + 2 * q][r0 + 8], sW[k0 + 2 * q + 1][r0 + 8]);
+                const uint32_t a2 = pack_bf16(sW[k0 + 2 * q + 8][r0], sW[k0 + 2 * q + 9][r0]);
+                const uint32_t a3 = pack_bf16(sW[k0 + 2 * q + 8][r0 + 8], sW[k0 + 2 * q + 9][r0 + 8]);
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) mma_bf16(acc[a][nt], a0, a1, a2, a3, bf[nt][0], bf[nt][1]);
+            }
+        }
+        __syncthreads();
+    }
+
+#pragma unroll
+    for (int a = 0; a < MT; ++a) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int row = a * 16 + g + h * 8;
+            if (row >= t.n_rows) continue;
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int col = n0 + nt * 8 + 2 * q + j;
+                    const int b = b0 + col;
+                    if (b >= B) continue;
+                    const float m = sMax[col];
+                    const float v = acc[a][nt][h * 2 + j];
+                    float o;
+                    if (MODE == 0) {
+                        o = (m == -INFINITY) ? -INFINITY : logf(v) + m;
+                    } else {
+                        const float x = __ldg(aux + ((int64_t)t.aux_row + row) * ld + b);
+                        o = (m == -INFINITY) ? 0.f : v * __expf(x + m);
+                    }
+                    out[((int64_t)t.out_row + row) * ld + b] = o;
+                }
+            }
+        }
+    }
+}
+
+template <int TM>
+int launch(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B, const float* params,
+           const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw, int w_stride, int mode,
+           cudaStream_t s, bool vec) {
+    dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, TB));
+    if (mode == 0)
+        lse_bf16_kernel<TM, 0><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+    else if (mode == 1)
+        lse_bf16_kernel<TM, 1><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+    else
+        lse_bf16_kernel<TM, 2><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+    return pcb::check_launch("pcb_lse_contract(bf16)");
+}
+
+}  // namespace
+
+int pcb_lse_contract_bf16(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
+                          const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows,
+                          const int* krow, const int* kw, int w_stride, int mode, cudaStream_t s) {
+    const bool vec = pcb::vec_ok(src, ld) && (!src2 || pcb::vec_ok(src2, ld));
+    if (tile_rows == 32)
+        return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, mode, s, vec);
+    if (tile_rows == 16)
+        return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, mode, s, vec);
+    return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: the bf16 form needs tile_rows 16 or 32, got %d", tile_rows);
+}

@@ -1,0 +1,537 @@
+"""Compiled layers: input (Categorical), product and sum layers, and layer groups.
+
+Each layer keeps the reference's compiled tables (``partitioned_*``, ``_layer_nid_range``
+and friends, see ``compilation.py``) and, per CUDA device, a set of compact int32 kernel
+descriptors derived from them (tile lists and block lists without the power-of-2
+padding). ``forward`` / ``backward`` launch the sm_100a kernels of ``libpcb200.so``
+through ``_native``; there is no CPU path.
+
+Interfaces follow the reference's ``SumLayer`` (src/pyjuice/layer/sum_layer.py:30-384),
+``ProdLayer`` (src/pyjuice/layer/prod_layer.py:28-237), ``InputLayer``
+(src/pyjuice/layer/input_layer.py:32-724) and ``LayerGroup``
+(src/pyjuice/layer/layer_group.py:14-108).
+"""
+
+from __future__ import annotations
+
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from .compilation import compile_prod_layer, compile_sum_layer
+from .input_layer_compile import compile_input_layer
+
+
+def _i32(x) -> torch.Tensor:
+    a = np.asarray(x, dtype=np.int64)
+    if a.size and (a.max() >= 2 ** 31 or a.min() < -2 ** 31):
+        raise ValueError("index exceeds the int32 range of the kernel tables")
+    return torch.from_numpy(a.astype(np.int32))
+
+
+def _tile_rows(max_rows: int) -> int:
+    t = 1
+    while t < max_rows and t < 32:
+        t *= 2
+    return t
+
+
+class Layer:
+    propagation_alg_mapping = {"LL": 0, "MPE": 1, "GeneralLL": 2}
+
+    def __init__(self, nodes):
+        self.nodes = list(nodes)
+        self.scopes = []
+        for ns in self.nodes:
+            if ns.scope not in self.scopes:
+                self.scopes.append(ns.scope)
+        self.device = torch.device("cpu")
+        self._dev = {}
+
+    def is_sum(self):
+        return False
+
+    def is_prod(self):
+        return False
+
+    def is_input(self):
+        return False
+
+    def provided(self, name):
+        return hasattr(self, name) and getattr(self, name) is not None
+
+    def _desc(self, device: torch.device):
+        key = (device.type, device.index)
+        d = self._dev.get(key)
+        if d is None:
+            d = {k: (v.to(device) if isinstance(v, torch.Tensor) else v) for k, v in self._host_desc().items()}
+            self._dev[key] = d
+        return d
+
+    def _host_desc(self):
+        raise NotImplementedError()
+
+    def to(self, device):
+        device = torch.device(device)
+        for name in self._tensor_lists:
+            setattr(self, name, [t.to(device) for t in getattr(self, name)])
+        self.device = device
+        return self
+
+
+class SumLayer(Layer):
+    """A layer of sum node vectors with the same block size."""
+
+    _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
+                     "partitioned_chids", "partitioned_parids", "partitioned_parpids")
+
+    def __init__(self, nodes: Sequence, global_nid_start: int, global_pid_start: int, global_pfid_start: int,
+                 node2tiednodes: dict, layer_sparsity_tol: Optional[float] = None,
+                 max_num_partitions: Optional[int] = None, max_tied_ns_per_parflow_block: int = 8, **kwargs):
+        super().__init__(nodes)
+        if len(self.nodes) == 0 or len(set(self.nodes)) != len(self.nodes):
+            raise ValueError("a sum layer needs distinct node vectors")
+        self.block_size = self.nodes[0].block_size
+        for ns in self.nodes:
+            if ns.block_size != self.block_size:
+                raise ValueError("`block_size` of nodes in the same layer must be identical.")
+        c = compile_sum_layer(self.nodes, global_nid_start, global_pid_start, global_pfid_start, node2tiednodes,
+                              layer_sparsity_tol, max_num_partitions, max_tied_ns_per_parflow_block)
+        self.num_nodes = c["num_nodes"]
+        self.num_edges = c["num_edges"]
+        self._layer_nid_range = c["nid_range"]
+        self._layer_pid_range = c["pid_range"]
+        self._layer_pfid_range = c["pfid_range"]
+        self.partitioned_nids, self.partitioned_cids = c["nids"], c["cids"]
+        self.partitioned_pids, self.partitioned_pfids = c["pids"], c["pfids"]
+        self.partitioned_chids, self.partitioned_parids = c["chids"], c["parids"]
+        self.partitioned_parpids = c["parpids"]
+        self.cs_block_sizes = c["cs_block_sizes"]
+        self.num_fw_partitions = len(self.partitioned_nids)
+        self.num_bk_partitions = len(self.partitioned_chids)
+        self._has_tied = any(ns.is_tied() for ns in self.nodes)
+
+    @property
+    def num_parameters(self):
+        return self._layer_pid_range[1] - self._layer_pid_range[0]
+
+    @property
+    def num_param_flows(self):
+        return self._layer_pfid_range[1] - self._layer_pfid_range[0]
+
+    @property
+    def nid_range(self):
+        return self._layer_nid_range
+
+    def is_sum(self):
+        return True
+
+    # ---- kernel descriptors ----
+    def _host_desc(self):
+        bs = self.block_size
+        # forward blocks (shared with sampling and parameter flows)
+        blk_nid, blk_koff, blk_kcnt, krow, kw, kpf = [], [], [], [], [], []
+        off = 0
+        for nids, cids, pids, pfids in zip(self.partitioned_nids, self.partitioned_cids, self.partitioned_pids,
+                                           self.partitioned_pfids):
+            n_np, c_np, p_np, f_np = nids.cpu().numpy(), cids.cpu().numpy(), pids.cpu().numpy(), pfids.cpu().numpy()
+            for l in range(n_np.shape[0]):
+                real = c_np[l] != 0
+                cnt = int(real.sum())
+                if not np.all(real[:cnt]):
+                    raise RuntimeError("sum layer children are not a prefix of the padded row")
+                blk_nid.append(int(n_np[l]))
+                blk_koff.append(off)
+                blk_kcnt.append(cnt)
+                krow.append(c_np[l, :cnt])
+                kw.append(p_np[l, :cnt])
+                kpf.append(f_np[l, :cnt])
+                off += cnt
+        krow = np.concatenate(krow) if krow else np.zeros([0], np.int64)
+        kw = np.concatenate(kw) if kw else np.zeros([0], np.int64)
+        kpf = np.concatenate(kpf) if kpf else np.zeros([0], np.int64)
+        blk_nid = np.asarray(blk_nid, np.int64)
+        blk_koff = np.asarray(blk_koff, np.int64)
+        blk_kcnt = np.asarray(blk_kcnt, np.int64)
+
+        tm = _tile_rows(bs)
+        fw_tiles = []
+        for g in range(blk_nid.shape[0]):
+            for i0 in range(0, bs, tm):
+                fw_tiles.append((blk_nid[g] + i0, min(tm, bs - i0), blk_koff[g], blk_kcnt[g], i0, 0))
+        pf_tiles = []
+        for g in range(blk_nid.shape[0]):
+            for i0 in range(0, bs, 32):
+                for k0 in range(0, int(blk_kcnt[g]), 64):
+                    pf_tiles.append((blk_nid[g] + i0, min(32, bs - i0), blk_koff[g] + k0,
+                                     min(64, int(blk_kcnt[g]) - k0), i0))
+        node2blk = np.zeros([self.num_nodes // bs], np.int64)
+        node2blk[(blk_nid - self._layer_nid_range[0]) // bs] = np.arange(blk_nid.shape[0])
+
+        # element-flow tiles
+        ekrow, ekw, etiles = [], [], []
+        eoff = 0
+        max_cbs = max(self.cs_block_sizes) if self.cs_block_sizes else 1
+        etm = _tile_rows(max_cbs)
+        for chids, parids, parpids, cbs in zip(self.partitioned_chids, self.partitioned_parids,
+                                               self.partitioned_parpids, self.cs_block_sizes):
+            ch_np, pa_np, pp_np = chids.cpu().numpy(), parids.cpu().numpy(), parpids.cpu().numpy()
+            for l in range(ch_np.shape[0]):
+                real = pa_np[l] != 0
+                npar = int(real.sum())
+                par = pa_np[l, :npar]
+                ppar = pp_np[l, :npar]
+                rows = (par[:, None] + np.arange(bs)[None, :]).reshape(-1)
+                wts = (ppar[:, None] + np.arange(bs)[None, :]).reshape(-1)
+                ekrow.append(rows)
+                ekw.append(wts)
+                for j0 in range(0, cbs, etm):
+                    etiles.append((ch_np[l] + j0, min(etm, cbs - j0), eoff, rows.shape[0], j0 * bs, ch_np[l] + j0))
+                eoff += rows.shape[0]
+        ekrow = np.concatenate(ekrow) if ekrow else np.zeros([0], np.int64)
+        ekw = np.concatenate(ekw) if ekw else np.zeros([0], np.int64)
+
+        return dict(
+            fw_tiles=_i32(np.asarray(fw_tiles, np.int64).reshape(-1, 6)), fw_tm=tm,
+            krow=_i32(krow), kw=_i32(kw), kpf=_i32(kpf),
+            blk_nid=_i32(blk_nid), blk_koff=_i32(blk_koff), blk_kcnt=_i32(blk_kcnt), node2blk=_i32(node2blk),
+            min_kcnt=int(blk_kcnt.min()) if blk_kcnt.size else 0,
+            pf_tiles=_i32(np.asarray(pf_tiles, np.int64).reshape(-1, 5)),
+            el_tiles=_i32(np.asarray(etiles, np.int64).reshape(-1, 6)), el_tm=etm,
+            ekrow=_i32(ekrow), ekw=_i32(ekw),
+        )
+
+    # ---- forward / backward ----
+    def _use_bf16(self, d, B, force_use_bf16, force_use_fp32):
+        if force_use_bf16 and force_use_fp32:
+            raise ValueError("`force_use_bf16` and `force_use_fp32` are exclusive")
+        eligible = d["fw_tm"] >= 16
+        if force_use_bf16:
+            return eligible
+        if force_use_fp32:
+            return False
+        # Reference default: tensor-core contraction when the tiles are at least 16 wide
+        # (sum_layer.py:871-880).
+        return eligible and d["min_kcnt"] >= 16 and B >= 16
+
+    def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, params: torch.Tensor,
+                force_use_bf16: bool = False, force_use_fp32: bool = False, propagation_alg: str = "LL",
+                **kwargs) -> None:
+        if propagation_alg != "LL":
+            raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
+        if params.dim() != 1:
+            raise ValueError("Expecting a 1D `params`.")
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        if element_mars.stride(0) != ld or node_mars.stride(1) != 1 or element_mars.stride(1) != 1:
+            raise ValueError("node_mars and element_mars must share a row-major layout")
+        prec = 1 if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
+        t = d["fw_tiles"]
+        nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
+                 nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0,
+                 prec, nat.stream())
+
+    __call__ = forward
+
+    def backward(self, node_flows: torch.Tensor, element_flows: torch.Tensor, node_mars: torch.Tensor,
+                 element_mars: torch.Tensor, params: torch.Tensor, param_flows: Optional[torch.Tensor] = None,
+                 allow_modify_flows: bool = False, propagation_alg: str = "LL", logspace_flows: bool = False,
+                 negate_pflows: bool = False, accumulate_ch_flows: bool = False, allow_neg_flows: bool = False,
+                 force_use_fp32: bool = False, **kwargs) -> None:
+        if propagation_alg != "LL":
+            raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
+        if logspace_flows or negate_pflows or accumulate_ch_flows or allow_neg_flows:
+            raise NotImplementedError("logspace / negated / accumulated / negative flows are not supported by the CUDA path")
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        for t in (node_flows, element_flows, element_mars):
+            if t.stride(0) != ld or t.stride(1) != 1:
+                raise ValueError("node/element mars/flows must share a row-major layout")
+        if allow_modify_flows:
+            nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
+                     self._layer_nid_range[1], nat.stream())
+        # element flows
+        et = d["el_tiles"]
+        prec = 1 if (not force_use_fp32 and d["el_tm"] >= 16 and B >= 16) else 0
+        nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
+                 nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
+                 d["el_tm"], nat.ptr(d["ekrow"]), nat.ptr(d["ekw"]), self.block_size, 1 if allow_modify_flows else 2,
+                 prec, nat.stream())
+        # parameter flows
+        if param_flows is not None:
+            pt = d["pf_tiles"]
+            nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
+                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), nat.ptr(d["krow"]),
+                     nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0, 1 if self._has_tied else 0,
+                     nat.stream())
+
+    def __repr__(self):
+        return f"SumLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
+
+
+class ProdLayer(Layer):
+    """A layer of product node vectors."""
+
+    _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_u_cids", "partitioned_parids")
+
+    def __init__(self, nodes: Sequence, global_nid_start: Optional[int] = None,
+                 layer_sparsity_tol: Optional[float] = None, max_num_partitions: Optional[int] = None, **kwargs):
+        super().__init__(nodes)
+        if len(self.nodes) == 0 or len(set(self.nodes)) != len(self.nodes):
+            raise ValueError("a product layer needs distinct node vectors")
+        bs0 = self.nodes[0].block_size
+        if global_nid_start is None:
+            global_nid_start = bs0
+        c = compile_prod_layer(self.nodes, global_nid_start, layer_sparsity_tol, max_num_partitions)
+        self.use_block_sparse_edges = c["use_block_sparse"]
+        self.block_size = c["block_size"]
+        self.num_nodes = c["num_nodes"]
+        self.num_edges = c["num_edges"]
+        self._layer_nid_range = c["nid_range"]
+        self.partitioned_nids, self.partitioned_cids = c["nids"], c["cids"]
+        self.partitioned_u_cids, self.partitioned_parids = c["u_cids"], c["parids"]
+        self.num_fw_partitions = len(self.partitioned_nids)
+        self.num_bk_partitions = len(self.partitioned_u_cids)
+
+    def is_prod(self):
+        return True
+
+    def _host_desc(self):
+        def blocks(rows_list, chs_list):
+            row, off, cnt, chs = [], [], [], []
+            o = 0
+            for r, c in zip(rows_list, chs_list):
+                r_np, c_np = r.cpu().numpy(), c.cpu().numpy()
+                for l in range(r_np.shape[0]):
+                    real = c_np[l][c_np[l] != 0]
+                    row.append(int(r_np[l]))
+                    off.append(o)
+                    cnt.append(real.shape[0])
+                    chs.append(real)
+                    o += real.shape[0]
+            chs = np.concatenate(chs) if chs else np.zeros([0], np.int64)
+            return _i32(row), _i32(off), _i32(cnt), _i32(chs)
+
+        fr, fo, fc, fch = blocks(self.partitioned_nids, self.partitioned_cids)
+        br, bo, bc, bch = blocks(self.partitioned_u_cids, self.partitioned_parids)
+        lo, hi = self._layer_nid_range
+        elem2blk = np.full([hi - lo], -1, np.int64)
+        rows = fr.numpy().astype(np.int64)
+        for i in range(self.block_size):
+            elem2blk[rows + i - lo] = np.arange(rows.shape[0])
+        return dict(fw_row=fr, fw_off=fo, fw_cnt=fc, fw_chs=fch, bk_row=br, bk_off=bo, bk_cnt=bc, bk_chs=bch,
+                    elem2blk=_i32(elem2blk))
+
+    def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, _for_backward: bool = False, **kwargs):
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        if element_mars.stride(0) != ld:
+            raise ValueError("node_mars and element_mars must share a row-major layout")
+        nat.call("pcb_prod_gather_sum", nat.ptr(node_mars), nat.ptr(element_mars), ld, B, nat.ptr(d["fw_row"]),
+                 nat.ptr(d["fw_off"]), nat.ptr(d["fw_cnt"]), nat.ptr(d["fw_chs"]), d["fw_row"].size(0),
+                 self.block_size, 0, 0, nat.stream())
+
+    __call__ = forward
+
+    def backward(self, node_flows: torch.Tensor, element_flows: torch.Tensor, logspace_flows: bool = False, **kwargs):
+        d = self._desc(node_flows.device)
+        B = node_flows.size(1)
+        ld = node_flows.stride(0)
+        if element_flows.stride(0) != ld:
+            raise ValueError("node_flows and element_flows must share a row-major layout")
+        nat.call("pcb_prod_gather_sum", nat.ptr(element_flows), nat.ptr(node_flows), ld, B, nat.ptr(d["bk_row"]),
+                 nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]), d["bk_row"].size(0),
+                 self.block_size, 1, 1 if logspace_flows else 0, nat.stream())
+
+    def __repr__(self):
+        return f"ProdLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
+
+
+class InputLayer(Layer, torch.nn.Module):
+    """A layer of Categorical input node vectors."""
+
+    _tensor_lists = ()
+
+    def __init__(self, nodes: Sequence, cum_nodes: int = 0, pc_num_vars: int = 0,
+                 max_tied_ns_per_parflow_block: int = 4):
+        torch.nn.Module.__init__(self)
+        c = compile_input_layer(nodes, cum_nodes, max_tied_ns_per_parflow_block)
+        Layer.__init__(self, c["nodes"])
+        self.pc_num_vars = pc_num_vars
+        if c["signature"] != "Categorical":
+            raise NotImplementedError(f"input distribution {c['signature']} has no CUDA path")
+        if c["num_vars_per_node"] != 1:
+            raise NotImplementedError("multivariate input nodes have no CUDA path")
+        self._output_ind_range = c["nid_range"]
+        self.num_nodes = c["num_nodes"]
+        self.num_parameters = c["num_parameters"]
+        self.num_param_flows = c["num_param_flows"]
+        self.dist_signature = c["signature"]
+        self.num_vars_per_node = 1
+        for name in ("vids", "s_pids", "s_pfids", "metadata", "s_mids", "nids", "source_nids", "node_id2source_id"):
+            self.register_buffer(name, c[name])
+        self.tied2source_nids = c["tied2source_nids"]
+        self.params = torch.nn.Parameter(torch.empty([max(self.num_parameters, 1)], dtype=torch.float32),
+                                         requires_grad=False)
+        self.param_flows = None
+
+    def is_input(self):
+        return True
+
+    def get_dist(self):
+        return self.nodes[0].dist
+
+    def get_data_dtype(self):
+        return self.nodes[0].get_data_dtype()
+
+    def to(self, device):
+        torch.nn.Module.to(self, device)
+        self.device = torch.device(device)
+        if self.param_flows is not None:
+            self.param_flows = self.param_flows.to(device)
+        return self
+
+    def _host_desc(self):
+        vids = self.vids[:, 0].cpu().numpy()
+        ncats = self.metadata.cpu()[self.s_mids.cpu()].long().numpy()
+        # runs of consecutive nodes over the same variable
+        change = np.ones(vids.shape[0], dtype=bool)
+        change[1:] = vids[1:] != vids[:-1]
+        starts = np.nonzero(change)[0]
+        counts = np.diff(np.append(starts, vids.shape[0]))
+        tied = []
+        for dst, n, ch in self.tied2source_nids:
+            tied.append((int(dst), int(n), ch.clone().long()))
+        return dict(vids=_i32(vids), s_pids=_i32(self.s_pids.cpu()), s_pfids=_i32(self.s_pfids.cpu()),
+                    ncats=_i32(ncats), source_nids=_i32(self.source_nids.cpu()),
+                    grp_var=_i32(vids[starts]), grp_node0=_i32(starts), grp_count=_i32(counts),
+                    grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), tied=tied)
+
+    def _init_parameters(self, perturbation: float = 2.0):
+        p0 = 0
+        with torch.no_grad():
+            for ns in self.nodes:
+                if ns.is_tied():
+                    continue
+                p1 = p0 + ns.num_nodes * ns.dist.num_parameters()
+                src = ns._params if ns.has_params() else ns.init_parameters(perturbation=perturbation, ret_params=True)
+                self.params[p0:p1] = src.to(self.params.device, torch.float32)
+                p0 = p1
+
+    def init_param_flows(self, flows_memory: float = 1.0):
+        if self.param_flows is None or self.param_flows.device != self.params.device:
+            self.param_flows = torch.zeros([max(self.num_param_flows, 1)], device=self.params.device)
+        elif flows_memory < 1.0:
+            self.param_flows.mul_(flows_memory)
+
+    def forward(self, data: torch.Tensor, node_mars: torch.Tensor, params=None, missing_mask=None, **kwargs):
+        """``data`` is ``[num_vars, B]`` (int64), as passed by ``TensorCircuit.forward``."""
+        if params is not None or missing_mask is not None:
+            raise NotImplementedError("external input parameters / missing masks have no CUDA path")
+        d = self._desc(node_mars.device)
+        data = data.to(torch.long)
+        if data.stride(1) != 1:
+            data = data.contiguous()
+        B = node_mars.size(1)
+        nat.call("pcb_input_cat_fwd", nat.ptr(data), data.stride(0), nat.ptr(self.params), nat.ptr(d["vids"]),
+                 nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), self.num_nodes, self._output_ind_range[0],
+                 nat.ptr(node_mars), node_mars.stride(0), B, nat.stream())
+
+    __call__ = forward
+
+    def backward(self, data: torch.Tensor, node_flows: torch.Tensor, node_mars: torch.Tensor, params=None,
+                 logspace_flows: bool = False, missing_mask=None, **kwargs):
+        if params is not None or missing_mask is not None:
+            raise NotImplementedError("external input parameters / missing masks have no CUDA path")
+        d = self._desc(node_flows.device)
+        if self.param_flows is None:
+            self.init_param_flows(0.0)
+        data = data.to(torch.long)
+        if data.stride(1) != 1:
+            data = data.contiguous()
+        B = node_flows.size(1)
+        nat.call("pcb_input_cat_bwd", nat.ptr(data), data.stride(0), nat.ptr(node_flows), node_flows.stride(0), B,
+                 nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
+                 d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
+                 nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.stream())
+
+    def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False):
+        d = self._desc(self.params.device)
+        for dst, n, ch in d["tied"]:
+            nat.call("pcb_pflow_accum", nat.ptr(self.param_flows), dst, n, nat.ptr(ch), ch.size(0), nat.stream())
+        nat.call("pcb_input_cat_em", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(d["s_pids"]),
+                 nat.ptr(d["s_pfids"]), nat.ptr(d["ncats"]), nat.ptr(d["source_nids"]), d["source_nids"].size(0),
+                 float(step_size), float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
+
+    def update_parameters(self):
+        for ns in self.nodes:
+            if ns.is_tied():
+                continue
+            p0, p1 = ns._param_range
+            ns._params = self.params.data[p0:p1].detach().cpu().clone()
+            ns._param_initialized = True
+
+    def __repr__(self):
+        return f"InputLayer(nid_range={self._output_ind_range}, num_nodes={self.num_nodes})"
+
+
+class LayerGroup:
+    """Layers of one type at one depth, run one after another."""
+
+    def __init__(self, layers: Sequence[Layer]):
+        if len(layers) == 0:
+            raise ValueError("A `LayerGroup` must contain at least 1 layer.")
+        for l in layers:
+            if type(l) is not type(layers[0]):
+                raise ValueError("layers of a group must have the same type")
+        self.layers = list(layers)
+        self.num_layers = len(self.layers)
+        if layers[0].is_input():
+            self.layer_type = "input"
+        elif layers[0].is_prod():
+            self.layer_type = "prod"
+        else:
+            self.layer_type = "sum"
+
+    def to(self, device):
+        for l in self.layers:
+            l.to(device)
+        return self
+
+    def forward(self, *args, **kwargs):
+        for l in self.layers:
+            l.forward(*args, **kwargs)
+
+    __call__ = forward
+
+    def backward(self, *args, **kwargs):
+        for l in self.layers:
+            l.backward(*args, **kwargs)
+
+    def callback(self, fn, *args, **kwargs):
+        if fn is not None:
+            for l in self.layers:
+                fn(l, *args, **kwargs)
+
+    def is_input(self):
+        return self.layer_type == "input"
+
+    def is_prod(self):
+        return self.layer_type == "prod"
+
+    def is_sum(self):
+        return self.layer_type == "sum"
+
+    def __len__(self):
+        return self.num_layers
+
+    def __getitem__(self, idx):
+        return self.layers[idx]
+
+    def __iter__(self):
+        return iter(self.layers)

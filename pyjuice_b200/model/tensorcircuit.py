@@ -1,0 +1,579 @@
+"""``TensorCircuit``: a compiled circuit whose passes run on the sm_100a kernels.
+
+Drop-in for the reference's ``TensorCircuit`` (src/pyjuice/model/tensorcircuit.py:94-1261):
+same constructor arguments, buffers (``node_mars``, ``element_mars``, ``node_flows``,
+``element_flows``, ``params``, ``param_flows``), layer groups, ``forward`` /
+``backward`` / ``mini_batch_em`` semantics, the autograd hook that turns
+``lls.mean().backward()`` into a circuit backward pass, and the accessors
+(``get_node_mars``, ``get_node_flows``, ``update_parameters``, ...).
+
+Differences that are deliberate:
+* buffers are only initialised where a kernel reads them before writing (dummy rows;
+  ``node_flows`` which is accumulated), instead of full re-initialisation each pass;
+* the running total of root flows (``_cum_flow``) is kept on the device, so
+  ``backward`` does not synchronise with the host;
+* EM and normalisation accumulate in FP64 per node block (``pcb_sum_em``), without
+  atomics.
+"""
+
+from __future__ import annotations
+
+from functools import partial
+from typing import Callable, Optional, Sequence, Union
+
+import numpy as np
+import torch
+import torch.nn as nn
+
+from .. import _native as nat
+from ..layer.layers import InputLayer, LayerGroup, ProdLayer, SumLayer
+from ..nodes import CircuitNodes, multiply, summate
+
+
+def _pc_model_backward_hook(grad, pc, inputs, record_cudagraph, apply_cudagraph, propagation_alg, **kwargs):
+    """Gradient hook on the returned log-likelihoods (tensorcircuit.py:24-37).
+
+    The weights are normalised to sum to the batch size, so ``lls.mean()`` and
+    ``lls.sum()`` produce the same flows, as in the reference.
+    """
+    grad = grad.permute(1, 0)
+    pc.backward(inputs=inputs, ll_weights=grad / grad.sum() * grad.size(1),
+                compute_param_flows=pc._optim_hyperparams["compute_param_flows"],
+                flows_memory=pc._optim_hyperparams["flows_memory"], record_cudagraph=record_cudagraph,
+                apply_cudagraph=apply_cudagraph, propagation_alg=propagation_alg, **kwargs)
+    return None
+
+
+class TensorCircuit(nn.Module):
+    def __init__(self, root_ns: CircuitNodes, layer_sparsity_tol: float = 0.5,
+                 max_num_partitions: Optional[int] = None, disable_gpu_compilation: bool = False,
+                 force_gpu_compilation: bool = False, max_tied_ns_per_parflow_block: int = 8,
+                 device: Optional[Union[int, torch.device]] = None, verbose: bool = False) -> None:
+        super().__init__()
+        if not isinstance(root_ns, CircuitNodes):
+            raise TypeError("`root_ns` should be an instance of `CircuitNodes`.")
+        self.root_ns = root_ns
+        self.device = torch.device("cpu")
+        self.num_vars = max(root_ns.scope.to_list()) + 1
+        self.node_mars = None
+        self.element_mars = None
+        self.node_flows = None
+        self.element_flows = None
+        self.param_flows = None
+        self._init_layers(layer_sparsity_tol=layer_sparsity_tol, max_num_partitions=max_num_partitions,
+                          max_tied_ns_per_parflow_block=max_tied_ns_per_parflow_block)
+        self._optim_hyperparams = {"compute_param_flows": True, "flows_memory": 1.0}
+        self._recorded_cuda_graphs = dict()
+        self.default_propagation_alg = "LL"
+        self.propagation_alg_kwargs = dict()
+        self._run_params = dict()
+        self._cum_flow_dev = None
+        self._dev_tables = {}
+        if device is not None:
+            self.to(device)
+
+    # ------------------------------------------------------------------ compile
+    def _create_node_layers(self):
+        """Depth assignment with pass-through insertion (tensorcircuit.py:1122-1191)."""
+        depth2nodes = dict()
+        nodes2depth = dict()
+        num_layers = 1
+        max_node_bs = 0
+        max_ele_bs = 0
+        order = list(self.root_ns)  # post-order: children first
+        for ns in order:
+            if ns in nodes2depth:
+                continue
+            if ns.is_input():
+                nodes2depth[ns] = 0
+                depth2nodes.setdefault(0, {"input": []})["input"].append(ns)
+                continue
+            depth = max(nodes2depth[cs] for cs in ns.chs) + (1 if ns.is_prod() else 0)
+            num_layers = max(depth + 1, num_layers)
+            nodes2depth[ns] = depth
+            if depth not in depth2nodes:
+                depth2nodes[depth] = {"sum": [], "prod": []}
+            if ns.is_sum():
+                for idx, cs in enumerate(ns.chs):
+                    cs_depth = nodes2depth[cs]
+                    if cs_depth < depth:
+                        pass_sum = summate(cs, num_node_blocks=cs.num_node_blocks, block_size=cs.block_size,
+                                           edge_ids=torch.arange(0, cs.num_node_blocks)[None, :].repeat(2, 1),
+                                           params=torch.eye(cs.block_size)[None, :, :].repeat(cs.num_node_blocks, 1, 1))
+                        pass_prod = multiply(pass_sum)
+                        ns.chs[idx] = pass_prod
+                        depth2nodes[cs_depth]["sum"].append(pass_sum)
+                        nodes2depth[pass_sum] = cs_depth
+                        nodes2depth[pass_prod] = depth
+                depth2nodes[depth]["sum"].append(ns)
+                max_node_bs = max(max_node_bs, ns.block_size)
+            else:
+                max_ele_bs = max(max_ele_bs, ns.block_size)
+        pns2layer = dict()
+        for layer in range(1, len(depth2nodes)):
+            for ns in depth2nodes[layer]["sum"]:
+                for cs in ns.chs:
+                    if cs.is_prod():
+                        if id(cs) in pns2layer:
+                            if pns2layer[id(cs)] != layer:
+                                raise ValueError("a product node is requested by sum nodes at different layers")
+                        else:
+                            depth2nodes[layer]["prod"].append(cs)
+                            pns2layer[id(cs)] = layer
+        return depth2nodes, num_layers, max_node_bs, max_ele_bs
+
+    def _init_layers(self, layer_sparsity_tol, max_num_partitions, max_tied_ns_per_parflow_block):
+        """Layer construction and global numbering (tensorcircuit.py:920-1092)."""
+        self.root_ns._clear_tensor_circuit_hooks()
+        depth2nodes, num_layers, max_node_bs, max_ele_bs = self._create_node_layers()
+        self.num_dummy_nodes = max_ele_bs
+        self.num_dummy_eles = max_node_bs
+        self.num_dummy_params = max_node_bs * max_ele_bs
+        num_nodes = self.num_dummy_nodes
+        num_edges = 0
+        num_elements = self.num_dummy_eles
+        num_parameters = self.num_dummy_params
+        num_param_flows = 0
+        node2tiednodes = dict()
+        self.inner_layer_groups = []
+        self.input_layer_group = None
+        input_layers = []
+        for depth in range(num_layers):
+            if depth == 0:
+                sig2nodes = dict()
+                for ns in depth2nodes[0]["input"]:
+                    sig2nodes.setdefault(ns.dist.get_signature(), []).append(ns)
+                for sig, nodes in sig2nodes.items():
+                    layer = InputLayer(nodes, cum_nodes=num_nodes, pc_num_vars=self.num_vars,
+                                       max_tied_ns_per_parflow_block=max_tied_ns_per_parflow_block)
+                    input_layers.append(layer)
+                    num_nodes += layer.num_nodes
+                self.input_layer_group = LayerGroup(input_layers)
+                self.input_layers = nn.ModuleList(input_layers)
+                continue
+            if not depth2nodes[depth]["prod"] or not depth2nodes[depth]["sum"]:
+                raise ValueError(f"depth {depth} has no product or no sum nodes")
+            gsize2prod = dict()
+            for ns in depth2nodes[depth]["prod"]:
+                gsize2prod.setdefault(ns.block_size, []).append(ns)
+            layer_num_elements = max_node_bs
+            prod_layers = []
+            for _, nodes in gsize2prod.items():
+                pl = ProdLayer(nodes, global_nid_start=layer_num_elements, layer_sparsity_tol=layer_sparsity_tol,
+                               max_num_partitions=max_num_partitions)
+                layer_num_elements += pl.num_nodes
+                num_edges += pl.num_edges
+                prod_layers.append(pl)
+            self.inner_layer_groups.append(LayerGroup(prod_layers))
+            num_elements = max(num_elements, layer_num_elements)
+            gsize2sum = dict()
+            for ns in depth2nodes[depth]["sum"]:
+                gsize2sum.setdefault(ns.block_size, []).append(ns)
+            sum_layers = []
+            for _, nodes in gsize2sum.items():
+                sl = SumLayer(nodes, global_nid_start=num_nodes, global_pid_start=num_parameters,
+                              global_pfid_start=num_param_flows, node2tiednodes=node2tiednodes,
+                              layer_sparsity_tol=layer_sparsity_tol, max_num_partitions=max_num_partitions,
+                              max_tied_ns_per_parflow_block=max_tied_ns_per_parflow_block)
+                num_nodes += sl.num_nodes
+                num_edges += sl.num_edges
+                num_parameters += sl.num_parameters
+                num_param_flows += sl.num_param_flows
+                sum_layers.append(sl)
+            self.inner_layer_groups.append(LayerGroup(sum_layers))
+
+        self.num_nodes = num_nodes
+        self.num_edges = num_edges
+        self.num_elements = num_elements
+        self.num_sum_params = num_parameters
+        self.num_param_flows = num_param_flows
+        self.num_root_nodes = self.root_ns.num_nodes
+        self._root_node_range = (self.num_nodes - self.num_root_nodes, self.num_nodes)
+        self._node2tiednodes = node2tiednodes
+        self._build_em_tables()
+        self._init_parameters()
+
+    def _build_em_tables(self):
+        """Per sum node block: parameter / flow base, #children, block size (untied vectors only).
+
+        The reference enumerates the same (node, child) parameters per row of at most 32
+        children (par_update.py:15-171); here one entry covers a whole node block, whose
+        parameters are the contiguous [nch x block_size] slab ``base + k * bs + i``.
+        """
+        pb, fb, nch, bsz = [], [], [], []
+        for ns in self.root_ns:
+            if not ns.is_sum() or ns.is_tied():
+                continue
+            e0 = ns.edge_ids[0].numpy()
+            cnt = np.bincount(e0, minlength=ns.num_node_blocks) * ns.ch_block_size
+            cum = np.zeros(ns.num_node_blocks, np.int64)
+            cum[1:] = np.cumsum(cnt)[:-1]
+            pb.append(ns._param_range[0] + cum * ns.block_size)
+            fb.append(ns._param_flow_range[0] + cum * ns.block_size)
+            nch.append(cnt)
+            bsz.append(np.full(ns.num_node_blocks, ns.block_size, np.int64))
+        cat = lambda xs: np.concatenate(xs) if xs else np.zeros([0], np.int64)
+        self._em_pbase = torch.from_numpy(cat(pb).astype(np.int64))
+        self._em_pfbase = torch.from_numpy(cat(fb).astype(np.int64))
+        self._em_nch = torch.from_numpy(cat(nch).astype(np.int32))
+        self._em_bs = torch.from_numpy(cat(bsz).astype(np.int32))
+        # tied sum vectors whose flows live in several slots (parflow_fusing.py:11-78)
+        self._tied_sum_fusing = []
+        for src, item in self._node2tiednodes.items():
+            if len(item[0]) > 1:
+                n = src._param_flow_range[1] - src._param_flow_range[0]
+                srcs = torch.tensor([r[0] for r in item[1]], dtype=torch.long)
+                self._tied_sum_fusing.append((src._param_flow_range[0], n, srcs))
+
+    def _normalize_host(self, params: torch.Tensor, pseudocount: float = 0.0):
+        """FP64 sum-to-one normalisation on the host (used at construction)."""
+        p = params.double().numpy()
+        for pbase, k, bs in zip(self._em_pbase.tolist(), self._em_nch.tolist(), self._em_bs.tolist()):
+            slab = p[pbase:pbase + k * bs].reshape(k, bs)
+            tot = slab.sum(axis=0)
+            p[pbase:pbase + k * bs] = ((slab + pseudocount / k) / (tot + pseudocount)).reshape(-1)
+        params.copy_(torch.from_numpy(p).float())
+
+    def _init_parameters(self, perturbation: float = 4.0, pseudocount: float = 0.0):
+        """Random / node-provided parameters, normalised (tensorcircuit.py:1094-1120)."""
+        for ns in self.root_ns:
+            if not ns.is_tied() and (ns.is_sum() or ns.is_input()) and not ns.has_params():
+                ns.init_parameters(perturbation=perturbation, recursive=False)
+        params = torch.exp(torch.rand([self.num_sum_params]) * -perturbation)
+        params[:self.num_dummy_params] = 0.0
+        for ns in self.root_ns:
+            if ns.is_sum() and not ns.is_tied() and ns.has_params():
+                ns.gather_parameters(params)
+        self._normalize_host(params, pseudocount)
+        self.params = nn.Parameter(params, requires_grad=False)
+        for layer in self.input_layer_group:
+            layer._init_parameters(perturbation)
+
+    # ------------------------------------------------------------------ device
+    def to(self, device):
+        device = torch.device(device) if not isinstance(device, int) else torch.device(f"cuda:{device}")
+        super().to(device)
+        for g in self.inner_layer_groups:
+            g.to(device)
+        self.input_layer_group.to(device)
+        self.device = device
+        return self
+
+    def cuda(self, device=None):
+        return self.to(torch.device("cuda", device if device is not None else torch.cuda.current_device()))
+
+    def _tables(self):
+        key = (self.device.type, self.device.index)
+        t = self._dev_tables.get(key)
+        if t is None:
+            t = dict(pbase=self._em_pbase.to(self.device), pfbase=self._em_pfbase.to(self.device),
+                     nch=self._em_nch.to(self.device), bs=self._em_bs.to(self.device),
+                     fusing=[(d, n, s.to(self.device)) for d, n, s in self._tied_sum_fusing])
+            self._dev_tables[key] = t
+        return t
+
+    def _buffer(self, name: str, rows: int, B: int, fresh_value: float):
+        t = self.__dict__.get(name)
+        if not isinstance(t, torch.Tensor) or t.shape != (rows, B) or t.device != self.device:
+            t = torch.full((rows, B), fresh_value, device=self.device, dtype=torch.float32)
+            self.__dict__[name] = t
+        return t
+
+    # ------------------------------------------------------------------ passes
+    def set_propagation_alg(self, propagation_alg: str, **kwargs):
+        if propagation_alg != "LL":
+            raise NotImplementedError("only the LL propagation algorithm runs on the CUDA path")
+        self.default_propagation_alg = "LL"
+        self.propagation_alg_kwargs.clear()
+
+    def _run_inner_forward(self, force_use_bf16, force_use_fp32, propagation_alg, **kwargs):
+        for group in self.inner_layer_groups:
+            if group.is_prod():
+                group(self.node_mars, self.element_mars)
+            else:
+                group(self.node_mars, self.element_mars, self.params, force_use_bf16=force_use_bf16,
+                      force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, **kwargs)
+
+    def forward(self, inputs: torch.Tensor, input_layer_fn: Optional[Union[str, Callable]] = None,
+                cache: Optional[dict] = None, return_cache: bool = False, record_cudagraph: bool = False,
+                apply_cudagraph: bool = True, force_use_bf16: bool = False, force_use_fp32: bool = False,
+                propagation_alg: Optional[str] = None, _inner_layers_only: bool = False,
+                _no_buffer_reset: bool = False, **kwargs):
+        """Log-likelihoods ``[B, num_root_nodes]`` of ``inputs`` (``[B, num_vars]`` int64)."""
+        if self.device.type != "cuda":
+            raise RuntimeError("TensorCircuit runs on CUDA only: call pc.to('cuda') first")
+        if propagation_alg is None:
+            propagation_alg = self.default_propagation_alg
+        with torch.no_grad():
+            B = inputs.size(0)
+            origin_inputs = inputs
+            if input_layer_fn is None:
+                if inputs.dim() != 2:
+                    raise ValueError("inputs must be [B, num_vars]")
+                data = inputs.permute(1, 0).to(self.device, torch.long).contiguous()
+            nm = self._buffer("node_mars", self.num_nodes, B, 0.0)
+            em = self._buffer("element_mars", self.num_elements, B, -float("inf"))
+            if not _no_buffer_reset:
+                nat.call("pcb_fill_rows", nat.ptr(nm), B, 0, self.num_dummy_nodes, 0.0, nat.stream())
+                nat.call("pcb_fill_rows", nat.ptr(em), B, 0, self.num_dummy_eles, -float("inf"), nat.stream())
+            if cache is not None and "node_mars" in cache and cache["node_mars"].shape == nm.shape:
+                nm.copy_(cache["node_mars"])
+            if not _inner_layers_only:
+                for layer in self.input_layer_group:
+                    if input_layer_fn is None:
+                        layer(data, nm, **kwargs)
+                    elif isinstance(input_layer_fn, str):
+                        getattr(layer, input_layer_fn)(inputs, nm, **kwargs)
+                    else:
+                        ret = input_layer_fn(layer, inputs, nm, **kwargs)
+                        if not ret and ret is not None:
+                            layer(data, nm, **kwargs)
+            sig = (0, id(nm), id(em), id(self.params), B, force_use_bf16, force_use_fp32)
+            run = partial(self._run_inner_forward, force_use_bf16, force_use_fp32, propagation_alg, **kwargs)
+            if record_cudagraph and sig not in self._recorded_cuda_graphs:
+                self._recorded_cuda_graphs[sig] = self._capture(run)
+            if apply_cudagraph and sig in self._recorded_cuda_graphs:
+                self._recorded_cuda_graphs[sig].replay()
+            else:
+                run()
+            lls = nm[self._root_node_range[0]:self._root_node_range[1], :].permute(1, 0)
+        if return_cache:
+            cache = dict() if cache is None else cache
+            cache["node_mars"] = nm.clone()
+        out = lls.clone()
+        if torch.is_grad_enabled():
+            out.requires_grad = True
+            out.register_hook(partial(_pc_model_backward_hook, pc=self, inputs=origin_inputs,
+                                      record_cudagraph=record_cudagraph, apply_cudagraph=apply_cudagraph,
+                                      propagation_alg=propagation_alg, **kwargs))
+        if return_cache:
+            return out, cache
+        return out
+
+    def _capture(self, fn):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(2):
+                fn()
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        return g
+
+    def _run_inner_backward(self, compute_param_flows, allow_modify_flows, logspace_flows, force_use_fp32, **kwargs):
+        for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
+            group = self.inner_layer_groups[layer_id]
+            if group.is_prod():
+                group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows)
+            else:
+                self.inner_layer_groups[layer_id - 1].forward(self.node_mars, self.element_mars, _for_backward=True)
+                group.backward(self.node_flows, self.element_flows, self.node_mars, self.element_mars, self.params,
+                               param_flows=self.param_flows if compute_param_flows else None,
+                               allow_modify_flows=allow_modify_flows, logspace_flows=logspace_flows,
+                               force_use_fp32=force_use_fp32, **kwargs)
+
+    def backward(self, inputs: Optional[torch.Tensor] = None, ll_weights: Optional[torch.Tensor] = None,
+                 compute_param_flows: bool = True, flows_memory: float = 1.0,
+                 input_layer_fn: Optional[Union[str, Callable]] = None, cache: Optional[dict] = None,
+                 sum_layer_pre_backward_callback: Optional[Callable] = None,
+                 sum_layer_post_backward_callback: Optional[Callable] = None, return_cache: bool = False,
+                 record_cudagraph: bool = False, apply_cudagraph: bool = True, allow_modify_flows: bool = True,
+                 propagation_alg: str = "LL", logspace_flows: bool = False, negate_pflows: bool = False,
+                 _inner_layers_only: bool = False, _disable_buffer_init: bool = False, force_use_fp32: bool = False,
+                 **kwargs):
+        """Node flows, element flows and (accumulated) parameter flows of the last forward batch."""
+        if self.node_mars is None or self.element_mars is None:
+            raise RuntimeError("Should run forward path first.")
+        if propagation_alg != "LL" or negate_pflows:
+            raise NotImplementedError("only LL flows run on the CUDA path")
+        if allow_modify_flows and logspace_flows:
+            raise ValueError("`allow_modify_flows` should be set to `False` when using `logspace_flows`.")
+        if sum_layer_pre_backward_callback is not None or sum_layer_post_backward_callback is not None:
+            raise NotImplementedError("sum-layer callbacks are not supported")
+        self._run_params.update(allow_modify_flows=allow_modify_flows, propagation_alg=propagation_alg,
+                                logspace_flows=logspace_flows, negate_pflows=negate_pflows,
+                                force_use_fp32=force_use_fp32)
+        with torch.no_grad():
+            B = self.node_mars.size(1)
+            if input_layer_fn is None:
+                if inputs is None or inputs.dim() != 2 or inputs.size(1) != self.num_vars:
+                    raise ValueError("inputs must be [B, num_vars]")
+                data = inputs.permute(1, 0).to(self.device, torch.long).contiguous()
+            init = -float("inf") if logspace_flows else 0.0
+            nf = self._buffer("node_flows", self.num_nodes, B, init)
+            ef = self._buffer("element_flows", self.num_elements, B, init)
+            if not _disable_buffer_init:
+                nf.fill_(init)
+                nat.call("pcb_fill_rows", nat.ptr(ef), B, 0, self.num_dummy_eles, init, nat.stream())
+            r0, r1 = self._root_node_range
+            if ll_weights is None:
+                nf[r0:r1, :] = 0.0 if logspace_flows else 1.0
+            else:
+                w = ll_weights.unsqueeze(0) if ll_weights.dim() == 1 else ll_weights
+                if w.size(0) != self.num_root_nodes:
+                    raise ValueError("ll_weights must be [num_root_nodes, B]")
+                nf[r0:r1, :] = w.log() if logspace_flows else w
+            if compute_param_flows:
+                if self._cum_flow_dev is None or self._cum_flow_dev.device != self.device:
+                    self._cum_flow_dev = torch.zeros([], dtype=torch.float64, device=self.device)
+                if ll_weights is None:
+                    self._cum_flow_dev += float((r1 - r0) * B)
+                else:
+                    self._cum_flow_dev += ll_weights.double().sum()
+            if cache is not None and "node_flows" in cache and cache["node_flows"].shape == nf.shape:
+                nf.copy_(cache["node_flows"])
+            if compute_param_flows:
+                self.init_param_flows(flows_memory=flows_memory)
+            sig = (1, id(nf), id(ef), id(self.node_mars), id(self.element_mars), id(self.params),
+                   id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows)
+            run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,
+                          force_use_fp32, **kwargs)
+            if record_cudagraph and sig not in self._recorded_cuda_graphs:
+                saved = nf.clone()
+                self._recorded_cuda_graphs[sig] = self._capture(run)
+                nf.copy_(saved)
+                if compute_param_flows:
+                    self.init_param_flows(flows_memory=0.0)
+            if apply_cudagraph and sig in self._recorded_cuda_graphs:
+                self._recorded_cuda_graphs[sig].replay()
+            else:
+                run()
+            if not _inner_layers_only:
+                for layer in self.input_layer_group:
+                    if input_layer_fn is None:
+                        layer.backward(data, nf, self.node_mars, logspace_flows=logspace_flows, **kwargs)
+                    elif isinstance(input_layer_fn, str):
+                        getattr(layer, input_layer_fn)(inputs, nf, self.node_mars, logspace_flows=logspace_flows, **kwargs)
+                    else:
+                        ret = input_layer_fn(layer, inputs, nf, self.node_mars, logspace_flows=logspace_flows, **kwargs)
+                        if not ret and ret is not None:
+                            layer.backward(data, nf, self.node_mars, logspace_flows=logspace_flows, **kwargs)
+        if return_cache:
+            cache = dict() if cache is None else cache
+            cache["node_flows"] = nf.clone()
+            return cache
+        return None
+
+    @property
+    def _cum_flow(self) -> float:
+        return 0.0 if self._cum_flow_dev is None else float(self._cum_flow_dev.item())
+
+    def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
+                      step_size_rescaling: bool = False, use_cudagraph: bool = True):
+        """EM update from the accumulated parameter flows (tensorcircuit.py:549-590)."""
+        if step_size_rescaling:
+            raise NotImplementedError("step_size_rescaling needs top-down probabilities, which have no CUDA path yet")
+        if not (0.0 < step_size <= 1.0):
+            raise ValueError("`step_size` should be between 0 and 1.")
+        if self.param_flows is None:
+            raise RuntimeError("run a backward pass before mini_batch_em")
+        with torch.no_grad():
+            for layer in self.input_layer_group:
+                layer.mini_batch_em(step_size=step_size, pseudocount=pseudocount, keep_zero_params=keep_zero_params)
+            t = self._tables()
+            for dst, n, srcs in t["fusing"]:
+                nat.call("pcb_pflow_accum", nat.ptr(self.param_flows), dst, n, nat.ptr(srcs), srcs.size(0), nat.stream())
+            nat.call("pcb_sum_em", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(t["pbase"]),
+                     nat.ptr(t["pfbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0), float(step_size),
+                     float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
+
+    def normalize_parameters(self, pseudocount: float = 0.0):
+        """Renormalise the sum parameters in place on the device (FP64)."""
+        t = self._tables()
+        nat.call("pcb_sum_normalize", nat.ptr(self.params), nat.ptr(t["pbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]),
+                 t["nch"].size(0), float(pseudocount), nat.stream())
+
+    def cumulate_flows(self, inputs: torch.Tensor):
+        with torch.no_grad():
+            self.forward(inputs)
+            self.backward(inputs=inputs, compute_param_flows=True, flows_memory=1.0)
+
+    def init_param_flows(self, flows_memory: float = 1.0, batch_size: Optional[int] = None):
+        if not (0.0 <= flows_memory <= 1.0):
+            raise ValueError("`flows_memory` should be in [0.0, 1.0]")
+        if batch_size is not None:
+            raise NotImplementedError("per-sample parameter flows are not supported")
+        pf = self.param_flows
+        if not isinstance(pf, torch.Tensor) or pf.shape != (self.num_param_flows,) or pf.device != self.device:
+            self.param_flows = torch.zeros([self.num_param_flows], device=self.device)
+        elif flows_memory != 1.0:
+            self.param_flows.mul_(flows_memory)
+        for layer in self.input_layer_group:
+            layer.init_param_flows(flows_memory=flows_memory)
+
+    def zero_param_flows(self):
+        self.init_param_flows(flows_memory=0.0)
+
+    def update_parameters(self, clone: bool = True):
+        params = self.params.detach().cpu()
+        for ns in self.root_ns:
+            if ns.is_sum() and not ns.is_tied():
+                ns.update_parameters(params, clone=clone)
+        for layer in self.input_layer_group:
+            layer.update_parameters()
+
+    def update_param_flows(self, clone: bool = True, origin_ns_only: bool = True):
+        pf = self.param_flows.detach().cpu()
+        for ns in self.root_ns:
+            if ns.is_sum() and not ns.is_tied():
+                ns.update_param_flows(pf, clone=clone, origin_ns_only=origin_ns_only)
+
+    def print_statistics(self):
+        print(f"> Number of nodes: {self.num_nodes}")
+        print(f"> Number of edges: {self.num_edges}")
+        print(f"> Number of sum parameters: {self.num_sum_params}")
+        print(f"> Number of input parameters: {sum(l.params.numel() for l in self.input_layer_group)}")
+
+    def get_node_mars(self, ns: CircuitNodes):
+        nsid, neid = ns._output_ind_range
+        if ns.is_sum() or ns.is_input():
+            return self.node_mars[nsid:neid, :].detach()
+        for group in self.inner_layer_groups:
+            for layer in group:
+                if layer.is_prod() and any(n is ns for n in layer.nodes):
+                    layer(self.node_mars, self.element_mars)
+                    return self.element_mars[nsid:neid, :].detach()
+        raise ValueError("node not found in the circuit")
+
+    def get_node_flows(self, ns: CircuitNodes, **kwargs):
+        nsid, neid = ns._output_ind_range
+        if ns.is_sum() or ns.is_input():
+            return self.node_flows[nsid:neid, :].detach()
+        for idx, group in enumerate(self.inner_layer_groups):
+            for layer in group:
+                if layer.is_prod() and any(n is ns for n in layer.nodes):
+                    self.inner_layer_groups[idx].forward(self.node_mars, self.element_mars, _for_backward=True)
+                    self.inner_layer_groups[idx + 1].backward(
+                        self.node_flows, self.element_flows, self.node_mars, self.element_mars, self.params,
+                        param_flows=None, allow_modify_flows=False, force_use_fp32=True)
+                    return self.element_flows[nsid:neid, :].detach()
+        raise ValueError("node not found in the circuit")
+
+    def layers(self, reverse: bool = False, ret_layer_groups: bool = False, ignore_input_layers: bool = False):
+        groups = ([] if ignore_input_layers else [self.input_layer_group]) + list(self.inner_layer_groups)
+        if reverse:
+            groups = groups[::-1]
+        for g in groups:
+            if ret_layer_groups:
+                yield g
+            else:
+                for l in g:
+                    yield l
+
+    def dataset_ll_accumulate(self, lls: torch.Tensor, acc: torch.Tensor):
+        """Adds sum_b lls[b, 0] to the FP64 device scalar ``acc`` (dataset-level LL, FP64)."""
+        if acc.dtype != torch.float64 or not acc.is_cuda:
+            raise ValueError("acc must be a float64 CUDA tensor")
+        x = lls[:, 0].contiguous()
+        nat.call("pcb_ll_sum_f64", nat.ptr(x), x.numel(), x.numel(), 0, nat.ptr(acc), nat.stream())
+
+
+def compile(ns: CircuitNodes, layer_sparsity_tol: float = 0.5, max_num_partitions: Optional[int] = None,
+            disable_gpu_compilation: bool = False, force_gpu_compilation: bool = False,
+            max_tied_ns_per_parflow_block: int = 8, device: Optional[Union[int, torch.device]] = None,
+            verbose: bool = False) -> TensorCircuit:
+    """Compile a circuit DAG into a ``TensorCircuit`` (reference: tensorcircuit.py:1224-1261)."""
+    return TensorCircuit(ns, layer_sparsity_tol=layer_sparsity_tol, max_num_partitions=max_num_partitions,
+                         max_tied_ns_per_parflow_block=max_tied_ns_per_parflow_block, device=device, verbose=verbose)

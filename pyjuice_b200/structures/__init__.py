@@ -1,0 +1,1 @@
+from .hclt import HCLT, hclt_from_tree, chow_liu_tree, mutual_information, mutual_information_chunked

@@ -1,0 +1,52 @@
+"""Circuit recipes shared by the fixture generator and the tests.
+
+Each recipe only uses the construction API that the reference and ``pyjuice_b200``
+have in common (``inputs`` / ``multiply`` / ``summate`` / ``set_block_size`` /
+``duplicate``), so the same call builds the same DAG in both packages.
+"""
+
+from __future__ import annotations
+
+import torch
+
+
+def build_tiny_dag(juice, dists):
+    """A small DAG exercising the compiler's corner cases.
+
+    * sum vectors with different child counts in one layer (several partitions);
+    * a block-sparse sum (explicit ``edge_ids``) and a sparse product (explicit ``edge_ids``);
+    * a sum whose children sit at different depths (pass-through insertion);
+    * tied sum vectors and tied input vectors;
+    * a block-size-1 root.
+    """
+    with juice.set_block_size(4):
+        i = [juice.inputs(v, num_node_blocks=2, dist=dists.Categorical(num_cats=4)) for v in range(5)]
+        i.append(i[4].duplicate(5, tie_params=True))
+        p01 = juice.multiply(i[0], i[1])
+        p01b = juice.multiply(i[0], i[1], edge_ids=torch.tensor([[1, 0], [0, 1]]))
+        p23 = juice.multiply(i[2], i[3])
+        p45 = juice.multiply(i[4], i[5])
+        s01 = juice.summate(p01, p01b, num_node_blocks=3)
+        s23 = juice.summate(p23, edge_ids=torch.tensor([[0, 0, 1], [0, 1, 1]]))
+        s23t = s23.duplicate(tie_params=True)
+        s45 = juice.summate(p45, num_node_blocks=2)
+        q = juice.multiply(s01, s23, edge_ids=torch.tensor([[0, 0], [1, 1], [2, 0]]))
+        q2 = juice.multiply(s01, s23t, edge_ids=torch.tensor([[2, 1], [0, 0], [1, 0]]))
+        p0123 = juice.multiply(i[0], i[1], i[2], i[3])
+        r = juice.summate(q, q2, p0123, num_node_blocks=2)
+        top = juice.multiply(r, s45)
+        root = juice.summate(top, num_node_blocks=1, block_size=1)
+    return root
+
+
+def build_layer_test_nodes(juice, dists, block_size: int = 16):
+    """The node vectors of the reference's sum-layer unit test (tests/layer/sum_layer_test.py:17-48)."""
+    with juice.set_block_size(block_size):
+        ni = [juice.inputs(v, num_node_blocks=2, dist=dists.Categorical(num_cats=2)) for v in range(4)]
+        np0 = juice.multiply(ni[0], ni[1])
+        np1 = juice.multiply(ni[2], ni[3])
+        np2 = juice.multiply(ni[1], ni[2])
+        ns0 = juice.summate(np0, num_node_blocks=2)
+        ns1 = juice.summate(np1, num_node_blocks=2)
+        ns2 = juice.summate(np2, num_node_blocks=2)
+    return ni, [np0, np1, np2], [ns0, ns1, ns2]

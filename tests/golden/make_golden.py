@@ -1,0 +1,192 @@
+"""Generate the golden fixtures in this directory by running the reference PyJuice.
+
+Run from the repository root in a container that holds the reference sources
+(``PYJUICE_REF_SRC``, default ``/root/reference/src``):
+
+    python tests/golden/make_golden.py [tiny] [hclt64] [hclt784]
+
+The reference executes on CPU through Triton's interpreter (``ref_shim.py``) in its
+plain FP32 mode (``force_use_fp32=True``). Outputs (``.npz``) hold the compiled index
+tensors (or their SHA-256 digests for the large circuit), the initial parameters and
+the results of one forward / backward / ``mini_batch_em`` step:
+
+* ``tiny.npz``      the DAG of ``tests/circuits.py:build_tiny_dag`` (partitions, block-sparse
+                    edges, pass-through insertion, tied sums and inputs), B = 64;
+* ``hclt64.npz``    HCLT, 64 variables x 4 categories, 16 latents, block size 16, B = 512,
+                    data from a seeded random tree Bayesian network;
+* ``hclt784.npz``   HCLT, 28x28 variables x 256 categories, 128 latents, block size 32:
+                    structure, index digests and the log-likelihoods of 8 samples.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from ref_shim import load_reference  # noqa: E402
+
+juice = load_reference()
+import torch  # noqa: E402
+import networkx as nx  # noqa: E402
+import pyjuice.nodes.distributions as dists  # noqa: E402
+from pyjuice.structures.hclt import mutual_information_chunked, chow_liu_tree  # noqa: E402
+from pyjuice.structures.compilation import BayesianTreeToHiddenRegionGraph  # noqa: E402
+
+from circuits import build_tiny_dag  # noqa: E402
+from pyjuice_b200.synthetic import gaussian_field_data, tree_bayes_net_data  # noqa: E402
+
+
+def digest(t: torch.Tensor) -> str:
+    return hashlib.sha256(t.detach().cpu().long().contiguous().numpy().tobytes()).hexdigest()
+
+
+def collect_layout(pc, out: dict, full: bool = True):
+    """Index tensors of every layer, flattened into ``out``."""
+    gi = 0
+    for group in pc.inner_layer_groups:
+        for li, layer in enumerate(group):
+            pre = f"g{gi}_l{li}_"
+            if layer.is_sum():
+                names = ["nids", "cids", "pids", "pfids", "chids", "parids", "parpids"]
+                out[pre + "nid_range"] = np.array(layer._layer_nid_range)
+                out[pre + "pid_range"] = np.array(layer._layer_pid_range)
+                out[pre + "pfid_range"] = np.array(layer._layer_pfid_range)
+                out[pre + "cs_block_sizes"] = np.array(layer.cs_block_sizes)
+            else:
+                names = ["nids", "cids", "u_cids", "parids"]
+                out[pre + "nid_range"] = np.array(layer._layer_nid_range)
+            for n in names:
+                tl = getattr(layer, "partitioned_" + n)
+                out[pre + n + "_count"] = np.array(len(tl))
+                for p, t in enumerate(tl):
+                    if full:
+                        out[f"{pre}{n}_{p}"] = t.detach().cpu().numpy()
+                    else:
+                        out[f"{pre}{n}_{p}_sha"] = np.array(digest(t))
+                        out[f"{pre}{n}_{p}_shape"] = np.array(tuple(t.shape))
+        gi += 1
+    il = pc.input_layer_group[0]
+    for n in ("vids", "s_pids", "s_pfids", "s_mids", "nids", "source_nids", "node_id2source_id"):
+        t = getattr(il, n)
+        if full:
+            out["in_" + n] = t.detach().cpu().numpy()
+        else:
+            out["in_" + n + "_sha"] = np.array(digest(t))
+    out["num_nodes"] = np.array(pc.num_nodes)
+    out["num_elements"] = np.array(pc.num_elements)
+    out["num_sum_params"] = np.array(pc.num_sum_params)
+    out["num_param_flows"] = np.array(pc.num_param_flows)
+    out["num_groups"] = np.array(len(pc.inner_layer_groups))
+    out["root_range"] = np.array(pc._root_node_range)
+
+
+def run_step(pc, x, out: dict, keep_buffers: bool):
+    """forward (FP32) -> backward (default flags) -> mini_batch_em(0.1, 0.1)."""
+    out["params0"] = pc.params.detach().cpu().numpy().copy()
+    out["in_params0"] = pc.input_layer_group[0].params.detach().cpu().numpy().copy()
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    out["lls"] = lls.detach().cpu().numpy()
+    if keep_buffers:
+        out["node_mars"] = pc.node_mars.detach().cpu().numpy().copy()
+    lls.mean().backward()
+    if keep_buffers:
+        out["node_flows"] = pc.node_flows.detach().cpu().numpy().copy()
+    out["param_flows"] = pc.param_flows.detach().cpu().numpy().copy()
+    out["in_param_flows"] = pc.input_layer_group[0].param_flows.detach().cpu().numpy().copy()
+    pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+    out["params1"] = pc.params.detach().cpu().numpy().copy()
+    out["in_params1"] = pc.input_layer_group[0].params.detach().cpu().numpy().copy()
+
+
+def hclt_tree(x: torch.Tensor, num_bins=32, sigma=0.5 / 32, chunk_size=64):
+    mi = mutual_information_chunked(x, x, num_bins, sigma, chunk_size=chunk_size).detach().cpu().numpy()
+    T = chow_liu_tree(mi)
+    root = nx.center(T)[0]
+    clt = nx.bfs_tree(T, root)
+    seq = list(nx.dfs_postorder_nodes(T, root))
+    children = {int(v): [int(c) for c in clt.successors(v)] for v in clt.nodes}
+    return mi, T, root, seq, children
+
+
+def pack_tree(out, mi, root, seq, children):
+    out["tree_mi"] = mi.astype(np.float32)
+    out["tree_root"] = np.array(root)
+    out["tree_seq"] = np.array(seq)
+    ch_flat, ch_off = [], [0]
+    for v in range(len(seq)):
+        ch_flat.extend(children.get(v, []))
+        ch_off.append(len(ch_flat))
+    out["tree_children"] = np.array(ch_flat, dtype=np.int64)
+    out["tree_children_off"] = np.array(ch_off, dtype=np.int64)
+
+
+def make_tiny():
+    torch.manual_seed(1)
+    root = build_tiny_dag(juice, dists)
+    pc = juice.compile(root, max_tied_ns_per_parflow_block=1, verbose=False)
+    out = {}
+    collect_layout(pc, out, full=True)
+    gen = torch.Generator().manual_seed(2)
+    x = torch.randint(0, 4, (64, 6), generator=gen)
+    out["x"] = x.numpy()
+    run_step(pc, x, out, keep_buffers=True)
+    np.savez_compressed(os.path.join(HERE, "tiny.npz"), **out)
+
+
+def make_hclt64():
+    data = tree_bayes_net_data(num_vars=64, num_cats=4, num_samples=8192, seed=0)
+    mi, T, root, seq, children = hclt_tree(data.float())
+    torch.manual_seed(3)
+    with juice.set_block_size(16):
+        r = BayesianTreeToHiddenRegionGraph(T, root, 16, dists.Categorical, {"num_cats": 4}, num_root_ns=1,
+                                            block_size=16)
+    pc = juice.compile(r, verbose=False)
+    out = {}
+    pack_tree(out, mi, root, seq, children)
+    collect_layout(pc, out, full=True)
+    x = data[:512]
+    out["x"] = x.numpy()
+    run_step(pc, x, out, keep_buffers=False)
+    np.savez_compressed(os.path.join(HERE, "hclt64.npz"), **out)
+
+
+def make_hclt784():
+    data = gaussian_field_data(8192, side=28, num_cats=256, length_scale=3.0, seed=0)
+    mi, T, root, seq, children = hclt_tree(data.float())
+    torch.manual_seed(4)
+    r = BayesianTreeToHiddenRegionGraph(T, root, 128, dists.Categorical, {"num_cats": 256}, num_root_ns=1,
+                                        block_size=32)
+    t = time.time()
+    pc = juice.compile(r, verbose=False)
+    print("hclt784 compile", time.time() - t, flush=True)
+    out = {}
+    pack_tree(out, mi, root, seq, children)
+    collect_layout(pc, out, full=False)
+    out["params0_sha"] = np.array(hashlib.sha256(pc.params.detach().numpy().tobytes()).hexdigest())
+    x = data[:8]
+    out["x"] = x.numpy()
+    out["params0"] = pc.params.detach().cpu().numpy().astype(np.float32)
+    out["in_params0"] = pc.input_layer_group[0].params.detach().cpu().numpy().astype(np.float32)
+    t = time.time()
+    lls = pc(x, force_use_fp32=True)
+    print("hclt784 forward", time.time() - t, flush=True)
+    out["lls"] = lls.detach().cpu().numpy()
+    np.savez_compressed(os.path.join(HERE, "hclt784.npz"), **out)
+
+
+if __name__ == "__main__":
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784"]
+    for w in which:
+        t = time.time()
+        {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784}[w]()
+        print(w, "done in", round(time.time() - t, 1), "s", flush=True)

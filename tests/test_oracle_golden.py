@@ -1,0 +1,57 @@
+"""Pins the CPU oracle to the reference: its FP64 restatement reproduces the outputs that
+the reference itself produced on the same circuits, parameters and data (golden fixtures
+from ``tests/golden/make_golden.py``). CPU only."""
+
+import numpy as np
+import pytest
+
+from conftest import load_fixture
+from oracle import pc_oracle as orc
+
+NCATS = {"tiny": 4, "hclt64": 4}
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_oracle_forward_backward_em(name):
+    fx = load_fixture(name)
+    lay = orc.layout_from_fixture(fx, ncats=NCATS[name])
+    nm, ems, lls = orc.forward(lay, fx["params0"], fx["in_params0"], fx["x"])
+    # the reference ran in FP32: agreement to FP32 rounding of the LL scale
+    assert np.allclose(lls, fx["lls"], rtol=1e-6, atol=1e-5)
+    nf, pf, in_pf = orc.backward(lay, fx["params0"], fx["x"], nm, ems)
+    scale = np.abs(fx["param_flows"]).max()
+    assert np.abs(pf - fx["param_flows"]).max() <= 1e-5 * scale
+    assert np.abs(in_pf - fx["in_param_flows"]).max() <= 1e-5 * np.abs(fx["in_param_flows"]).max()
+    p1, ip1 = orc.em_update(lay, fx["params0"], fx["param_flows"].astype(np.float64), fx["in_params0"],
+                            fx["in_param_flows"].astype(np.float64), 0.1, 0.1)
+    assert np.abs(p1 - fx["params1"]).max() <= 1e-6
+    assert np.abs(ip1 - fx["in_params1"]).max() <= 1e-6
+
+
+def test_oracle_node_values_tiny():
+    fx = load_fixture("tiny")
+    lay = orc.layout_from_fixture(fx, ncats=4)
+    nm, ems, _ = orc.forward(lay, fx["params0"], fx["in_params0"], fx["x"])
+    ref = fx["node_mars"]
+    fin = np.isfinite(ref)
+    assert np.array_equal(fin, np.isfinite(nm))
+    assert np.abs(nm[fin] - ref[fin]).max() < 1e-5
+
+
+def test_oracle_probabilities_sum_to_one():
+    """Sum of p(x) over every assignment of the tiny circuit is 1 (a size-independent property)."""
+    import itertools
+    fx = load_fixture("tiny")
+    lay = orc.layout_from_fixture(fx, ncats=4)
+    x = np.array(list(itertools.product(range(4), repeat=6)), dtype=np.int64)
+    _, _, lls = orc.forward(lay, fx["params0"], fx["in_params0"], x)
+    # parameters are FP32-normalised, so the total is 1 up to FP32 rounding
+    assert abs(np.exp(lls).sum() - 1.0) < 2e-6
+
+
+def test_uniform_hash_known_values():
+    # SplitMix64 of the counter: fixed outputs guard the sampler's draw contract
+    u = [float(orc.uniform(0, 0, 0)), float(orc.uniform(12345, 7, 3)), float(orc.uniform(2 ** 62, 2 ** 31, 1023))]
+    assert all(0.0 <= v < 1.0 for v in u)
+    assert len(set(u)) == 3
+    assert orc.uniform(1, 2, 3) == orc.uniform(1, 2, 3)
