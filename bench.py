@@ -1,0 +1,408 @@
+"""EM-step throughput of a compiled HCLT on B200 (one JSON line on rank 0).
+
+Workload: HCLT over 28x28 variables with 256 categories, 128 latents, block size 32,
+batch 512; data = seeded Gaussian random fields (length scale 3 px) quantised to 256
+levels (stand-in for MNIST, same shapes). One step = ``init_param_flows(0)`` ->
+forward -> backward -> ``mini_batch_em(step_size=0.1, pseudocount=0.1)``.
+
+* ``value``: samples/s of the BF16 tensor-core form, whole step captured in one CUDA
+  graph, inputs resident in HBM, device time (CUDA events), max over ranks;
+* ``fp32_plain``: the same for the plain FP32 form;
+* ``e2e``: the BF16 form through the public API (``lls = pc(x)``,
+  ``lls.mean().backward()``, ``pc.mini_batch_em``) with the batch copied from pinned
+  host memory and the log-likelihoods read back every step;
+* ``roofline``: the sum-layer forward contraction, timed per launch with CUDA events;
+* ``cpu_baseline``: the FP64 CPU restatement (oracle port) on a bounded sample.
+
+``--impl reference`` times the CPU implementation of the same step instead (the
+reference itself is Python + Triton with no CPU path; its arithmetic is restated by
+``oracle/``), on all host cores, rank 0 only.
+
+Multi-GPU (``torchrun``): data-parallel replicas; each rank runs its own batch and the
+parameter flows are summed with an NCCL all-reduce before every EM update
+(weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIDE = 28
+NUM_CATS = 256
+LATENTS = 128
+BLOCK = 32
+BATCH = 512
+STEP_SIZE = 0.1
+PSEUDOCOUNT = 0.1
+METRIC = "EM samples/s (fwd+bwd+update) 1xB200, BF16-TC vs FP32 plain; dLL vs FP64 oracle"
+WORKLOAD = "HCLT 28x28 vars x 256 cats, 128 latents, block 32, EM step (fwd+bwd+mini_batch_em)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=BATCH)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_data(num_samples: int):
+    from pyjuice_b200.synthetic import gaussian_field_data
+    return gaussian_field_data(num_samples, side=SIDE, num_cats=NUM_CATS, length_scale=3.0, seed=0)
+
+
+def build_circuit(data: torch.Tensor, device):
+    """HCLT over the data's Chow-Liu tree (mutual information from the first 8192 samples)."""
+    import pyjuice_b200 as juice
+    from pyjuice_b200.nodes.distributions import Categorical
+    from pyjuice_b200.structures import hclt_from_tree, chow_liu_tree
+    from pyjuice_b200.structures.hclt import mutual_information_chunked
+    x = data[:8192].float()
+    if device.type == "cuda":
+        x = x.to(device)
+    mi = mutual_information_chunked(x, x, 32, 0.5 / 32, chunk_size=64).cpu().numpy()
+    tree = chow_liu_tree(mi)
+    root = tree.center()
+    torch.manual_seed(0)
+    ns = hclt_from_tree(tree.dfs_postorder(root), tree.bfs_children(root), root, LATENTS,
+                        input_dist=Categorical(num_cats=NUM_CATS), block_size=BLOCK)
+    return juice.compile(ns)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def sum_forward_roofline(pc, x, precision_kw, reps=3):
+    """Per-launch CUDA-event timing of the sum-layer forward contractions of one forward pass.
+
+    Algorithmic bytes per launch: each child row read once (4 B x batch), each node row
+    written once (4 B x batch), each edge weight read once (4 B).
+    """
+    with torch.no_grad():
+        pc(x, **precision_kw)
+    s = torch.cuda.current_stream()
+    B = x.size(0)
+    rows = []
+    for g in pc.inner_layer_groups:
+        if g.is_sum():
+            for layer in g:
+                d = layer._desc(x.device)
+                child_rows = int(torch.unique(d["krow"]).numel())
+                rows.append((layer, 4 * B * (child_rows + layer.num_nodes) + 4 * layer.num_edges,
+                             2 * layer.num_edges * B))
+    tot_ms, bytes_alg, flops = 0.0, 0, 0
+    for _ in range(reps):
+        for g in pc.inner_layer_groups:
+            if g.is_prod():
+                g(pc.node_mars, pc.element_mars)
+                continue
+            for layer in g:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                layer(pc.node_mars, pc.element_mars, pc.params, **precision_kw)
+                e1.record(s)
+                e1.synchronize()
+                tot_ms += e0.elapsed_time(e1)
+        for _, b, f in rows:
+            bytes_alg += b
+            flops += f
+    n = reps * len(rows)
+    return bytes_alg / n, flops / n, tot_ms / 1e3 / n, len(rows)
+
+
+def cpu_step_rate(layout, params, in_params, data, budget_s):
+    """FP64 oracle port: forward + backward + EM, batches doubling until ~budget seconds."""
+    from oracle import pc_oracle as orc
+    B, t_used, samples = 8, 0.0, 0
+    while t_used < budget_s:
+        x = data[:B].numpy()
+        t0 = time.perf_counter()
+        nm, ems, _ = orc.forward(layout, params, in_params, x)
+        _, pf, ipf = orc.backward(layout, params, x, nm, ems)
+        orc.em_update(layout, params, pf, in_params, ipf, STEP_SIZE, PSEUDOCOUNT)
+        dt = time.perf_counter() - t0
+        t_used += dt
+        samples += B
+        if dt < budget_s / 4 and B < 512:
+            B *= 2
+    return samples / t_used, f"FP64 numpy oracle, batches of 8..{B} samples, {samples} samples in {t_used:.1f} s"
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    data = make_data(8192)
+    # mutual information is structure building, not the timed path: use a GPU when present
+    pc = build_circuit(data, torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu"))
+    from oracle import pc_oracle as orc
+    lay = orc.layout_from_circuit(pc)
+    params = pc.params.detach().numpy().astype(np.float64)
+    in_params = pc.input_layer_group[0].params.detach().numpy().astype(np.float64)
+    B = 32
+    x = data[:B].numpy()
+    warm = max(1, min(args.warmup, 1))
+    steps = max(1, min(args.steps, 3))
+    times = []
+    for i in range(warm + steps):
+        t0 = time.perf_counter()
+        nm, ems, _ = orc.forward(lay, params, in_params, x)
+        _, pf, ipf = orc.backward(lay, params, x, nm, ems)
+        orc.em_update(lay, params, pf, in_params, ipf, STEP_SIZE, PSEUDOCOUNT)
+        if i >= warm:
+            times.append(time.perf_counter() - t0)
+    v = B / statistics.median(times)
+    sample = f"FP64 CPU restatement (oracle port), {B} samples per step, median of {len(times)} steps"
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": args.gpus,
+                      "steps": len(times), "warmup": warm, "ms_per_step": 1e3 * statistics.median(times),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": {"workload": WORKLOAD, "batch": B},
+                      "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    ws, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    group = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+        group = dist.group.WORLD
+    from pyjuice_b200 import _native as nat
+    nat.load()
+    B = args.batch
+    n_data = max(8192, B * 8)
+    data = make_data(n_data)
+    pc = build_circuit(data, device).to(device)
+    data_dev = data[torch.arange(rank * B, rank * B + B * 8) % n_data].to(device)  # 8 resident batches per rank
+
+    def allreduce_flows():
+        if group is not None:
+            import torch.distributed as dist
+            dist.all_reduce(pc.param_flows, group=group)
+            dist.all_reduce(pc.input_layer_group[0].param_flows, group=group)
+
+    def step(x, kw):
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            pc(x, **kw)
+        pc.backward(inputs=x, allow_modify_flows=True, force_use_fp32=kw.get("force_use_fp32", False))
+        allreduce_flows()
+        pc.mini_batch_em(step_size=STEP_SIZE, pseudocount=PSEUDOCOUNT)
+
+    # kernels per step: every C-ABI call launches one kernel
+    n0 = nat.CALLS
+    step(data_dev[:B], {"force_use_bf16": True})
+    kernels_per_step = nat.CALLS - n0
+
+    def timed(kw, use_graph):
+        x_static = data_dev[:B].clone()
+        g = None
+        if use_graph:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                for _ in range(2):
+                    step(x_static, kw)
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                step(x_static, kw)
+        for i in range(args.warmup):
+            x_static.copy_(data_dev[(i % 8) * B:(i % 8 + 1) * B])
+            g.replay() if g is not None else step(x_static, kw)
+        torch.cuda.synchronize()
+        if group is not None:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(args.steps):
+            x_static.copy_(data_dev[(i % 8) * B:(i % 8 + 1) * B])
+            g.replay() if g is not None else step(x_static, kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        if group is not None:
+            import torch.distributed as dist
+            t = torch.tensor([ms], device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        del g
+        return ms, ck
+
+    use_graph = ws == 1
+    ms_bf16, clocks = timed({"force_use_bf16": True}, use_graph)
+    ms_fp32, _ = timed({"force_use_fp32": True}, use_graph)
+    value = ws * B * args.steps / (ms_bf16 / 1e3)
+    value_fp32 = ws * B * args.steps / (ms_fp32 / 1e3)
+
+    # end to end through the public API, host buffers, LLs read back every step
+    host = data[:B * 8].pin_memory()
+    ll_host = torch.empty([B, 1], dtype=torch.float32).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+
+    def e2e_step(i):
+        x = host[(i % 8) * B:(i % 8 + 1) * B].to(device, non_blocking=True)
+        pc.init_param_flows(flows_memory=0.0)
+        lls = pc(x, force_use_bf16=True)
+        lls.mean().backward()
+        allreduce_flows()
+        pc.mini_batch_em(step_size=STEP_SIZE, pseudocount=PSEUDOCOUNT)
+        ll_host.copy_(lls.detach(), non_blocking=True)
+
+    for i in range(2):
+        e2e_step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(e2e_steps):
+        e2e_step(i)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if group is not None:
+        import torch.distributed as dist
+        t = torch.tensor([ms_e2e], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = ws * B * e2e_steps / (ms_e2e / 1e3)
+
+    result = None
+    if rank == 0:
+        from oracle import pc_oracle as orc
+        lay = orc.layout_from_circuit(pc)
+        params = pc.params.detach().cpu().numpy().astype(np.float64)
+        in_params = pc.input_layer_group[0].params.detach().cpu().numpy().astype(np.float64)
+        xs = data[:64]
+        _, _, lls_o = orc.forward(lay, params, in_params, xs.numpy())
+        with torch.no_grad():
+            l_bf = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
+            l_32 = pc(xs.to(device), force_use_fp32=True).double().cpu().numpy()
+        ll_err = {"bf16_dmean_ll_nats": float(abs(l_bf.mean() - lls_o.mean())),
+                  "bf16_mean_abs_dll_nats": float(np.abs(l_bf - lls_o).mean()),
+                  "fp32_max_rel_dll": float((np.abs(l_32 - lls_o) / np.abs(lls_o)).max()),
+                  "fp32_dmean_ll_nats": float(abs(l_32.mean() - lls_o.mean())),
+                  "mean_ll_nats": float(lls_o.mean()), "samples": int(xs.size(0))}
+        hbm, tflops, src = peaks()
+        bytes_l, flops_l, avg_s, nl = sum_forward_roofline(pc, data_dev[:B], {"force_use_bf16": True})
+        achieved = bytes_l / avg_s / 1e9
+        roof = {"kernel": "pcb_lse_contract, sum-layer forward, bf16 form", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak_source": f"{src} hbm_gbs", "launches_per_forward": nl, "avg_launch_us": avg_s * 1e6,
+                "alg_bytes_per_launch": bytes_l, "tensor_tflops_achieved": flops_l / avg_s / 1e12}
+        threads = os.cpu_count() or 1
+        torch.set_num_threads(threads)
+        v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0)
+        cpu = {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample}
+        result = {
+            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_bf16 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "batch_per_gpu": B, "num_nodes": pc.num_nodes,
+                       "num_edges": pc.num_edges, "parallelism": f"dp{ws}" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (node_mars alone is 4*N*B bytes > 126 MB); no flush",
+                       "cuda_graph": use_graph},
+            "fp32_plain": {"value": value_fp32, "unit": "samples/s", "ms_per_step": ms_fp32 / args.steps},
+            "ll_error_vs_fp64": ll_err,
+            "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": B * SIDE * SIDE * 8,
+                    "d2h_bytes_per_step": B * 4},
+            "gpu_launches": kernels_per_step * args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+    if group is not None:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

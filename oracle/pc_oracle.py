@@ -138,14 +138,15 @@ def forward(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarr
                 for nids, cids, pids in zip(l["nids"], l["cids"], l["pids"]):
                     G, C = cids.shape
                     e = em[cids.reshape(-1)].reshape(G, C, B)                  # [G, C, B]
-                    w = logw[pids[:, :, None] + np.arange(bs)[None, None, :]]   # [G, C, bs]
-                    w = np.where(cids[:, :, None] == 0, -np.inf, w)
-                    t = w.transpose(0, 2, 1)[:, :, :, None] + e[:, None, :, :]  # [G, bs, C, B]
-                    m = np.max(t, axis=2, keepdims=True)
-                    with np.errstate(invalid="ignore", divide="ignore"):
-                        s = np.log(np.sum(np.exp(t - np.where(np.isfinite(m), m, 0.0)), axis=2)) + \
-                            np.where(np.isfinite(m[:, :, 0]), m[:, :, 0], 0.0)
-                    s = np.where(np.isfinite(m[:, :, 0]), s, -np.inf)
+                    e = np.where(cids[:, :, None] == 0, -np.inf, e)
+                    w = np.exp(logw[pids[:, :, None] + np.arange(bs)[None, None, :]])   # [G, C, bs]
+                    w = np.where(cids[:, :, None] == 0, 0.0, w)
+                    m = np.max(e, axis=1)                                       # [G, B]
+                    fin = np.isfinite(m)
+                    m0 = np.where(fin, m, 0.0)
+                    s = np.einsum("gci,gcb->gib", w, np.exp(e - m0[:, None, :]))  # [G, bs, B]
+                    with np.errstate(divide="ignore"):
+                        s = np.where(fin[:, None, :], np.log(s) + m0[:, None, :], -np.inf)
                     nm[_rows(nids, bs)] = s.reshape(G * bs, B)
     r0, r1 = layout["root_range"]
     return nm, ems, nm[r0:r1].T.copy()
@@ -184,37 +185,39 @@ def backward(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, em
             with np.errstate(divide="ignore", invalid="ignore"):
                 lr = np.where(np.isfinite(nm) & (nf > 0), np.log(nf) - np.where(np.isfinite(nm), nm, 0.0), -np.inf)
 
-            def shifted(rows):
-                a = lr[rows]
-                m = np.max(a, axis=0)
+            def shifted(rows, real):
+                """exp(lr[rows] - M) with M the max over axis 1 (the nodes involved), per sample."""
+                a = np.where(real[..., None], lr[rows], -np.inf)               # [R, K, B]
+                m = np.max(a, axis=1)
                 m = np.where(np.isfinite(m), m, 0.0)
-                return np.exp(a - m[None, :]), m
+                return np.exp(a - m[:, None, :]), m
 
+            ar = None
             for l in g["layers"]:
                 bs = l["block_size"]
-                # element flows
+                ar = np.arange(bs)
+                # element flows: one batched contraction per partition
                 for chids, parids, parpids, cbs in zip(l["chids"], l["parids"], l["parpids"], l["cs_block_sizes"]):
-                    for r in range(chids.shape[0]):
-                        npar = int((parids[r] != 0).sum())
-                        prow = _rows(parids[r, :npar], bs)                       # parent node rows
-                        a, m = shifted(prow)
-                        acc = np.zeros([cbs, B])
-                        for j in range(cbs):
-                            wj = w[(parpids[r, :npar][:, None] + j * bs + np.arange(bs)[None, :]).reshape(-1)]
-                            acc[j] = wj @ a
-                        crow = chids[r] + np.arange(cbs)
-                        ef[crow] = acc * np.exp(em[crow] + m[None, :])
-                # parameter flows
+                    R, P = parids.shape
+                    real = np.repeat(parids != 0, bs, axis=1)                      # [R, P*bs]
+                    prow = (parids[:, :, None] + ar).reshape(R, P * bs)
+                    a, m = shifted(prow, real)
+                    wid = parpids[:, None, :, None] + np.arange(cbs)[None, :, None, None] * bs + ar
+                    wj = np.where(real[:, None, :], w[wid.reshape(R, cbs, P * bs)], 0.0)   # [R, cbs, P*bs]
+                    acc = np.einsum("rjk,rkb->rjb", wj, a)
+                    crow = chids[:, None] + np.arange(cbs)[None, :]                 # [R, cbs]
+                    ef[crow.reshape(-1)] = (acc * np.exp(em[crow] + m[:, None, :])).reshape(R * cbs, B)
+                # parameter flows: one batched contraction (over the batch) per partition
                 for nids, cids, pids, pfids in zip(l["nids"], l["cids"], l["pids"], l["pfids"]):
-                    for r in range(nids.shape[0]):
-                        cnt = int((cids[r] != 0).sum())
-                        nrow = nids[r] + np.arange(bs)
-                        a, m = shifted(nrow)
-                        ce = np.exp(em[cids[r, :cnt]] + m[None, :])               # [C, B]
-                        s = a @ ce.T                                               # [bs, C]
-                        slots = pfids[r, :cnt][None, :] + np.arange(bs)[:, None]
-                        ws = w[pids[r, :cnt][None, :] + np.arange(bs)[:, None]]
-                        np.add.at(pf, slots.reshape(-1), (ws * s).reshape(-1))
+                    R, C = cids.shape
+                    nrow = nids[:, None] + ar                                       # [R, bs]
+                    a, m = shifted(nrow, np.ones_like(nrow, dtype=bool))
+                    ce = np.exp(em[cids] + m[:, None, :])                           # [R, C, B]
+                    s = np.einsum("rib,rcb->ric", a, ce)                            # [R, bs, C]
+                    real = np.broadcast_to((cids != 0)[:, None, :], s.shape)
+                    slots = pfids[:, None, :] + ar[None, :, None]
+                    ws = w[pids[:, None, :] + ar[None, :, None]]
+                    np.add.at(pf, slots[real], (ws * s)[real])
     inp = layout["input"]
     n_in = inp["vids"].shape[0]
     npf = inp["num_param_flows"] if inp.get("num_param_flows") else int(inp["s_pfids"].max() + inp["ncats"].max())
@@ -225,48 +228,53 @@ def backward(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, em
     return nf, pf, in_pf
 
 
-def _sum_node_table(layout: dict):
-    """(param ids row, flow ids row) of every sum node, one entry per node of every block."""
-    out = []
+def _sum_block_table(layout: dict):
+    """Per distinct parameter slab: (first param id, #children, block size, set of first flow ids).
+
+    In the compiled layout the weights of a node block are ``pids[r, 0] + k * bs + i`` and
+    its flows ``pfids[r, 0] + k * bs + i``; tied node blocks share ``pids[r, 0]`` and may
+    own separate flow slots, which EM sums first.
+    """
+    table: Dict[int, list] = {}
     for g in layout["groups"]:
         if g["kind"] != "sum":
             continue
         for l in g["layers"]:
             bs = l["block_size"]
             for cids, pids, pfids in zip(l["cids"], l["pids"], l["pfids"]):
+                cnts = (cids != 0).sum(axis=1)
                 for r in range(cids.shape[0]):
-                    cnt = int((cids[r] != 0).sum())
-                    for i in range(bs):
-                        out.append((pids[r, :cnt] + i, pfids[r, :cnt] + i))
-    return out
+                    ent = table.setdefault(int(pids[r, 0]), [int(cnts[r]), bs, set()])
+                    ent[2].add(int(pfids[r, 0]))
+    return table
 
 
 def em_update(layout: dict, params: np.ndarray, pf: np.ndarray, in_params: np.ndarray, in_pf: np.ndarray,
               step_size: float, pseudocount: float):
     """One EM step (keep_zero_params=False); returns new (params, in_params) as float64."""
     newp = params.astype(np.float64).copy()
-    groups: Dict[tuple, set] = {}
-    for prow, frow in _sum_node_table(layout):
-        key = tuple(prow.tolist())
-        groups.setdefault(key, set()).add(tuple(frow.tolist()))
-    for key, frows in groups.items():
-        prow = np.array(key, dtype=np.int64)
-        f = np.zeros(prow.shape[0])
-        for fr in frows:
-            f += pf[np.array(fr, dtype=np.int64)]
-        nch = prow.shape[0]
-        tot = f.sum()
-        newp[prow] = (1 - step_size) * newp[prow] + step_size * (f + pseudocount / nch) / (tot + pseudocount)
+    for p0, (nch, bs, f0s) in _sum_block_table(layout).items():
+        n = nch * bs
+        f = np.zeros(n)
+        for f0 in f0s:
+            f += pf[f0:f0 + n]
+        f = f.reshape(nch, bs)
+        tot = f.sum(axis=0)                                    # per node of the block
+        old = newp[p0:p0 + n].reshape(nch, bs)
+        newp[p0:p0 + n] = ((1 - step_size) * old + step_size * (f + pseudocount / nch) / (tot + pseudocount)).reshape(-1)
     inp = layout["input"]
     new_in = in_params.astype(np.float64).copy()
-    by_pid: Dict[int, set] = {}
-    for sp, spf, k in zip(inp["s_pids"], inp["s_pfids"], inp["ncats"]):
-        by_pid.setdefault((int(sp), int(k)), set()).add(int(spf))
-    for (sp, K), spfs in by_pid.items():
-        f = np.zeros(K)
-        for s in spfs:
-            f += in_pf[s:s + K]
-        new_in[sp:sp + K] = (1 - step_size) * new_in[sp:sp + K] + step_size * (f + pseudocount / K) / (f.sum() + pseudocount)
+    pairs = np.unique(np.stack([inp["s_pids"], inp["s_pfids"], inp["ncats"]], axis=1), axis=0)
+    for K in np.unique(pairs[:, 2]):
+        sel = pairs[pairs[:, 2] == K]
+        ar = np.arange(int(K))
+        acc = np.zeros([new_in.shape[0]])
+        np.add.at(acc, (sel[:, 0:1] + ar).reshape(-1), in_pf[(sel[:, 1:2] + ar).reshape(-1)])
+        sp = np.unique(sel[:, 0])
+        rows = sp[:, None] + ar                                # [n, K]
+        f = acc[rows]
+        new_in[rows] = (1 - step_size) * new_in[rows] + step_size * (f + pseudocount / K) / (
+            f.sum(axis=1, keepdims=True) + pseudocount)
     return newp, new_in
 
 
@@ -287,10 +295,12 @@ def sample(layout: dict, params: np.ndarray, in_params: np.ndarray, num_samples:
     """Top-down sampling with the device sampler's draw rules (small circuits only)."""
     p32 = params.astype(np.float32)
     ip32 = in_params.astype(np.float32)
-    # node id -> (children element ids, param ids) for sum nodes; element id -> child node ids
+    # node id -> (children element ids, param ids, product group) for sum nodes;
+    # (product group, element id) -> child node ids. Element ids are reused by every
+    # product layer group, so they are only meaningful together with their group.
     sum_ch: Dict[int, tuple] = {}
-    prod_ch: Dict[int, List[int]] = {}
-    for g in layout["groups"]:
+    prod_ch: Dict[tuple, List[int]] = {}
+    for gi, g in enumerate(layout["groups"]):
         for l in g["layers"]:
             bs = l["block_size"]
             if l["kind"] == "sum":
@@ -298,13 +308,13 @@ def sample(layout: dict, params: np.ndarray, in_params: np.ndarray, num_samples:
                     for r in range(nids.shape[0]):
                         cnt = int((cids[r] != 0).sum())
                         for i in range(bs):
-                            sum_ch[int(nids[r]) + i] = (cids[r, :cnt], pids[r, :cnt] + i)
+                            sum_ch[int(nids[r]) + i] = (cids[r, :cnt], pids[r, :cnt] + i, gi - 1)
             else:
                 for nids, cids in zip(l["nids"], l["cids"]):
                     for r in range(nids.shape[0]):
                         real = cids[r][cids[r] != 0]
                         for i in range(bs):
-                            prod_ch[int(nids[r]) + i] = [int(c) + i for c in real]
+                            prod_ch[(gi, int(nids[r]) + i)] = [int(c) + i for c in real]
     inp = layout["input"]
     in0 = inp["nid_start"]
     out = np.zeros([num_samples, num_vars], dtype=np.int64)
@@ -314,7 +324,7 @@ def sample(layout: dict, params: np.ndarray, in_params: np.ndarray, num_samples:
         while stack:
             n = stack.pop()
             if n in sum_ch:
-                ch, pid = sum_ch[n]
+                ch, pid, pg = sum_ch[n]
                 u = uniform(seed, n, s)
                 cum = np.float32(0.0)
                 pick, last_nz = -1, 0
@@ -328,7 +338,7 @@ def sample(layout: dict, params: np.ndarray, in_params: np.ndarray, num_samples:
                         break
                 if pick < 0:
                     pick = last_nz
-                stack.extend(prod_ch[int(ch[pick])])
+                stack.extend(prod_ch[(pg, int(ch[pick]))])
             else:
                 li = n - in0
                 K = int(inp["ncats"][li])

@@ -109,8 +109,13 @@ def load() -> ctypes.CDLL:
     return lib
 
 
+CALLS = 0  # number of entry-point calls (each launches at most one kernel)
+
+
 def call(name: str, *args):
+    global CALLS
     lib = load()
+    CALLS += 1
     rc = getattr(lib, name)(*args)
     if rc != 0:
         msg = lib.pcb_last_error().decode(errors="replace")

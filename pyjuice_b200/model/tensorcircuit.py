@@ -343,9 +343,10 @@ class TensorCircuit(nn.Module):
         out = lls.clone()
         if torch.is_grad_enabled():
             out.requires_grad = True
+            # the backward contraction runs in the precision form the forward used
             out.register_hook(partial(_pc_model_backward_hook, pc=self, inputs=origin_inputs,
                                       record_cudagraph=record_cudagraph, apply_cudagraph=apply_cudagraph,
-                                      propagation_alg=propagation_alg, **kwargs))
+                                      propagation_alg=propagation_alg, force_use_fp32=force_use_fp32, **kwargs))
         if return_cache:
             return out, cache
         return out

@@ -39,6 +39,24 @@ def build_tiny_dag(juice, dists):
     return root
 
 
+def seeded_params(em_pbase, em_nch, em_bs, num_sum_params, in_num_nodes, in_ncats, seed: int):
+    """Normalised random parameters for a compiled layout, regenerable from a seed.
+
+    Sum weights: each node's weights over its children sum to one (the node-block slab
+    ``base + k * bs + i`` of the compiled layout); input nodes: each row of ``in_ncats``
+    probabilities sums to one. Used instead of storing large parameter vectors in fixtures.
+    """
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p = np.zeros(num_sum_params, dtype=np.float64)
+    for base, k, bs in zip(em_pbase, em_nch, em_bs):
+        slab = np.exp(-4.0 * rng.random((int(k), int(bs))))
+        p[int(base):int(base) + int(k) * int(bs)] = (slab / slab.sum(axis=0, keepdims=True)).reshape(-1)
+    q = np.exp(-4.0 * rng.random((in_num_nodes, in_ncats)))
+    q /= q.sum(axis=1, keepdims=True)
+    return p.astype(np.float32), q.reshape(-1).astype(np.float32)
+
+
 def build_layer_test_nodes(juice, dists, block_size: int = 16):
     """The node vectors of the reference's sum-layer unit test (tests/layer/sum_layer_test.py:17-48)."""
     with juice.set_block_size(block_size):

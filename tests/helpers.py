@@ -70,8 +70,20 @@ def layout_mismatches(pc, fx, full: bool = True):
     return bad
 
 
+def fixture_params(pc, fx):
+    """(sum params, input params) of a fixture: stored, or regenerated from its seed."""
+    if "params0" in fx:
+        return fx["params0"], fx["in_params0"]
+    from circuits import seeded_params
+    il = pc.input_layer_group[0]
+    ncats = int(il.metadata[0].item())
+    return seeded_params(pc._em_pbase.tolist(), pc._em_nch.tolist(), pc._em_bs.tolist(), pc.num_sum_params,
+                         il.num_nodes, ncats, seed=int(fx["param_seed"]))
+
+
 def load_fixture_params(pc, fx):
+    p, q = fixture_params(pc, fx)
     with torch.no_grad():
-        pc.params.copy_(torch.from_numpy(fx["params0"]).to(pc.params.device))
+        pc.params.copy_(torch.from_numpy(p).to(pc.params.device))
         il = pc.input_layer_group[0]
-        il.params.copy_(torch.from_numpy(fx["in_params0"]).to(il.params.device))
+        il.params.copy_(torch.from_numpy(q).to(il.params.device))

@@ -1,0 +1,195 @@
+"""Full-circuit parity on the GPU: CUDA path vs the reference's own outputs (golden
+fixtures) and vs the FP64 oracle, through pyjuice_b200's public API."""
+
+import itertools
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_fixture
+from helpers import build_fixture_circuit, fixture_params, load_fixture_params
+from oracle import pc_oracle as orc
+
+import pyjuice_b200 as juice
+
+pytestmark = pytest.mark.gpu
+
+# FP32 plain path vs the reference: per-sample LL within 1e-5 relative.
+LL_RTOL = 1e-5
+
+
+def _step(pc, x, **fw):
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, **fw)
+    lls.mean().backward()
+    return lls
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_fp32_step_matches_reference(name, cuda_device):
+    fx = load_fixture(name)
+    torch.manual_seed(0)
+    pc = build_fixture_circuit(name, fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    lls = _step(pc, x, force_use_fp32=True)
+    ref = fx["lls"]
+    got = lls.detach().cpu().numpy()
+    assert np.all(np.abs(got - ref) <= LL_RTOL * np.abs(ref) + 1e-6)
+    pf = pc.param_flows.cpu().numpy()
+    assert np.abs(pf - fx["param_flows"]).max() <= 1e-4 * np.abs(fx["param_flows"]).max()
+    ipf = pc.input_layer_group[0].param_flows.cpu().numpy()[: fx["in_param_flows"].shape[0]]
+    assert np.abs(ipf - fx["in_param_flows"]).max() <= 1e-4 * np.abs(fx["in_param_flows"]).max()
+    pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+    assert np.abs(pc.params.cpu().numpy() - fx["params1"]).max() <= 1e-5
+    ip1 = pc.input_layer_group[0].params.cpu().numpy()[: fx["in_params1"].shape[0]]
+    assert np.abs(ip1 - fx["in_params1"]).max() <= 1e-5
+
+
+def test_fp32_node_values_match_reference_tiny(cuda_device):
+    fx = load_fixture("tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    with torch.no_grad():
+        pc(x, force_use_fp32=True)
+    nm = pc.node_mars.cpu().numpy()
+    ref = fx["node_mars"]
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(nm), fin)
+    assert np.abs(nm[fin] - ref[fin]).max() <= 1e-5 * max(1.0, np.abs(ref[fin]).max())
+
+
+def test_fp32_hclt784_matches_reference(cuda_device):
+    fx = load_fixture("hclt784")
+    pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    with torch.no_grad():
+        lls = pc(x, force_use_fp32=True).cpu().numpy()
+    ref = fx["lls"]
+    assert np.all(np.abs(lls - ref) <= LL_RTOL * np.abs(ref))
+
+
+@pytest.mark.parametrize("B", [1, 3, 17, 64, 200])
+def test_fp32_batch_sizes_vs_oracle(B, cuda_device):
+    """Ragged batches (not multiples of 4 or of the sample tile) against the oracle."""
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"][:B]).to(cuda_device)
+    lay = orc.layout_from_circuit(pc)
+    nm, ems, lls_o = orc.forward(lay, fx["params0"], fx["in_params0"], fx["x"][:B])
+    lls = _step(pc, x, force_use_fp32=True).detach().cpu().numpy()
+    assert np.all(np.abs(lls - lls_o) <= LL_RTOL * np.abs(lls_o))
+    _, pf, ipf = orc.backward(lay, fx["params0"], fx["x"][:B], nm, ems)
+    assert np.abs(pc.param_flows.cpu().numpy() - pf).max() <= 1e-4 * max(np.abs(pf).max(), 1e-6)
+    got_ipf = pc.input_layer_group[0].param_flows.cpu().numpy()[: ipf.shape[0]]
+    assert np.abs(got_ipf - ipf).max() <= 1e-4 * max(np.abs(ipf).max(), 1e-6)
+
+
+def test_probabilities_sum_to_one_tiny(cuda_device):
+    fx = load_fixture("tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.tensor(list(itertools.product(range(4), repeat=6)), device=cuda_device)
+    with torch.no_grad():
+        lls = pc(x, force_use_fp32=True)
+    assert abs(lls.double().exp().sum().item() - 1.0) < 1e-5
+
+
+def test_bf16_forward_error_vs_fp64(cuda_device):
+    """BF16 tensor-core form on HCLT-784 (128 latents, block size 32): mean LL within
+    1e-3 nats of the FP64 oracle; FP32 form within 1e-5 relative per sample."""
+    fx = load_fixture("hclt784")
+    pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    lay = orc.layout_from_circuit(pc)
+    p0, q0 = fixture_params(pc, fx)
+    _, _, lls_o = orc.forward(lay, p0, q0, fx["x"])
+    with torch.no_grad():
+        lls_bf = pc(x, force_use_bf16=True).double().cpu().numpy()
+        lls_32 = pc(x, force_use_fp32=True).double().cpu().numpy()
+    assert np.all(np.abs(lls_32 - lls_o) <= LL_RTOL * np.abs(lls_o))
+    assert abs(lls_bf.mean() - lls_o.mean()) < 1e-3
+
+
+def test_cuda_graph_replay_matches_eager(cuda_device):
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    with torch.no_grad():
+        eager = pc(x, force_use_fp32=True).clone()
+        pc(x, force_use_fp32=True, record_cudagraph=True)
+        replay = pc(x, force_use_fp32=True, apply_cudagraph=True)
+    assert torch.equal(eager, replay)
+
+
+def test_deterministic_flows(cuda_device):
+    """Parameter flows carry no float atomics on untied circuits: two runs are bit-identical."""
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    _step(pc, x, force_use_fp32=True)
+    a = pc.param_flows.clone()
+    ai = pc.input_layer_group[0].param_flows.clone()
+    _step(pc, x, force_use_fp32=True)
+    assert torch.equal(a, pc.param_flows)
+    assert torch.equal(ai, pc.input_layer_group[0].param_flows)
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_sampling_bit_exact_vs_oracle(name, cuda_device):
+    fx = load_fixture(name)
+    pc = build_fixture_circuit(name, fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    S, seed = 64, 1234567
+    got = juice.queries.sample(pc, S, seed=seed).cpu().numpy()
+    lay = orc.layout_from_circuit(pc)
+    ref = orc.sample(lay, fx["params0"], fx["in_params0"], S, seed, pc.num_vars)
+    assert np.array_equal(got, ref)
+
+
+def test_sampling_marginals(cuda_device):
+    """Empirical single-variable marginals of 20k samples match the exact marginals of the tiny circuit."""
+    fx = load_fixture("tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    S = 20000
+    s = juice.queries.sample(pc, S, seed=7).cpu().numpy()
+    lay = orc.layout_from_circuit(pc)
+    allx = np.array(list(itertools.product(range(4), repeat=6)), dtype=np.int64)
+    _, _, lls = orc.forward(lay, fx["params0"], fx["in_params0"], allx)
+    p = np.exp(lls[:, 0])
+    for v in range(6):
+        exact = np.array([p[allx[:, v] == k].sum() for k in range(4)])
+        emp = np.bincount(s[:, v], minlength=4) / S
+        assert np.abs(exact - emp).max() < 0.02
+
+
+def test_invalid_category_gives_nan_not_fault(cuda_device):
+    fx = load_fixture("tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"][:8]).to(cuda_device).clone()
+    x[0, 0] = 99
+    with torch.no_grad():
+        lls = pc(x, force_use_fp32=True)
+    assert torch.isnan(lls[0, 0])
+    assert torch.isfinite(lls[1:]).all()
+
+
+def test_errors_are_raised(cuda_device):
+    fx = load_fixture("tiny")
+    cpu_pc = build_fixture_circuit("tiny", fx)
+    with pytest.raises(RuntimeError):
+        cpu_pc(torch.from_numpy(fx["x"][:4]))  # there is no CPU path
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    with pytest.raises(RuntimeError):
+        pc.mini_batch_em(step_size=0.1)  # no flows yet
+    with pytest.raises(ValueError):
+        pc.mini_batch_em(step_size=0.0)

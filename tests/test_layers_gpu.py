@@ -1,0 +1,108 @@
+"""Layer-level kernels on the GPU, checked with the formulas of the reference's layer tests
+(tests/layer/sum_layer_test.py:17-143, tests/layer/prod_layer_test.py:17-91) in FP64 torch."""
+
+import pytest
+import torch
+
+import pyjuice_b200 as juice
+from pyjuice_b200.nodes import distributions as dists
+
+from circuits import build_layer_test_nodes
+
+pytestmark = pytest.mark.gpu
+
+
+def _layers(bs):
+    ni, nps, nss = build_layer_test_nodes(juice, dists, bs)
+    juice.InputLayer(ni, cum_nodes=bs)
+    prod = juice.ProdLayer(nps)
+    layer = juice.SumLayer(nss, global_nid_start=bs, global_pid_start=bs ** 2, global_pfid_start=0,
+                           node2tiednodes=dict())
+    return prod, layer
+
+
+@pytest.mark.parametrize("bs,B,fp32", [(16, 16, True), (16, 16, False), (4, 7, True), (32, 130, True),
+                                       (32, 256, False)])
+def test_sum_layer_forward_backward(bs, B, fp32, cuda_device):
+    torch.manual_seed(63892)
+    prod, layer = _layers(bs)
+    layer.to(cuda_device)
+    em = torch.rand([bs + 3 * 2 * 2 * bs, B]).log().to(cuda_device)
+    em[:bs] = -float("inf")
+    nm = torch.zeros([bs + bs * 2 * 3, B], device=cuda_device)
+    params = torch.rand([bs ** 2 + 3 * 4 * bs * bs], device=cuda_device)
+    layer(nm, em, params, force_use_fp32=fp32, force_use_bf16=not fp32)
+    tol = 1e-5 if fp32 else 2e-2
+    cids, pids = layer.partitioned_cids[0], layer.partitioned_pids[0]
+    for j in range(6):
+        for i in range(bs):
+            ref = (params[pids[j] + i].double()[:, None] * em[cids[j]].double().exp()).sum(0).log()
+            assert torch.all((nm[(j + 1) * bs + i].double() - ref).abs() <= tol * ref.abs().clamp(min=1.0))
+
+    nf = torch.rand([bs + bs * 2 * 3, B], device=cuda_device)
+    ef = torch.zeros([bs + 3 * 2 * 2 * bs, B], device=cuda_device)
+    pf = torch.zeros_like(params)
+    nm64 = nm.double()
+    layer.backward(nf, ef, nm, em, params, pf, force_use_fp32=fp32)
+    chids, parids, parpids = layer.partitioned_chids[0], layer.partitioned_parids[0], layer.partitioned_parpids[0]
+    etol = 1e-4 if fp32 else 3e-2
+    for j in range(6):
+        prow = (parids[j][:, None] + torch.arange(bs, device=cuda_device)[None, :]).reshape(-1)
+        for i in range(bs):
+            w = (parpids[j][:, None] + i * bs + torch.arange(bs, device=cuda_device)[None, :]).reshape(-1)
+            ref = (nf[prow].double() * params[w].double()[:, None] * em[chids[j] + i].double().exp()[None, :]
+                   / nm64[prow].exp()).sum(0)
+            assert torch.all((ef[chids[j] + i].double() - ref).abs() <= etol * ref.abs().max())
+    my_pf = torch.zeros_like(params, dtype=torch.float64)
+    for j in range(6):
+        for i in range(bs):
+            row = (j + 1) * bs + i
+            my_pf[layer.partitioned_pfids[0][j] + i] = params[pids[j] + i].double() * (
+                nf[row].double()[None, :] * em[cids[j]].double().exp() / nm64[row].exp()[None, :]).sum(1)
+    assert torch.all((pf.double() - my_pf).abs() <= 1e-4 * my_pf.abs().max())
+
+
+def test_sum_layer_unmodified_flows_equal_modified(cuda_device):
+    """allow_modify_flows=False (log f - log m computed on the fly) gives the same flows."""
+    bs, B = 16, 64
+    torch.manual_seed(1)
+    prod, layer = _layers(bs)
+    layer.to(cuda_device)
+    em = torch.rand([bs + 12 * bs, B]).log().to(cuda_device)
+    em[:bs] = -float("inf")
+    nm = torch.zeros([7 * bs, B], device=cuda_device)
+    params = torch.rand([bs ** 2 + 12 * bs * bs], device=cuda_device)
+    layer(nm, em, params, force_use_fp32=True)
+    nf = torch.rand([7 * bs, B], device=cuda_device)
+    ef1, ef2 = torch.zeros_like(em), torch.zeros_like(em)
+    pf1, pf2 = torch.zeros_like(params), torch.zeros_like(params)
+    layer.backward(nf.clone(), ef1, nm, em, params, pf1, allow_modify_flows=True, force_use_fp32=True)
+    layer.backward(nf.clone(), ef2, nm, em, params, pf2, allow_modify_flows=False, force_use_fp32=True)
+    assert torch.allclose(ef1, ef2, rtol=1e-5, atol=1e-6)
+    assert torch.allclose(pf1, pf2, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("B", [16, 5])
+def test_prod_layer_forward_backward(B, cuda_device):
+    bs = 16
+    torch.manual_seed(2)
+    prod, _ = _layers(bs)
+    prod.to(cuda_device)
+    nm = torch.rand([bs + 4 * 2 * bs, B], device=cuda_device)
+    nm[:bs] = 0.0
+    em = torch.full([bs + 3 * 2 * bs, B], -float("inf"), device=cuda_device)
+    prod(nm, em)
+    for nids, cids in zip(prod.partitioned_nids, prod.partitioned_cids):
+        for g in range(nids.size(0)):
+            for i in range(bs):
+                ref = sum(nm[cids[g, j] + i] for j in range(cids.size(1)))
+                assert torch.allclose(em[nids[g] + i], ref, atol=1e-6)
+    ef = torch.rand_like(em)
+    ef[:bs] = 0.0
+    nf = torch.zeros_like(nm)
+    prod.backward(nf, ef)
+    for u, par in zip(prod.partitioned_u_cids, prod.partitioned_parids):
+        for g in range(u.size(0)):
+            for i in range(bs):
+                ref = sum(ef[par[g, q] + i] for q in range(par.size(1)))
+                assert torch.allclose(nf[u[g] + i], ref, atol=1e-6)
