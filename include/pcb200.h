@@ -28,23 +28,39 @@ extern "C" {
 #define PCB_E_LAUNCH -2    /* CUDA launch error */
 #define PCB_E_CUDA -3      /* other CUDA runtime error */
 
-/* One tile of an LSE contraction (sum forward / element flows). */
+/*
+ * One tile of an LSE contraction (sum forward / element flows). A tile covers n_rows
+ * consecutive output rows made of consecutive blocks of `rows_per_block` rows (the
+ * launch argument) that share the same contraction terms; row r of the tile uses weight
+ *   params[kw[k] + w_add + (r / rows_per_block) * g_stride + (r % rows_per_block) * w_stride].
+ */
 typedef struct {
-    int32_t out_row;  /* first output row of the tile */
-    int32_t n_rows;   /* rows in the tile (<= tile height of the launch) */
-    int32_t k_off;    /* offset into krow[] / kw[] */
-    int32_t k_cnt;    /* number of contraction terms */
-    int32_t w_add;    /* added to kw[k] for tile row 0 */
-    int32_t aux_row;  /* element-flow epilogue: first element_mars row of the tile */
+    int32_t out_row;   /* first output row of the tile */
+    int32_t n_rows;    /* rows in the tile (<= tile height of the launch) */
+    int32_t k_off;     /* offset into krow[] / kw[] */
+    int32_t k_cnt;     /* number of contraction terms */
+    int32_t w_add;     /* added to kw[k] for tile row 0 */
+    int32_t aux_row;   /* element-flow epilogue: first element_mars row of the tile */
+    int32_t g_stride;  /* weight offset between consecutive blocks of the tile */
+    int32_t reserved;
 } PcbLseTile;
 
-/* One tile of the sum-parameter-flow contraction (contraction over the batch). */
+/*
+ * One tile of the sum-parameter-flow contraction (contraction over the batch): nodes
+ * nid + r (r < n_rows, consecutive blocks of `rows_per_block` nodes sharing children)
+ * and children k_off .. k_off + k_cnt - 1. Node r of child k uses
+ *   weight  params[pids[k] + p_add + (r / rows_per_block) * gs_p + r % rows_per_block]
+ *   flow    param_flows[pfids[k] + p_add + (r / rows_per_block) * gs_pf + r % rows_per_block].
+ */
 typedef struct {
-    int32_t nid;      /* first node row of the tile */
-    int32_t n_rows;   /* nodes in the tile */
-    int32_t k_off;    /* offset into cids[] / pids[] / pfids[] of the tile's first child */
-    int32_t k_cnt;    /* children in the tile */
-    int32_t p_add;    /* index of the tile's first node within its block (added to pids / pfids) */
+    int32_t nid;       /* first node row of the tile */
+    int32_t n_rows;    /* nodes in the tile (<= 128) */
+    int32_t k_off;     /* offset into cids[] / pids[] / pfids[] of the tile's first child */
+    int32_t k_cnt;     /* children in the tile (<= 64) */
+    int32_t p_add;     /* added to pids / pfids for tile row 0 */
+    int32_t gs_p;      /* parameter offset between consecutive blocks of the tile */
+    int32_t gs_pf;     /* flow offset between consecutive blocks of the tile */
+    int32_t reserved;
 } PcbPflowTile;
 
 /* Version of the library ABI (currently 1). */
@@ -127,7 +143,8 @@ int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int32_t B,
 /*
  * Log-sum-exp contraction over tiles, FP32 FMA (plain) or BF16 tensor-core (prec=1):
  *   acc[r, b] = sum_k W(k, r) * exp(src[krow[k], b] - m_b),  m_b = max_k src[krow[k], b]
- *   W(k, r)   = params[kw[k] + w_add + r * w_stride]
+ *   W(k, r)   = params[kw[k] + w_add + (r / rows_per_block) * g_stride + (r % rows_per_block) * w_stride]
+ * tile_rows (power of 2, <= 128) is the launch's tile height; rows_per_block a power of 2.
  * mode 0 (sum forward):    out[out_row + r, b] = log(acc) + m_b
  * mode 1 (element flows):  out[out_row + r, b] = acc * exp(aux[aux_row + r, b] + m_b)
  * mode 2 (element flows, unmodified node flows): as mode 1 with src = log(src) - src2.
@@ -138,8 +155,8 @@ int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int32_t B,
  */
 int pcb_lse_contract(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
                      const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t tile_rows,
-                     const int32_t* krow, const int32_t* kw, int32_t w_stride, int32_t mode, int32_t prec,
-                     void* stream);
+                     int32_t rows_per_block, const int32_t* krow, const int32_t* kw, int32_t w_stride, int32_t mode,
+                     int32_t prec, void* stream);
 
 /*
  * In place on rows [row0, row1) of node_flows: f <- (m == -inf) ? -inf : log(f) - m.
@@ -149,18 +166,20 @@ int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int3
                      int64_t row0, int64_t row1, void* stream);
 
 /*
- * Sum-layer parameter flows, contraction over the batch:
- *   pf[pfids[k] + p_add + i] += params[pids[k] + p_add + i] * sum_b exp(lf[nid + i, b] - M_b) * exp(em[cids[k], b] + M_b)
+ * Sum-layer parameter flows, contraction over the batch (see PcbPflowTile for the ids):
+ *   pf(r, k) += params(r, k) * sum_b exp(lf[nid + r, b] - M_b) * exp(em[cids[k], b] + M_b)
  * with lf = node_flows already in "log f - log m" form (modified=1) or computed as
  * log(node_flows) - node_mars (modified=0), M_b the max over the tile's nodes.
+ * The batch is split over a cluster of CTAs whose partial sums are added in a fixed
+ * order through distributed shared memory (deterministic, no scratch memory).
  * atomic=1 when flow slots are shared by tied nodes.
  * Replaces SumLayer._bk_triton_block_sparse_par_kernel / _csmm2 / sparse par kernel
  * (src/pyjuice/layer/sum_layer.py:2052-2282, 2795-2902).
  */
 int pcb_sum_pflows(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld, int32_t B,
                    const float* params, float* param_flows, const PcbPflowTile* tiles, int32_t num_tiles,
-                   const int32_t* cids, const int32_t* pids, const int32_t* pfids, int32_t modified, int32_t atomic,
-                   void* stream);
+                   int32_t rows_per_block, const int32_t* cids, const int32_t* pids, const int32_t* pfids,
+                   int32_t modified, int32_t atomic, void* stream);
 
 /*
  * Sum-parameter EM update, per node block (FP64 normalisation):

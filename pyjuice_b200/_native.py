@@ -53,11 +53,6 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB_PATH
 
 
-class _LseTile(ctypes.Structure):
-    _fields_ = [("out_row", c_int32), ("n_rows", c_int32), ("k_off", c_int32), ("k_cnt", c_int32),
-                ("w_add", c_int32), ("aux_row", c_int32)]
-
-
 _SIGS = {
     "pcb_version": ([], c_int32),
     "pcb_last_error": ([], ctypes.c_char_p),
@@ -73,10 +68,10 @@ _SIGS = {
     "pcb_prod_gather_sum": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
-                          c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
+                          c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_modify_flows": ([c_void_p, c_void_p, c_int64, c_int32, c_int64, c_int64, c_void_p], c_int32),
     "pcb_sum_pflows": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
-                        c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p], c_int32),
+                        c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p], c_int32),
     "pcb_sum_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double, c_int32,
                     c_void_p], c_int32),
     "pcb_sum_normalize": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_void_p], c_int32),

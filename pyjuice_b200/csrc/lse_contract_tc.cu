@@ -1,9 +1,11 @@
 // BF16 tensor-core form of the log-sum-exp contraction (see lse_contract.cu).
 //
-// Same tiling and online-max scheme as the FP32 kernel; the contraction of each staged
-// chunk runs on the tensor cores: A = W (rows x K, rounded to bf16), B = exp(src - m)
-// (K x samples, rounded to bf16), FP32 accumulators. max / exp / log stay in FP32.
-// Tile: TM (16 or 32) rows x 128 samples, 8 warps, warp w owns samples [16w, 16w + 16).
+// Same tiles and online-max scheme as the FP32 kernel; each staged chunk is contracted on
+// the tensor cores: A = W (rows x K, rounded to bf16), B = exp(src - m) (K x samples,
+// rounded to bf16), FP32 accumulators; max / exp / log stay in FP32.
+// Operands are kept in shared memory as packed bf16 pairs along K, so every mma fragment
+// register is one 32-bit shared load. Tile: TM (16..128) rows x 128 samples, 8 warps:
+// TM/16 warps along the rows, the rest along the samples.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -12,8 +14,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int TB = 128;
-constexpr int KC = 64;
-constexpr int ES = TB + 4;  // padded shared-memory row strides (conflict-free fragment loads)
+constexpr int KC = 32;
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -33,11 +34,15 @@ __global__ void __launch_bounds__(kThreads)
 lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
-                int w_stride, bool vec) {
-    constexpr int MT = TM / 16;  // m16 tiles per warp
-    constexpr int WS = TM + 4;
-    __shared__ __align__(16) float sE[KC][ES];
-    __shared__ __align__(16) float sW[KC][WS];
+                int w_stride, int rpb_log2, bool vec) {
+    constexpr int WM = TM / 16;          // warps along rows
+    constexpr int WN = 8 / WM;           // warps along samples
+    constexpr int NT = TB / 8 / WN;      // n8 tiles per warp
+    constexpr int ES = TB + 8;           // packed row strides (conflict-free fragment loads)
+    constexpr int WS = TM + 8;
+    __shared__ __align__(16) float sE[KC][TB];
+    __shared__ uint32_t sE2[KC / 2][ES];
+    __shared__ uint32_t sW2[KC / 2][WS];
     __shared__ float sMax[TB];
     __shared__ float sScale[TB];
 
@@ -48,17 +53,19 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     const int lane = tid & 31;
     const int g = lane >> 2;
     const int q = lane & 3;
-    const int n0 = warp * 16;
+    const int wm = warp % WM;
+    const int wn = warp / WM;
+    const int m0 = wm * 16;
+    const int nb = wn * (TB / WN);
+    const int rpb_mask = (1 << rpb_log2) - 1;
 
     for (int i = tid; i < TB; i += kThreads) sMax[i] = -INFINITY;
 
-    float acc[MT][2][4];
+    float acc[NT][4];
 #pragma unroll
-    for (int a = 0; a < MT; ++a)
+    for (int a = 0; a < NT; ++a)
 #pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
 
     for (int kc = 0; kc < t.k_cnt; kc += KC) {
         const int n = min(KC, t.k_cnt - kc);
@@ -80,12 +87,18 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
             }
             *reinterpret_cast<float4*>(&sE[k][c4 * 4]) = v;
         }
-        for (int idx = tid; idx < KC * TM; idx += kThreads) {
-            const int k = idx / TM;
+        // weights, packed along K: sW2[k/2][r] = (W(k, r), W(k + 1, r))
+        for (int idx = tid; idx < (KC / 2) * TM; idx += kThreads) {
+            const int kk = idx / TM;
             const int r = idx % TM;
-            float w = 0.f;
-            if (k < n && r < t.n_rows) w = __ldg(params + (int64_t)kw[t.k_off + kc + k] + t.w_add + (int64_t)r * w_stride);
-            sW[k][r] = w;
+            float w0 = 0.f, w1 = 0.f;
+            if (r < t.n_rows) {
+                const int64_t roff = (int64_t)t.w_add + (int64_t)(r >> rpb_log2) * t.g_stride +
+                                     (int64_t)(r & rpb_mask) * w_stride;
+                if (2 * kk < n) w0 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk] + roff);
+                if (2 * kk + 1 < n) w1 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk + 1] + roff);
+            }
+            sW2[kk][r] = pack_bf16(w0, w1);
         }
         __syncthreads();
         for (int b = tid; b < TB; b += kThreads) {
@@ -97,72 +110,64 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
             sMax[b] = nm;
         }
         __syncthreads();
-        for (int idx = tid; idx < KC * TB; idx += kThreads) {
-            const int k = idx / TB;
+        for (int idx = tid; idx < (KC / 2) * TB; idx += kThreads) {
+            const int kk = idx / TB;
             const int b = idx % TB;
             const float m = sMax[b];
-            sE[k][b] = (m == -INFINITY || k >= n) ? 0.f : __expf(sE[k][b] - m);
+            float e0 = 0.f, e1 = 0.f;
+            if (m != -INFINITY) {
+                if (2 * kk < n) e0 = __expf(sE[2 * kk][b] - m);
+                if (2 * kk + 1 < n) e1 = __expf(sE[2 * kk + 1][b] - m);
+            }
+            sE2[kk][b] = pack_bf16(e0, e1);
         }
         __syncthreads();
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const float s0 = sScale[n0 + nt * 8 + 2 * q];
-            const float s1 = sScale[n0 + nt * 8 + 2 * q + 1];
-#pragma unroll
-            for (int a = 0; a < MT; ++a) {
-                acc[a][nt][0] *= s0;
-                acc[a][nt][1] *= s1;
-                acc[a][nt][2] *= s0;
-                acc[a][nt][3] *= s1;
-            }
+        for (int nt = 0; nt < NT; ++nt) {
+            const float s0 = sScale[nb + nt * 8 + 2 * q];
+            const float s1 = sScale[nb + nt * 8 + 2 * q + 1];
+            acc[nt][0] *= s0;
+            acc[nt][1] *= s1;
+            acc[nt][2] *= s0;
+            acc[nt][3] *= s1;
         }
         const int kend = (n + 15) & ~15;
         for (int k0 = 0; k0 < kend; k0 += 16) {
-            uint32_t bf[2][2];
+            const int kk = k0 >> 1;
+            const uint32_t a0 = sW2[kk + q][m0 + g];
+            const uint32_t a1 = sW2[kk + q][m0 + g + 8];
+            const uint32_t a2 = sW2[kk + 4 + q][m0 + g];
+            const uint32_t a3 = sW2[kk + 4 + q][m0 + g + 8];
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                const int col = n0 + nt * 8 + g;
-                bf[nt][0] = pack_bf16(sE[k0 + 2 * q][col], sE[k0 + 2 * q + 1][col]);
-                bf[nt][1] = pack_bf16(sE[k0 + 2 * q + 8][col], sE[k0 + 2 * q + 9][col]);
-            }
-#pragma unroll
-            for (int a = 0; a < MT; ++a) {
-                const int r0 = a * 16 + g;
-                const uint32_t a0 = pack_bf16(sW[k0 + 2 * q][r0], sW[k0 + 2 * q + 1][r0]);
-                const uint32_t a1 = pack_bf16(sW[k0 + 2 * q][r0 + 8], sW[k0 + 2 * q + 1][r0 + 8]);
-                const uint32_t a2 = pack_bf16(sW[k0 + 2 * q + 8][r0], sW[k0 + 2 * q + 9][r0]);
-                const uint32_t a3 = pack_bf16(sW[k0 + 2 * q + 8][r0 + 8], sW[k0 + 2 * q + 9][r0 + 8]);
-#pragma unroll
-                for (int nt = 0; nt < 2; ++nt) mma_bf16(acc[a][nt], a0, a1, a2, a3, bf[nt][0], bf[nt][1]);
+            for (int nt = 0; nt < NT; ++nt) {
+                const int col = nb + nt * 8 + g;
+                mma_bf16(acc[nt], a0, a1, a2, a3, sE2[kk + q][col], sE2[kk + 4 + q][col]);
             }
         }
         __syncthreads();
     }
 
 #pragma unroll
-    for (int a = 0; a < MT; ++a) {
+    for (int h = 0; h < 2; ++h) {
+        const int row = m0 + g + h * 8;
+        if (row >= t.n_rows) continue;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int row = a * 16 + g + h * 8;
-            if (row >= t.n_rows) continue;
+        for (int nt = 0; nt < NT; ++nt) {
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int col = n0 + nt * 8 + 2 * q + j;
-                    const int b = b0 + col;
-                    if (b >= B) continue;
-                    const float m = sMax[col];
-                    const float v = acc[a][nt][h * 2 + j];
-                    float o;
-                    if (MODE == 0) {
-                        o = (m == -INFINITY) ? -INFINITY : logf(v) + m;
-                    } else {
-                        const float x = __ldg(aux + ((int64_t)t.aux_row + row) * ld + b);
-                        o = (m == -INFINITY) ? 0.f : v * __expf(x + m);
-                    }
-                    out[((int64_t)t.out_row + row) * ld + b] = o;
+            for (int j = 0; j < 2; ++j) {
+                const int col = nb + nt * 8 + 2 * q + j;
+                const int b = b0 + col;
+                if (b >= B) continue;
+                const float m = sMax[col];
+                const float v = acc[nt][h * 2 + j];
+                float o;
+                if (MODE == 0) {
+                    o = (m == -INFINITY) ? -INFINITY : logf(v) + m;
+                } else {
+                    const float x = __ldg(aux + ((int64_t)t.aux_row + row) * ld + b);
+                    o = (m == -INFINITY) ? 0.f : v * __expf(x + m);
                 }
+                out[((int64_t)t.out_row + row) * ld + b] = o;
             }
         }
     }
@@ -170,27 +175,31 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
 
 template <int TM>
 int launch(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B, const float* params,
-           const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw, int w_stride, int mode,
-           cudaStream_t s, bool vec) {
+           const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw, int w_stride, int rpb_log2,
+           int mode, cudaStream_t s, bool vec) {
     dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, TB));
+    if (grid.y > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: batch too large");
     if (mode == 0)
-        lse_bf16_kernel<TM, 0><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+        lse_bf16_kernel<TM, 0><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
     else if (mode == 1)
-        lse_bf16_kernel<TM, 1><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+        lse_bf16_kernel<TM, 1><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
     else
-        lse_bf16_kernel<TM, 2><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, vec);
+        lse_bf16_kernel<TM, 2><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
     return pcb::check_launch("pcb_lse_contract(bf16)");
 }
 
 }  // namespace
 
 int pcb_lse_contract_bf16(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
-                          const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows,
+                          const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows, int rpb_log2,
                           const int* krow, const int* kw, int w_stride, int mode, cudaStream_t s) {
     const bool vec = pcb::vec_ok(src, ld) && (!src2 || pcb::vec_ok(src2, ld));
-    if (tile_rows == 32)
-        return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, mode, s, vec);
-    if (tile_rows == 16)
-        return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, mode, s, vec);
-    return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: the bf16 form needs tile_rows 16 or 32, got %d", tile_rows);
+    switch (tile_rows) {
+        case 16: return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
+        case 32: return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
+        case 64: return launch<64>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
+        case 128: return launch<128>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
+        default:
+            return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: the bf16 form needs tile_rows 16..128, got %d", tile_rows);
+    }
 }

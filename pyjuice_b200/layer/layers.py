@@ -31,11 +31,51 @@ def _i32(x) -> torch.Tensor:
     return torch.from_numpy(a.astype(np.int32))
 
 
+_MAX_ROWS = 128  # tallest contraction tile (rows that share one staged set of terms)
+
+
 def _tile_rows(max_rows: int) -> int:
     t = 1
-    while t < max_rows and t < 32:
+    while t < max_rows and t < _MAX_ROWS:
         t *= 2
     return t
+
+
+def _merge_chains(starts, klists, wlists, flists, rpb: int):
+    """Group consecutive blocks into tiles that share one set of contraction terms.
+
+    Blocks ``i .. i + c - 1`` merge when their term lists (``klists``) are identical, their
+    first rows are ``rpb`` apart, and their weight (and flow) offsets differ by one constant
+    stride; at most ``_MAX_ROWS`` rows per chain. Returns ``(first, count, w_stride, f_stride)``.
+    In a structured circuit every region (the node blocks of one sum vector over one
+    product vector) becomes one chain.
+    """
+    chains = []
+    n = len(starts)
+    max_blocks = max(1, _MAX_ROWS // rpb)
+    i = 0
+    while i < n:
+        j = i + 1
+        gs_w = gs_f = 0
+        while j < n and j - i < max_blocks:
+            if starts[j] != starts[j - 1] + rpb or klists[j].shape != klists[i].shape or \
+                    not np.array_equal(klists[j], klists[i]) or klists[i].size == 0:
+                break
+            dw = wlists[j] - wlists[j - 1]
+            if not np.all(dw == dw[0]) or (j - i > 1 and int(dw[0]) != gs_w):
+                break
+            if flists is not None:
+                df = flists[j] - flists[j - 1]
+                if not np.all(df == df[0]) or (j - i > 1 and int(df[0]) != gs_f):
+                    break
+                if j - i == 1:
+                    gs_f = int(df[0])
+            if j - i == 1:
+                gs_w = int(dw[0])
+            j += 1
+        chains.append((i, j - i, gs_w, gs_f))
+        i = j
+    return chains
 
 
 class Layer:
@@ -66,7 +106,13 @@ class Layer:
         key = (device.type, device.index)
         d = self._dev.get(key)
         if d is None:
-            d = {k: (v.to(device) if isinstance(v, torch.Tensor) else v) for k, v in self._host_desc().items()}
+            def mv(v):
+                if isinstance(v, torch.Tensor):
+                    return v.to(device)
+                if isinstance(v, (list, tuple)):
+                    return type(v)(mv(x) for x in v)
+                return v
+            d = {k: mv(v) for k, v in self._host_desc().items()}
             self._dev[key] = d
         return d
 
@@ -149,58 +195,63 @@ class SumLayer(Layer):
                 kw.append(p_np[l, :cnt])
                 kpf.append(f_np[l, :cnt])
                 off += cnt
-        krow = np.concatenate(krow) if krow else np.zeros([0], np.int64)
-        kw = np.concatenate(kw) if kw else np.zeros([0], np.int64)
-        kpf = np.concatenate(kpf) if kpf else np.zeros([0], np.int64)
+        chains = _merge_chains(blk_nid, krow, kw, kpf, bs)
+        krow_c = np.concatenate(krow) if krow else np.zeros([0], np.int64)
+        kw_c = np.concatenate(kw) if kw else np.zeros([0], np.int64)
+        kpf_c = np.concatenate(kpf) if kpf else np.zeros([0], np.int64)
         blk_nid = np.asarray(blk_nid, np.int64)
         blk_koff = np.asarray(blk_koff, np.int64)
         blk_kcnt = np.asarray(blk_kcnt, np.int64)
 
-        tm = _tile_rows(bs)
-        fw_tiles = []
-        for g in range(blk_nid.shape[0]):
-            for i0 in range(0, bs, tm):
-                fw_tiles.append((blk_nid[g] + i0, min(tm, bs - i0), blk_koff[g], blk_kcnt[g], i0, 0))
-        pf_tiles = []
-        for g in range(blk_nid.shape[0]):
-            for i0 in range(0, bs, 32):
+        fw_tiles, pf_tiles = [], []
+        for g, cnt, gs_w, gs_f in chains:
+            rows = cnt * bs
+            for i0 in range(0, rows, _MAX_ROWS):
+                nr = min(_MAX_ROWS, rows - i0)
+                fw_tiles.append((blk_nid[g] + i0, nr, blk_koff[g], blk_kcnt[g], i0, 0, gs_w, 0))
                 for k0 in range(0, int(blk_kcnt[g]), 64):
-                    pf_tiles.append((blk_nid[g] + i0, min(32, bs - i0), blk_koff[g] + k0,
-                                     min(64, int(blk_kcnt[g]) - k0), i0))
+                    pf_tiles.append((blk_nid[g] + i0, nr, blk_koff[g] + k0, min(64, int(blk_kcnt[g]) - k0), i0,
+                                     gs_w, gs_f, 0))
+        fw_tm = _tile_rows(max(t[1] for t in fw_tiles)) if fw_tiles else 1
         node2blk = np.zeros([self.num_nodes // bs], np.int64)
         node2blk[(blk_nid - self._layer_nid_range[0]) // bs] = np.arange(blk_nid.shape[0])
 
-        # element-flow tiles
-        ekrow, ekw, etiles = [], [], []
-        eoff = 0
-        max_cbs = max(self.cs_block_sizes) if self.cs_block_sizes else 1
-        etm = _tile_rows(max_cbs)
-        for chids, parids, parpids, cbs in zip(self.partitioned_chids, self.partitioned_parids,
-                                               self.partitioned_parpids, self.cs_block_sizes):
-            ch_np, pa_np, pp_np = chids.cpu().numpy(), parids.cpu().numpy(), parpids.cpu().numpy()
-            for l in range(ch_np.shape[0]):
-                real = pa_np[l] != 0
-                npar = int(real.sum())
-                par = pa_np[l, :npar]
-                ppar = pp_np[l, :npar]
-                rows = (par[:, None] + np.arange(bs)[None, :]).reshape(-1)
-                wts = (ppar[:, None] + np.arange(bs)[None, :]).reshape(-1)
-                ekrow.append(rows)
-                ekw.append(wts)
-                for j0 in range(0, cbs, etm):
-                    etiles.append((ch_np[l] + j0, min(etm, cbs - j0), eoff, rows.shape[0], j0 * bs, ch_np[l] + j0))
-                eoff += rows.shape[0]
-        ekrow = np.concatenate(ekrow) if ekrow else np.zeros([0], np.int64)
-        ekw = np.concatenate(ekw) if ekw else np.zeros([0], np.int64)
+        # element-flow tiles, one launch per child block size
+        el_groups = []
+        for cbs in sorted(set(self.cs_block_sizes)):
+            starts, klist, wlist = [], [], []
+            for chids, parids, parpids, pcbs in zip(self.partitioned_chids, self.partitioned_parids,
+                                                    self.partitioned_parpids, self.cs_block_sizes):
+                if pcbs != cbs:
+                    continue
+                ch_np, pa_np, pp_np = chids.cpu().numpy(), parids.cpu().numpy(), parpids.cpu().numpy()
+                for l in range(ch_np.shape[0]):
+                    npar = int((pa_np[l] != 0).sum())
+                    starts.append(int(ch_np[l]))
+                    klist.append((pa_np[l, :npar][:, None] + np.arange(bs)[None, :]).reshape(-1))
+                    wlist.append((pp_np[l, :npar][:, None] + np.arange(bs)[None, :]).reshape(-1))
+            if not starts:
+                continue
+            ech = _merge_chains(starts, klist, wlist, None, cbs)
+            offs = np.zeros(len(klist) + 1, np.int64)
+            offs[1:] = np.cumsum([k.shape[0] for k in klist])
+            tiles = []
+            for g, cnt, gs_w, _ in ech:
+                rows = cnt * cbs
+                for j0 in range(0, rows, _MAX_ROWS):
+                    nr = min(_MAX_ROWS, rows - j0)
+                    tiles.append((starts[g] + j0, nr, offs[g], klist[g].shape[0], j0 * bs, starts[g] + j0, gs_w, 0))
+            el_groups.append(dict(
+                cbs=cbs, tm=_tile_rows(max(t[1] for t in tiles)), tiles=_i32(np.asarray(tiles, np.int64).reshape(-1, 8)),
+                krow=_i32(np.concatenate(klist)), kw=_i32(np.concatenate(wlist))))
 
         return dict(
-            fw_tiles=_i32(np.asarray(fw_tiles, np.int64).reshape(-1, 6)), fw_tm=tm,
-            krow=_i32(krow), kw=_i32(kw), kpf=_i32(kpf),
+            fw_tiles=_i32(np.asarray(fw_tiles, np.int64).reshape(-1, 8)), fw_tm=fw_tm,
+            krow=_i32(krow_c), kw=_i32(kw_c), kpf=_i32(kpf_c),
             blk_nid=_i32(blk_nid), blk_koff=_i32(blk_koff), blk_kcnt=_i32(blk_kcnt), node2blk=_i32(node2blk),
             min_kcnt=int(blk_kcnt.min()) if blk_kcnt.size else 0,
-            pf_tiles=_i32(np.asarray(pf_tiles, np.int64).reshape(-1, 5)),
-            el_tiles=_i32(np.asarray(etiles, np.int64).reshape(-1, 6)), el_tm=etm,
-            ekrow=_i32(ekrow), ekw=_i32(ekw),
+            pf_tiles=_i32(np.asarray(pf_tiles, np.int64).reshape(-1, 8)),
+            el_groups=el_groups,
         )
 
     # ---- forward / backward ----
@@ -231,8 +282,8 @@ class SumLayer(Layer):
         prec = 1 if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
         t = d["fw_tiles"]
         nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
-                 nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0,
-                 prec, nat.stream())
+                 nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
+                 nat.ptr(d["kw"]), 1, 0, prec, nat.stream())
 
     __call__ = forward
 
@@ -255,17 +306,18 @@ class SumLayer(Layer):
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
                      self._layer_nid_range[1], nat.stream())
         # element flows
-        et = d["el_tiles"]
-        prec = 1 if (not force_use_fp32 and d["el_tm"] >= 16 and B >= 16) else 0
-        nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
-                 nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
-                 d["el_tm"], nat.ptr(d["ekrow"]), nat.ptr(d["ekw"]), self.block_size, 1 if allow_modify_flows else 2,
-                 prec, nat.stream())
+        for eg in d["el_groups"]:
+            et = eg["tiles"]
+            prec = 1 if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
+            nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
+                     nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
+                     eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
+                     1 if allow_modify_flows else 2, prec, nat.stream())
         # parameter flows
         if param_flows is not None:
             pt = d["pf_tiles"]
             nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
-                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), nat.ptr(d["krow"]),
+                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size, nat.ptr(d["krow"]),
                      nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0, 1 if self._has_tied else 0,
                      nat.stream())
 
