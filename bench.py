@@ -315,11 +315,16 @@ def main():
         del g
         return ms, ck
 
+    from pyjuice_b200.layer.layers import SumLayer
     use_graph = ws == 1
+    SumLayer.bf16_form = 1
+    ms_bf16p, _ = timed({"force_use_bf16": True}, use_graph)
+    SumLayer.bf16_form = 2
     ms_bf16, clocks = timed({"force_use_bf16": True}, use_graph)
     ms_fp32, _ = timed({"force_use_fp32": True}, use_graph)
     value = ws * B * args.steps / (ms_bf16 / 1e3)
     value_fp32 = ws * B * args.steps / (ms_fp32 / 1e3)
+    value_bf16p = ws * B * args.steps / (ms_bf16p / 1e3)
 
     # end to end through the public API, host buffers, LLs read back every step
     host = data[:B * 8].pin_memory()
@@ -361,10 +366,15 @@ def main():
         xs = data[:64]
         _, _, lls_o = orc.forward(lay, params, in_params, xs.numpy())
         with torch.no_grad():
+            SumLayer.bf16_form = 1
+            l_bp = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
+            SumLayer.bf16_form = 2
             l_bf = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
             l_32 = pc(xs.to(device), force_use_fp32=True).double().cpu().numpy()
         ll_err = {"bf16_dmean_ll_nats": float(abs(l_bf.mean() - lls_o.mean())),
                   "bf16_mean_abs_dll_nats": float(np.abs(l_bf - lls_o).mean()),
+                  "bf16_single_dmean_ll_nats": float(abs(l_bp.mean() - lls_o.mean())),
+                  "bf16_single_mean_abs_dll_nats": float(np.abs(l_bp - lls_o).mean()),
                   "fp32_max_rel_dll": float((np.abs(l_32 - lls_o) / np.abs(lls_o)).max()),
                   "fp32_dmean_ll_nats": float(abs(l_32.mean() - lls_o.mean())),
                   "mean_ll_nats": float(lls_o.mean()), "samples": int(xs.size(0))}
@@ -387,7 +397,9 @@ def main():
                        "num_edges": pc.num_edges, "parallelism": f"dp{ws}" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (node_mars alone is 4*N*B bytes > 126 MB); no flush",
                        "cuda_graph": use_graph},
+            "precision_form": "bf16 tensor cores, operands split into bf16 hi + lo (3 MMAs), FP32 accumulate",
             "fp32_plain": {"value": value_fp32, "unit": "samples/s", "ms_per_step": ms_fp32 / args.steps},
+            "bf16_single": {"value": value_bf16p, "unit": "samples/s", "ms_per_step": ms_bf16p / args.steps},
             "ll_error_vs_fp64": ll_err,
             "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": B * SIDE * SIDE * 8,
                     "d2h_bytes_per_step": B * 4},

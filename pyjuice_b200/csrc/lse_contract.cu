@@ -176,7 +176,7 @@ int ilog2(int v) {
 // Tensor-core (BF16) variant, defined in lse_contract_tc.cu.
 int pcb_lse_contract_bf16(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                           const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows, int rpb_log2,
-                          const int* krow, const int* kw, int w_stride, int mode, cudaStream_t s);
+                          const int* krow, const int* kw, int w_stride, int mode, bool split, cudaStream_t s);
 
 extern "C" int pcb_lse_contract(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
                                 int32_t B, const float* params, const PcbLseTile* tiles, int32_t num_tiles,
@@ -190,10 +190,11 @@ extern "C" int pcb_lse_contract(const float* src, const float* src2, const float
     if (rpb_log2 < 0) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: rows_per_block must be a power of 2");
     if (num_tiles == 0) return PCB_OK;
     cudaStream_t s = pcb::as_stream(stream);
-    if (prec == 1) {
+    if (prec == 1 || prec == 2) {
         return pcb_lse_contract_bf16(src, src2, aux, out, ld, B, params, tiles, num_tiles, tile_rows, rpb_log2, krow, kw,
-                                     w_stride, mode, s);
+                                     w_stride, mode, prec == 2, s);
     }
+    if (prec != 0) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: prec must be 0, 1 or 2");
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!aux || pcb::vec_ok(aux, ld)) &&
                      (!src2 || pcb::vec_ok(src2, ld));
 #define PCB_LSE(TM, TB, KC) launch_cfg<TM, TB, KC>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec)

@@ -6,6 +6,11 @@
 // Operands are kept in shared memory as packed bf16 pairs along K, so every mma fragment
 // register is one 32-bit shared load. Tile: TM (16..128) rows x 128 samples, 8 warps:
 // TM/16 warps along the rows, the rest along the samples.
+//
+// SPLIT: each operand x is held as hi = bf16(x) plus lo = bf16(x - hi) and the product is
+// accumulated as hi*hi + lo*hi + hi*lo (three bf16 MMAs). This keeps the contraction on
+// the bf16 tensor cores while removing the bf16 rounding of the weights, whose per-node
+// sums would otherwise drift from one and bias every sample's log-likelihood the same way.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -29,7 +34,15 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-template <int TM, int MODE>
+__device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, uint32_t& l) {
+    __nv_bfloat162 hv = __floats2bfloat162_rn(lo_k, hi_k);
+    const float2 hf = __bfloat1622float2(hv);
+    __nv_bfloat162 lv = __floats2bfloat162_rn(lo_k - hf.x, hi_k - hf.y);
+    h = *reinterpret_cast<uint32_t*>(&hv);
+    l = *reinterpret_cast<uint32_t*>(&lv);
+}
+
+template <int TM, int MODE, bool SPLIT>
 __global__ void __launch_bounds__(kThreads)
 lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
@@ -40,11 +53,14 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     constexpr int NT = TB / 8 / WN;      // n8 tiles per warp
     constexpr int ES = TB + 8;           // packed row strides (conflict-free fragment loads)
     constexpr int WS = TM + 8;
-    __shared__ __align__(16) float sE[KC][TB];
-    __shared__ uint32_t sE2[KC / 2][ES];
-    __shared__ uint32_t sW2[KC / 2][WS];
-    __shared__ float sMax[TB];
-    __shared__ float sScale[TB];
+    extern __shared__ __align__(16) unsigned char dsm[];
+    float (*sE)[TB] = reinterpret_cast<float (*)[TB]>(dsm);
+    uint32_t (*sE2)[ES] = reinterpret_cast<uint32_t (*)[ES]>(dsm + sizeof(float) * KC * TB);
+    uint32_t (*sW2)[WS] = reinterpret_cast<uint32_t (*)[WS]>(reinterpret_cast<unsigned char*>(sE2) + 4 * (KC / 2) * ES);
+    uint32_t (*sE2l)[ES] = reinterpret_cast<uint32_t (*)[ES]>(reinterpret_cast<unsigned char*>(sW2) + 4 * (KC / 2) * WS);
+    uint32_t (*sW2l)[WS] = reinterpret_cast<uint32_t (*)[WS]>(reinterpret_cast<unsigned char*>(sE2l) + (SPLIT ? 4 * (KC / 2) * ES : 0));
+    float* sMax = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sW2l) + (SPLIT ? 4 * (KC / 2) * WS : 0));
+    float* sScale = sMax + TB;
 
     const PcbLseTile t = tiles[blockIdx.x];
     const int b0 = blockIdx.y * TB;
@@ -98,7 +114,8 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
                 if (2 * kk < n) w0 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk] + roff);
                 if (2 * kk + 1 < n) w1 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk + 1] + roff);
             }
-            sW2[kk][r] = pack_bf16(w0, w1);
+            if (SPLIT) split_bf16(w0, w1, sW2[kk][r], sW2l[kk][r]);
+            else sW2[kk][r] = pack_bf16(w0, w1);
         }
         __syncthreads();
         for (int b = tid; b < TB; b += kThreads) {
@@ -119,7 +136,8 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
                 if (2 * kk < n) e0 = __expf(sE[2 * kk][b] - m);
                 if (2 * kk + 1 < n) e1 = __expf(sE[2 * kk + 1][b] - m);
             }
-            sE2[kk][b] = pack_bf16(e0, e1);
+            if (SPLIT) split_bf16(e0, e1, sE2[kk][b], sE2l[kk][b]);
+            else sE2[kk][b] = pack_bf16(e0, e1);
         }
         __syncthreads();
 #pragma unroll
@@ -138,10 +156,25 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
             const uint32_t a1 = sW2[kk + q][m0 + g + 8];
             const uint32_t a2 = sW2[kk + 4 + q][m0 + g];
             const uint32_t a3 = sW2[kk + 4 + q][m0 + g + 8];
+            if (SPLIT) {
+                const uint32_t l0 = sW2l[kk + q][m0 + g];
+                const uint32_t l1 = sW2l[kk + q][m0 + g + 8];
+                const uint32_t l2 = sW2l[kk + 4 + q][m0 + g];
+                const uint32_t l3 = sW2l[kk + 4 + q][m0 + g + 8];
 #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const int col = nb + nt * 8 + g;
-                mma_bf16(acc[nt], a0, a1, a2, a3, sE2[kk + q][col], sE2[kk + 4 + q][col]);
+                for (int nt = 0; nt < NT; ++nt) {
+                    const int col = nb + nt * 8 + g;
+                    const uint32_t bh0 = sE2[kk + q][col], bh1 = sE2[kk + 4 + q][col];
+                    mma_bf16(acc[nt], a0, a1, a2, a3, bh0, bh1);
+                    mma_bf16(acc[nt], l0, l1, l2, l3, bh0, bh1);
+                    mma_bf16(acc[nt], a0, a1, a2, a3, sE2l[kk + q][col], sE2l[kk + 4 + q][col]);
+                }
+            } else {
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    const int col = nb + nt * 8 + g;
+                    mma_bf16(acc[nt], a0, a1, a2, a3, sE2[kk + q][col], sE2[kk + 4 + q][col]);
+                }
             }
         }
         __syncthreads();
@@ -173,32 +206,53 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     }
 }
 
+template <int TM, int MODE, bool SPLIT>
+int launch_one(dim3 grid, const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
+               const float* params, const PcbLseTile* tiles, const int* krow, const int* kw, int w_stride,
+               int rpb_log2, cudaStream_t s, bool vec) {
+    constexpr int ES = TB + 8, WS = TM + 8;
+    constexpr size_t smem = sizeof(float) * KC * TB + 4 * (KC / 2) * (ES + WS) * (SPLIT ? 2 : 1) + 2 * sizeof(float) * TB;
+    static bool configured = false;  // per instantiation; the attribute is per function, not per device state
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(lse_bf16_kernel<TM, MODE, SPLIT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract(bf16): %s", cudaGetErrorString(e));
+        configured = true;
+    }
+    lse_bf16_kernel<TM, MODE, SPLIT><<<grid, kThreads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw,
+                                                                  w_stride, rpb_log2, vec);
+    return pcb::check_launch("pcb_lse_contract(bf16)");
+}
+
 template <int TM>
 int launch(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B, const float* params,
            const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw, int w_stride, int rpb_log2,
-           int mode, cudaStream_t s, bool vec) {
+           int mode, bool split, cudaStream_t s, bool vec) {
     dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, TB));
     if (grid.y > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: batch too large");
-    if (mode == 0)
-        lse_bf16_kernel<TM, 0><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    else if (mode == 1)
-        lse_bf16_kernel<TM, 1><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    else
-        lse_bf16_kernel<TM, 2><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    return pcb::check_launch("pcb_lse_contract(bf16)");
+#define PCB_L1(M, S) launch_one<TM, M, S>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec)
+    if (split) {
+        if (mode == 0) return PCB_L1(0, true);
+        if (mode == 1) return PCB_L1(1, true);
+        return PCB_L1(2, true);
+    }
+    if (mode == 0) return PCB_L1(0, false);
+    if (mode == 1) return PCB_L1(1, false);
+    return PCB_L1(2, false);
+#undef PCB_L1
 }
 
 }  // namespace
 
 int pcb_lse_contract_bf16(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                           const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows, int rpb_log2,
-                          const int* krow, const int* kw, int w_stride, int mode, cudaStream_t s) {
+                          const int* krow, const int* kw, int w_stride, int mode, bool split, cudaStream_t s) {
     const bool vec = pcb::vec_ok(src, ld) && (!src2 || pcb::vec_ok(src2, ld));
     switch (tile_rows) {
-        case 16: return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
-        case 32: return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
-        case 64: return launch<64>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
-        case 128: return launch<128>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec);
+        case 16: return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
+        case 32: return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
+        case 64: return launch<64>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
+        case 128: return launch<128>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
         default:
             return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: the bf16 form needs tile_rows 16..128, got %d", tile_rows);
     }

@@ -111,6 +111,8 @@ class Layer:
                     return v.to(device)
                 if isinstance(v, (list, tuple)):
                     return type(v)(mv(x) for x in v)
+                if isinstance(v, dict):
+                    return {kk: mv(vv) for kk, vv in v.items()}
                 return v
             d = {k: mv(v) for k, v in self._host_desc().items()}
             self._dev[key] = d
@@ -128,7 +130,15 @@ class Layer:
 
 
 class SumLayer(Layer):
-    """A layer of sum node vectors with the same block size."""
+    """A layer of sum node vectors with the same block size.
+
+    Precision forms of the sum contractions: plain FP32 (``force_use_fp32``) or the BF16
+    tensor-core form. ``SumLayer.bf16_form`` selects the latter's variant: 2 (default)
+    splits both operands into bf16 hi + lo parts (three MMAs, FP32-like accuracy), 1 uses
+    single bf16 operands.
+    """
+
+    bf16_form = 2
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -279,7 +289,7 @@ class SumLayer(Layer):
         ld = node_mars.stride(0)
         if element_mars.stride(0) != ld or node_mars.stride(1) != 1 or element_mars.stride(1) != 1:
             raise ValueError("node_mars and element_mars must share a row-major layout")
-        prec = 1 if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
+        prec = SumLayer.bf16_form if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
         t = d["fw_tiles"]
         nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
                  nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
@@ -308,7 +318,7 @@ class SumLayer(Layer):
         # element flows
         for eg in d["el_groups"]:
             et = eg["tiles"]
-            prec = 1 if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
+            prec = SumLayer.bf16_form if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
             nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
                      nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
                      eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,

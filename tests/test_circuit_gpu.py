@@ -116,6 +116,25 @@ def test_bf16_forward_error_vs_fp64(cuda_device):
     assert abs(lls_bf.mean() - lls_o.mean()) < 1e-3
 
 
+def test_bf16_single_operand_form(cuda_device):
+    """The single-bf16 variant (one MMA per fragment) stays within its rounding error."""
+    from pyjuice_b200.layer.layers import SumLayer
+    fx = load_fixture("hclt784")
+    pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    p0, q0 = fixture_params(pc, fx)
+    _, _, lls_o = orc.forward(orc.layout_from_circuit(pc), p0, q0, fx["x"])
+    saved = SumLayer.bf16_form
+    try:
+        SumLayer.bf16_form = 1
+        with torch.no_grad():
+            lls = pc(x, force_use_bf16=True).double().cpu().numpy()
+    finally:
+        SumLayer.bf16_form = saved
+    assert np.abs(lls - lls_o).max() < 0.05
+
+
 def test_cuda_graph_replay_matches_eager(cuda_device):
     fx = load_fixture("hclt64")
     pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
