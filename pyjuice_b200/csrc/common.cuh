@@ -73,6 +73,23 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Asynchronous global -> shared copies (no register round trip, so a thread can have many
+// in flight). 16-byte copies need 16-byte aligned addresses on both sides.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Vectorised access needs ld % 4 == 0 and a 16-byte aligned base.
 inline bool vec_ok(const void* p, int64_t ld) {
     return (ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);

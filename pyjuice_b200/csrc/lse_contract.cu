@@ -6,41 +6,40 @@
 // rescaling, one max per sample, shared by all rows of the tile). A tile spans several
 // node blocks that share their children (a whole region of a structured circuit), so
 // every staged child value is exponentiated once and reused by up to 128 output rows.
-// Terms are staged in shared memory in chunks of KC rows.
 //   W(k, r) = params[kw[k] + w_add + (r >> rpb_log2) * g_stride + (r & (rpb - 1)) * w_stride]
+//
+// Terms are staged in chunks of KC with asynchronous copies (cp.async) into two shared
+// buffers: the copies of chunk c + 1 are in flight while chunk c is reduced, so a CTA
+// pays one memory latency per tile rather than one per staged value.
 //
 // Epilogues: mode 0 writes log(acc) + m (sum forward); modes 1/2 write
 // acc * exp(aux + m) (element flows; mode 2 first turns node flows into log f - log m).
-#include "common.cuh"
+#include "lse_stage.cuh"
 
 namespace {
 
-constexpr int kThreads = 256;
-
-template <int TM, int TB, int KC, int MODE>
-__global__ void __launch_bounds__(kThreads)
+template <int TM, int TB, int RN, int MODE>
+__global__ void __launch_bounds__(TB / 4 * (TM / RN))
 lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                int w_stride, int rpb_log2, bool vec) {
     constexpr int NX = TB / 4;           // threads along the batch (4 samples each)
-    constexpr int NY = kThreads / NX;    // threads along rows
-    constexpr int RN = TM / NY;          // rows per thread
-    static_assert(NY * RN == TM && RN >= 1, "tile shape");
-
-    __shared__ __align__(16) float sE[KC][TB];
-    __shared__ __align__(16) float sW[KC][TM];
-    __shared__ float sMax[TB];
-    __shared__ float sScale[TB];
+    constexpr int NY = TM / RN;          // threads along rows
+    constexpr int NT = NX * NY;
+    using St = pcb::LseStage<TM, TB, MODE == 2>;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    St st(dsm);
+    float* sMax = st.end();
+    float* sScale = sMax + TB;
 
     const PcbLseTile t = tiles[blockIdx.x];
     const int b0 = blockIdx.y * TB;
     const int tid = threadIdx.x;
     const int tx = tid % NX;
     const int ty = tid / NX;
-    const int rpb_mask = (1 << rpb_log2) - 1;
 
-    for (int i = tid; i < TB; i += kThreads) sMax[i] = -INFINITY;
+    for (int i = tid; i < TB; i += NT) sMax[i] = -INFINITY;
 
     float acc[RN][4];
 #pragma unroll
@@ -48,48 +47,23 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[r][j] = 0.f;
 
-    for (int kc = 0; kc < t.k_cnt; kc += KC) {
-        const int n = min(KC, t.k_cnt - kc);
-        for (int idx = tid; idx < KC * NX; idx += kThreads) {
-            const int k = idx / NX;
-            const int c4 = idx % NX;
-            float4 v = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
-            if (k < n) {
-                const int row = krow[t.k_off + kc + k];
-                v = pcb::load4(src, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
-                if (MODE == 2) {
-                    const float4 m = pcb::load4(src2, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float mm = pcb::get(m, j);
-                        pcb::set(v, j, (mm == -INFINITY) ? -INFINITY : logf(pcb::get(v, j)) - mm);
-                    }
-                }
-            }
-            *reinterpret_cast<float4*>(&sE[k][c4 * 4]) = v;
-        }
-        for (int idx = tid; idx < KC * TM; idx += kThreads) {
-            const int k = idx / TM;
-            const int r = idx % TM;
-            float w = 0.f;
-            if (k < n && r < t.n_rows) {
-                const int64_t wi = (int64_t)kw[t.k_off + kc + k] + t.w_add + (int64_t)(r >> rpb_log2) * t.g_stride +
-                                   (int64_t)(r & rpb_mask) * w_stride;
-                w = __ldg(params + wi);
-            }
-            sW[k][r] = w;
+    const int nchunks = (t.k_cnt + pcb::kLseKC - 1) / pcb::kLseKC;
+    st.template issue<NT>(0, 0, t, src, src2, params, krow, kw, ld, B, b0, w_stride, rpb_log2, vec, tid);
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c & 1;
+        if (c + 1 < nchunks) {
+            st.template issue<NT>(c + 1, s ^ 1, t, src, src2, params, krow, kw, ld, B, b0, w_stride, rpb_log2, vec, tid);
+            pcb::cp_async_wait<1>();
+        } else {
+            pcb::cp_async_wait<0>();
         }
         __syncthreads();
-        for (int b = tid; b < TB; b += kThreads) {
-            float cm = -INFINITY;
-            for (int k = 0; k < n; ++k) cm = fmaxf(cm, sE[k][b]);
-            const float old = sMax[b];
-            const float nm = fmaxf(old, cm);
-            sScale[b] = (nm == -INFINITY) ? 1.f : __expf(old - nm);
-            sMax[b] = nm;
-        }
+        const int n = min(pcb::kLseKC, t.k_cnt - c * pcb::kLseKC);
+        float (*sE)[TB] = st.E(s);
+        float (*sW)[TM] = st.W(s);
+        st.transform_and_max(s, n, sMax, sScale, tid, NT);
         __syncthreads();
-        for (int idx = tid; idx < n * TB; idx += kThreads) {
+        for (int idx = tid; idx < n * TB; idx += NT) {
             const int k = idx / TB;
             const int b = idx % TB;
             const float m = sMax[b];
@@ -98,9 +72,9 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float s = sScale[tx * 4 + j];
+            const float sc = sScale[tx * 4 + j];
 #pragma unroll
-            for (int r = 0; r < RN; ++r) acc[r][j] *= s;
+            for (int r = 0; r < RN; ++r) acc[r][j] *= sc;
         }
         for (int k = 0; k < n; ++k) {
             const float4 e = *reinterpret_cast<const float4*>(&sE[k][tx * 4]);
@@ -150,19 +124,36 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
     }
 }
 
-template <int TM, int TB, int KC>
+template <int TM, int TB, int RN, int MODE>
+int launch_mode(dim3 grid, const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
+                const float* params, const PcbLseTile* tiles, const int* krow, const int* kw, int w_stride,
+                int rpb_log2, cudaStream_t s, bool vec) {
+    constexpr int threads = TB / 4 * (TM / RN);
+    constexpr size_t smem = pcb::LseStage<TM, TB, MODE == 2>::bytes() + 2 * sizeof(float) * TB;
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev = dev < 0 ? 0 : (dev > 63 ? 63 : dev);
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(lse_f32_kernel<TM, TB, RN, MODE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract: %s", cudaGetErrorString(e));
+        configured[dev] = true;
+    }
+    lse_f32_kernel<TM, TB, RN, MODE><<<grid, threads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw,
+                                                                 w_stride, rpb_log2, vec);
+    return pcb::check_launch("pcb_lse_contract");
+}
+
+template <int TM, int TB, int RN>
 int launch_cfg(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                const float* params, const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw,
                int w_stride, int rpb_log2, int mode, cudaStream_t s, bool vec) {
     dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, TB));
     if (grid.y > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: batch too large");
-    if (mode == 0)
-        lse_f32_kernel<TM, TB, KC, 0><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    else if (mode == 1)
-        lse_f32_kernel<TM, TB, KC, 1><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    else
-        lse_f32_kernel<TM, TB, KC, 2><<<grid, kThreads, 0, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, vec);
-    return pcb::check_launch("pcb_lse_contract");
+    if (mode == 0) return launch_mode<TM, TB, RN, 0>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec);
+    if (mode == 1) return launch_mode<TM, TB, RN, 1>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec);
+    return launch_mode<TM, TB, RN, 2>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec);
 }
 
 int ilog2(int v) {
@@ -197,16 +188,16 @@ extern "C" int pcb_lse_contract(const float* src, const float* src2, const float
     if (prec != 0) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: prec must be 0, 1 or 2");
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!aux || pcb::vec_ok(aux, ld)) &&
                      (!src2 || pcb::vec_ok(src2, ld));
-#define PCB_LSE(TM, TB, KC) launch_cfg<TM, TB, KC>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec)
+#define PCB_LSE(TM, TB, RN) launch_cfg<TM, TB, RN>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec)
     switch (tile_rows) {
-        case 1: return PCB_LSE(1, 1024, 8);
-        case 2: return PCB_LSE(2, 1024, 8);
-        case 4: return PCB_LSE(4, 1024, 8);
-        case 8: return PCB_LSE(8, 512, 16);
-        case 16: return PCB_LSE(16, 256, 32);
-        case 32: return PCB_LSE(32, 128, 64);
-        case 64: return PCB_LSE(64, 128, 32);
-        case 128: return PCB_LSE(128, 128, 32);
+        case 1: return PCB_LSE(1, 128, 1);
+        case 2: return PCB_LSE(2, 128, 1);
+        case 4: return PCB_LSE(4, 128, 1);
+        case 8: return PCB_LSE(8, 128, 1);
+        case 16: return PCB_LSE(16, 128, 2);
+        case 32: return PCB_LSE(32, 128, 4);
+        case 64: return PCB_LSE(64, 64, 4);
+        case 128: return PCB_LSE(128, 32, 4);
         default:
             return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: tile_rows must be a power of 2 <= 128, got %d", tile_rows);
     }

@@ -1,11 +1,11 @@
 // BF16 tensor-core form of the log-sum-exp contraction (see lse_contract.cu).
 //
-// Same tiles and online-max scheme as the FP32 kernel; each staged chunk is contracted on
-// the tensor cores: A = W (rows x K, rounded to bf16), B = exp(src - m) (K x samples,
-// rounded to bf16), FP32 accumulators; max / exp / log stay in FP32.
-// Operands are kept in shared memory as packed bf16 pairs along K, so every mma fragment
-// register is one 32-bit shared load. Tile: TM (16..128) rows x 128 samples, 8 warps:
-// TM/16 warps along the rows, the rest along the samples.
+// Same tiles, asynchronous double-buffered staging (lse_stage.cuh) and online-max scheme
+// as the FP32 kernel; each staged chunk is contracted on the tensor cores: A = W (rows x K)
+// and B = exp(src - m) (K x samples) in bf16, FP32 accumulators; max / exp / log stay in
+// FP32. Operands are repacked in shared memory as bf16 pairs along K, so every mma
+// fragment register is one 32-bit shared load. 8 warps: TM/16 along the rows, the rest
+// along the samples.
 //
 // SPLIT: each operand x is held as hi = bf16(x) plus lo = bf16(x - hi) and the product is
 // accumulated as hi*hi + lo*hi + hi*lo (three bf16 MMAs). This keeps the contraction on
@@ -13,25 +13,16 @@
 // sums would otherwise drift from one and bias every sample's log-likelihood the same way.
 #include <cuda_bf16.h>
 
-#include "common.cuh"
+#include "lse_stage.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int TB = 128;
-constexpr int KC = 32;
+constexpr int KC = pcb::kLseKC;
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
 __device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, uint32_t& l) {
@@ -42,7 +33,30 @@ __device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, 
     l = *reinterpret_cast<uint32_t*>(&lv);
 }
 
-template <int TM, int MODE, bool SPLIT>
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int TM, int TB, bool SPLIT>
+struct Packed {
+    static constexpr int ES = TB + 8;  // packed row strides: conflict-free fragment loads
+    static constexpr int WS = TM + 8;
+    static constexpr int NB = SPLIT ? 2 : 1;
+    static constexpr size_t bytes() { return 4ull * (KC / 2) * (ES + WS) * NB; }
+    uint32_t* p;
+    __device__ explicit Packed(float* base) : p(reinterpret_cast<uint32_t*>(base)) {}
+    __device__ uint32_t (*E(int h))[ES] { return reinterpret_cast<uint32_t(*)[ES]>(p + h * (KC / 2) * ES); }
+    __device__ uint32_t (*W(int h))[WS] {
+        return reinterpret_cast<uint32_t(*)[WS]>(p + NB * (KC / 2) * ES + h * (KC / 2) * WS);
+    }
+    __device__ float* end() { return reinterpret_cast<float*>(p + NB * (KC / 2) * (ES + WS)); }
+};
+
+template <int TM, int TB, int MODE, bool SPLIT>
 __global__ void __launch_bounds__(kThreads)
 lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
@@ -51,15 +65,12 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     constexpr int WM = TM / 16;          // warps along rows
     constexpr int WN = 8 / WM;           // warps along samples
     constexpr int NT = TB / 8 / WN;      // n8 tiles per warp
-    constexpr int ES = TB + 8;           // packed row strides (conflict-free fragment loads)
-    constexpr int WS = TM + 8;
+    using St = pcb::LseStage<TM, TB, MODE == 2>;
+    using Pk = Packed<TM, TB, SPLIT>;
     extern __shared__ __align__(16) unsigned char dsm[];
-    float (*sE)[TB] = reinterpret_cast<float (*)[TB]>(dsm);
-    uint32_t (*sE2)[ES] = reinterpret_cast<uint32_t (*)[ES]>(dsm + sizeof(float) * KC * TB);
-    uint32_t (*sW2)[WS] = reinterpret_cast<uint32_t (*)[WS]>(reinterpret_cast<unsigned char*>(sE2) + 4 * (KC / 2) * ES);
-    uint32_t (*sE2l)[ES] = reinterpret_cast<uint32_t (*)[ES]>(reinterpret_cast<unsigned char*>(sW2) + 4 * (KC / 2) * WS);
-    uint32_t (*sW2l)[WS] = reinterpret_cast<uint32_t (*)[WS]>(reinterpret_cast<unsigned char*>(sE2l) + (SPLIT ? 4 * (KC / 2) * ES : 0));
-    float* sMax = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(sW2l) + (SPLIT ? 4 * (KC / 2) * WS : 0));
+    St st(dsm);
+    Pk pk(st.end());
+    float* sMax = pk.end();
     float* sScale = sMax + TB;
 
     const PcbLseTile t = tiles[blockIdx.x];
@@ -69,11 +80,8 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     const int lane = tid & 31;
     const int g = lane >> 2;
     const int q = lane & 3;
-    const int wm = warp % WM;
-    const int wn = warp / WM;
-    const int m0 = wm * 16;
-    const int nb = wn * (TB / WN);
-    const int rpb_mask = (1 << rpb_log2) - 1;
+    const int m0 = (warp % WM) * 16;
+    const int nb = (warp / WM) * (TB / WN);
 
     for (int i = tid; i < TB; i += kThreads) sMax[i] = -INFINITY;
 
@@ -83,49 +91,22 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
 
-    for (int kc = 0; kc < t.k_cnt; kc += KC) {
-        const int n = min(KC, t.k_cnt - kc);
-        for (int idx = tid; idx < KC * (TB / 4); idx += kThreads) {
-            const int k = idx / (TB / 4);
-            const int c4 = idx % (TB / 4);
-            float4 v = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
-            if (k < n) {
-                const int row = krow[t.k_off + kc + k];
-                v = pcb::load4(src, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
-                if (MODE == 2) {
-                    const float4 m = pcb::load4(src2, row, ld, b0 + c4 * 4, B, vec, -INFINITY);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float mm = pcb::get(m, j);
-                        pcb::set(v, j, (mm == -INFINITY) ? -INFINITY : logf(pcb::get(v, j)) - mm);
-                    }
-                }
-            }
-            *reinterpret_cast<float4*>(&sE[k][c4 * 4]) = v;
-        }
-        // weights, packed along K: sW2[k/2][r] = (W(k, r), W(k + 1, r))
-        for (int idx = tid; idx < (KC / 2) * TM; idx += kThreads) {
-            const int kk = idx / TM;
-            const int r = idx % TM;
-            float w0 = 0.f, w1 = 0.f;
-            if (r < t.n_rows) {
-                const int64_t roff = (int64_t)t.w_add + (int64_t)(r >> rpb_log2) * t.g_stride +
-                                     (int64_t)(r & rpb_mask) * w_stride;
-                if (2 * kk < n) w0 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk] + roff);
-                if (2 * kk + 1 < n) w1 = __ldg(params + (int64_t)kw[t.k_off + kc + 2 * kk + 1] + roff);
-            }
-            if (SPLIT) split_bf16(w0, w1, sW2[kk][r], sW2l[kk][r]);
-            else sW2[kk][r] = pack_bf16(w0, w1);
+    const int nchunks = (t.k_cnt + KC - 1) / KC;
+    st.template issue<kThreads>(0, 0, t, src, src2, params, krow, kw, ld, B, b0, w_stride, rpb_log2, vec, tid);
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c & 1;
+        if (c + 1 < nchunks) {
+            st.template issue<kThreads>(c + 1, s ^ 1, t, src, src2, params, krow, kw, ld, B, b0, w_stride, rpb_log2,
+                                        vec, tid);
+            pcb::cp_async_wait<1>();
+        } else {
+            pcb::cp_async_wait<0>();
         }
         __syncthreads();
-        for (int b = tid; b < TB; b += kThreads) {
-            float cm = -INFINITY;
-            for (int k = 0; k < n; ++k) cm = fmaxf(cm, sE[k][b]);
-            const float old = sMax[b];
-            const float nm = fmaxf(old, cm);
-            sScale[b] = (nm == -INFINITY) ? 1.f : __expf(old - nm);
-            sMax[b] = nm;
-        }
+        const int n = min(KC, t.k_cnt - c * KC);
+        float(*sE)[TB] = st.E(s);
+        float(*sW)[TM] = st.W(s);
+        st.transform_and_max(s, n, sMax, sScale, tid, kThreads);
         __syncthreads();
         for (int idx = tid; idx < (KC / 2) * TB; idx += kThreads) {
             const int kk = idx / TB;
@@ -136,8 +117,16 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
                 if (2 * kk < n) e0 = __expf(sE[2 * kk][b] - m);
                 if (2 * kk + 1 < n) e1 = __expf(sE[2 * kk + 1][b] - m);
             }
-            if (SPLIT) split_bf16(e0, e1, sE2[kk][b], sE2l[kk][b]);
-            else sE2[kk][b] = pack_bf16(e0, e1);
+            if (SPLIT) split_bf16(e0, e1, pk.E(0)[kk][b], pk.E(1)[kk][b]);
+            else pk.E(0)[kk][b] = pack_bf16(e0, e1);
+        }
+        for (int idx = tid; idx < (KC / 2) * TM; idx += kThreads) {
+            const int kk = idx / TM;
+            const int r = idx % TM;
+            const float w0 = sW[2 * kk][r];
+            const float w1 = sW[2 * kk + 1][r];
+            if (SPLIT) split_bf16(w0, w1, pk.W(0)[kk][r], pk.W(1)[kk][r]);
+            else pk.W(0)[kk][r] = pack_bf16(w0, w1);
         }
         __syncthreads();
 #pragma unroll
@@ -152,28 +141,28 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
         const int kend = (n + 15) & ~15;
         for (int k0 = 0; k0 < kend; k0 += 16) {
             const int kk = k0 >> 1;
-            const uint32_t a0 = sW2[kk + q][m0 + g];
-            const uint32_t a1 = sW2[kk + q][m0 + g + 8];
-            const uint32_t a2 = sW2[kk + 4 + q][m0 + g];
-            const uint32_t a3 = sW2[kk + 4 + q][m0 + g + 8];
+            const uint32_t a0 = pk.W(0)[kk + q][m0 + g];
+            const uint32_t a1 = pk.W(0)[kk + q][m0 + g + 8];
+            const uint32_t a2 = pk.W(0)[kk + 4 + q][m0 + g];
+            const uint32_t a3 = pk.W(0)[kk + 4 + q][m0 + g + 8];
             if (SPLIT) {
-                const uint32_t l0 = sW2l[kk + q][m0 + g];
-                const uint32_t l1 = sW2l[kk + q][m0 + g + 8];
-                const uint32_t l2 = sW2l[kk + 4 + q][m0 + g];
-                const uint32_t l3 = sW2l[kk + 4 + q][m0 + g + 8];
+                const uint32_t l0 = pk.W(1)[kk + q][m0 + g];
+                const uint32_t l1 = pk.W(1)[kk + q][m0 + g + 8];
+                const uint32_t l2 = pk.W(1)[kk + 4 + q][m0 + g];
+                const uint32_t l3 = pk.W(1)[kk + 4 + q][m0 + g + 8];
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
                     const int col = nb + nt * 8 + g;
-                    const uint32_t bh0 = sE2[kk + q][col], bh1 = sE2[kk + 4 + q][col];
+                    const uint32_t bh0 = pk.E(0)[kk + q][col], bh1 = pk.E(0)[kk + 4 + q][col];
                     mma_bf16(acc[nt], a0, a1, a2, a3, bh0, bh1);
                     mma_bf16(acc[nt], l0, l1, l2, l3, bh0, bh1);
-                    mma_bf16(acc[nt], a0, a1, a2, a3, sE2l[kk + q][col], sE2l[kk + 4 + q][col]);
+                    mma_bf16(acc[nt], a0, a1, a2, a3, pk.E(1)[kk + q][col], pk.E(1)[kk + 4 + q][col]);
                 }
             } else {
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
                     const int col = nb + nt * 8 + g;
-                    mma_bf16(acc[nt], a0, a1, a2, a3, sE2[kk + q][col], sE2[kk + 4 + q][col]);
+                    mma_bf16(acc[nt], a0, a1, a2, a3, pk.E(0)[kk + q][col], pk.E(0)[kk + 4 + q][col]);
                 }
             }
         }
@@ -186,51 +175,63 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
         if (row >= t.n_rows) continue;
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
+            const int col = nb + nt * 8 + 2 * q;
+            const int b = b0 + col;
+            float o[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int col = nb + nt * 8 + 2 * q + j;
-                const int b = b0 + col;
-                if (b >= B) continue;
-                const float m = sMax[col];
+                const float m = sMax[col + j];
                 const float v = acc[nt][h * 2 + j];
-                float o;
                 if (MODE == 0) {
-                    o = (m == -INFINITY) ? -INFINITY : logf(v) + m;
+                    o[j] = (m == -INFINITY) ? -INFINITY : logf(v) + m;
                 } else {
-                    const float x = __ldg(aux + ((int64_t)t.aux_row + row) * ld + b);
-                    o = (m == -INFINITY) ? 0.f : v * __expf(x + m);
+                    const float x = (b + j < B) ? __ldg(aux + ((int64_t)t.aux_row + row) * ld + b + j) : 0.f;
+                    o[j] = (m == -INFINITY) ? 0.f : v * __expf(x + m);
                 }
-                out[((int64_t)t.out_row + row) * ld + b] = o;
+            }
+            float* dst = out + ((int64_t)t.out_row + row) * ld + b;
+            if (vec && b + 1 < B) {
+                *reinterpret_cast<float2*>(dst) = make_float2(o[0], o[1]);
+            } else {
+                if (b < B) dst[0] = o[0];
+                if (b + 1 < B) dst[1] = o[1];
             }
         }
     }
 }
 
-template <int TM, int MODE, bool SPLIT>
+int current_device() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d < 0 ? 0 : (d > 63 ? 63 : d);
+}
+
+template <int TM, int TB, int MODE, bool SPLIT>
 int launch_one(dim3 grid, const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                const float* params, const PcbLseTile* tiles, const int* krow, const int* kw, int w_stride,
                int rpb_log2, cudaStream_t s, bool vec) {
-    constexpr int ES = TB + 8, WS = TM + 8;
-    constexpr size_t smem = sizeof(float) * KC * TB + 4 * (KC / 2) * (ES + WS) * (SPLIT ? 2 : 1) + 2 * sizeof(float) * TB;
-    static bool configured = false;  // per instantiation; the attribute is per function, not per device state
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(lse_bf16_kernel<TM, MODE, SPLIT>,
+    constexpr size_t smem = pcb::LseStage<TM, TB, MODE == 2>::bytes() + Packed<TM, TB, SPLIT>::bytes() +
+                            2 * sizeof(float) * TB;
+    static bool configured[64] = {false};
+    const int dev = current_device();
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(lse_bf16_kernel<TM, TB, MODE, SPLIT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract(bf16): %s", cudaGetErrorString(e));
-        configured = true;
+        configured[dev] = true;
     }
-    lse_bf16_kernel<TM, MODE, SPLIT><<<grid, kThreads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw,
-                                                                  w_stride, rpb_log2, vec);
+    lse_bf16_kernel<TM, TB, MODE, SPLIT><<<grid, kThreads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow,
+                                                                      kw, w_stride, rpb_log2, vec);
     return pcb::check_launch("pcb_lse_contract(bf16)");
 }
 
-template <int TM>
+template <int TM, int TB>
 int launch(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B, const float* params,
            const PcbLseTile* tiles, int num_tiles, const int* krow, const int* kw, int w_stride, int rpb_log2,
            int mode, bool split, cudaStream_t s, bool vec) {
     dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, TB));
     if (grid.y > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: batch too large");
-#define PCB_L1(M, S) launch_one<TM, M, S>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec)
+#define PCB_L1(M, S) launch_one<TM, TB, M, S>(grid, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec)
     if (split) {
         if (mode == 0) return PCB_L1(0, true);
         if (mode == 1) return PCB_L1(1, true);
@@ -247,13 +248,15 @@ int launch(const float* src, const float* src2, const float* aux, float* out, in
 int pcb_lse_contract_bf16(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                           const float* params, const PcbLseTile* tiles, int num_tiles, int tile_rows, int rpb_log2,
                           const int* krow, const int* kw, int w_stride, int mode, bool split, cudaStream_t s) {
-    const bool vec = pcb::vec_ok(src, ld) && (!src2 || pcb::vec_ok(src2, ld));
+    const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!src2 || pcb::vec_ok(src2, ld));
+#define PCB_LB(TM, TB) launch<TM, TB>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec)
     switch (tile_rows) {
-        case 16: return launch<16>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
-        case 32: return launch<32>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
-        case 64: return launch<64>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
-        case 128: return launch<128>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, split, s, vec);
+        case 16: return PCB_LB(16, 128);
+        case 32: return PCB_LB(32, 128);
+        case 64: return PCB_LB(64, 64);
+        case 128: return PCB_LB(128, 64);
         default:
             return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: the bf16 form needs tile_rows 16..128, got %d", tile_rows);
     }
+#undef PCB_LB
 }

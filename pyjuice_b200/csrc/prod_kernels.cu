@@ -22,10 +22,19 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
     float4 acc;
     if (!LSE) {
         acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int j = 0; j < cnt; ++j) {
-            const int c = __ldg(chs + off + j);
-            const float4 v = pcb::load4(in, (int64_t)c + i, ld, b, B, vec, 0.f);
-            acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+        // 8 children at a time: all index loads, then all row loads, are independent
+        for (int j0 = 0; j0 < cnt; j0 += 8) {
+            int c[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) c[j] = (j0 + j < cnt) ? __ldg(chs + off + j0 + j) : -1;
+            float4 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                v[j] = (c[j] >= 0) ? pcb::load4(in, (int64_t)c[j] + i, ld, b, B, vec, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                acc.x += v[j].x; acc.y += v[j].y; acc.z += v[j].z; acc.w += v[j].w;
+            }
         }
     } else {
         float4 m = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);

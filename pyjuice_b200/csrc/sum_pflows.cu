@@ -7,13 +7,14 @@
 // with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b].
 //
 // The batch is split over a thread-block cluster of CS CTAs (one batch slice each). Each
-// CTA stages its slice in chunks of 32 samples (every exponential taken once) and keeps
-// an 8 x 4 register tile per thread. At the end the CTAs exchange their partial tiles
-// through distributed shared memory and each adds the CS partials of its share of the
-// outputs in rank order: the result does not depend on timing (no float atomics), and no
-// global scratch is needed. Each (node, child) flow slot is owned by one tile, so the
-// final update is a plain read-modify-write unless slots are shared by tied nodes
-// (atomic = 1).
+// CTA stages its slice in chunks of 32 samples with asynchronous copies into two shared
+// buffers (the next chunk's copies fly while the current one is reduced), takes every
+// exponential once, and keeps an 8 x 4 register tile per thread. At the end the CTAs
+// exchange their partial tiles through distributed shared memory and each adds the CS
+// partials of its share of the outputs in rank order: the result does not depend on
+// timing (no float atomics) and no global scratch is needed. Each (node, child) flow slot
+// is owned by one tile, so the final update is a plain read-modify-write unless slots are
+// shared by tied nodes (atomic = 1).
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -25,66 +26,133 @@ namespace {
 constexpr int TMN = 128;  // nodes per tile
 constexpr int TKC = 64;   // children per tile
 constexpr int KB = 32;    // samples per staged chunk
-constexpr int AS = TMN + 4;
-constexpr int CSS = TKC + 4;
+constexpr int RS = KB + 4;  // shared row stride (floats): 16-byte rows, conflict-free float4 reads
+
+template <bool MODIFIED>
+struct PfStage {
+    static constexpr int kA = TMN * RS;
+    static constexpr int kC = TKC * RS;
+    static constexpr int kPer = kA * (MODIFIED ? 1 : 2) + kC;
+    static constexpr size_t bytes() { return sizeof(float) * (2 * kPer + KB + 8 * KB) + sizeof(int) * TKC; }
+    float* base;
+    __device__ explicit PfStage(float* p) : base(p) {}
+    __device__ float* A(int s) { return base + s * kPer; }
+    __device__ float* A2(int s) { return base + s * kPer + kA; }
+    __device__ float* C(int s) { return base + s * kPer + kA * (MODIFIED ? 1 : 2); }
+    __device__ float* M() { return base + 2 * kPer; }
+    __device__ float* Part() { return base + 2 * kPer + KB; }
+    __device__ int* Cid() { return reinterpret_cast<int*>(base + 2 * kPer + KB + 8 * KB); }
+};
+
+__device__ __forceinline__ void stage_row(float* d, const float* g, int b, int bend, bool vec, float fill) {
+    // 32 samples of one row, copied by the calling thread in 8 pieces of 4
+#pragma unroll
+    for (int j4 = 0; j4 < KB / 4; ++j4) {
+        const int bb = b + j4 * 4;
+        if (vec && bb + 3 < bend) {
+            pcb::cp_async16(d + j4 * 4, g + j4 * 4);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (bb + j < bend) pcb::cp_async4(d + j4 * 4 + j, g + j4 * 4 + j);
+                else d[j4 * 4 + j] = fill;
+            }
+        }
+    }
+}
 
 template <bool MODIFIED, bool ATOMIC>
 __global__ void __launch_bounds__(256)
 sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, const float* __restrict__ em,
                   int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                   const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
-                  const int* __restrict__ pids, const int* __restrict__ pfids, int slice) {
-    // staging buffers during the loop; the partial-result tile [TMN][TKC] afterwards
-    __shared__ __align__(16) float smem[TMN * TKC];
-    float* sA = smem;                       // [KB][AS]   exp(lf - M), sample-major
-    float* sC = smem + KB * AS;             // [KB][CSS]  exp(em + M)
-    float* sM = sC + KB * CSS;              // [KB]
-    float* sPart = sM + KB;                 // [8][KB]
-    __shared__ int sCid[TKC];
+                  const int* __restrict__ pids, const int* __restrict__ pfids, int slice, bool vec) {
+    extern __shared__ __align__(16) float dsm[];
+    PfStage<MODIFIED> st(dsm);
+    float* sM = st.M();
+    float* sPart = st.Part();
+    int* sCid = st.Cid();
 
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int csize = (int)cluster.num_blocks();
     const PcbPflowTile t = tiles[blockIdx.x / csize];
     const int tid = threadIdx.x;
-    const int tx = tid % 16;   // children tx*4 .. +4
-    const int ty = tid / 16;   // nodes ty*8 .. +8
+    const int tx = tid % 16;   // children tx + 16 * kk, kk < 4
+    const int ty = tid / 16;   // nodes ty * 8 .. + 8
     const int rpb_mask = (1 << rpb_log2) - 1;
 
-    if (tid < TKC) sCid[tid] = (tid < t.k_cnt) ? cids[t.k_off + tid] : 0;
+    if (tid < TKC) sCid[tid] = (tid < t.k_cnt) ? cids[t.k_off + tid] : -1;
+    __syncthreads();
 
     float acc[8][4];
 #pragma unroll
     for (int a = 0; a < 8; ++a)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[a][q] = 0.f;
-    __syncthreads();
 
     const int bs0 = crank * slice;
     const int bs1 = min(B, bs0 + slice);
-    for (int b0 = bs0; b0 < bs1; b0 += KB) {
-        for (int idx = tid; idx < TMN * KB; idx += 256) {
-            const int i = idx / KB;
-            const int b = idx % KB;
-            float v = -INFINITY;
-            if (i < t.n_rows && b0 + b < bs1) {
-                const int64_t off = ((int64_t)t.nid + i) * ld + b0 + b;
-                if (MODIFIED) {
-                    v = __ldg(nf + off);
-                } else {
-                    const float m = __ldg(nm + off);
-                    v = (m == -INFINITY) ? -INFINITY : logf(__ldg(nf + off)) - m;
-                }
+    const int nchunks = bs1 > bs0 ? (bs1 - bs0 + KB - 1) / KB : 0;
+
+    auto issue = [&](int c, int s) {
+        const int b0 = bs0 + c * KB;
+        // 128 node rows (+ mars rows), 64 child rows: one row per thread-iteration
+        for (int i = tid; i < TMN; i += 256) {
+            float* dA = st.A(s) + i * RS;
+            if (i < t.n_rows) {
+                const int64_t off = ((int64_t)t.nid + i) * ld + b0;
+                stage_row(dA, nf + off, b0, bs1, vec, -INFINITY);
+                if (!MODIFIED) stage_row(st.A2(s) + i * RS, nm + off, b0, bs1, vec, -INFINITY);
+            } else {
+#pragma unroll
+                for (int j = 0; j < KB; ++j) dA[j] = -INFINITY;
+                if (!MODIFIED)
+#pragma unroll
+                    for (int j = 0; j < KB; ++j) st.A2(s)[i * RS + j] = -INFINITY;
             }
-            sA[b * AS + i] = v;
+        }
+        for (int k = tid; k < TKC; k += 256) {
+            float* dC = st.C(s) + k * RS;
+            const int row = sCid[k];
+            if (row >= 0) {
+                stage_row(dC, em + (int64_t)row * ld + b0, b0, bs1, vec, -INFINITY);
+            } else {
+#pragma unroll
+                for (int j = 0; j < KB; ++j) dC[j] = -INFINITY;
+            }
+        }
+        pcb::cp_async_commit();
+    };
+
+    if (nchunks > 0) issue(0, 0);
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c & 1;
+        if (c + 1 < nchunks) {
+            issue(c + 1, s ^ 1);
+            pcb::cp_async_wait<1>();
+        } else {
+            pcb::cp_async_wait<0>();
         }
         __syncthreads();
+        float* sA = st.A(s);
+        float* sC = st.C(s);
+        if (!MODIFIED) {
+            float* sA2 = st.A2(s);
+            for (int idx = tid; idx < TMN * KB; idx += 256) {
+                const int i = idx / KB;
+                const int b = idx % KB;
+                const float m = sA2[i * RS + b];
+                sA[i * RS + b] = (m == -INFINITY) ? -INFINITY : logf(sA[i * RS + b]) - m;
+            }
+            __syncthreads();
+        }
         {
             const int b = tid % KB;
-            const int part = tid / KB;      // 8 parts of 16 rows
+            const int part = tid / KB;  // 8 parts of 16 rows
             float m = -INFINITY;
 #pragma unroll 4
-            for (int i = part * 16; i < part * 16 + 16; ++i) m = fmaxf(m, sA[b * AS + i]);
+            for (int i = part * 16; i < part * 16 + 16; ++i) m = fmaxf(m, sA[i * RS + b]);
             sPart[part * KB + b] = m;
         }
         __syncthreads();
@@ -96,43 +164,44 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
         }
         __syncthreads();
         for (int idx = tid; idx < TMN * KB; idx += 256) {
-            const int b = idx / TMN;
-            const int i = idx % TMN;
+            const int i = idx / KB;
+            const int b = idx % KB;
             const float m = sM[b];
-            sA[b * AS + i] = (m == -INFINITY) ? 0.f : __expf(sA[b * AS + i] - m);
+            sA[i * RS + b] = (m == -INFINITY) ? 0.f : __expf(sA[i * RS + b] - m);
         }
         for (int idx = tid; idx < TKC * KB; idx += 256) {
             const int k = idx / KB;
             const int b = idx % KB;
-            float v = 0.f;
             const float m = sM[b];
-            if (k < t.k_cnt && b0 + b < bs1 && m != -INFINITY) {
-                v = __expf(__ldg(em + (int64_t)sCid[k] * ld + b0 + b) + m);
-            }
-            sC[b * CSS + k] = v;
+            sC[k * RS + b] = (m == -INFINITY) ? 0.f : __expf(sC[k * RS + b] + m);
         }
         __syncthreads();
-#pragma unroll 4
-        for (int b = 0; b < KB; ++b) {
-            const float4 a0 = *reinterpret_cast<const float4*>(&sA[b * AS + ty * 8]);
-            const float4 a1 = *reinterpret_cast<const float4*>(&sA[b * AS + ty * 8 + 4]);
-            const float4 c = *reinterpret_cast<const float4*>(&sC[b * CSS + tx * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll 2
+        for (int b = 0; b < KB; b += 4) {
+            float4 cv[4];
 #pragma unroll
-            for (int a = 0; a < 8; ++a)
+            for (int kk = 0; kk < 4; ++kk) cv[kk] = *reinterpret_cast<const float4*>(&sC[(tx + 16 * kk) * RS + b]);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[a][q] = fmaf(av[a], cv[q], acc[a][q]);
+            for (int a = 0; a < 8; ++a) {
+                const float4 av = *reinterpret_cast<const float4*>(&sA[(ty * 8 + a) * RS + b]);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    acc[a][kk] = fmaf(av.x, cv[kk].x, acc[a][kk]);
+                    acc[a][kk] = fmaf(av.y, cv[kk].y, acc[a][kk]);
+                    acc[a][kk] = fmaf(av.z, cv[kk].z, acc[a][kk]);
+                    acc[a][kk] = fmaf(av.w, cv[kk].w, acc[a][kk]);
+                }
+            }
         }
         __syncthreads();
     }
 
-    // partial tile -> shared memory; cluster-wide exchange; fixed-order sum
+    // partial tile -> shared memory (aliases the stage buffers); cluster-wide fixed-order sum
+    float* red = dsm;  // [TMN][TKC]
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        float4 v = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
-        *reinterpret_cast<float4*>(&smem[(ty * 8 + a) * TKC + tx * 4]) = v;
-    }
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) red[(ty * 8 + a) * TKC + tx + 16 * kk] = acc[a][kk];
     cluster.sync();
     const int per = (TMN * TKC) / csize;
     for (int idx = crank * per + tid; idx < (crank + 1) * per; idx += 256) {
@@ -140,7 +209,7 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
         const int k = idx % TKC;
         if (i >= t.n_rows || k >= t.k_cnt) continue;
         float s = 0.f;
-        for (int r = 0; r < csize; ++r) s += cluster.map_shared_rank(smem, r)[idx];
+        for (int r = 0; r < csize; ++r) s += cluster.map_shared_rank(red, r)[idx];
         const int64_t roff = (int64_t)t.p_add + (int64_t)(i & rpb_mask);
         const int blk = i >> rpb_log2;
         const float w = __ldg(params + (int64_t)pids[t.k_off + k] + roff + (int64_t)blk * t.gs_p);
@@ -154,12 +223,24 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
 template <bool MODIFIED, bool ATOMIC>
 int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld, int B, const float* params,
            float* pf, const PcbPflowTile* tiles, int num_tiles, int rpb_log2, const int* cids, const int* pids,
-           const int* pfids, cudaStream_t s) {
+           const int* pfids, cudaStream_t s, bool vec) {
     const int slice = (int)pcb::cdiv(pcb::cdiv(B, cs), KB) * KB;
+    constexpr size_t smem = PfStage<MODIFIED>::bytes();
+    static_assert(PfStage<MODIFIED>::bytes() >= sizeof(float) * TMN * TKC, "reduction tile must fit");
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev = dev < 0 ? 0 : (dev > 63 ? 63 : dev);
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(sum_pflows_kernel<MODIFIED, ATOMIC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_sum_pflows: %s", cudaGetErrorString(e));
+        configured[dev] = true;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)num_tiles * cs);
     cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -169,7 +250,7 @@ int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, sum_pflows_kernel<MODIFIED, ATOMIC>, nf, nm, em, ld, B, params, pf, tiles,
-                                       rpb_log2, cids, pids, pfids, slice);
+                                       rpb_log2, cids, pids, pfids, slice, vec);
     if (e != cudaSuccess) return pcb::set_error(PCB_E_LAUNCH, "pcb_sum_pflows: %s", cudaGetErrorString(e));
     return pcb::check_launch("pcb_sum_pflows");
 }
@@ -189,10 +270,11 @@ extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, c
     // batch slices of >= 128 samples, up to 4 CTAs per cluster
     const int cs = B >= 512 ? 4 : (B >= 256 ? 2 : 1);
     if ((int64_t)num_tiles * cs > 2147483647) return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows: too many tiles");
+    const bool vec = pcb::vec_ok(node_flows, ld) && pcb::vec_ok(node_mars, ld) && pcb::vec_ok(element_mars, ld);
     cudaStream_t s = pcb::as_stream(stream);
     const float *nf = node_flows, *nm = node_mars, *em = element_mars;
-    if (modified && atomic) return launch<true, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s);
-    if (modified) return launch<true, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s);
-    if (atomic) return launch<false, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s);
-    return launch<false, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s);
+    if (modified && atomic) return launch<true, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
+    if (modified) return launch<true, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
+    if (atomic) return launch<false, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
+    return launch<false, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
 }
