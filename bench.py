@@ -257,11 +257,13 @@ def main():
     pc = build_circuit(data, device).to(device)
     data_dev = data[torch.arange(rank * B, rank * B + B * 8) % n_data].to(device)  # 8 resident batches per rank
 
+    from pyjuice_b200.distributed import allreduce_param_flows, broadcast_parameters
+    if group is not None:
+        broadcast_parameters(pc, src=0, group=group)
+
     def allreduce_flows():
         if group is not None:
-            import torch.distributed as dist
-            dist.all_reduce(pc.param_flows, group=group)
-            dist.all_reduce(pc.input_layer_group[0].param_flows, group=group)
+            allreduce_param_flows(pc, group=group)
 
     def step(x, kw):
         pc.init_param_flows(flows_memory=0.0)
