@@ -237,6 +237,54 @@ int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32
                      const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, const float* params,
                      int64_t* samples, int64_t sld, uint64_t seed, void* stream);
 
+/*
+ * Whole-circuit sampling that allocates nothing. No counterpart in the reference: the
+ * reference samples layer by layer with host-side tensors; this entry point exists for
+ * callers that may not allocate device memory when they sample (a fixed pre-reserved
+ * memory pool, a plugin inside another framework's allocator, a loop that must not call
+ * cudaMalloc because it can synchronise the device). Neither this function nor its
+ * kernel allocates; the caller passes only inputs and outputs.
+ *
+ * One step per layer, in the order the per-layer entry points above would be called
+ * (sum and product layers top-down, then the input layers); the table lives in device
+ * memory the caller owns. Draws are the same as pcb_sample_sum / pcb_sample_prod /
+ * pcb_sample_input with the same seed, so the samples are identical.
+ *   kind 0 (sum layer, nodes [lo, hi), block size bs): node2blk, blk_first (= blk_nid),
+ *          blk_off, blk_cnt, children (= krow), weight_base (= kw), params.
+ *   kind 1 (product layer, elements [lo, hi)): node2blk (= elem2blk), blk_first (= blk_row),
+ *          blk_off, blk_cnt, children (= chs).
+ *   kind 2 (input layer, nodes [lo, hi)): vids, s_pids, ncats, params.
+ *
+ * Working lists: S * (cap_n + cap_e) int32 in a fixed 8 MiB device array inside the
+ * library (PCB_SAMPLE_NOALLOC_MAX_INTS entries); larger requests are rejected with
+ * PCB_E_ARG before anything is launched (sample in smaller batches). The array is per
+ * device and shared by all calls: two calls that overlap in time on the same device
+ * (two streams, two host threads) overwrite each other's lists, so serialise them.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress; with lazy module loading the runtime loads the module and
+ * reserves the array at that point); make that first call before any stream capture.
+ * *err is set to zero by the call (cudaMemsetAsync on `stream`), then to 1 on list
+ * overflow, 2 on an element outside its product layer. samples[s * sld + v] is written
+ * for every variable v that sample s draws; other entries are left as they are.
+ */
+#define PCB_SAMPLE_NOALLOC_MAX_INTS (1 << 21)
+typedef struct {
+    int32_t kind, lo, hi, bs;
+    const int32_t* node2blk;
+    const int32_t* blk_first;
+    const int32_t* blk_off;
+    const int32_t* blk_cnt;
+    const int32_t* children;
+    const int32_t* weight_base;
+    const float* params;
+    const int32_t* vids;
+    const int32_t* s_pids;
+    const int32_t* ncats;
+} PcbSampleStep;
+int pcb_sample_circuit_noalloc(const PcbSampleStep* steps, int32_t num_steps, int32_t root_id, int32_t S,
+                               int32_t cap_n, int32_t cap_e, int64_t* samples, int64_t sld, uint64_t seed,
+                               int32_t* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpcb200.so")
 CSRC = os.path.join(_HERE, "csrc")
 SOURCES = ["capi_common.cu", "lse_contract.cu", "lse_contract_tc.cu", "prod_kernels.cu", "sum_pflows.cu",
-           "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu"]
+           "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-shared",
               "-Xcompiler", "-fPIC"]
 
@@ -37,7 +37,8 @@ def _nvcc():
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile ``libpcb200.so`` for sm_100a if it is missing or older than its sources."""
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(_HERE, "..", "include", "pcb200.h")]
+    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "lse_stage.cuh"),
+                   os.path.join(_HERE, "..", "include", "pcb200.h")]
     if not force and os.path.exists(LIB_PATH):
         lib_m = os.path.getmtime(LIB_PATH)
         if all(os.path.getmtime(d) <= lib_m for d in deps if os.path.exists(d)):
@@ -83,6 +84,8 @@ _SIGS = {
                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
     "pcb_sample_input": ([c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
+    "pcb_sample_circuit_noalloc": ([c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p, c_int64, c_uint64,
+                                    c_void_p, c_void_p], c_int32),
 }
 
 EXPORTED_SYMBOLS = sorted(_SIGS.keys())

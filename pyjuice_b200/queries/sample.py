@@ -12,6 +12,7 @@ sample carries its active node / element lists on the device
 
 from __future__ import annotations
 
+import ctypes
 import random
 from typing import Optional
 
@@ -89,3 +90,80 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
         raise RuntimeError(f"sampling failed on the device (code {e}: "
                            f"{'active list overflow' if e == 1 else 'element outside its product layer'})")
     return samples
+
+
+class _SampleStep(ctypes.Structure):
+    """Mirror of ``PcbSampleStep`` (include/pcb200.h)."""
+    _fields_ = [("kind", ctypes.c_int32), ("lo", ctypes.c_int32), ("hi", ctypes.c_int32), ("bs", ctypes.c_int32),
+                ("node2blk", ctypes.c_void_p), ("blk_first", ctypes.c_void_p), ("blk_off", ctypes.c_void_p),
+                ("blk_cnt", ctypes.c_void_p), ("children", ctypes.c_void_p), ("weight_base", ctypes.c_void_p),
+                ("params", ctypes.c_void_p), ("vids", ctypes.c_void_p), ("s_pids", ctypes.c_void_p),
+                ("ncats", ctypes.c_void_p)]
+
+
+def noalloc_sample_plan(pc):
+    """Step table for ``pcb_sample_circuit_noalloc``: ``(table, num_steps, root_id, cap_n, cap_e)``.
+
+    Building the plan allocates (the table is copied to the device once); the calls that
+    use it do not. The table holds raw pointers to the circuit's index tables and
+    parameters, so it is valid while ``pc`` keeps those tensors; it is cached on ``pc``
+    and rebuilt when a parameter tensor moves.
+    """
+    if pc.num_root_nodes != 1:
+        raise ValueError("It is ambiguous to sample from multi-head PCs.")
+    if pc.device.type != "cuda":
+        raise RuntimeError("sampling runs on CUDA only")
+    dev = pc.device
+    key = (str(dev), pc.params.data_ptr(), tuple(layer.params.data_ptr() for layer in pc.input_layer_group))
+    cached = getattr(pc, "_noalloc_sample_plan", None)
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    steps = []
+    for layer_id in range(len(pc.inner_layer_groups) - 1, -1, -1):
+        group = pc.inner_layer_groups[layer_id]
+        for layer in group:
+            d = layer._desc(dev)
+            lo, hi = layer._layer_nid_range
+            if group.is_sum():
+                steps.append(_SampleStep(0, lo, hi, layer.block_size, d["node2blk"].data_ptr(),
+                                         d["blk_nid"].data_ptr(), d["blk_koff"].data_ptr(), d["blk_kcnt"].data_ptr(),
+                                         d["krow"].data_ptr(), d["kw"].data_ptr(), pc.params.data_ptr(), None, None,
+                                         None))
+            else:
+                steps.append(_SampleStep(1, lo, hi, 1, d["elem2blk"].data_ptr(), d["fw_row"].data_ptr(),
+                                         d["fw_off"].data_ptr(), d["fw_cnt"].data_ptr(), d["fw_chs"].data_ptr(),
+                                         None, None, None, None, None))
+    for layer in pc.input_layer_group:
+        d = layer._desc(dev)
+        lo, hi = layer._output_ind_range
+        steps.append(_SampleStep(2, lo, hi, 1, None, None, None, None, None, None, layer.params.data_ptr(),
+                                 d["vids"].data_ptr(), d["s_pids"].data_ptr(), d["ncats"].data_ptr()))
+    arr = (_SampleStep * len(steps))(*steps)
+    table = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(dev)
+    cap_n, cap_e = _scope_bounds(pc)
+    plan = (table, len(steps), int(pc._root_node_range[0]), max(cap_n, 1), max(cap_e, 1))
+    pc._noalloc_sample_plan = (key, plan)
+    return plan
+
+
+def sample_noalloc(pc, samples: torch.Tensor, err: torch.Tensor, seed: int, plan=None) -> None:
+    """Fill ``samples`` ([S, num_vars] int64, caller-allocated) without any device allocation.
+
+    Same draws as :func:`sample` with the same ``seed``. ``err`` (one int32 on the device)
+    receives 0, or 1 on list overflow, 2 on an element outside its product layer; the
+    call does not synchronise, so read it when the stream reaches that point. Variables a
+    sample does not draw keep their value in ``samples``. At most
+    ``PCB_SAMPLE_NOALLOC_MAX_INTS // (cap_n + cap_e)`` samples per call; calls that
+    overlap in time on one device share the library's working lists and must be
+    serialised. For callers that cannot allocate when they sample (a pre-reserved memory
+    pool, a plugin inside another framework's allocator).
+    """
+    if plan is None:
+        plan = noalloc_sample_plan(pc)
+    table, num_steps, root_id, cap_n, cap_e = plan
+    if samples.dtype != torch.long or samples.dim() != 2 or samples.stride(1) != 1:
+        raise ValueError("`samples` must be a row-major int64 tensor [S, num_vars]")
+    if err.dtype != torch.int32 or err.numel() < 1:
+        raise ValueError("`err` must hold one int32")
+    nat.call("pcb_sample_circuit_noalloc", nat.ptr(table), num_steps, root_id, samples.size(0), cap_n, cap_e,
+             nat.ptr(samples), samples.stride(0), int(seed), nat.ptr(err), nat.stream())
