@@ -159,6 +159,43 @@ int pcb_lse_contract(const float* src, const float* src2, const float* aux, floa
                      int32_t prec, void* stream);
 
 /*
+ * Same contraction, epilogues and precision forms (prec 0 FP32, 1 bf16, 2 split bf16) as
+ * pcb_lse_contract for tiles of at most 128 terms, built for latency: each CTA stages all
+ * its terms at once and computes a slice of RM rows (32 when tile_rows <= 32, else 64) by
+ * batch_tile samples (16, 32 or 64), so small layers launch many CTAs.
+ * wlayout: 0 = weights copied one by one; 1 = groups of 4 consecutive rows have
+ * consecutive, 16-byte aligned weights (forward tables); 2 = groups of 4 consecutive terms
+ * do (element-flow tables). The caller guarantees k_cnt <= 128 and the wlayout property;
+ * a tile with more terms produces NaN rows.
+ * Replaces the same sum-layer kernels as pcb_lse_contract (small-K case).
+ */
+int pcb_lse_contract_short(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
+                           const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t tile_rows,
+                           int32_t rows_per_block, const int32_t* krow, const int32_t* kw, int32_t w_stride,
+                           int32_t mode, int32_t prec, int32_t wlayout, int32_t batch_tile, void* stream);
+
+/*
+ * Weights of LSE-contraction tiles (at most 128 rows x 128 terms each, same tile table,
+ * kw, rows_per_block and w_stride as pcb_lse_contract) packed for
+ * pcb_lse_contract_tc05: for tile t, 65536 bytes at packed + t * 65536 hold W(k, r)
+ * rounded to bf16 (first 32 KB) and the bf16 rounding of the remainder (next 32 KB), in
+ * the canonical no-swizzle K-major layout of a 128 x 128 tensor-core operand; rows and
+ * terms beyond the tile are zero. packed must be 16-byte aligned.
+ */
+int pcb_pack_weights(const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t rows_per_block,
+                     const int32_t* kw, int32_t w_stride, uint8_t* packed, void* stream);
+
+/*
+ * Same contraction and epilogues as pcb_lse_contract (BF16 forms, prec 1 or 2) on the
+ * tcgen05 tensor cores with tensor-memory accumulators, for tiles of at most 128 terms,
+ * using the weights packed by pcb_pack_weights from the same tile table. One CTA per
+ * tile and batch_tile (32 or 64) samples. A tile with more terms produces NaN rows.
+ */
+int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
+                          const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles, const int32_t* krow,
+                          int32_t mode, int32_t prec, int32_t batch_tile, void* stream);
+
+/*
  * In place on rows [row0, row1) of node_flows: f <- (m == -inf) ? -inf : log(f) - m.
  * Replaces SumLayer._bk_triton_modify_flow_kernel (src/pyjuice/layer/sum_layer.py:1355-1515).
  */
@@ -170,16 +207,18 @@ int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int3
  *   pf(r, k) += params(r, k) * sum_b exp(lf[nid + r, b] - M_b) * exp(em[cids[k], b] + M_b)
  * with lf = node_flows already in "log f - log m" form (modified=1) or computed as
  * log(node_flows) - node_mars (modified=0), M_b the max over the tile's nodes.
- * The batch is split over a cluster of CTAs whose partial sums are added in a fixed
- * order through distributed shared memory (deterministic, no scratch memory).
- * atomic=1 when flow slots are shared by tied nodes.
+ * The batch is split over a cluster of up to 8 CTAs (64 samples per CTA and staged
+ * chunk) whose partial sums are added in a fixed order through distributed shared memory
+ * (deterministic, no scratch memory). Tiles hold at most tile_children (32 or 64)
+ * children. prec: 0 = FP32 FMA, 1 = bf16 tensor cores, 2 = split bf16 (hi + lo, three
+ * MMAs). atomic=1 when flow slots are shared by tied nodes.
  * Replaces SumLayer._bk_triton_block_sparse_par_kernel / _csmm2 / sparse par kernel
  * (src/pyjuice/layer/sum_layer.py:2052-2282, 2795-2902).
  */
 int pcb_sum_pflows(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld, int32_t B,
                    const float* params, float* param_flows, const PcbPflowTile* tiles, int32_t num_tiles,
                    int32_t rows_per_block, const int32_t* cids, const int32_t* pids, const int32_t* pfids,
-                   int32_t modified, int32_t atomic, void* stream);
+                   int32_t modified, int32_t atomic, int32_t tile_children, int32_t prec, void* stream);
 
 /*
  * Sum-parameter EM update, per node block (FP64 normalisation):

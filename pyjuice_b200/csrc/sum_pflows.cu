@@ -1,21 +1,24 @@
-// Sum-layer parameter flows (plain FP32 path): a contraction over the batch.
+// Sum-layer parameter flows: a contraction over the batch.
 //
 // A tile covers up to 128 nodes (rows nid + r: consecutive node blocks that share their
-// children) and up to 64 children (element rows cids[k]):
+// children) and up to TKC children (element rows cids[k], TKC = 32 or 64):
 //   pf(r, k) += params(r, k) * sum_b A[r, b] * C[k, b]
 //   A[r, b] = exp(lf[nid + r, b] - M_b),  C[k, b] = exp(em[cids[k], b] + M_b)
-// with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b].
+// with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b]: every
+// exponential is taken once per (row, sample), not once per (node, child, sample).
 //
-// The batch is split over a thread-block cluster of CS CTAs (one batch slice each). Each
-// CTA stages its slice in chunks of 32 samples with asynchronous copies into two shared
-// buffers (the next chunk's copies fly while the current one is reduced), takes every
-// exponential once, and keeps an 8 x 4 register tile per thread. At the end the CTAs
-// exchange their partial tiles through distributed shared memory and each adds the CS
-// partials of its share of the outputs in rank order: the result does not depend on
-// timing (no float atomics) and no global scratch is needed. Each (node, child) flow slot
-// is owned by one tile, so the final update is a plain read-modify-write unless slots are
-// shared by tied nodes (atomic = 1).
+// The batch is split over a thread-block cluster of up to 8 CTAs. A CTA copies 64
+// samples of its slice at a time (all node rows and child rows in one batch of
+// asynchronous copies), forms A and C, and contracts them either with FP32 FMA (prec 0)
+// or on the tensor cores (prec 1: bf16 operands; prec 2: both operands split into
+// bf16 hi + lo, three MMAs, FP32 accumulators). At the end the CTAs exchange their
+// partial tiles through distributed shared memory and each adds the partials of its
+// share of the outputs in rank order: the result does not depend on timing (no float
+// atomics) and no global scratch is needed. Each (node, child) flow slot is owned by one
+// tile, so the final update is a plain read-modify-write unless slots are shared by tied
+// nodes (atomic = 1).
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include "common.cuh"
 
@@ -23,188 +26,275 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr int TMN = 128;  // nodes per tile
-constexpr int TKC = 64;   // children per tile
-constexpr int KB = 32;    // samples per staged chunk
-constexpr int RS = KB + 4;  // shared row stride (floats): 16-byte rows, conflict-free float4 reads
+constexpr int kThreads = 256;
+constexpr int TMN = 128;      // nodes per tile
+constexpr int KB = 64;        // samples per staged chunk
+constexpr int RS = KB + 4;    // fp32 staging row stride (16-byte rows)
+constexpr int PS = KB / 2 + 4;  // packed bf16-pair row stride (conflict-free fragment loads)
+constexpr int kMaxCluster = 8;
 
-template <bool MODIFIED>
-struct PfStage {
-    static constexpr int kA = TMN * RS;
-    static constexpr int kC = TKC * RS;
-    static constexpr int kPer = kA * (MODIFIED ? 1 : 2) + kC;
-    static constexpr size_t bytes() { return sizeof(float) * (2 * kPer + KB + 8 * KB) + sizeof(int) * TKC; }
-    float* base;
-    __device__ explicit PfStage(float* p) : base(p) {}
-    __device__ float* A(int s) { return base + s * kPer; }
-    __device__ float* A2(int s) { return base + s * kPer + kA; }
-    __device__ float* C(int s) { return base + s * kPer + kA * (MODIFIED ? 1 : 2); }
-    __device__ float* M() { return base + 2 * kPer; }
-    __device__ float* Part() { return base + 2 * kPer + KB; }
-    __device__ int* Cid() { return reinterpret_cast<int*>(base + 2 * kPer + KB + 8 * KB); }
-};
-
-__device__ __forceinline__ void stage_row(float* d, const float* g, int b, int bend, bool vec, float fill) {
-    // 32 samples of one row, copied by the calling thread in 8 pieces of 4
-#pragma unroll
-    for (int j4 = 0; j4 < KB / 4; ++j4) {
-        const int bb = b + j4 * 4;
-        if (vec && bb + 3 < bend) {
-            pcb::cp_async16(d + j4 * 4, g + j4 * 4);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (bb + j < bend) pcb::cp_async4(d + j4 * 4 + j, g + j4 * 4 + j);
-                else d[j4 * 4 + j] = fill;
-            }
-        }
-    }
+__device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, uint32_t& l) {
+    __nv_bfloat162 hv = __floats2bfloat162_rn(lo_k, hi_k);
+    const float2 hf = __bfloat1622float2(hv);
+    __nv_bfloat162 lv = __floats2bfloat162_rn(lo_k - hf.x, hi_k - hf.y);
+    h = *reinterpret_cast<uint32_t*>(&hv);
+    l = *reinterpret_cast<uint32_t*>(&lv);
 }
 
-template <bool MODIFIED, bool ATOMIC>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Shared-memory plan in 4-byte words (16-byte aligned arrays).
+template <int TKC, bool MODIFIED, int PREC>
+struct Plan {
+    static constexpr int NB = PREC == 2 ? 2 : (PREC == 1 ? 1 : 0);
+    static constexpr int oA = 0;
+    static constexpr int oA2 = oA + TMN * RS;
+    static constexpr int oC = oA2 + (MODIFIED ? 0 : TMN * RS);
+    static constexpr int oPA = oC + TKC * RS;
+    static constexpr int oPC = oPA + NB * TMN * PS;
+    static constexpr int oPart = oPC + NB * TKC * PS;
+    static constexpr int oM = oPart + kThreads;
+    static constexpr int oCid = oM + KB;
+    static constexpr int words = oCid + TKC;
+    static_assert(words >= TMN * TKC, "the partial tile aliases the staging area");
+    static constexpr size_t bytes() { return 4ull * words; }
+};
+
+template <int TKC, bool MODIFIED, bool ATOMIC, int PREC>
+__global__ void __launch_bounds__(kThreads)
 sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, const float* __restrict__ em,
                   int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                   const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
                   const int* __restrict__ pids, const int* __restrict__ pfids, int slice, bool vec) {
+    using P = Plan<TKC, MODIFIED, PREC>;
     extern __shared__ __align__(16) float dsm[];
-    PfStage<MODIFIED> st(dsm);
-    float* sM = st.M();
-    float* sPart = st.Part();
-    int* sCid = st.Cid();
+    float(*sA)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oA);
+    float(*sA2)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oA2);
+    float(*sC)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oC);
+    uint32_t* pA = reinterpret_cast<uint32_t*>(dsm + P::oPA);
+    uint32_t* pC = reinterpret_cast<uint32_t*>(dsm + P::oPC);
+    float* sPart = dsm + P::oPart;
+    float* sM = dsm + P::oM;
+    int* sCid = reinterpret_cast<int*>(dsm + P::oCid);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int csize = (int)cluster.num_blocks();
     const PcbPflowTile t = tiles[blockIdx.x / csize];
     const int tid = threadIdx.x;
-    const int tx = tid % 16;   // children tx + 16 * kk, kk < 4
-    const int ty = tid / 16;   // nodes ty * 8 .. + 8
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
     const int rpb_mask = (1 << rpb_log2) - 1;
 
-    if (tid < TKC) sCid[tid] = (tid < t.k_cnt) ? cids[t.k_off + tid] : -1;
+    if (tid < TKC) sCid[tid] = (tid < t.k_cnt) ? __ldg(cids + t.k_off + tid) : -1;
     __syncthreads();
 
-    float acc[8][4];
+    // FP32: thread (ty, tx) owns nodes ty * 8 .. + 8 and children tx + 16 * j.
+    // Tensor cores: warp w owns nodes 16 w .. 16 w + 15 and all TKC children.
+    constexpr int FJ = TKC / 16;
+    constexpr int NT = TKC / 8;
+    float acc[PREC == 0 ? 8 : NT][PREC == 0 ? FJ : 4];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < (PREC == 0 ? 8 : NT); ++a)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[a][q] = 0.f;
+        for (int j = 0; j < (PREC == 0 ? FJ : 4); ++j) acc[a][j] = 0.f;
 
     const int bs0 = crank * slice;
     const int bs1 = min(B, bs0 + slice);
-    const int nchunks = bs1 > bs0 ? (bs1 - bs0 + KB - 1) / KB : 0;
-
-    auto issue = [&](int c, int s) {
-        const int b0 = bs0 + c * KB;
-        // 128 node rows (+ mars rows), 64 child rows: one row per thread-iteration
-        for (int i = tid; i < TMN; i += 256) {
-            float* dA = st.A(s) + i * RS;
-            if (i < t.n_rows) {
-                const int64_t off = ((int64_t)t.nid + i) * ld + b0;
-                stage_row(dA, nf + off, b0, bs1, vec, -INFINITY);
-                if (!MODIFIED) stage_row(st.A2(s) + i * RS, nm + off, b0, bs1, vec, -INFINITY);
-            } else {
+    for (int b0 = bs0; b0 < bs1; b0 += KB) {
+        // ---- one batch of asynchronous copies: node rows (flows, mars) and child rows ----
+        {
+            constexpr int NX = KB / 4;
 #pragma unroll
-                for (int j = 0; j < KB; ++j) dA[j] = -INFINITY;
-                if (!MODIFIED)
+            for (int it = 0; it < TMN * NX / kThreads; ++it) {
+                const int idx = tid + it * kThreads;
+                const int r = idx / NX;
+                const int c4 = (idx % NX) * 4;
+                const int b = b0 + c4;
 #pragma unroll
-                    for (int j = 0; j < KB; ++j) st.A2(s)[i * RS + j] = -INFINITY;
+                for (int h = 0; h < (MODIFIED ? 1 : 2); ++h) {
+                    float* d = h == 0 ? &sA[r][c4] : &sA2[r][c4];
+                    if (r < t.n_rows) {
+                        const float* g = (h == 0 ? nf : nm) + ((int64_t)t.nid + r) * ld + b;
+                        if (vec && b + 3 < bs1) {
+                            pcb::cp_async16(d, g);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                if (b + j < bs1) pcb::cp_async4(d + j, g + j);
+                                else d[j] = -INFINITY;
+                            }
+                        }
+                    } else {
+                        *reinterpret_cast<float4*>(d) = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+                    }
+                }
             }
-        }
-        for (int k = tid; k < TKC; k += 256) {
-            float* dC = st.C(s) + k * RS;
-            const int row = sCid[k];
-            if (row >= 0) {
-                stage_row(dC, em + (int64_t)row * ld + b0, b0, bs1, vec, -INFINITY);
-            } else {
 #pragma unroll
-                for (int j = 0; j < KB; ++j) dC[j] = -INFINITY;
+            for (int it = 0; it < TKC * NX / kThreads; ++it) {
+                const int idx = tid + it * kThreads;
+                const int k = idx / NX;
+                const int c4 = (idx % NX) * 4;
+                const int b = b0 + c4;
+                float* d = &sC[k][c4];
+                const int row = sCid[k];
+                if (row >= 0) {
+                    const float* g = em + (int64_t)row * ld + b;
+                    if (vec && b + 3 < bs1) {
+                        pcb::cp_async16(d, g);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            if (b + j < bs1) pcb::cp_async4(d + j, g + j);
+                            else d[j] = -INFINITY;
+                        }
+                    }
+                } else {
+                    *reinterpret_cast<float4*>(d) = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+                }
             }
-        }
-        pcb::cp_async_commit();
-    };
-
-    if (nchunks > 0) issue(0, 0);
-    for (int c = 0; c < nchunks; ++c) {
-        const int s = c & 1;
-        if (c + 1 < nchunks) {
-            issue(c + 1, s ^ 1);
-            pcb::cp_async_wait<1>();
-        } else {
+            pcb::cp_async_commit();
             pcb::cp_async_wait<0>();
         }
         __syncthreads();
-        float* sA = st.A(s);
-        float* sC = st.C(s);
-        if (!MODIFIED) {
-            float* sA2 = st.A2(s);
-            for (int idx = tid; idx < TMN * KB; idx += 256) {
-                const int i = idx / KB;
-                const int b = idx % KB;
-                const float m = sA2[i * RS + b];
-                sA[i * RS + b] = (m == -INFINITY) ? -INFINITY : logf(sA[i * RS + b]) - m;
-            }
-            __syncthreads();
-        }
+
+        // ---- lf = log f - log m (unmodified flows), then M_b = max over the tile's nodes ----
         {
             const int b = tid % KB;
-            const int part = tid / KB;  // 8 parts of 16 rows
-            float m = -INFINITY;
-#pragma unroll 4
-            for (int i = part * 16; i < part * 16 + 16; ++i) m = fmaxf(m, sA[i * RS + b]);
-            sPart[part * KB + b] = m;
+            const int part = tid / KB;  // 4 parts of 32 rows
+            float mx = -INFINITY;
+            for (int r = part * (TMN / 4); r < (part + 1) * (TMN / 4); ++r) {
+                float v = sA[r][b];
+                if (!MODIFIED) {
+                    const float m2 = sA2[r][b];
+                    v = (m2 == -INFINITY) ? -INFINITY : logf(v) - m2;
+                    sA[r][b] = v;
+                }
+                mx = fmaxf(mx, v);
+            }
+            sPart[part * KB + b] = mx;
         }
         __syncthreads();
-        if (tid < KB) {
-            float m = -INFINITY;
-#pragma unroll
-            for (int p = 0; p < 8; ++p) m = fmaxf(m, sPart[p * KB + tid]);
-            sM[tid] = m;
-        }
+        if (tid < KB) sM[tid] = fmaxf(fmaxf(sPart[tid], sPart[KB + tid]), fmaxf(sPart[2 * KB + tid], sPart[3 * KB + tid]));
         __syncthreads();
-        for (int idx = tid; idx < TMN * KB; idx += 256) {
-            const int i = idx / KB;
-            const int b = idx % KB;
-            const float m = sM[b];
-            sA[i * RS + b] = (m == -INFINITY) ? 0.f : __expf(sA[i * RS + b] - m);
-        }
-        for (int idx = tid; idx < TKC * KB; idx += 256) {
-            const int k = idx / KB;
-            const int b = idx % KB;
-            const float m = sM[b];
-            sC[k * RS + b] = (m == -INFINITY) ? 0.f : __expf(sC[k * RS + b] + m);
-        }
-        __syncthreads();
+
+        if constexpr (PREC == 0) {
+            for (int idx = tid; idx < TMN * KB; idx += kThreads) {
+                const int r = idx / KB, b = idx % KB;
+                const float m = sM[b];
+                sA[r][b] = (m == -INFINITY) ? 0.f : __expf(sA[r][b] - m);
+            }
+            for (int idx = tid; idx < TKC * KB; idx += kThreads) {
+                const int k = idx / KB, b = idx % KB;
+                const float m = sM[b];
+                sC[k][b] = (m == -INFINITY) ? 0.f : __expf(sC[k][b] + m);
+            }
+            __syncthreads();
+            const int tx = tid % 16;
+            const int ty = tid / 16;
 #pragma unroll 2
-        for (int b = 0; b < KB; b += 4) {
-            float4 cv[4];
+            for (int b = 0; b < KB; b += 4) {
+                float4 cv[FJ];
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) cv[kk] = *reinterpret_cast<const float4*>(&sC[(tx + 16 * kk) * RS + b]);
+                for (int j = 0; j < FJ; ++j) cv[j] = *reinterpret_cast<const float4*>(&sC[tx + 16 * j][b]);
 #pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                const float4 av = *reinterpret_cast<const float4*>(&sA[(ty * 8 + a) * RS + b]);
+                for (int a = 0; a < 8; ++a) {
+                    const float4 av = *reinterpret_cast<const float4*>(&sA[ty * 8 + a][b]);
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    acc[a][kk] = fmaf(av.x, cv[kk].x, acc[a][kk]);
-                    acc[a][kk] = fmaf(av.y, cv[kk].y, acc[a][kk]);
-                    acc[a][kk] = fmaf(av.z, cv[kk].z, acc[a][kk]);
-                    acc[a][kk] = fmaf(av.w, cv[kk].w, acc[a][kk]);
+                    for (int j = 0; j < FJ; ++j) {
+                        acc[a][j] = fmaf(av.x, cv[j].x, acc[a][j]);
+                        acc[a][j] = fmaf(av.y, cv[j].y, acc[a][j]);
+                        acc[a][j] = fmaf(av.z, cv[j].z, acc[a][j]);
+                        acc[a][j] = fmaf(av.w, cv[j].w, acc[a][j]);
+                    }
+                }
+            }
+        } else {
+            constexpr bool SPLIT = PREC == 2;
+            // ---- exponentiate and pack sample pairs as bf16 (hi, lo) ----
+            for (int idx = tid; idx < TMN * (KB / 2); idx += kThreads) {
+                const int r = idx / (KB / 2), j = idx % (KB / 2);
+                const float2 v = *reinterpret_cast<const float2*>(&sA[r][2 * j]);
+                const float m0 = sM[2 * j], m1 = sM[2 * j + 1];
+                const float e0 = (m0 == -INFINITY) ? 0.f : __expf(v.x - m0);
+                const float e1 = (m1 == -INFINITY) ? 0.f : __expf(v.y - m1);
+                if (SPLIT) split_bf16(e0, e1, pA[r * PS + j], pA[TMN * PS + r * PS + j]);
+                else pA[r * PS + j] = pack_bf16(e0, e1);
+            }
+            for (int idx = tid; idx < TKC * (KB / 2); idx += kThreads) {
+                const int k = idx / (KB / 2), j = idx % (KB / 2);
+                const float2 v = *reinterpret_cast<const float2*>(&sC[k][2 * j]);
+                const float m0 = sM[2 * j], m1 = sM[2 * j + 1];
+                const float e0 = (m0 == -INFINITY) ? 0.f : __expf(v.x + m0);
+                const float e1 = (m1 == -INFINITY) ? 0.f : __expf(v.y + m1);
+                if (SPLIT) split_bf16(e0, e1, pC[k * PS + j], pC[TKC * PS + k * PS + j]);
+                else pC[k * PS + j] = pack_bf16(e0, e1);
+            }
+            __syncthreads();
+            const int g = lane >> 2, q = lane & 3;
+            const int mr = warp * 16 + g;
+#pragma unroll
+            for (int kk = 0; kk < KB / 2; kk += 8) {
+                const uint32_t a0 = pA[mr * PS + kk + q], a1 = pA[(mr + 8) * PS + kk + q];
+                const uint32_t a2 = pA[mr * PS + kk + 4 + q], a3 = pA[(mr + 8) * PS + kk + 4 + q];
+                uint32_t l0 = 0, l1 = 0, l2 = 0, l3 = 0;
+                if (SPLIT) {
+                    l0 = pA[TMN * PS + mr * PS + kk + q];
+                    l1 = pA[TMN * PS + (mr + 8) * PS + kk + q];
+                    l2 = pA[TMN * PS + mr * PS + kk + 4 + q];
+                    l3 = pA[TMN * PS + (mr + 8) * PS + kk + 4 + q];
+                }
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    const int n = nt * 8 + g;
+                    const uint32_t b0v = pC[n * PS + kk + q], b1v = pC[n * PS + kk + 4 + q];
+                    mma_bf16(acc[nt], a0, a1, a2, a3, b0v, b1v);
+                    if (SPLIT) {
+                        mma_bf16(acc[nt], l0, l1, l2, l3, b0v, b1v);
+                        mma_bf16(acc[nt], a0, a1, a2, a3, pC[TKC * PS + n * PS + kk + q],
+                                 pC[TKC * PS + n * PS + kk + 4 + q]);
+                    }
                 }
             }
         }
-        __syncthreads();
+        __syncthreads();  // the next chunk (or the partial tile) overwrites the staging area
     }
 
-    // partial tile -> shared memory (aliases the stage buffers); cluster-wide fixed-order sum
+    // ---- partial tile -> shared memory; cluster-wide fixed-order sum ----
     float* red = dsm;  // [TMN][TKC]
+    if constexpr (PREC == 0) {
+        const int tx = tid % 16, ty = tid / 16;
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+        for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) red[(ty * 8 + a) * TKC + tx + 16 * kk] = acc[a][kk];
+            for (int j = 0; j < FJ; ++j) red[(ty * 8 + a) * TKC + tx + 16 * j] = acc[a][j];
+    } else {
+        const int g = lane >> 2, q = lane & 3;
+        const int mr = warp * 16 + g;
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int n = nt * 8 + 2 * q;
+            red[mr * TKC + n] = acc[nt][0];
+            red[mr * TKC + n + 1] = acc[nt][1];
+            red[(mr + 8) * TKC + n] = acc[nt][2];
+            red[(mr + 8) * TKC + n + 1] = acc[nt][3];
+        }
+    }
     cluster.sync();
-    const int per = (TMN * TKC) / csize;
-    for (int idx = crank * per + tid; idx < (crank + 1) * per; idx += 256) {
+    const int per = (TMN * TKC + csize - 1) / csize;
+    const int end = min(TMN * TKC, (crank + 1) * per);
+    for (int idx = crank * per + tid; idx < end; idx += kThreads) {
         const int i = idx / TKC;
         const int k = idx % TKC;
         if (i >= t.n_rows || k >= t.k_cnt) continue;
@@ -220,26 +310,27 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
     cluster.sync();  // keep every CTA's shared memory alive until all reads are done
 }
 
-template <bool MODIFIED, bool ATOMIC>
+template <int TKC, bool MODIFIED, bool ATOMIC, int PREC>
 int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld, int B, const float* params,
            float* pf, const PcbPflowTile* tiles, int num_tiles, int rpb_log2, const int* cids, const int* pids,
            const int* pfids, cudaStream_t s, bool vec) {
     const int slice = (int)pcb::cdiv(pcb::cdiv(B, cs), KB) * KB;
-    constexpr size_t smem = PfStage<MODIFIED>::bytes();
-    static_assert(PfStage<MODIFIED>::bytes() >= sizeof(float) * TMN * TKC, "reduction tile must fit");
+    using P = Plan<TKC, MODIFIED, PREC>;
+    constexpr size_t smem = P::bytes();
+    static_assert(P::bytes() <= 227 * 1024, "shared memory");
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     dev = dev < 0 ? 0 : (dev > 63 ? 63 : dev);
     if (!configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(sum_pflows_kernel<MODIFIED, ATOMIC>,
+        cudaError_t e = cudaFuncSetAttribute(sum_pflows_kernel<TKC, MODIFIED, ATOMIC, PREC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_sum_pflows: %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)num_tiles * cs);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -249,10 +340,21 @@ int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, sum_pflows_kernel<MODIFIED, ATOMIC>, nf, nm, em, ld, B, params, pf, tiles,
-                                       rpb_log2, cids, pids, pfids, slice, vec);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, sum_pflows_kernel<TKC, MODIFIED, ATOMIC, PREC>, nf, nm, em, ld, B,
+                                       params, pf, tiles, rpb_log2, cids, pids, pfids, slice, vec);
     if (e != cudaSuccess) return pcb::set_error(PCB_E_LAUNCH, "pcb_sum_pflows: %s", cudaGetErrorString(e));
     return pcb::check_launch("pcb_sum_pflows");
+}
+
+template <int TKC, int PREC>
+int launch_flags(int cs, bool modified, bool atomic, const float* nf, const float* nm, const float* em, int64_t ld,
+                 int B, const float* params, float* pf, const PcbPflowTile* tiles, int num_tiles, int rpb_log2,
+                 const int* cids, const int* pids, const int* pfids, cudaStream_t s, bool vec) {
+#define PCB_PF(M, A) \
+    launch<TKC, M, A, PREC>(cs, nf, nm, em, ld, B, params, pf, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec)
+    if (modified) return atomic ? PCB_PF(true, true) : PCB_PF(true, false);
+    return atomic ? PCB_PF(false, true) : PCB_PF(false, false);
+#undef PCB_PF
 }
 
 }  // namespace
@@ -260,21 +362,25 @@ int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld
 extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld,
                               int32_t B, const float* params, float* param_flows, const PcbPflowTile* tiles,
                               int32_t num_tiles, int32_t rows_per_block, const int32_t* cids, const int32_t* pids,
-                              const int32_t* pfids, int32_t modified, int32_t atomic, void* stream) {
+                              const int32_t* pfids, int32_t modified, int32_t atomic, int32_t tile_children,
+                              int32_t prec, void* stream) {
     if (!node_flows || !node_mars || !element_mars || !params || !param_flows || !tiles || !cids || !pids || !pfids ||
-        B <= 0 || ld < B || num_tiles < 0 || rows_per_block <= 0 || (rows_per_block & (rows_per_block - 1)))
+        B <= 0 || ld < B || num_tiles < 0 || rows_per_block <= 0 || (rows_per_block & (rows_per_block - 1)) ||
+        (tile_children != 32 && tile_children != 64) || prec < 0 || prec > 2)
         return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows: bad arguments");
     if (num_tiles == 0) return PCB_OK;
     int rpb_log2 = 0;
     while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
-    // batch slices of >= 128 samples, up to 4 CTAs per cluster
-    const int cs = B >= 512 ? 4 : (B >= 256 ? 2 : 1);
+    // one CTA per 64-sample slice, up to 8 CTAs per cluster (a power of two)
+    int cs = 1;
+    while (cs < kMaxCluster && (int64_t)cs * KB < B) cs *= 2;
     if ((int64_t)num_tiles * cs > 2147483647) return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows: too many tiles");
     const bool vec = pcb::vec_ok(node_flows, ld) && pcb::vec_ok(node_mars, ld) && pcb::vec_ok(element_mars, ld);
     cudaStream_t s = pcb::as_stream(stream);
-    const float *nf = node_flows, *nm = node_mars, *em = element_mars;
-    if (modified && atomic) return launch<true, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
-    if (modified) return launch<true, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
-    if (atomic) return launch<false, true>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
-    return launch<false, false>(cs, nf, nm, em, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec);
+    const bool mod = modified != 0, at = atomic != 0;
+#define PCB_PK(T, P) \
+    launch_flags<T, P>(cs, mod, at, node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec)
+    if (tile_children == 32) return prec == 0 ? PCB_PK(32, 0) : (prec == 1 ? PCB_PK(32, 1) : PCB_PK(32, 2));
+    return prec == 0 ? PCB_PK(64, 0) : (prec == 1 ? PCB_PK(64, 1) : PCB_PK(64, 2));
+#undef PCB_PK
 }

@@ -41,6 +41,53 @@ def _tile_rows(max_rows: int) -> int:
     return t
 
 
+_SHORT_K = 128  # terms per tile handled by the single-stage kernels (pcb_lse_contract_short)
+_NUM_SMS = None
+_PACK_BYTES = 65536  # packed bf16 hi + lo weights of one tile (pcb_pack_weights)
+
+
+def _num_sms() -> int:
+    global _NUM_SMS
+    if _NUM_SMS is None:
+        _NUM_SMS = max(1, int(nat.load().pcb_num_sms()))
+    return _NUM_SMS
+
+
+def _short_batch_tile(num_tiles: int, tile_rows: int, B: int) -> int:
+    """Samples per CTA for pcb_lse_contract_short: the widest slice that still launches two
+    CTAs per SM (small layers get narrow slices and therefore more CTAs)."""
+    splits = 1 if tile_rows <= 32 else -(-tile_rows // 64)
+    for tb in (64, 32):
+        if num_tiles * splits * -(-B // tb) >= 2 * _num_sms():
+            return tb
+    return 16
+
+
+def _tc05_batch_tile(num_tiles: int, B: int) -> int:
+    """Samples per CTA for pcb_lse_contract_tc05 (two CTAs per SM fit in shared memory)."""
+    return 64 if num_tiles * -(-B // 64) >= 2 * _num_sms() else 32
+
+
+def _rows_vec4(tiles: np.ndarray, kw: np.ndarray, rpb: int, w_stride: int) -> bool:
+    """Weights of 4 consecutive rows are consecutive and 16-byte aligned (forward tables)."""
+    return (w_stride == 1 and rpb % 4 == 0 and bool(np.all(kw % 4 == 0)) and bool(np.all(tiles[:, 4] % 4 == 0))
+            and bool(np.all(tiles[:, 6] % 4 == 0)))
+
+
+def _terms_vec4(tiles: np.ndarray, kw: np.ndarray, w_stride: int) -> bool:
+    """Weights of 4 consecutive terms (aligned groups of each tile) are consecutive and
+    16-byte aligned (element-flow tables)."""
+    if w_stride % 4 or not np.all(tiles[:, 4] % 4 == 0) or not np.all(tiles[:, 6] % 4 == 0):
+        return False
+    for k_off, k_cnt in zip(tiles[:, 2].tolist(), tiles[:, 3].tolist()):
+        seg = kw[k_off:k_off + k_cnt]
+        full = (k_cnt // 4) * 4
+        g = seg[:full].reshape(-1, 4)
+        if g.size and (np.any(g[:, 0] % 4) or np.any(g - g[:, :1] != np.arange(4)[None, :])):
+            return False
+    return True
+
+
 def _merge_chains(starts, klists, wlists, flists, rpb: int):
     """Group consecutive blocks into tiles that share one set of contraction terms.
 
@@ -139,6 +186,8 @@ class SumLayer(Layer):
     """
 
     bf16_form = 2
+    short_kernels = True  # single-stage kernels for tiles of <= 128 terms
+    tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -213,15 +262,16 @@ class SumLayer(Layer):
         blk_koff = np.asarray(blk_koff, np.int64)
         blk_kcnt = np.asarray(blk_kcnt, np.int64)
 
-        fw_tiles, pf_tiles = [], []
+        fw_tiles, pf_tiles, pf_tiles32 = [], [], []
         for g, cnt, gs_w, gs_f in chains:
             rows = cnt * bs
             for i0 in range(0, rows, _MAX_ROWS):
                 nr = min(_MAX_ROWS, rows - i0)
                 fw_tiles.append((blk_nid[g] + i0, nr, blk_koff[g], blk_kcnt[g], i0, 0, gs_w, 0))
-                for k0 in range(0, int(blk_kcnt[g]), 64):
-                    pf_tiles.append((blk_nid[g] + i0, nr, blk_koff[g] + k0, min(64, int(blk_kcnt[g]) - k0), i0,
-                                     gs_w, gs_f, 0))
+                for kc, lst in ((64, pf_tiles), (32, pf_tiles32)):
+                    for k0 in range(0, int(blk_kcnt[g]), kc):
+                        lst.append((blk_nid[g] + i0, nr, blk_koff[g] + k0, min(kc, int(blk_kcnt[g]) - k0), i0,
+                                    gs_w, gs_f, 0))
         fw_tm = _tile_rows(max(t[1] for t in fw_tiles)) if fw_tiles else 1
         node2blk = np.zeros([self.num_nodes // bs], np.int64)
         node2blk[(blk_nid - self._layer_nid_range[0]) // bs] = np.arange(blk_nid.shape[0])
@@ -251,16 +301,26 @@ class SumLayer(Layer):
                 for j0 in range(0, rows, _MAX_ROWS):
                     nr = min(_MAX_ROWS, rows - j0)
                     tiles.append((starts[g] + j0, nr, offs[g], klist[g].shape[0], j0 * bs, starts[g] + j0, gs_w, 0))
+            tiles_np = np.asarray(tiles, np.int64).reshape(-1, 8)
+            kw_np = np.concatenate(wlist)
             el_groups.append(dict(
-                cbs=cbs, tm=_tile_rows(max(t[1] for t in tiles)), tiles=_i32(np.asarray(tiles, np.int64).reshape(-1, 8)),
-                krow=_i32(np.concatenate(klist)), kw=_i32(np.concatenate(wlist))))
+                cbs=cbs, tm=_tile_rows(max(t[1] for t in tiles)), tiles=_i32(tiles_np),
+                krow=_i32(np.concatenate(klist)), kw=_i32(kw_np),
+                short=int(tiles_np[:, 3].max()) <= _SHORT_K,
+                wlayout=2 if _terms_vec4(tiles_np, kw_np, bs) else 0,
+                pack=torch.empty([tiles_np.shape[0] * _PACK_BYTES], dtype=torch.uint8)))
 
+        fw_np = np.asarray(fw_tiles, np.int64).reshape(-1, 8)
         return dict(
-            fw_tiles=_i32(np.asarray(fw_tiles, np.int64).reshape(-1, 8)), fw_tm=fw_tm,
+            fw_tiles=_i32(fw_np), fw_tm=fw_tm,
+            fw_short=bool(fw_np.shape[0]) and int(fw_np[:, 3].max()) <= _SHORT_K,
+            fw_wlayout=1 if (fw_np.shape[0] and _rows_vec4(fw_np, kw_c, bs, 1)) else 0,
+            fw_pack=torch.empty([fw_np.shape[0] * _PACK_BYTES], dtype=torch.uint8),
             krow=_i32(krow_c), kw=_i32(kw_c), kpf=_i32(kpf_c),
             blk_nid=_i32(blk_nid), blk_koff=_i32(blk_koff), blk_kcnt=_i32(blk_kcnt), node2blk=_i32(node2blk),
             min_kcnt=int(blk_kcnt.min()) if blk_kcnt.size else 0,
             pf_tiles=_i32(np.asarray(pf_tiles, np.int64).reshape(-1, 8)),
+            pf_tiles32=_i32(np.asarray(pf_tiles32, np.int64).reshape(-1, 8)),
             el_groups=el_groups,
         )
 
@@ -291,6 +351,20 @@ class SumLayer(Layer):
             raise ValueError("node_mars and element_mars must share a row-major layout")
         prec = SumLayer.bf16_form if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
         t = d["fw_tiles"]
+        st = nat.stream()
+        if prec > 0 and d["fw_short"] and t.size(0) >= SumLayer.tc05_min_tiles:
+            nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
+                     nat.ptr(d["fw_pack"]), st)
+            nat.call("pcb_lse_contract_tc05", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
+                     nat.ptr(node_mars), ld, B, nat.ptr(d["fw_pack"]), nat.ptr(t), t.size(0), nat.ptr(d["krow"]), 0,
+                     prec, _tc05_batch_tile(t.size(0), B), st)
+            return
+        if d["fw_short"] and SumLayer.short_kernels:
+            nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
+                     ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
+                     nat.ptr(d["kw"]), 1, 0, prec, d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B),
+                     nat.stream())
+            return
         nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
                  nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
                  nat.ptr(d["kw"]), 1, 0, prec, nat.stream())
@@ -319,17 +393,39 @@ class SumLayer(Layer):
         for eg in d["el_groups"]:
             et = eg["tiles"]
             prec = SumLayer.bf16_form if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
+            if prec > 0 and eg["short"] and et.size(0) >= SumLayer.tc05_min_tiles:
+                st = nat.stream()
+                nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
+                         self.block_size, nat.ptr(eg["pack"]), st)
+                nat.call("pcb_lse_contract_tc05", nat.ptr(node_flows),
+                         nat.ptr(None if allow_modify_flows else node_mars), nat.ptr(element_mars),
+                         nat.ptr(element_flows), ld, B, nat.ptr(eg["pack"]), nat.ptr(et), et.size(0),
+                         nat.ptr(eg["krow"]), 1 if allow_modify_flows else 2, prec,
+                         _tc05_batch_tile(et.size(0), B), st)
+                continue
+            if eg["short"] and SumLayer.short_kernels:
+                nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
+                         nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et),
+                         et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
+                         1 if allow_modify_flows else 2, prec, eg["wlayout"],
+                         _short_batch_tile(et.size(0), eg["tm"], B), nat.stream())
+                continue
             nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
                      nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
                      eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
                      1 if allow_modify_flows else 2, prec, nat.stream())
         # parameter flows
         if param_flows is not None:
-            pt = d["pf_tiles"]
+            # 64-child tiles unless that leaves the GPU short of CTAs (cluster of up to 8 per tile)
+            cs = min(8, 1 << max(0, (B - 1).bit_length() - 6))
+            pt, kc = d["pf_tiles"], 64
+            if pt.size(0) * cs < 2 * _num_sms():
+                pt, kc = d["pf_tiles32"], 32
+            prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
             nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
                      nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size, nat.ptr(d["krow"]),
                      nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0, 1 if self._has_tied else 0,
-                     nat.stream())
+                     kc, prec, nat.stream())
 
     def __repr__(self):
         return f"SumLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"

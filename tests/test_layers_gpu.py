@@ -106,3 +106,42 @@ def test_prod_layer_forward_backward(B, cuda_device):
             for i in range(bs):
                 ref = sum(ef[par[g, q] + i] for q in range(par.size(1)))
                 assert torch.allclose(nf[u[g] + i], ref, atol=1e-6)
+
+
+@pytest.mark.parametrize("path", ["short", "tc05"])
+@pytest.mark.parametrize("bs,B,form", [(8, 7, 2), (16, 130, 2), (32, 256, 2), (32, 512, 1), (64, 33, 2)])
+def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
+    """The single-stage contractions (<= 128 terms: mma.sync or tcgen05) agree with the chunked ones."""
+    from pyjuice_b200.layer.layers import SumLayer
+    torch.manual_seed(1234 + bs + B)
+    prod, layer = _layers(bs)
+    layer.to(cuda_device)
+    n_el = bs + 3 * 2 * 2 * bs
+    n_nd = bs + bs * 2 * 3
+    em = (torch.rand([n_el, B]) * 4 - 6).to(cuda_device)
+    em[:bs] = -float("inf")
+    params = torch.rand([bs ** 2 + 3 * 4 * bs * bs], device=cuda_device)
+    nf0 = torch.rand([n_nd, B], device=cuda_device)
+    outs = {}
+    saved = (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles)
+    try:
+        SumLayer.bf16_form = form
+        for short in (False, True):
+            SumLayer.short_kernels = short
+            SumLayer.tc05_min_tiles = 1 if (short and path == "tc05") else 1 << 30
+            nm = torch.zeros([n_nd, B], device=cuda_device)
+            layer(nm, em, params, force_use_bf16=True)
+            ef = torch.zeros([n_el, B], device=cuda_device)
+            pf = torch.zeros_like(params)
+            nf = nf0.clone()
+            layer.backward(nf, ef, nm, em, params, pf)
+            ef2 = torch.zeros([n_el, B], device=cuda_device)
+            nf2 = nf0.clone()
+            layer.backward(nf2, ef2, nm, em, params, None, allow_modify_flows=True)
+            outs[short] = (nm[bs:], ef[bs:], ef2[bs:], pf)
+    finally:
+        SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles = saved
+    tol = 2e-5 if form == 2 else 2e-2
+    for a, b in zip(outs[False], outs[True]):
+        assert torch.isfinite(b).all()
+        assert torch.all((a - b).abs() <= tol * a.abs().clamp(min=1.0)), (a - b).abs().max()
