@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=BATCH)
+    p.add_argument("--profile-step", action="store_true",
+                   help="run one warm-up step and one EM step (BF16 form) inside the NVTX range 'em_step', "
+                        "for kernel profilers; prints the kernels launched per step")
     return p.parse_args()
 
 
@@ -141,42 +144,58 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-def sum_forward_roofline(pc, x, precision_kw, reps=3):
-    """Per-launch CUDA-event timing of the sum-layer forward contractions of one forward pass.
+def sum_forward_roofline(pc, x, precision_kw, reps=10):
+    """Device time of every sum layer's forward (its weight-pack and contraction launches),
+    each captured ``reps`` times in one CUDA graph and timed with CUDA events on the
+    launching stream; element_mars holds the layer's children from the preceding product
+    layers.
 
-    Algorithmic bytes per launch: each child row read once (4 B x batch), each node row
-    written once (4 B x batch), each edge weight read once (4 B).
+    Algorithmic bytes of a layer: each child row read once (4 B x batch), each node row
+    written once (4 B x batch), each edge weight read once (4 B). Returns totals over the
+    layers and the figures of the largest layer.
     """
     with torch.no_grad():
         pc(x, **precision_kw)
-    s = torch.cuda.current_stream()
     B = x.size(0)
-    rows = []
-    for g in pc.inner_layer_groups:
-        if g.is_sum():
-            for layer in g:
-                d = layer._desc(x.device)
-                child_rows = int(torch.unique(d["krow"]).numel())
-                rows.append((layer, 4 * B * (child_rows + layer.num_nodes) + 4 * layer.num_edges,
-                             2 * layer.num_edges * B))
-    tot_ms, bytes_alg, flops = 0.0, 0, 0
-    for _ in range(reps):
-        for g in pc.inner_layer_groups:
+    per_layer = []
+    with torch.no_grad():
+        for gi, g in enumerate(pc.inner_layer_groups):
             if g.is_prod():
                 g(pc.node_mars, pc.element_mars)
                 continue
             for layer in g:
+                d = layer._desc(x.device)
+                child_rows = int(torch.unique(d["krow"]).numel())
+                nbytes = 4 * B * (child_rows + layer.num_nodes) + 4 * layer.num_edges
+
+                def fwd():
+                    layer(pc.node_mars, pc.element_mars, pc.params, **precision_kw)
+
+                side = torch.cuda.Stream()
+                side.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(side):
+                    fwd()
+                torch.cuda.current_stream().wait_stream(side)
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph):
+                    for _ in range(reps):
+                        fwd()
+                graph.replay()
+                torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(s)
-                layer(pc.node_mars, pc.element_mars, pc.params, **precision_kw)
-                e1.record(s)
+                e0.record()
+                graph.replay()
+                e1.record()
                 e1.synchronize()
-                tot_ms += e0.elapsed_time(e1)
-        for _, b, f in rows:
-            bytes_alg += b
-            flops += f
-    n = reps * len(rows)
-    return bytes_alg / n, flops / n, tot_ms / 1e3 / n, len(rows)
+                per_layer.append((nbytes, 2 * layer.num_edges * B, e0.elapsed_time(e1) / 1e3 / reps,
+                                  d["fw_tiles"].size(0)))
+                del graph
+    tot_b = sum(r[0] for r in per_layer)
+    tot_f = sum(r[1] for r in per_layer)
+    tot_s = sum(r[2] for r in per_layer)
+    big = max(per_layer, key=lambda r: r[0])
+    return {"layers": len(per_layer), "bytes": tot_b, "flops": tot_f, "seconds": tot_s,
+            "largest": {"bytes": big[0], "flops": big[1], "seconds": big[2], "tiles": big[3]}}
 
 
 def cpu_step_rate(layout, params, in_params, data, budget_s):
@@ -277,6 +296,15 @@ def main():
     n0 = nat.CALLS
     step(data_dev[:B], {"force_use_bf16": True})
     kernels_per_step = nat.CALLS - n0
+    if args.profile_step:
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("em_step")
+        step(data_dev[B:2 * B], {"force_use_bf16": True})
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        if rank == 0:
+            print(json.dumps({"profile_step": True, "kernels_per_step": kernels_per_step}), flush=True)
+        return
 
     def timed(kw, use_graph):
         x_static = data_dev[:B].clone()
@@ -381,12 +409,18 @@ def main():
                   "fp32_dmean_ll_nats": float(abs(l_32.mean() - lls_o.mean())),
                   "mean_ll_nats": float(lls_o.mean()), "samples": int(xs.size(0))}
         hbm, tflops, src = peaks()
-        bytes_l, flops_l, avg_s, nl = sum_forward_roofline(pc, data_dev[:B], {"force_use_bf16": True})
-        achieved = bytes_l / avg_s / 1e9
-        roof = {"kernel": "pcb_lse_contract, sum-layer forward, bf16 form", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                "peak_source": f"{src} hbm_gbs", "launches_per_forward": nl, "avg_launch_us": avg_s * 1e6,
-                "alg_bytes_per_launch": bytes_l, "tensor_tflops_achieved": flops_l / avg_s / 1e12}
+        rf = sum_forward_roofline(pc, data_dev[:B], {"force_use_bf16": True})
+        big = rf["largest"]
+        achieved = big["bytes"] / big["seconds"] / 1e9
+        roof = {"kernel": "sum-layer forward of the largest layer (pcb_pack_weights + pcb_lse_contract_tc05, "
+                          "split-bf16 tcgen05)",
+                "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "peak_source": f"{src} hbm_gbs (of measured)" if src == "measured" else src,
+                "alg_bytes_per_launch": big["bytes"], "us_per_launch": big["seconds"] * 1e6,
+                "tiles": big["tiles"], "tensor_tflops_achieved": big["flops"] / big["seconds"] / 1e12,
+                "all_sum_layers": {"layers": rf["layers"], "us_total": rf["seconds"] * 1e6,
+                                   "achieved_gbs": rf["bytes"] / rf["seconds"] / 1e9,
+                                   "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm}}
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
         v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0)

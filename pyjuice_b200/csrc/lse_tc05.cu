@@ -131,15 +131,21 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4& h, uint4& l) 
 }
 
 // ---------------------------------------------------------------------------------------
-// Weight packing: one CTA per tile, 16-byte chunks (8 terms of one row).
+// Weight packing: 8 CTAs per tile, one 16-byte chunk (8 terms of one row) per thread;
+// consecutive threads take consecutive rows, so each weight load is coalesced along the
+// rows of the forward tables.
+constexpr int kPackSplit = (128 * (KT / 8)) / 256;
+
 __global__ void __launch_bounds__(256)
 pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
                     const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
-    const PcbLseTile t = tiles[blockIdx.x];
-    uint8_t* dst = packed + (size_t)blockIdx.x * kTileBytes;
+    const int tile = blockIdx.x / kPackSplit;
+    const PcbLseTile t = tiles[tile];
+    uint8_t* dst = packed + (size_t)tile * kTileBytes;
     const int rpb_mask = (1 << rpb_log2) - 1;
     const int nk = min(t.k_cnt, KT);
-    for (int c = threadIdx.x; c < 128 * (KT / 8); c += 256) {
+    {
+        const int c = (blockIdx.x % kPackSplit) * 256 + threadIdx.x;
         const int r = c % 128;
         const int kg = c / 128;
         float w[8];
@@ -435,8 +441,9 @@ extern "C" int pcb_pack_weights(const float* params, const PcbLseTile* tiles, in
     if (num_tiles == 0) return PCB_OK;
     int rpb_log2 = 0;
     while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
-    pack_weights_kernel<<<(unsigned)num_tiles, 256, 0, pcb::as_stream(stream)>>>(params, tiles, rpb_log2, kw,
-                                                                                w_stride, packed);
+    if ((int64_t)num_tiles * kPackSplit > 2147483647) return pcb::set_error(PCB_E_ARG, "pcb_pack_weights: too many tiles");
+    pack_weights_kernel<<<(unsigned)(num_tiles * kPackSplit), 256, 0, pcb::as_stream(stream)>>>(params, tiles, rpb_log2,
+                                                                                              kw, w_stride, packed);
     return pcb::check_launch("pcb_pack_weights");
 }
 

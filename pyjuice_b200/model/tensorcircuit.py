@@ -136,6 +136,7 @@ class TensorCircuit(nn.Module):
         num_param_flows = 0
         node2tiednodes = dict()
         self.inner_layer_groups = []
+        em_regions = []
         self.input_layer_group = None
         input_layers = []
         for depth in range(num_layers):
@@ -165,6 +166,7 @@ class TensorCircuit(nn.Module):
                 num_edges += pl.num_edges
                 prod_layers.append(pl)
             self.inner_layer_groups.append(LayerGroup(prod_layers))
+            em_regions.append((len(self.inner_layer_groups) - 1, layer_num_elements))
             num_elements = max(num_elements, layer_num_elements)
             gsize2sum = dict()
             for ns in depth2nodes[depth]["sum"]:
@@ -185,6 +187,14 @@ class TensorCircuit(nn.Module):
         self.num_nodes = num_nodes
         self.num_edges = num_edges
         self.num_elements = num_elements
+        # Every product layer group keeps its element values in its own row region of one
+        # resident buffer, so the backward pass reads them instead of recomputing them.
+        self._em_region = dict()
+        off = 0
+        for gi, rows in em_regions:
+            self._em_region[gi] = (off, rows)
+            off += rows
+        self._em_rows = off
         self.num_sum_params = num_parameters
         self.num_param_flows = num_param_flows
         self.num_root_nodes = self.root_ns.num_nodes
@@ -286,12 +296,17 @@ class TensorCircuit(nn.Module):
         self.default_propagation_alg = "LL"
         self.propagation_alg_kwargs.clear()
 
+    def _em_view(self, group_id: int) -> torch.Tensor:
+        """Element values of product layer group ``group_id`` (rows indexed like ``element_mars``)."""
+        off, rows = self._em_region[group_id]
+        return self._em_resident[off:off + rows]
+
     def _run_inner_forward(self, force_use_bf16, force_use_fp32, propagation_alg, **kwargs):
-        for group in self.inner_layer_groups:
+        for gi, group in enumerate(self.inner_layer_groups):
             if group.is_prod():
-                group(self.node_mars, self.element_mars)
+                group(self.node_mars, self._em_view(gi))
             else:
-                group(self.node_mars, self.element_mars, self.params, force_use_bf16=force_use_bf16,
+                group(self.node_mars, self._em_view(gi - 1), self.params, force_use_bf16=force_use_bf16,
                       force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, **kwargs)
 
     def forward(self, inputs: torch.Tensor, input_layer_fn: Optional[Union[str, Callable]] = None,
@@ -313,6 +328,8 @@ class TensorCircuit(nn.Module):
                 data = inputs.permute(1, 0).to(self.device, torch.long).contiguous()
             nm = self._buffer("node_mars", self.num_nodes, B, 0.0)
             em = self._buffer("element_mars", self.num_elements, B, -float("inf"))
+            # dummy rows of every region keep their initial -inf (nothing writes them)
+            self._buffer("_em_resident", self._em_rows, B, -float("inf"))
             if not _no_buffer_reset:
                 nat.call("pcb_fill_rows", nat.ptr(nm), B, 0, self.num_dummy_nodes, 0.0, nat.stream())
                 nat.call("pcb_fill_rows", nat.ptr(em), B, 0, self.num_dummy_eles, -float("inf"), nat.stream())
@@ -328,7 +345,7 @@ class TensorCircuit(nn.Module):
                         ret = input_layer_fn(layer, inputs, nm, **kwargs)
                         if not ret and ret is not None:
                             layer(data, nm, **kwargs)
-            sig = (0, id(nm), id(em), id(self.params), B, force_use_bf16, force_use_fp32)
+            sig = (0, id(nm), id(em), id(self._em_resident), id(self.params), B, force_use_bf16, force_use_fp32)
             run = partial(self._run_inner_forward, force_use_bf16, force_use_fp32, propagation_alg, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
                 self._recorded_cuda_graphs[sig] = self._capture(run)
@@ -369,10 +386,16 @@ class TensorCircuit(nn.Module):
             if group.is_prod():
                 group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows)
             else:
-                self.inner_layer_groups[layer_id - 1].forward(self.node_mars, self.element_mars, _for_backward=True)
-                group.backward(self.node_flows, self.element_flows, self.node_mars, self.element_mars, self.params,
+                # The element values of the forward pass are still resident (no recomputation). Small
+                # layers form log f - log m inside the flow kernels instead of rewriting the node flows
+                # in place (one launch fewer); large ones rewrite them once (allow_modify_flows) so that
+                # the two flow kernels read one row per node instead of two.
+                modify = allow_modify_flows and any(
+                    layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles for layer in group)
+                group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
+                               self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
-                               allow_modify_flows=allow_modify_flows, logspace_flows=logspace_flows,
+                               allow_modify_flows=modify, logspace_flows=logspace_flows,
                                force_use_fp32=force_use_fp32, **kwargs)
 
     def backward(self, inputs: Optional[torch.Tensor] = None, ll_weights: Optional[torch.Tensor] = None,
@@ -427,7 +450,7 @@ class TensorCircuit(nn.Module):
                 nf.copy_(cache["node_flows"])
             if compute_param_flows:
                 self.init_param_flows(flows_memory=flows_memory)
-            sig = (1, id(nf), id(ef), id(self.node_mars), id(self.element_mars), id(self.params),
+            sig = (1, id(nf), id(ef), id(self.node_mars), id(self._em_resident), id(self.params),
                    id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows)
             run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,
                           force_use_fp32, **kwargs)
