@@ -2,6 +2,8 @@
 #include <cstdarg>
 #include <cstring>
 
+#include <cstdlib>
+
 #include "common.cuh"
 
 namespace pcb {
@@ -14,6 +16,22 @@ int set_error(int code, const char* fmt, ...) {
     vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
     va_end(ap);
     return code;
+}
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("PCB_NO_PDL");
+        return !(v && v[0] == '1');
+    }();
+    return on;
+}
+
+int launch_status(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PCB_E_LAUNCH, "%s: launch failed: %s", what, cudaGetErrorString(e));
+    }
+    return PCB_OK;
 }
 
 int check_launch(const char* what) {
@@ -29,12 +47,14 @@ int check_launch(const char* what) {
 namespace {
 
 __global__ void fill_rows_kernel(float* __restrict__ mat, int64_t n, float value) {
+    pcb::pdl_begin();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n; i += stride) mat[i] = value;
 }
 
 __global__ void ll_sum_kernel(const float* __restrict__ lls, int B, double* __restrict__ out) {
+    pcb::pdl_begin();
     __shared__ double part[8];
     double s = 0.0;
     for (int b = threadIdx.x; b < B; b += blockDim.x) s += (double)lls[b];
@@ -50,6 +70,7 @@ __global__ void ll_sum_kernel(const float* __restrict__ lls, int B, double* __re
 
 __global__ void pflow_accum_kernel(float* __restrict__ pf, int64_t dst, int64_t n, const int64_t* __restrict__ srcs,
                                    int nsrc) {
+    pcb::pdl_begin();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     float s = 0.f;
@@ -79,21 +100,23 @@ int pcb_fill_rows(float* mat, int64_t ld, int64_t row0, int64_t row1, float valu
     if (n == 0) return PCB_OK;
     int64_t blocks = pcb::cdiv(n, 256);
     if (blocks > 4 * 148 * 8) blocks = 4 * 148 * 8;
-    fill_rows_kernel<<<(unsigned)blocks, 256, 0, pcb::as_stream(stream)>>>(mat + row0 * ld, n, value);
-    return pcb::check_launch("pcb_fill_rows");
+    return pcb::launch_status(pcb::launch_k(fill_rows_kernel, dim3((unsigned)blocks), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, mat + row0 * ld, n, value),
+                              "pcb_fill_rows");
 }
 
 int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double* out, void* stream) {
     if (!lls || !out || B <= 0 || row < 0) return pcb::set_error(PCB_E_ARG, "pcb_ll_sum_f64: bad arguments");
-    ll_sum_kernel<<<1, 256, 0, pcb::as_stream(stream)>>>(lls + row * ld, B, out);
-    return pcb::check_launch("pcb_ll_sum_f64");
+    return pcb::launch_status(pcb::launch_k(ll_sum_kernel, dim3(1), dim3(256), 0, pcb::as_stream(stream), 1u,
+                                            lls + row * ld, B, out), "pcb_ll_sum_f64");
 }
 
 int pcb_pflow_accum(float* param_flows, int64_t dst, int64_t n, const int64_t* srcs, int32_t nsrc, void* stream) {
     if (!param_flows || !srcs || n < 0 || nsrc <= 0) return pcb::set_error(PCB_E_ARG, "pcb_pflow_accum: bad arguments");
     if (n == 0) return PCB_OK;
-    pflow_accum_kernel<<<(unsigned)pcb::cdiv(n, 256), 256, 0, pcb::as_stream(stream)>>>(param_flows, dst, n, srcs, nsrc);
-    return pcb::check_launch("pcb_pflow_accum");
+    return pcb::launch_status(pcb::launch_k(pflow_accum_kernel, dim3((unsigned)pcb::cdiv(n, 256)), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, param_flows, dst, n, srcs, nsrc),
+                              "pcb_pflow_accum");
 }
 
 }  // extern "C"

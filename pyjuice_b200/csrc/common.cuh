@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cmath>
+#include <utility>
 
 #include "../../include/pcb200.h"
 
@@ -89,6 +90,51 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Programmatic dependent launch. Every kernel starts with pdl_begin(): it lets the next
+// kernel of the stream be scheduled as soon as all of this grid's CTAs are running, then
+// waits until the previous grid has completed and its memory is visible. Kernels launched
+// without the attribute pass through both instructions at once.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
+// Whether launches carry the programmatic-stream-serialization attribute (on unless the
+// environment sets PCB_NO_PDL=1).
+bool pdl_enabled();
+
+// Launch with the programmatic-stream-serialization attribute (and an optional cluster
+// size along x); returns the launch status.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            unsigned cluster_x, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
+    if (pdl_enabled()) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        ++n;
+    }
+    if (cluster_x > 1) {
+        attr[n].id = cudaLaunchAttributeClusterDimension;
+        attr[n].val.clusterDim.x = cluster_x;
+        attr[n].val.clusterDim.y = 1;
+        attr[n].val.clusterDim.z = 1;
+        ++n;
+    }
+    cfg.attrs = attr;
+    cfg.numAttrs = n;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Status of a launch_k call: PCB_OK, or PCB_E_LAUNCH with the message recorded.
+int launch_status(cudaError_t e, const char* what);
 
 // Vectorised access needs ld % 4 == 0 and a 16-byte aligned base.
 inline bool vec_ok(const void* p, int64_t ld) {

@@ -15,6 +15,7 @@ __global__ void __launch_bounds__(256)
 sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int64_t* __restrict__ pbase,
               const int64_t* __restrict__ pfbase, const int* __restrict__ nchs, const int* __restrict__ bss,
               double step, double pc) {
+    pcb::pdl_begin();
     __shared__ double part[256];
     const int g = blockIdx.x;
     const int64_t pb = pbase[g];
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(256)
 input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int* __restrict__ s_pids,
                 const int* __restrict__ s_pfids, const int* __restrict__ ncats, const int* __restrict__ source_nids,
                 int num_src, double step, double pc) {
+    pcb::pdl_begin();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= num_src) return;
@@ -113,11 +115,15 @@ extern "C" int pcb_sum_em(float* params, const float* param_flows, const int64_t
     if (!(step_size > 0.0 && step_size <= 1.0)) return pcb::set_error(PCB_E_ARG, "pcb_sum_em: step_size must be in (0, 1]");
     if (num_blocks == 0) return PCB_OK;
     cudaStream_t s = pcb::as_stream(stream);
-    if (keep_zero_params)
-        sum_em_kernel<true, true><<<num_blocks, 256, 0, s>>>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, step_size, pseudocount);
-    else
-        sum_em_kernel<true, false><<<num_blocks, 256, 0, s>>>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, step_size, pseudocount);
-    return pcb::check_launch("pcb_sum_em");
+    if (keep_zero_params) {
+        return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, true>, dim3(num_blocks), dim3(256), 0, s, 1u,
+                                                params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs,
+                                                step_size, pseudocount), "pcb_sum_em");
+    } else {
+        return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, false>, dim3(num_blocks), dim3(256), 0, s, 1u,
+                                                params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs,
+                                                step_size, pseudocount), "pcb_sum_em");
+    }
 }
 
 extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const int32_t* blk_nch, const int32_t* blk_bs,
@@ -125,9 +131,9 @@ extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const 
     if (!params || !blk_pbase || !blk_nch || !blk_bs || num_blocks < 0)
         return pcb::set_error(PCB_E_ARG, "pcb_sum_normalize: bad arguments");
     if (num_blocks == 0) return PCB_OK;
-    sum_em_kernel<false, false><<<num_blocks, 256, 0, pcb::as_stream(stream)>>>(params, nullptr, blk_pbase, nullptr, blk_nch,
-                                                                                 blk_bs, 1.0, pseudocount);
-    return pcb::check_launch("pcb_sum_normalize");
+    return pcb::launch_status(pcb::launch_k(sum_em_kernel<false, false>, dim3(num_blocks), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, params, nullptr, blk_pbase, nullptr, blk_nch,
+                                            blk_bs, 1.0, pseudocount), "pcb_sum_normalize");
 }
 
 extern "C" int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_pids, const int32_t* s_pfids,
@@ -140,9 +146,13 @@ extern "C" int pcb_input_cat_em(float* params, const float* param_flows, const i
     if (num_source_nodes == 0) return PCB_OK;
     const unsigned grid = (unsigned)pcb::cdiv((int64_t)num_source_nodes * 32, 256);
     cudaStream_t s = pcb::as_stream(stream);
-    if (keep_zero_params)
-        input_em_kernel<true><<<grid, 256, 0, s>>>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes, step_size, pseudocount);
-    else
-        input_em_kernel<false><<<grid, 256, 0, s>>>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes, step_size, pseudocount);
-    return pcb::check_launch("pcb_input_cat_em");
+    if (keep_zero_params) {
+        return pcb::launch_status(pcb::launch_k(input_em_kernel<true>, dim3(grid), dim3(256), 0, s, 1u, params,
+                                                param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                                step_size, pseudocount), "pcb_input_cat_em");
+    } else {
+        return pcb::launch_status(pcb::launch_k(input_em_kernel<false>, dim3(grid), dim3(256), 0, s, 1u, params,
+                                                param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                                step_size, pseudocount), "pcb_input_cat_em");
+    }
 }

@@ -9,6 +9,7 @@ __global__ void __launch_bounds__(256)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
                      int node_offset, float* __restrict__ nm, int64_t ld, int B, int ngrp, int64_t total, bool vec) {
+    pcb::pdl_begin();
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int b = (int)(idx % ngrp) * 4;
@@ -37,6 +38,7 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                      int B, const int* __restrict__ grp_var, const int* __restrict__ grp_node0,
                      const int* __restrict__ grp_count, const int* __restrict__ grp_ncats,
                      const int* __restrict__ s_pfids, int node_offset, float* __restrict__ pf, bool logspace, int CB) {
+    pcb::pdl_begin();
     extern __shared__ int smem[];
     const int g = blockIdx.x;
     const int K = grp_ncats[g];
@@ -117,9 +119,9 @@ extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const flo
     const int ngrp = (int)pcb::cdiv(B, 4);
     const int64_t total = (int64_t)num_nodes * ngrp;
     const bool vec = pcb::vec_ok(node_mars, ld);
-    input_cat_fwd_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
-        data, data_ld, params, vids, s_pids, ncats, node_offset, node_mars, ld, B, ngrp, total, vec);
-    return pcb::check_launch("pcb_input_cat_fwd");
+    return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(total, 256)), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, data, data_ld, params, vids, s_pids, ncats,
+                                            node_offset, node_mars, ld, B, ngrp, total, vec), "pcb_input_cat_fwd");
 }
 
 extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,
@@ -138,8 +140,8 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
         cudaError_t e = cudaFuncSetAttribute(input_cat_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_input_cat_bwd: %s", cudaGetErrorString(e));
     }
-    input_cat_bwd_kernel<<<num_groups, 256, smem, pcb::as_stream(stream)>>>(
-        data, data_ld, node_flows, ld, B, grp_var, grp_node0, grp_count, grp_ncats, s_pfids, node_offset, param_flows,
-        logspace_flows != 0, CB);
-    return pcb::check_launch("pcb_input_cat_bwd");
+    return pcb::launch_status(pcb::launch_k(input_cat_bwd_kernel, dim3(num_groups), dim3(256), smem,
+                                            pcb::as_stream(stream), 1u, data, data_ld, node_flows, ld, B, grp_var,
+                                            grp_node0, grp_count, grp_ncats, s_pfids, node_offset, param_flows,
+                                            logspace_flows != 0, CB), "pcb_input_cat_bwd");
 }

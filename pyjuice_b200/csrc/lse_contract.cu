@@ -24,6 +24,7 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
                float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                int w_stride, int rpb_log2, bool vec) {
+    pcb::pdl_begin();
     constexpr int NX = TB / 4;           // threads along the batch (4 samples each)
     constexpr int NY = TM / RN;          // threads along rows
     constexpr int NT = NX * NY;
@@ -140,9 +141,9 @@ int launch_mode(dim3 grid, const float* src, const float* src2, const float* aux
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract: %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
-    lse_f32_kernel<TM, TB, RN, MODE><<<grid, threads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow, kw,
-                                                                 w_stride, rpb_log2, vec);
-    return pcb::check_launch("pcb_lse_contract");
+    return pcb::launch_status(pcb::launch_k(lse_f32_kernel<TM, TB, RN, MODE>, dim3(grid), dim3(threads), smem, s, 1u,
+                                            src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2,
+                                            vec), "pcb_lse_contract");
 }
 
 template <int TM, int TB, int RN>

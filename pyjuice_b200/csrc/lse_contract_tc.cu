@@ -62,6 +62,7 @@ lse_bf16_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                 int w_stride, int rpb_log2, bool vec) {
+    pcb::pdl_begin();
     constexpr int WM = TM / 16;          // warps along rows
     constexpr int WN = 8 / WM;           // warps along samples
     constexpr int NT = TB / 8 / WN;      // n8 tiles per warp
@@ -220,9 +221,9 @@ int launch_one(dim3 grid, const float* src, const float* src2, const float* aux,
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract(bf16): %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
-    lse_bf16_kernel<TM, TB, MODE, SPLIT><<<grid, kThreads, smem, s>>>(src, src2, aux, out, ld, B, params, tiles, krow,
-                                                                      kw, w_stride, rpb_log2, vec);
-    return pcb::check_launch("pcb_lse_contract(bf16)");
+    return pcb::launch_status(pcb::launch_k(lse_bf16_kernel<TM, TB, MODE, SPLIT>, dim3(grid), dim3(kThreads), smem, s,
+                                            1u, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride,
+                                            rpb_log2, vec), "pcb_lse_contract(bf16)");
 }
 
 template <int TM, int TB>

@@ -75,6 +75,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                  float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                  const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                  int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec) {
+    pcb::pdl_begin();
     using S = Smem<RM, TB, MODE, PREC, WK>;
     constexpr int ES = S::ES, WS = S::WS, WROW = S::WROW;
     constexpr int PARTS = kThreads / TB;  // threads per sample column in the max / exp passes
@@ -397,9 +398,10 @@ int launch_one(int num_tiles, int row_splits, const float* src, const float* src
     const int64_t gx = (int64_t)num_tiles * row_splits;
     const int64_t gy = pcb::cdiv(B, TB);
     if (gx > 2147483647 || gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: grid too large");
-    lse_short_kernel<RM, TB, MODE, PREC, WK><<<dim3((unsigned)gx, (unsigned)gy), kThreads, smem, s>>>(
-        src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, row_splits, vec, wvec);
-    return pcb::check_launch("pcb_lse_contract_short");
+    return pcb::launch_status(pcb::launch_k(lse_short_kernel<RM, TB, MODE, PREC, WK>,
+                                            dim3((unsigned)gx, (unsigned)gy), dim3(kThreads), smem, s, 1u, src,
+                                            src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2,
+                                            row_splits, vec, wvec), "pcb_lse_contract_short");
 }
 
 template <int RM, int TB, int PREC>

@@ -139,6 +139,7 @@ constexpr int kPackSplit = (128 * (KT / 8)) / 256;
 __global__ void __launch_bounds__(256)
 pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
                     const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
+    pcb::pdl_begin();
     const int tile = blockIdx.x / kPackSplit;
     const PcbLseTile t = tiles[tile];
     uint8_t* dst = packed + (size_t)tile * kTileBytes;
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(kThreads)
 lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const uint8_t* __restrict__ packed,
                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, bool vec) {
+    pcb::pdl_begin();
     static_assert(N == 32 || N == 64, "sample slice");
     using S = Tc05Smem<N>;
     constexpr int NQ = N / 32;          // groups of 4 x 8 samples
@@ -415,9 +417,10 @@ int launch(int num_tiles, const float* src, const float* src2, const float* aux,
     }
     const int64_t gy = pcb::cdiv(B, N);
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: batch too large");
-    lse_tc05_kernel<N, MODE, SPLIT><<<dim3((unsigned)num_tiles, (unsigned)gy), kThreads, smem, s>>>(
-        src, src2, aux, out, ld, B, packed, tiles, krow, vec);
-    return pcb::check_launch("pcb_lse_contract_tc05");
+    return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, SPLIT>,
+                                            dim3((unsigned)num_tiles, (unsigned)gy), dim3(kThreads), smem, s,
+                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, vec),
+                              "pcb_lse_contract_tc05");
 }
 
 template <int N>
@@ -442,9 +445,9 @@ extern "C" int pcb_pack_weights(const float* params, const PcbLseTile* tiles, in
     int rpb_log2 = 0;
     while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
     if ((int64_t)num_tiles * kPackSplit > 2147483647) return pcb::set_error(PCB_E_ARG, "pcb_pack_weights: too many tiles");
-    pack_weights_kernel<<<(unsigned)(num_tiles * kPackSplit), 256, 0, pcb::as_stream(stream)>>>(params, tiles, rpb_log2,
-                                                                                              kw, w_stride, packed);
-    return pcb::check_launch("pcb_pack_weights");
+    return pcb::launch_status(pcb::launch_k(pack_weights_kernel, dim3((unsigned)(num_tiles * kPackSplit)), dim3(256),
+                                            0, pcb::as_stream(stream), 1u, params, tiles, rpb_log2, kw, w_stride,
+                                            packed), "pcb_pack_weights");
 }
 
 extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld,

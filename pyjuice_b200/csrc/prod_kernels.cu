@@ -10,6 +10,7 @@ __global__ void __launch_bounds__(256)
 prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, int B, const int* __restrict__ blk_row,
             const int* __restrict__ blk_off, const int* __restrict__ blk_cnt, const int* __restrict__ chs,
             int blk_size, int ngrp, int64_t total, bool vec) {
+    pcb::pdl_begin();
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int grp = (int)(idx % ngrp);
@@ -75,6 +76,7 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
 __global__ void __launch_bounds__(256)
 modify_flows_kernel(float* __restrict__ nf, const float* __restrict__ nm, int64_t ld, int B, int64_t row0, int ngrp,
                     int64_t total, bool vec) {
+    pcb::pdl_begin();
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int b = (int)(idx % ngrp) * 4;
@@ -103,15 +105,23 @@ extern "C" int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int3
     const bool vec = pcb::vec_ok(in, ld) && pcb::vec_ok(out, ld);
     const unsigned grid = (unsigned)pcb::cdiv(total, 256);
     cudaStream_t s = pcb::as_stream(stream);
-    if (!accum && !logsumexp)
-        prod_kernel<false, false><<<grid, 256, 0, s>>>(in, out, ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec);
-    else if (accum && !logsumexp)
-        prod_kernel<true, false><<<grid, 256, 0, s>>>(in, out, ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec);
-    else if (!accum && logsumexp)
-        prod_kernel<false, true><<<grid, 256, 0, s>>>(in, out, ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec);
-    else
-        prod_kernel<true, true><<<grid, 256, 0, s>>>(in, out, ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec);
-    return pcb::check_launch("pcb_prod_gather_sum");
+    if (!accum && !logsumexp) {
+        return pcb::launch_status(pcb::launch_k(prod_kernel<false, false>, dim3(grid), dim3(256), 0, s, 1u, in, out,
+                                                ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec),
+                                  "pcb_prod_gather_sum");
+    } else if (accum && !logsumexp) {
+        return pcb::launch_status(pcb::launch_k(prod_kernel<true, false>, dim3(grid), dim3(256), 0, s, 1u, in, out,
+                                                ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec),
+                                  "pcb_prod_gather_sum");
+    } else if (!accum && logsumexp) {
+        return pcb::launch_status(pcb::launch_k(prod_kernel<false, true>, dim3(grid), dim3(256), 0, s, 1u, in, out,
+                                                ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec),
+                                  "pcb_prod_gather_sum");
+    } else {
+        return pcb::launch_status(pcb::launch_k(prod_kernel<true, true>, dim3(grid), dim3(256), 0, s, 1u, in, out, ld,
+                                                B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec),
+                                  "pcb_prod_gather_sum");
+    }
 }
 
 extern "C" int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int32_t B, int64_t row0,
@@ -122,7 +132,7 @@ extern "C" int pcb_modify_flows(float* node_flows, const float* node_mars, int64
     const int ngrp = (int)pcb::cdiv(B, 4);
     const int64_t total = (row1 - row0) * ngrp;
     const bool vec = pcb::vec_ok(node_flows, ld) && pcb::vec_ok(node_mars, ld);
-    modify_flows_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
-        node_flows, node_mars, ld, B, row0, ngrp, total, vec);
-    return pcb::check_launch("pcb_modify_flows");
+    return pcb::launch_status(pcb::launch_k(modify_flows_kernel, dim3((unsigned)pcb::cdiv(total, 256)), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, node_flows, node_mars, ld, B, row0, ngrp,
+                                            total, vec), "pcb_modify_flows");
 }

@@ -77,6 +77,7 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                   int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                   const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
                   const int* __restrict__ pids, const int* __restrict__ pfids, int slice, bool vec) {
+    pcb::pdl_begin();
     using P = Plan<TKC, MODIFIED, PREC>;
     extern __shared__ __align__(16) float dsm[];
     float(*sA)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oA);
@@ -328,22 +329,10 @@ int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_sum_pflows: %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)num_tiles * cs);
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, sum_pflows_kernel<TKC, MODIFIED, ATOMIC, PREC>, nf, nm, em, ld, B,
-                                       params, pf, tiles, rpb_log2, cids, pids, pfids, slice, vec);
-    if (e != cudaSuccess) return pcb::set_error(PCB_E_LAUNCH, "pcb_sum_pflows: %s", cudaGetErrorString(e));
-    return pcb::check_launch("pcb_sum_pflows");
+    return pcb::launch_status(pcb::launch_k(sum_pflows_kernel<TKC, MODIFIED, ATOMIC, PREC>, dim3((unsigned)num_tiles * cs),
+                                            dim3(kThreads), smem, s, (unsigned)cs, nf, nm, em, ld, B, params, pf,
+                                            tiles, rpb_log2, cids, pids, pfids, slice, vec),
+                              "pcb_sum_pflows");
 }
 
 template <int TKC, int PREC>
