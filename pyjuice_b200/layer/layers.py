@@ -389,6 +389,14 @@ class SumLayer(Layer):
         if allow_modify_flows:
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
                      self._layer_nid_range[1], nat.stream())
+        # The parameter flows only read this layer's node flows / mars and its children's element
+        # values, so with a side stream they run concurrently with the element flows (and with
+        # everything the caller issues next on the current stream).
+        pflow_stream = kwargs.get("_pflow_stream")
+        ready = None
+        if param_flows is not None and pflow_stream is not None:
+            ready = torch.cuda.Event()
+            ready.record()
         # element flows
         for eg in d["el_groups"]:
             et = eg["tiles"]
@@ -422,10 +430,13 @@ class SumLayer(Layer):
             if pt.size(0) * cs < 2 * _num_sms():
                 pt, kc = d["pf_tiles32"], 32
             prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
-            nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
-                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size, nat.ptr(d["krow"]),
-                     nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0, 1 if self._has_tied else 0,
-                     kc, prec, nat.stream())
+            if ready is not None:
+                pflow_stream.wait_event(ready)
+            with torch.cuda.stream(pflow_stream if ready is not None else torch.cuda.current_stream()):
+                nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
+                         nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size,
+                         nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0,
+                         1 if self._has_tied else 0, kc, prec, nat.stream())
 
     def __repr__(self):
         return f"SumLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"

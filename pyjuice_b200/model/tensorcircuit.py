@@ -68,6 +68,7 @@ class TensorCircuit(nn.Module):
         self.propagation_alg_kwargs = dict()
         self._run_params = dict()
         self._cum_flow_dev = None
+        self._side_streams = dict()
         self._dev_tables = {}
         if device is not None:
             self.to(device)
@@ -381,6 +382,14 @@ class TensorCircuit(nn.Module):
         return g
 
     def _run_inner_backward(self, compute_param_flows, allow_modify_flows, logspace_flows, force_use_fp32, **kwargs):
+        # Parameter flows go to a side stream: nothing later in the pass reads them, so they run
+        # alongside the element-flow / product chain and join before the pass ends.
+        main = torch.cuda.current_stream()
+        side = self._side_streams.get(main.device)
+        if side is None:
+            side = self._side_streams[main.device] = torch.cuda.Stream(device=main.device)
+        side.wait_stream(main)
+        kwargs = dict(kwargs, _pflow_stream=side)
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
             group = self.inner_layer_groups[layer_id]
             if group.is_prod():
@@ -397,6 +406,7 @@ class TensorCircuit(nn.Module):
                                param_flows=self.param_flows if compute_param_flows else None,
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
                                force_use_fp32=force_use_fp32, **kwargs)
+        main.wait_stream(side)
 
     def backward(self, inputs: Optional[torch.Tensor] = None, ll_weights: Optional[torch.Tensor] = None,
                  compute_param_flows: bool = True, flows_memory: float = 1.0,
