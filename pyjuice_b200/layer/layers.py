@@ -337,9 +337,44 @@ class SumLayer(Layer):
         # (sum_layer.py:871-880).
         return eligible and d["min_kcnt"] >= 16 and B >= 16
 
+    def _fw_tc05(self, d, B, force_use_bf16, force_use_fp32):
+        """Precision form of the forward and whether it runs on the tcgen05 kernel."""
+        prec = SumLayer.bf16_form if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
+        return prec, prec > 0 and d["fw_short"] and d["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles
+
+    def _el_prec(self, eg, B, force_use_fp32):
+        return SumLayer.bf16_form if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
+
+    def _el_tc05(self, eg, prec):
+        return prec > 0 and eg["short"] and eg["tiles"].size(0) >= SumLayer.tc05_min_tiles
+
+    def pack_forward_weights(self, params: torch.Tensor, B: int, force_use_bf16: bool = False,
+                             force_use_fp32: bool = False) -> bool:
+        """Pack the weights the forward's tcgen05 kernel reads (on the current stream); returns
+        whether this layer uses them. ``forward(..., _weights_packed=True)`` then skips the pack."""
+        d = self._desc(params.device)
+        prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
+        if tc05:
+            t = d["fw_tiles"]
+            nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
+                     nat.ptr(d["fw_pack"]), nat.stream())
+        return tc05
+
+    def pack_flow_weights(self, params: torch.Tensor, B: int, force_use_fp32: bool = False) -> bool:
+        """Pack the weights of the element-flow tcgen05 kernels (see pack_forward_weights)."""
+        d = self._desc(params.device)
+        any_tc05 = False
+        for eg in d["el_groups"]:
+            if self._el_tc05(eg, self._el_prec(eg, B, force_use_fp32)):
+                et = eg["tiles"]
+                nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
+                         self.block_size, nat.ptr(eg["pack"]), nat.stream())
+                any_tc05 = True
+        return any_tc05
+
     def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, params: torch.Tensor,
                 force_use_bf16: bool = False, force_use_fp32: bool = False, propagation_alg: str = "LL",
-                **kwargs) -> None:
+                _weights_packed: bool = False, **kwargs) -> None:
         if propagation_alg != "LL":
             raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
         if params.dim() != 1:
@@ -349,12 +384,12 @@ class SumLayer(Layer):
         ld = node_mars.stride(0)
         if element_mars.stride(0) != ld or node_mars.stride(1) != 1 or element_mars.stride(1) != 1:
             raise ValueError("node_mars and element_mars must share a row-major layout")
-        prec = SumLayer.bf16_form if self._use_bf16(d, B, force_use_bf16, force_use_fp32) else 0
+        prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
         t = d["fw_tiles"]
         st = nat.stream()
-        if prec > 0 and d["fw_short"] and t.size(0) >= SumLayer.tc05_min_tiles:
-            nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
-                     nat.ptr(d["fw_pack"]), st)
+        if tc05:
+            if not _weights_packed:
+                self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
             nat.call("pcb_lse_contract_tc05", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
                      nat.ptr(node_mars), ld, B, nat.ptr(d["fw_pack"]), nat.ptr(t), t.size(0), nat.ptr(d["krow"]), 0,
                      prec, _tc05_batch_tile(t.size(0), B), st)
@@ -375,7 +410,7 @@ class SumLayer(Layer):
                  element_mars: torch.Tensor, params: torch.Tensor, param_flows: Optional[torch.Tensor] = None,
                  allow_modify_flows: bool = False, propagation_alg: str = "LL", logspace_flows: bool = False,
                  negate_pflows: bool = False, accumulate_ch_flows: bool = False, allow_neg_flows: bool = False,
-                 force_use_fp32: bool = False, **kwargs) -> None:
+                 force_use_fp32: bool = False, _weights_packed: bool = False, **kwargs) -> None:
         if propagation_alg != "LL":
             raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
         if logspace_flows or negate_pflows or accumulate_ch_flows or allow_neg_flows:
@@ -398,13 +433,13 @@ class SumLayer(Layer):
             ready = torch.cuda.Event()
             ready.record()
         # element flows
+        if not _weights_packed:
+            self.pack_flow_weights(params, B, force_use_fp32)
         for eg in d["el_groups"]:
             et = eg["tiles"]
-            prec = SumLayer.bf16_form if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
-            if prec > 0 and eg["short"] and et.size(0) >= SumLayer.tc05_min_tiles:
+            prec = self._el_prec(eg, B, force_use_fp32)
+            if self._el_tc05(eg, prec):
                 st = nat.stream()
-                nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
-                         self.block_size, nat.ptr(eg["pack"]), st)
                 nat.call("pcb_lse_contract_tc05", nat.ptr(node_flows),
                          nat.ptr(None if allow_modify_flows else node_mars), nat.ptr(element_mars),
                          nat.ptr(element_flows), ld, B, nat.ptr(eg["pack"]), nat.ptr(et), et.size(0),

@@ -302,13 +302,41 @@ class TensorCircuit(nn.Module):
         off, rows = self._em_region[group_id]
         return self._em_resident[off:off + rows]
 
+    def _side_stream(self, main: torch.cuda.Stream) -> torch.cuda.Stream:
+        side = self._side_streams.get(main.device)
+        if side is None:
+            side = self._side_streams[main.device] = torch.cuda.Stream(device=main.device)
+        return side
+
+    def _prepack(self, side, pack_fn):
+        """Issue every sum group's weight packing on ``side`` (they only read the parameters);
+        returns {group id: event recorded after that group's packs}."""
+        events = dict()
+        with torch.cuda.stream(side):
+            for gi, group in enumerate(self.inner_layer_groups):
+                if group.is_sum() and any([pack_fn(layer) for layer in group]):
+                    ev = torch.cuda.Event()
+                    ev.record(side)
+                    events[gi] = ev
+        return events
+
     def _run_inner_forward(self, force_use_bf16, force_use_fp32, propagation_alg, **kwargs):
+        main = torch.cuda.current_stream()
+        side = self._side_stream(main)
+        side.wait_stream(main)
+        B = self.node_mars.size(1)
+        packed = self._prepack(side, lambda layer: layer.pack_forward_weights(self.params, B, force_use_bf16,
+                                                                              force_use_fp32))
         for gi, group in enumerate(self.inner_layer_groups):
             if group.is_prod():
                 group(self.node_mars, self._em_view(gi))
             else:
+                if gi in packed:
+                    main.wait_event(packed[gi])
                 group(self.node_mars, self._em_view(gi - 1), self.params, force_use_bf16=force_use_bf16,
-                      force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, **kwargs)
+                      force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, _weights_packed=True,
+                      **kwargs)
+        main.wait_stream(side)
 
     def forward(self, inputs: torch.Tensor, input_layer_fn: Optional[Union[str, Callable]] = None,
                 cache: Optional[dict] = None, return_cache: bool = False, record_cudagraph: bool = False,
@@ -385,11 +413,11 @@ class TensorCircuit(nn.Module):
         # Parameter flows go to a side stream: nothing later in the pass reads them, so they run
         # alongside the element-flow / product chain and join before the pass ends.
         main = torch.cuda.current_stream()
-        side = self._side_streams.get(main.device)
-        if side is None:
-            side = self._side_streams[main.device] = torch.cuda.Stream(device=main.device)
+        side = self._side_stream(main)
         side.wait_stream(main)
-        kwargs = dict(kwargs, _pflow_stream=side)
+        B = self.node_mars.size(1)
+        packed = self._prepack(side, lambda layer: layer.pack_flow_weights(self.params, B, force_use_fp32))
+        kwargs = dict(kwargs, _pflow_stream=side, _weights_packed=True)
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
             group = self.inner_layer_groups[layer_id]
             if group.is_prod():
@@ -401,6 +429,8 @@ class TensorCircuit(nn.Module):
                 # the two flow kernels read one row per node instead of two.
                 modify = allow_modify_flows and any(
                     layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles for layer in group)
+                if layer_id in packed:
+                    main.wait_event(packed[layer_id])
                 group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
