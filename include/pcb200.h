@@ -165,14 +165,17 @@ int pcb_lse_contract(const float* src, const float* src2, const float* aux, floa
  * batch_tile samples (16, 32 or 64), so small layers launch many CTAs.
  * wlayout: 0 = weights copied one by one; 1 = groups of 4 consecutive rows have
  * consecutive, 16-byte aligned weights (forward tables); 2 = groups of 4 consecutive terms
- * do (element-flow tables). The caller guarantees k_cnt <= 128 and the wlayout property;
- * a tile with more terms produces NaN rows.
+ * do (element-flow tables). packed (BF16 forms only, may be NULL): the same tiles' weights
+ * as written by pcb_pack_weights; the kernel then copies them instead of reading params.
+ * The caller guarantees k_cnt <= 128 and the wlayout property; a tile with more terms
+ * produces NaN rows.
  * Replaces the same sum-layer kernels as pcb_lse_contract (small-K case).
  */
 int pcb_lse_contract_short(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
                            const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t tile_rows,
                            int32_t rows_per_block, const int32_t* krow, const int32_t* kw, int32_t w_stride,
-                           int32_t mode, int32_t prec, int32_t wlayout, int32_t batch_tile, void* stream);
+                           int32_t mode, int32_t prec, const uint8_t* packed, int32_t wlayout, int32_t batch_tile,
+                           void* stream);
 
 /*
  * Weights of LSE-contraction tiles (at most 128 rows x 128 terms each, same tile table,

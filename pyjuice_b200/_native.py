@@ -71,8 +71,8 @@ _SIGS = {
     "pcb_lse_contract": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                           c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_short": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
-                                c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
-                                c_int32, c_void_p], c_int32),
+                                c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
+                                c_int32, c_int32, c_void_p], c_int32),
     "pcb_pack_weights": ([c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_lse_contract_tc05": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                                c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),

@@ -17,7 +17,10 @@
 // Weight copies are 16 bytes wide when the host has checked that groups of 4 weights are
 // contiguous and aligned: along the rows (wlayout 1, the forward: node-fastest parameter
 // blocks) or along the terms (wlayout 2, element flows: a child's weights over the
-// parents of one block are consecutive). wlayout 0 copies every weight on its own.
+// parents of one block are consecutive). wlayout 0 copies every weight on its own. In the
+// BF16 forms the weights can instead come already rounded and split (pcb_pack_weights):
+// the CTA then copies its rows of the packed tile as they are and reads the A fragments
+// straight from that core-matrix layout (no per-CTA conversion of the weights).
 //
 // Epilogues: mode 0 writes log(acc) + m (sum forward); modes 1/2 write
 // acc * exp(aux + m) (element flows; mode 2 first turns node flows into log f - log m).
@@ -74,7 +77,8 @@ __global__ void __launch_bounds__(kThreads)
 lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                  float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                  const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
-                 int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec) {
+                 int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
+                 const uint8_t* __restrict__ packed) {
     pcb::pdl_begin();
     using S = Smem<RM, TB, MODE, PREC, WK>;
     constexpr int ES = S::ES, WS = S::WS, WROW = S::WROW;
@@ -135,11 +139,28 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             }
         }
     }
+    // packed bf16 weights (hi, then lo): rows r0 .. r0 + RM - 1 are RM / 8 core-matrix row
+    // groups of 2048 bytes in each half of the tile's 64 KB block
+    constexpr int kPackHalf = RM * 256;
+    const bool pk = PREC > 0 && packed != nullptr;
+    if (pk) {
+        const uint8_t* srcp = packed + (size_t)(blockIdx.x / row_splits) * 65536 + (size_t)(r0 / 8) * 2048;
+        uint8_t* dstp = reinterpret_cast<uint8_t*>(pW);
+        constexpr int CH = kPackHalf / 16;
+        constexpr int IT = (PREC == 2 ? 2 : 1) * CH / kThreads;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int i = tid + it * kThreads;
+            const int h = i / CH, c = i % CH;
+            pcb::cp_async16(dstp + h * kPackHalf + c * 16, srcp + (size_t)h * 32768 + c * 16);
+        }
+    }
     auto wbase = [&](int r) -> int64_t {
         const int rr = r0 + r;
         return (int64_t)t.w_add + (int64_t)(rr >> rpb_log2) * t.g_stride + (int64_t)(rr & rpb_mask) * w_stride;
     };
-    if (WK) {
+    if (pk) {
+    } else if (WK) {
         // sW[r][k]: each thread copies groups of 4 consecutive terms of one row
         constexpr int IT = RM * (KMAX / 4) / kThreads;
 #pragma unroll
@@ -277,7 +298,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             if (SPLIT) split_bf16(e0, e1, pE[kk * ES + cb], pE[(KMAX / 2) * ES + kk * ES + cb]);
             else pE[kk * ES + cb] = pack_bf16(e0, e1);
         }
-        for (int idx = tid; idx < (KMAX / 2) * RM; idx += kThreads) {
+        for (int idx = tid; idx < (pk ? 0 : (KMAX / 2) * RM); idx += kThreads) {
             const int kk = idx / RM;
             const int r = idx % RM;
             float w0 = 0.f, w1 = 0.f;
@@ -319,14 +340,27 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
 #pragma unroll
             for (int a = 0; a < MT; ++a) {
                 const int mr = mw + a * 16 + g;
-                const uint32_t a0 = pW[(kk + q) * WS + mr], a1 = pW[(kk + q) * WS + mr + 8];
-                const uint32_t a2 = pW[(kk + 4 + q) * WS + mr], a3 = pW[(kk + 4 + q) * WS + mr + 8];
+                uint32_t a0, a1, a2, a3, l0 = 0, l1 = 0, l2 = 0, l3 = 0;
+                if (pk) {
+                    // word of (row group G, k group kg, row g of the group, pair q): G*512 + kg*32 + g*4 + q
+                    const int w0 = ((mw + a * 16) >> 3) * 512 + (k0 >> 3) * 32 + g * 4 + q;
+                    a0 = pW[w0]; a1 = pW[w0 + 512]; a2 = pW[w0 + 32]; a3 = pW[w0 + 544];
+                    if (SPLIT) {
+                        const int w1 = w0 + kPackHalf / 4;
+                        l0 = pW[w1]; l1 = pW[w1 + 512]; l2 = pW[w1 + 32]; l3 = pW[w1 + 544];
+                    }
+                } else {
+                    a0 = pW[(kk + q) * WS + mr]; a1 = pW[(kk + q) * WS + mr + 8];
+                    a2 = pW[(kk + 4 + q) * WS + mr]; a3 = pW[(kk + 4 + q) * WS + mr + 8];
+                    if (SPLIT) {
+                        const int o = (KMAX / 2) * WS;
+                        l0 = pW[o + (kk + q) * WS + mr]; l1 = pW[o + (kk + q) * WS + mr + 8];
+                        l2 = pW[o + (kk + 4 + q) * WS + mr]; l3 = pW[o + (kk + 4 + q) * WS + mr + 8];
+                    }
+                }
 #pragma unroll
                 for (int c = 0; c < NTL; ++c) mma_bf16(acc[a][c], a0, a1, a2, a3, bh[c][0], bh[c][1]);
                 if (SPLIT) {
-                    const int o = (KMAX / 2) * WS;
-                    const uint32_t l0 = pW[o + (kk + q) * WS + mr], l1 = pW[o + (kk + q) * WS + mr + 8];
-                    const uint32_t l2 = pW[o + (kk + 4 + q) * WS + mr], l3 = pW[o + (kk + 4 + q) * WS + mr + 8];
 #pragma unroll
                     for (int c = 0; c < NTL; ++c) {
                         mma_bf16(acc[a][c], l0, l1, l2, l3, bh[c][0], bh[c][1]);
@@ -356,7 +390,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                         if (bad) {
                             o[j] = __int_as_float(0x7fc00000);
                         } else if (MODE == 0) {
-                            o[j] = (mm == -INFINITY) ? -INFINITY : logf(v) + mm;
+                            o[j] = (mm == -INFINITY) ? -INFINITY : __logf(v) + mm;
                         } else {
                             const float x = (b + j < B) ? __ldg(aux + ((int64_t)t.aux_row + row) * ld + b + j) : 0.f;
                             o[j] = (mm == -INFINITY) ? 0.f : v * __expf(x + mm);
@@ -384,7 +418,7 @@ int current_device() {
 template <int RM, int TB, int MODE, int PREC, bool WK>
 int launch_one(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
-               int w_stride, int rpb_log2, cudaStream_t s, bool vec, bool wvec) {
+               int w_stride, int rpb_log2, cudaStream_t s, bool vec, bool wvec, const uint8_t* packed) {
     constexpr size_t smem = Smem<RM, TB, MODE, PREC, WK>::bytes();
     static_assert(smem <= 227 * 1024, "shared memory");
     static bool configured[64] = {false};
@@ -401,15 +435,16 @@ int launch_one(int num_tiles, int row_splits, const float* src, const float* src
     return pcb::launch_status(pcb::launch_k(lse_short_kernel<RM, TB, MODE, PREC, WK>,
                                             dim3((unsigned)gx, (unsigned)gy), dim3(kThreads), smem, s, 1u, src,
                                             src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2,
-                                            row_splits, vec, wvec), "pcb_lse_contract_short");
+                                            row_splits, vec, wvec, packed), "pcb_lse_contract_short");
 }
 
 template <int RM, int TB, int PREC>
 int launch_prec(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                 int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
-                int w_stride, int rpb_log2, int mode, bool wk, cudaStream_t s, bool vec, bool wvec) {
+                int w_stride, int rpb_log2, int mode, bool wk, cudaStream_t s, bool vec, bool wvec,
+                const uint8_t* packed) {
 #define PCB_LS(M, W) \
-    launch_one<RM, TB, M, PREC, W>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec, wvec)
+    launch_one<RM, TB, M, PREC, W>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec, wvec, packed)
     if (wk) return mode == 0 ? PCB_LS(0, true) : (mode == 1 ? PCB_LS(1, true) : PCB_LS(2, true));
     return mode == 0 ? PCB_LS(0, false) : (mode == 1 ? PCB_LS(1, false) : PCB_LS(2, false));
 #undef PCB_LS
@@ -418,9 +453,10 @@ int launch_prec(int num_tiles, int row_splits, const float* src, const float* sr
 template <int RM, int TB>
 int launch_shape(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                  int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
-                 int w_stride, int rpb_log2, int mode, int prec, bool wk, cudaStream_t s, bool vec, bool wvec) {
+                 int w_stride, int rpb_log2, int mode, int prec, bool wk, cudaStream_t s, bool vec, bool wvec,
+                 const uint8_t* packed) {
 #define PCB_LP(P) \
-    launch_prec<RM, TB, P>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, wk, s, vec, wvec)
+    launch_prec<RM, TB, P>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, wk, s, vec, wvec, packed)
     if (prec == 0) return PCB_LP(0);
     if (prec == 1) return PCB_LP(1);
     return PCB_LP(2);
@@ -433,13 +469,15 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
                                       int32_t B, const float* params, const PcbLseTile* tiles, int32_t num_tiles,
                                       int32_t tile_rows, int32_t rows_per_block, const int32_t* krow,
                                       const int32_t* kw, int32_t w_stride, int32_t mode, int32_t prec,
-                                      int32_t wlayout, int32_t batch_tile, void* stream) {
+                                      const uint8_t* packed, int32_t wlayout, int32_t batch_tile, void* stream) {
     if (!src || !out || !params || !tiles || !krow || !kw || B <= 0 || ld < B || num_tiles < 0 || mode < 0 ||
         mode > 2 || (mode == 2 && !src2) || (mode >= 1 && !aux) || rows_per_block <= 0 ||
         (rows_per_block & (rows_per_block - 1)) || tile_rows < 1 || tile_rows > 128 || prec < 0 || prec > 2 ||
         wlayout < 0 || wlayout > 2 || (batch_tile != 16 && batch_tile != 32 && batch_tile != 64))
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: bad arguments");
     if (num_tiles == 0) return PCB_OK;
+    if (packed && (prec == 0 || (reinterpret_cast<uintptr_t>(packed) & 15) != 0))
+        return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: packed weights need a BF16 form and 16-byte alignment");
     if (wlayout != 0 && (reinterpret_cast<uintptr_t>(params) & 15) != 0)
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: 16-byte weight copies need an aligned params base");
     int rpb_log2 = 0;
@@ -452,7 +490,7 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
     const int rm = tile_rows <= 32 ? 32 : 64;
     const int row_splits = (tile_rows + rm - 1) / rm;
 #define PCB_SH(RM, TB) \
-    launch_shape<RM, TB>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, prec, wk, s, vec, wvec)
+    launch_shape<RM, TB>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, prec, wk, s, vec, wvec, packed)
     if (rm == 32) {
         if (batch_tile == 16) return PCB_SH(32, 16);
         if (batch_tile == 32) return PCB_SH(32, 32);

@@ -353,19 +353,20 @@ class SumLayer(Layer):
         """Pack the weights the forward's tcgen05 kernel reads (on the current stream); returns
         whether this layer uses them. ``forward(..., _weights_packed=True)`` then skips the pack."""
         d = self._desc(params.device)
-        prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
-        if tc05:
+        prec, _ = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
+        use = prec > 0 and d["fw_short"]
+        if use:
             t = d["fw_tiles"]
             nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
                      nat.ptr(d["fw_pack"]), nat.stream())
-        return tc05
+        return use
 
     def pack_flow_weights(self, params: torch.Tensor, B: int, force_use_fp32: bool = False) -> bool:
         """Pack the weights of the element-flow tcgen05 kernels (see pack_forward_weights)."""
         d = self._desc(params.device)
         any_tc05 = False
         for eg in d["el_groups"]:
-            if self._el_tc05(eg, self._el_prec(eg, B, force_use_fp32)):
+            if self._el_prec(eg, B, force_use_fp32) > 0 and eg["short"]:
                 et = eg["tiles"]
                 nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
                          self.block_size, nat.ptr(eg["pack"]), nat.stream())
@@ -390,15 +391,17 @@ class SumLayer(Layer):
         if tc05:
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
+                _weights_packed = True
             nat.call("pcb_lse_contract_tc05", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
                      nat.ptr(node_mars), ld, B, nat.ptr(d["fw_pack"]), nat.ptr(t), t.size(0), nat.ptr(d["krow"]), 0,
                      prec, _tc05_batch_tile(t.size(0), B), st)
             return
         if d["fw_short"] and SumLayer.short_kernels:
+            packed = d["fw_pack"] if (_weights_packed and prec > 0) else None
             nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
                      ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
-                     nat.ptr(d["kw"]), 1, 0, prec, d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B),
-                     nat.stream())
+                     nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(packed), d["fw_wlayout"],
+                     _short_batch_tile(t.size(0), d["fw_tm"], B), nat.stream())
             return
         nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
                  nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
@@ -433,8 +436,10 @@ class SumLayer(Layer):
             ready = torch.cuda.Event()
             ready.record()
         # element flows
-        if not _weights_packed:
+        if not _weights_packed and any(self._el_tc05(eg, self._el_prec(eg, B, force_use_fp32))
+                                       for eg in d["el_groups"]):
             self.pack_flow_weights(params, B, force_use_fp32)
+            _weights_packed = True
         for eg in d["el_groups"]:
             et = eg["tiles"]
             prec = self._el_prec(eg, B, force_use_fp32)
@@ -447,10 +452,11 @@ class SumLayer(Layer):
                          _tc05_batch_tile(et.size(0), B), st)
                 continue
             if eg["short"] and SumLayer.short_kernels:
+                packed = eg["pack"] if (_weights_packed and prec > 0) else None
                 nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
                          nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et),
                          et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
-                         1 if allow_modify_flows else 2, prec, eg["wlayout"],
+                         1 if allow_modify_flows else 2, prec, nat.ptr(packed), eg["wlayout"],
                          _short_batch_tile(et.size(0), eg["tm"], B), nat.stream())
                 continue
             nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),

@@ -108,7 +108,7 @@ def test_prod_layer_forward_backward(B, cuda_device):
                 assert torch.allclose(nf[u[g] + i], ref, atol=1e-6)
 
 
-@pytest.mark.parametrize("path", ["short", "tc05"])
+@pytest.mark.parametrize("path", ["short", "short_packed", "tc05"])
 @pytest.mark.parametrize("bs,B,form", [(8, 7, 2), (16, 130, 2), (32, 256, 2), (32, 512, 1), (64, 33, 2)])
 def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
     """The single-stage contractions (<= 128 terms: mma.sync or tcgen05) agree with the chunked ones."""
@@ -129,15 +129,19 @@ def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
         for short in (False, True):
             SumLayer.short_kernels = short
             SumLayer.tc05_min_tiles = 1 if (short and path == "tc05") else 1 << 30
+            packed = short and path == "short_packed"
+            if packed:  # weights packed ahead of the contractions, as the circuit passes do
+                layer.pack_forward_weights(params, B, force_use_bf16=True)
+                layer.pack_flow_weights(params, B)
             nm = torch.zeros([n_nd, B], device=cuda_device)
-            layer(nm, em, params, force_use_bf16=True)
+            layer(nm, em, params, force_use_bf16=True, _weights_packed=packed)
             ef = torch.zeros([n_el, B], device=cuda_device)
             pf = torch.zeros_like(params)
             nf = nf0.clone()
-            layer.backward(nf, ef, nm, em, params, pf)
+            layer.backward(nf, ef, nm, em, params, pf, _weights_packed=packed)
             ef2 = torch.zeros([n_el, B], device=cuda_device)
             nf2 = nf0.clone()
-            layer.backward(nf2, ef2, nm, em, params, None, allow_modify_flows=True)
+            layer.backward(nf2, ef2, nm, em, params, None, allow_modify_flows=True, _weights_packed=packed)
             outs[short] = (nm[bs:], ef[bs:], ef2[bs:], pf)
     finally:
         SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles = saved
