@@ -188,6 +188,9 @@ class SumLayer(Layer):
     bf16_form = 2
     short_kernels = True  # single-stage kernels for tiles of <= 128 terms
     tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
+    # The single-stage kernels of small layers can read pre-packed weights too; off by default:
+    # packing every layer in each pass costs more side-stream time than it saves.
+    pack_short_weights = False
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -353,8 +356,8 @@ class SumLayer(Layer):
         """Pack the weights the forward's tcgen05 kernel reads (on the current stream); returns
         whether this layer uses them. ``forward(..., _weights_packed=True)`` then skips the pack."""
         d = self._desc(params.device)
-        prec, _ = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
-        use = prec > 0 and d["fw_short"]
+        prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
+        use = tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"])
         if use:
             t = d["fw_tiles"]
             nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
@@ -366,7 +369,8 @@ class SumLayer(Layer):
         d = self._desc(params.device)
         any_tc05 = False
         for eg in d["el_groups"]:
-            if self._el_prec(eg, B, force_use_fp32) > 0 and eg["short"]:
+            prec = self._el_prec(eg, B, force_use_fp32)
+            if self._el_tc05(eg, prec) or (SumLayer.pack_short_weights and prec > 0 and eg["short"]):
                 et = eg["tiles"]
                 nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
                          self.block_size, nat.ptr(eg["pack"]), nat.stream())
@@ -397,7 +401,7 @@ class SumLayer(Layer):
                      prec, _tc05_batch_tile(t.size(0), B), st)
             return
         if d["fw_short"] and SumLayer.short_kernels:
-            packed = d["fw_pack"] if (_weights_packed and prec > 0) else None
+            packed = d["fw_pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
             nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
                      ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
                      nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(packed), d["fw_wlayout"],
@@ -452,7 +456,7 @@ class SumLayer(Layer):
                          _tc05_batch_tile(et.size(0), B), st)
                 continue
             if eg["short"] and SumLayer.short_kernels:
-                packed = eg["pack"] if (_weights_packed and prec > 0) else None
+                packed = eg["pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
                 nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
                          nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et),
                          et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,

@@ -123,9 +123,10 @@ def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
     params = torch.rand([bs ** 2 + 3 * 4 * bs * bs], device=cuda_device)
     nf0 = torch.rand([n_nd, B], device=cuda_device)
     outs = {}
-    saved = (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles)
+    saved = (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights)
     try:
         SumLayer.bf16_form = form
+        SumLayer.pack_short_weights = path == "short_packed"
         for short in (False, True):
             SumLayer.short_kernels = short
             SumLayer.tc05_min_tiles = 1 if (short and path == "tc05") else 1 << 30
@@ -144,7 +145,7 @@ def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
             layer.backward(nf2, ef2, nm, em, params, None, allow_modify_flows=True, _weights_packed=packed)
             outs[short] = (nm[bs:], ef[bs:], ef2[bs:], pf)
     finally:
-        SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles = saved
+        SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights = saved
     tol = 2e-5 if form == 2 else 2e-2
     for a, b in zip(outs[False], outs[True]):
         assert torch.isfinite(b).all()
