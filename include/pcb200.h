@@ -56,7 +56,7 @@ typedef struct {
     int32_t nid;       /* first node row of the tile */
     int32_t n_rows;    /* nodes in the tile (<= 128) */
     int32_t k_off;     /* offset into cids[] / pids[] / pfids[] of the tile's first child */
-    int32_t k_cnt;     /* children in the tile (<= 64) */
+    int32_t k_cnt;     /* children in the tile (<= the launch's tile_children) */
     int32_t p_add;     /* added to pids / pfids for tile row 0 */
     int32_t gs_p;      /* parameter offset between consecutive blocks of the tile */
     int32_t gs_pf;     /* flow offset between consecutive blocks of the tile */
@@ -212,7 +212,7 @@ int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int3
  * log(node_flows) - node_mars (modified=0), M_b the max over the tile's nodes.
  * The batch is split over a cluster of up to 8 CTAs (64 samples per CTA and staged
  * chunk) whose partial sums are added in a fixed order through distributed shared memory
- * (deterministic, no scratch memory). Tiles hold at most tile_children (32 or 64)
+ * (deterministic, no scratch memory). Tiles hold at most tile_children (32, 64 or 128)
  * children. prec: 0 = FP32 FMA, 1 = bf16 tensor cores, 2 = split bf16 (hi + lo, three
  * MMAs). atomic=1 when flow slots are shared by tied nodes.
  * Replaces SumLayer._bk_triton_block_sparse_par_kernel / _csmm2 / sparse par kernel

@@ -1,7 +1,7 @@
 // Sum-layer parameter flows: a contraction over the batch.
 //
 // A tile covers up to 128 nodes (rows nid + r: consecutive node blocks that share their
-// children) and up to TKC children (element rows cids[k], TKC = 32 or 64):
+// children) and up to TKC children (element rows cids[k], TKC = 32, 64 or 128):
 //   pf(r, k) += params(r, k) * sum_b A[r, b] * C[k, b]
 //   A[r, b] = exp(lf[nid + r, b] - M_b),  C[k, b] = exp(em[cids[k], b] + M_b)
 // with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b]: every
@@ -355,7 +355,7 @@ extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, c
                               int32_t prec, void* stream) {
     if (!node_flows || !node_mars || !element_mars || !params || !param_flows || !tiles || !cids || !pids || !pfids ||
         B <= 0 || ld < B || num_tiles < 0 || rows_per_block <= 0 || (rows_per_block & (rows_per_block - 1)) ||
-        (tile_children != 32 && tile_children != 64) || prec < 0 || prec > 2)
+        (tile_children != 32 && tile_children != 64 && tile_children != 128) || prec < 0 || prec > 2)
         return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows: bad arguments");
     if (num_tiles == 0) return PCB_OK;
     int rpb_log2 = 0;
@@ -370,6 +370,7 @@ extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, c
 #define PCB_PK(T, P) \
     launch_flags<T, P>(cs, mod, at, node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec)
     if (tile_children == 32) return prec == 0 ? PCB_PK(32, 0) : (prec == 1 ? PCB_PK(32, 1) : PCB_PK(32, 2));
-    return prec == 0 ? PCB_PK(64, 0) : (prec == 1 ? PCB_PK(64, 1) : PCB_PK(64, 2));
+    if (tile_children == 64) return prec == 0 ? PCB_PK(64, 0) : (prec == 1 ? PCB_PK(64, 1) : PCB_PK(64, 2));
+    return prec == 0 ? PCB_PK(128, 0) : (prec == 1 ? PCB_PK(128, 1) : PCB_PK(128, 2));
 #undef PCB_PK
 }

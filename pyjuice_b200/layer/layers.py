@@ -191,6 +191,9 @@ class SumLayer(Layer):
     # The single-stage kernels of small layers can read pre-packed weights too; off by default:
     # packing every layer in each pass costs more side-stream time than it saves.
     pack_short_weights = False
+    # Children per parameter-flow tile (32, 64 or 128): with all children of a region in one
+    # tile, its node rows are exponentiated once per sample slice instead of once per chunk.
+    pflow_tile_children = 64
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -265,13 +268,13 @@ class SumLayer(Layer):
         blk_koff = np.asarray(blk_koff, np.int64)
         blk_kcnt = np.asarray(blk_kcnt, np.int64)
 
-        fw_tiles, pf_tiles, pf_tiles32 = [], [], []
+        fw_tiles, pf_tiles, pf_tiles32, pf_tiles128 = [], [], [], []
         for g, cnt, gs_w, gs_f in chains:
             rows = cnt * bs
             for i0 in range(0, rows, _MAX_ROWS):
                 nr = min(_MAX_ROWS, rows - i0)
                 fw_tiles.append((blk_nid[g] + i0, nr, blk_koff[g], blk_kcnt[g], i0, 0, gs_w, 0))
-                for kc, lst in ((64, pf_tiles), (32, pf_tiles32)):
+                for kc, lst in ((64, pf_tiles), (32, pf_tiles32), (128, pf_tiles128)):
                     for k0 in range(0, int(blk_kcnt[g]), kc):
                         lst.append((blk_nid[g] + i0, nr, blk_koff[g] + k0, min(kc, int(blk_kcnt[g]) - k0), i0,
                                     gs_w, gs_f, 0))
@@ -324,6 +327,7 @@ class SumLayer(Layer):
             min_kcnt=int(blk_kcnt.min()) if blk_kcnt.size else 0,
             pf_tiles=_i32(np.asarray(pf_tiles, np.int64).reshape(-1, 8)),
             pf_tiles32=_i32(np.asarray(pf_tiles32, np.int64).reshape(-1, 8)),
+            pf_tiles128=_i32(np.asarray(pf_tiles128, np.int64).reshape(-1, 8)),
             el_groups=el_groups,
         )
 
@@ -469,11 +473,8 @@ class SumLayer(Layer):
                      1 if allow_modify_flows else 2, prec, nat.stream())
         # parameter flows
         if param_flows is not None:
-            # 64-child tiles unless that leaves the GPU short of CTAs (cluster of up to 8 per tile)
-            cs = min(8, 1 << max(0, (B - 1).bit_length() - 6))
-            pt, kc = d["pf_tiles"], 64
-            if pt.size(0) * cs < 2 * _num_sms():
-                pt, kc = d["pf_tiles32"], 32
+            kc = SumLayer.pflow_tile_children
+            pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
             prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
             if ready is not None:
                 pflow_stream.wait_event(ready)
