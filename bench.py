@@ -8,10 +8,11 @@ forward -> backward -> ``mini_batch_em(step_size=0.1, pseudocount=0.1)``.
 * ``value``: samples/s of the BF16 tensor-core form, whole step captured in one CUDA
   graph, inputs resident in HBM, device time (CUDA events), max over ranks;
 * ``fp32_plain``: the same for the plain FP32 form;
-* ``e2e``: the BF16 form through the public API (``lls = pc(x)``,
+* ``e2e``: the BF16 form through the public API (``lls = pc(x, record_cudagraph=True)``,
   ``lls.mean().backward()``, ``pc.mini_batch_em``) with the batch copied from pinned
   host memory and the log-likelihoods read back every step;
-* ``roofline``: the sum-layer forward contraction, timed per launch with CUDA events;
+* ``roofline``: the parameter-flow launch of the largest sum layer (the kernel with the
+  largest share of the step), timed per launch with CUDA events;
 * ``cpu_baseline``: the FP64 CPU restatement (oracle port) on a bounded sample.
 
 ``--impl reference`` times the CPU implementation of the same step instead (the
@@ -47,6 +48,9 @@ BLOCK = 32
 BATCH = 512
 STEP_SIZE = 0.1
 PSEUDOCOUNT = 0.1
+# DRAM bytes (read + written) of the roofline launch, the largest layer's parameter flows,
+# from one ncu capture of `bench.py --profile-step` (-k regex:sum_pflows -s 63 -c 1).
+PFLOW_TRAFFIC_BYTES = 81_506_816
 METRIC = "EM samples/s (fwd+bwd+update) 1xB200, BF16-TC vs FP32 plain; dLL vs FP64 oracle"
 WORKLOAD = "HCLT 28x28 vars x 256 cats, 128 latents, block 32, EM step (fwd+bwd+mini_batch_em)"
 
@@ -54,7 +58,7 @@ WORKLOAD = "HCLT 28x28 vars x 256 cats, 128 latents, block 32, EM step (fwd+bwd+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=BATCH)
@@ -102,7 +106,7 @@ class Clocks:
         self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.FIELDS}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                       "--format=csv,noheader,nounits", "-lms", "20"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.p = None
@@ -196,6 +200,48 @@ def sum_forward_roofline(pc, x, precision_kw, reps=10):
     big = max(per_layer, key=lambda r: r[0])
     return {"layers": len(per_layer), "bytes": tot_b, "flops": tot_f, "seconds": tot_s,
             "largest": {"bytes": big[0], "flops": big[1], "seconds": big[2], "tiles": big[3]}}
+
+
+def pflows_roofline(pc, reps=10):
+    """Device time of the parameter-flow launch of the largest sum layer (after a full
+    forward + backward, so its node flows hold log f - log m), captured ``reps`` times in one
+    CUDA graph and timed with CUDA events on the launching stream.
+
+    Algorithmic bytes: the layer's node-flow rows and its children's element rows once
+    (4 B x batch each), every edge's parameter once (4 B) and its flow slot read and
+    written (8 B).
+    """
+    groups = pc.inner_layer_groups
+    gi, layer = max(((gi, l) for gi, g in enumerate(groups) if g.is_sum() for l in g.layers),
+                    key=lambda t: t[1].num_edges)
+    d = layer._desc(pc.node_mars.device)
+    B = pc.node_mars.size(1)
+    em = pc._em_view(gi - 1)
+    child_rows = int(torch.unique(d["krow"]).numel())
+    nbytes = 4 * B * (layer.num_nodes + child_rows) + 12 * layer.num_edges
+
+    def run():
+        layer.param_flows_only(pc.node_flows, pc.node_mars, em, pc.params, pc.param_flows, allow_modify_flows=True)
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        run()
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(reps):
+            run()
+    graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    graph.replay()
+    e1.record()
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3 / reps
+    return {"bytes": nbytes, "seconds": secs, "flops": 2 * layer.num_edges * B, "group": gi,
+            "tiles": d["pf_tiles"].size(0)}
 
 
 def cpu_step_rate(layout, params, in_params, data, budget_s):
@@ -364,7 +410,8 @@ def main():
     def e2e_step(i):
         x = host[(i % 8) * B:(i % 8 + 1) * B].to(device, non_blocking=True)
         pc.init_param_flows(flows_memory=0.0)
-        lls = pc(x, force_use_bf16=True)
+        # the public API's own CUDA-graph option: the inner passes are recorded once, then replayed
+        lls = pc(x, force_use_bf16=True, record_cudagraph=True)
         lls.mean().backward()
         allreduce_flows()
         pc.mini_batch_em(step_size=STEP_SIZE, pseudocount=PSEUDOCOUNT)
@@ -412,15 +459,23 @@ def main():
         rf = sum_forward_roofline(pc, data_dev[:B], {"force_use_bf16": True})
         big = rf["largest"]
         achieved = big["bytes"] / big["seconds"] / 1e9
-        roof = {"kernel": "sum-layer forward of the largest layer (pcb_pack_weights + pcb_lse_contract_tc05, "
-                          "split-bf16 tcgen05)",
+        pf = pflows_roofline(pc)
+        achieved = pf["bytes"] / pf["seconds"] / 1e9
+        roof = {"kernel": "pcb_sum_pflows (sum_pflows_kernel, split-bf16 form, 64-child tiles) of the largest "
+                          "sum layer: the kernel with the largest share of the step",
                 "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "peak_source": f"{src} hbm_gbs (of measured)" if src == "measured" else src,
-                "alg_bytes_per_launch": big["bytes"], "us_per_launch": big["seconds"] * 1e6,
-                "tiles": big["tiles"], "tensor_tflops_achieved": big["flops"] / big["seconds"] / 1e12,
-                "all_sum_layers": {"layers": rf["layers"], "us_total": rf["seconds"] * 1e6,
-                                   "achieved_gbs": rf["bytes"] / rf["seconds"] / 1e9,
-                                   "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm}}
+                "traffic": PFLOW_TRAFFIC_BYTES,
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of this launch, one ncu capture "
+                                  "of bench.py --profile-step (-k regex:sum_pflows -s 63 -c 1)",
+                "peak_source": f"{src} hbm_gbs (of measured)" if src == "measured" else f"{src} hbm_gbs",
+                "alg_bytes_per_launch": pf["bytes"], "us_per_launch": pf["seconds"] * 1e6,
+                "tensor_tflops_achieved": pf["flops"] / pf["seconds"] / 1e12,
+                "sum_forward_largest_layer": {"us": big["seconds"] * 1e6, "alg_bytes": big["bytes"],
+                                              "achieved_gbs": big["bytes"] / big["seconds"] / 1e9,
+                                              "kernels": "pcb_pack_weights + pcb_lse_contract_tc05"},
+                "all_sum_layers_forward": {"layers": rf["layers"], "us_total": rf["seconds"] * 1e6,
+                                           "achieved_gbs": rf["bytes"] / rf["seconds"] / 1e9,
+                                           "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm}}
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
         v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0)

@@ -473,16 +473,26 @@ class SumLayer(Layer):
                      1 if allow_modify_flows else 2, prec, nat.stream())
         # parameter flows
         if param_flows is not None:
-            kc = SumLayer.pflow_tile_children
-            pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
-            prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
             if ready is not None:
                 pflow_stream.wait_event(ready)
             with torch.cuda.stream(pflow_stream if ready is not None else torch.cuda.current_stream()):
-                nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
-                         nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size,
-                         nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 1 if allow_modify_flows else 0,
-                         1 if self._has_tied else 0, kc, prec, nat.stream())
+                self.param_flows_only(node_flows, node_mars, element_mars, params, param_flows,
+                                      allow_modify_flows=allow_modify_flows, force_use_fp32=force_use_fp32)
+
+    def param_flows_only(self, node_flows: torch.Tensor, node_mars: torch.Tensor, element_mars: torch.Tensor,
+                         params: torch.Tensor, param_flows: torch.Tensor, allow_modify_flows: bool = False,
+                         force_use_fp32: bool = False) -> None:
+        """Accumulate this layer's parameter flows on the current stream (``allow_modify_flows``:
+        node_flows already hold log f - log m for this layer's nodes)."""
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        kc = SumLayer.pflow_tile_children
+        pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
+        prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
+        nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
+                 node_mars.stride(0), B, nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0),
+                 self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]),
+                 1 if allow_modify_flows else 0, 1 if self._has_tied else 0, kc, prec, nat.stream())
 
     def __repr__(self):
         return f"SumLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
