@@ -45,6 +45,9 @@ def _pc_model_backward_hook(grad, pc, inputs, record_cudagraph, apply_cudagraph,
 
 
 class TensorCircuit(nn.Module):
+    # Side streams that the backward pass spreads the parameter-flow launches over.
+    pflow_streams = 4
+
     def __init__(self, root_ns: CircuitNodes, layer_sparsity_tol: float = 0.5,
                  max_num_partitions: Optional[int] = None, disable_gpu_compilation: bool = False,
                  force_gpu_compilation: bool = False, max_tied_ns_per_parflow_block: int = 8,
@@ -302,11 +305,12 @@ class TensorCircuit(nn.Module):
         off, rows = self._em_region[group_id]
         return self._em_resident[off:off + rows]
 
-    def _side_stream(self, main: torch.cuda.Stream) -> torch.cuda.Stream:
-        side = self._side_streams.get(main.device)
-        if side is None:
-            side = self._side_streams[main.device] = torch.cuda.Stream(device=main.device)
-        return side
+    def _side_stream(self, main: torch.cuda.Stream, i: int = 0) -> torch.cuda.Stream:
+        """Side stream ``i`` of the device of ``main`` (created on first use)."""
+        pool = self._side_streams.setdefault(main.device, [])
+        while len(pool) <= i:
+            pool.append(torch.cuda.Stream(device=main.device))
+        return pool[i]
 
     def _prepack(self, side, pack_fn):
         """Issue every sum group's weight packing on ``side`` (they only read the parameters);
@@ -410,14 +414,18 @@ class TensorCircuit(nn.Module):
         return g
 
     def _run_inner_backward(self, compute_param_flows, allow_modify_flows, logspace_flows, force_use_fp32, **kwargs):
-        # Parameter flows go to a side stream: nothing later in the pass reads them, so they run
-        # alongside the element-flow / product chain and join before the pass ends.
+        # Parameter flows go to side streams: nothing later in the pass reads them, so they run
+        # alongside the element-flow / product chain and join before the pass ends. The
+        # parameter-flow launches of the small levels are latency-bound, so consecutive levels
+        # take turns over several streams and overlap one another.
         main = torch.cuda.current_stream()
-        side = self._side_stream(main)
-        side.wait_stream(main)
+        sides = [self._side_stream(main, i) for i in range(max(1, TensorCircuit.pflow_streams))]
+        for side in sides:
+            side.wait_stream(main)
         B = self.node_mars.size(1)
-        packed = self._prepack(side, lambda layer: layer.pack_flow_weights(self.params, B, force_use_fp32))
-        kwargs = dict(kwargs, _pflow_stream=side, _weights_packed=True)
+        packed = self._prepack(sides[0], lambda layer: layer.pack_flow_weights(self.params, B, force_use_fp32))
+        kwargs = dict(kwargs, _weights_packed=True)
+        turn = 0
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
             group = self.inner_layer_groups[layer_id]
             if group.is_prod():
@@ -435,8 +443,10 @@ class TensorCircuit(nn.Module):
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
-                               force_use_fp32=force_use_fp32, **kwargs)
-        main.wait_stream(side)
+                               force_use_fp32=force_use_fp32, _pflow_stream=sides[turn % len(sides)], **kwargs)
+                turn += 1
+        for side in sides:
+            main.wait_stream(side)
 
     def backward(self, inputs: Optional[torch.Tensor] = None, ll_weights: Optional[torch.Tensor] = None,
                  compute_param_flows: bool = True, flows_memory: float = 1.0,
