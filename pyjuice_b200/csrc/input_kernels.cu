@@ -23,7 +23,7 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
         float r = 0.f;
         if (b + q < B) {
             const int64_t x = __ldg(data + v * data_ld + b + q);
-            r = (x >= 0 && x < K) ? logf(__ldg(params + sp + x)) : NAN;
+            r = (x >= 0 && x < K) ? __logf(__ldg(params + sp + x)) : NAN;
         }
         pcb::set(o, q, r);
     }
@@ -31,8 +31,10 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 }
 
 // One CTA per variable group: stable counting sort of the batch by category (chunks of
-// up to CB samples), then one warp per node sums its flows per category in sample order
-// and adds the sums to the node's flow slots. Deterministic: no float atomics.
+// up to CB samples; warp-parallel prefix sum of the category counts), then one warp per
+// node copies the node's flow row into shared memory with coalesced loads and sums it per
+// category in sample order, adding the sums to the node's flow slots. Deterministic: no
+// float atomics.
 __global__ void __launch_bounds__(256)
 input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ nf, int64_t ld,
                      int B, const int* __restrict__ grp_var, const int* __restrict__ grp_node0,
@@ -47,7 +49,8 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
     const int cnt = grp_count[g];
     int* keys = smem;              // [CB]
     int* perm = keys + CB;         // [CB]
-    int* seg = perm + CB;          // [K + 2]
+    float* rows = reinterpret_cast<float*>(perm + CB);  // [warps][CB]
+    int* seg = perm + CB + (blockDim.x >> 5) * CB;      // [K + 2]
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -63,8 +66,20 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
             atomicAdd(&seg[key + 1], 1);
         }
         __syncthreads();
-        if (tid == 0) {
-            for (int k = 1; k < K + 2; ++k) seg[k] += seg[k - 1];
+        if (warp == 0) {
+            int carry = 0;
+            for (int base = 0; base < K + 2; base += 32) {
+                const int i = base + lane;
+                int v = (i < K + 2) ? seg[i] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += t;
+                }
+                v += carry;
+                if (i < K + 2) seg[i] = v;
+                carry = __shfl_sync(0xffffffffu, v, 31);
+            }
         }
         __syncthreads();
         // Stable scatter by warp 0: 32 samples at a time, ranks from lane matching.
@@ -88,21 +103,25 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
         }
         __syncthreads();
         // seg[k] now holds the end of category k; its start is the end of category k-1.
+        float* wrow = rows + warp * CB;
         for (int n = warp; n < cnt; n += (blockDim.x >> 5)) {
             const int64_t row = (int64_t)node_offset + node0 + n;
             const float* frow = nf + row * ld + c0;
             const int64_t sf = s_pfids[node0 + n];
+            for (int i = lane; i < nb; i += 32) wrow[i] = __ldg(frow + i);
+            __syncwarp();
             for (int k = lane; k < K; k += 32) {
                 const int s = (k == 0) ? 0 : seg[k - 1];
                 const int e = seg[k];
                 if (e == s) continue;
                 float acc = 0.f;
                 for (int p = s; p < e; ++p) {
-                    const float f = __ldg(frow + perm[p]);
+                    const float f = wrow[perm[p]];
                     acc += logspace ? __expf(f) : f;
                 }
                 pf[sf + k] += acc;
             }
+            __syncwarp();  // the next node overwrites this warp's row
         }
         __syncthreads();
     }
@@ -133,8 +152,8 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
         B <= 0 || ld < B || data_ld < B || num_groups < 0 || max_ncats <= 0)
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: bad arguments");
     if (num_groups == 0) return PCB_OK;
-    const int CB = B < 8192 ? B : 8192;
-    const size_t smem = (size_t)(2 * CB + max_ncats + 2) * sizeof(int);
+    const int CB = B < 1024 ? B : 1024;
+    const size_t smem = (size_t)(2 * CB + 8 * CB + max_ncats + 2) * sizeof(int);
     if (smem > 200 * 1024) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: too many categories (%d)", max_ncats);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(input_cat_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
