@@ -401,11 +401,15 @@ class TensorCircuit(nn.Module):
             return out, cache
         return out
 
-    def _capture(self, fn):
+    def _capture(self, fn, reset=None):
+        """CUDA graph of ``fn`` after two warm-up runs; ``reset`` (if given) restores the state
+        that ``fn`` reads before each warm-up run."""
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             for _ in range(2):
+                if reset is not None:
+                    reset()
                 fn()
         torch.cuda.current_stream().wait_stream(s)
         g = torch.cuda.CUDAGraph()
@@ -505,11 +509,20 @@ class TensorCircuit(nn.Module):
             run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,
                           force_use_fp32, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
-                saved = nf.clone()
-                self._recorded_cuda_graphs[sig] = self._capture(run)
-                nf.copy_(saved)
-                if compute_param_flows:
-                    self.init_param_flows(flows_memory=0.0)
+                # The pass rewrites node flows in place and accumulates parameter flows, so each
+                # warm-up run starts from the state of this call and the state is put back after
+                # the capture (a second run on rewritten flows can overflow).
+                saved_nf = nf.clone()
+                saved_pf = self.param_flows.clone() if compute_param_flows else None
+
+                def reset():
+                    nf.copy_(saved_nf)
+                    if saved_pf is not None:
+                        self.param_flows.copy_(saved_pf)
+
+                self._recorded_cuda_graphs[sig] = self._capture(run, reset)
+                reset()
+                del saved_nf, saved_pf
             if apply_cudagraph and sig in self._recorded_cuda_graphs:
                 self._recorded_cuda_graphs[sig].replay()
             else:

@@ -147,6 +147,34 @@ def test_cuda_graph_replay_matches_eager(cuda_device):
     assert torch.equal(eager, replay)
 
 
+def test_recorded_backward_matches_eager(cuda_device):
+    """A backward pass recorded as a CUDA graph (through the autograd hook) leaves the same node
+    and parameter flows as the eager pass, including flows kept from an earlier batch
+    (flows_memory=1) and after EM steps have moved the parameters away from their start."""
+    fx = load_fixture("hclt784")
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    out = []
+    for rec in (False, True):
+        pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+        load_fixture_params(pc, fx)
+        for _ in range(3):
+            _step(pc, x, force_use_fp32=True)
+            pc.mini_batch_em(step_size=0.5, pseudocount=0.01)
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            pc(x, force_use_fp32=True)
+        pc.backward(inputs=x, allow_modify_flows=True, force_use_fp32=True)
+        pc._optim_hyperparams["flows_memory"] = 1.0
+        lls = pc(x, force_use_bf16=True, record_cudagraph=rec)
+        lls.mean().backward()
+        torch.cuda.synchronize()
+        out.append((pc.node_flows.clone(), pc.param_flows.clone()))
+    (nf_e, pf_e), (nf_r, pf_r) = out
+    assert torch.isfinite(pf_r).all()
+    assert torch.equal(nf_e, nf_r)
+    assert torch.equal(pf_e, pf_r)
+
+
 def test_deterministic_flows(cuda_device):
     """Parameter flows carry no float atomics on untied circuits: two runs are bit-identical."""
     fx = load_fixture("hclt64")
