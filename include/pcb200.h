@@ -210,8 +210,8 @@ int pcb_modify_flows(float* node_flows, const float* node_mars, int64_t ld, int3
  *   pf(r, k) += params(r, k) * sum_b exp(lf[nid + r, b] - M_b) * exp(em[cids[k], b] + M_b)
  * with lf = node_flows already in "log f - log m" form (modified=1) or computed as
  * log(node_flows) - node_mars (modified=0), M_b the max over the tile's nodes.
- * The batch is split over a cluster of up to 8 CTAs (64 samples per CTA and staged
- * chunk) whose partial sums are added in a fixed order through distributed shared memory
+ * The batch is split over a cluster of up to 8 CTAs (64-sample staged chunks; fewer CTAs
+ * per cluster when the tiles alone fill the GPU) whose partial sums are added in a fixed order through distributed shared memory
  * (deterministic, no scratch memory). Tiles hold at most tile_children (32, 64 or 128)
  * children. prec: 0 = FP32 FMA, 1 = bf16 tensor cores, 2 = split bf16 (hi + lo, three
  * MMAs). atomic=1 when flow slots are shared by tied nodes.

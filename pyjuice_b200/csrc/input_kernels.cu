@@ -5,29 +5,55 @@ namespace {
 
 // node_mars[node_offset + n, b] = log(params[s_pids[n] + x]) with x = data[vids[n], b].
 // A category outside [0, ncats) yields NaN (no out-of-range read).
+// A CTA covers kFwdNodes consecutive nodes over 1024 samples (4 per thread): the logs of
+// the nodes' parameter slabs (up to kFwdSlab categories) are taken once into shared
+// memory, each thread loads its 4 category values once and reuses them for every node of
+// the same variable, and each node row is written with 16-byte stores.
+constexpr int kFwdNodes = 8;
+constexpr int kFwdSlab = 256;
+
 __global__ void __launch_bounds__(256)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
-                     int node_offset, float* __restrict__ nm, int64_t ld, int B, int ngrp, int64_t total, bool vec) {
+                     int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec) {
     pcb::pdl_begin();
-    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (idx >= total) return;
-    const int b = (int)(idx % ngrp) * 4;
-    const int n = (int)(idx / ngrp);
-    const int64_t v = __ldg(vids + n);
-    const int64_t sp = __ldg(s_pids + n);
-    const int K = __ldg(ncats + n);
-    float4 o;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float r = 0.f;
-        if (b + q < B) {
-            const int64_t x = __ldg(data + v * data_ld + b + q);
-            r = (x >= 0 && x < K) ? __logf(__ldg(params + sp + x)) : NAN;
-        }
-        pcb::set(o, q, r);
+    __shared__ float slab[kFwdNodes][kFwdSlab];
+    __shared__ int sV[kFwdNodes], sK[kFwdNodes], sP[kFwdNodes];
+    const int n0 = blockIdx.x * kFwdNodes;
+    const int tid = threadIdx.x;
+    if (tid < kFwdNodes) {
+        const int n = n0 + tid;
+        sV[tid] = n < num_nodes ? __ldg(vids + n) : -1;
+        sK[tid] = n < num_nodes ? __ldg(ncats + n) : 0;
+        sP[tid] = n < num_nodes ? __ldg(s_pids + n) : 0;
     }
-    pcb::store4(nm, (int64_t)node_offset + n, ld, b, B, vec, o);
+    __syncthreads();
+    for (int i = tid; i < kFwdNodes * kFwdSlab; i += blockDim.x) {
+        const int j = i / kFwdSlab, k = i % kFwdSlab;
+        if (k < sK[j] && sK[j] <= kFwdSlab) slab[j][k] = __logf(__ldg(params + sP[j] + k));
+    }
+    __syncthreads();
+    const int b = blockIdx.y * 1024 + tid * 4;
+    if (b >= B) return;
+    const int v0 = sV[0];
+    int64_t x0[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x0[q] = (b + q < B) ? __ldg(data + (int64_t)v0 * data_ld + b + q) : 0;
+    for (int j = 0; j < kFwdNodes && n0 + j < num_nodes; ++j) {
+        const int v = sV[j], K = sK[j];
+        float4 o;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float r = 0.f;
+            if (b + q < B) {
+                const int64_t x = (v == v0) ? x0[q] : __ldg(data + (int64_t)v * data_ld + b + q);
+                if (x >= 0 && x < K) r = (K <= kFwdSlab) ? slab[j][x] : __logf(__ldg(params + sP[j] + x));
+                else r = NAN;
+            }
+            pcb::set(o, q, r);
+        }
+        pcb::store4(nm, (int64_t)node_offset + n0 + j, ld, b, B, vec, o);
+    }
 }
 
 // One CTA per variable group: stable counting sort of the batch by category (chunks of
@@ -104,11 +130,17 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
         __syncthreads();
         // seg[k] now holds the end of category k; its start is the end of category k-1.
         float* wrow = rows + warp * CB;
+        const bool vec4 = ((ld & 3) == 0) && ((c0 & 3) == 0) && ((reinterpret_cast<uintptr_t>(nf) & 15) == 0);
         for (int n = warp; n < cnt; n += (blockDim.x >> 5)) {
             const int64_t row = (int64_t)node_offset + node0 + n;
             const float* frow = nf + row * ld + c0;
             const int64_t sf = s_pfids[node0 + n];
-            for (int i = lane; i < nb; i += 32) wrow[i] = __ldg(frow + i);
+            if (vec4 && (nb & 3) == 0) {
+                for (int i = lane; i < nb / 4; i += 32)
+                    reinterpret_cast<float4*>(wrow)[i] = __ldg(reinterpret_cast<const float4*>(frow) + i);
+            } else {
+                for (int i = lane; i < nb; i += 32) wrow[i] = __ldg(frow + i);
+            }
             __syncwarp();
             for (int k = lane; k < K; k += 32) {
                 const int s = (k == 0) ? 0 : seg[k - 1];
@@ -135,12 +167,14 @@ extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const flo
     if (!data || !params || !vids || !s_pids || !ncats || !node_mars || B <= 0 || ld < B || data_ld < B || num_nodes < 0)
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: bad arguments");
     if (num_nodes == 0) return PCB_OK;
-    const int ngrp = (int)pcb::cdiv(B, 4);
-    const int64_t total = (int64_t)num_nodes * ngrp;
     const bool vec = pcb::vec_ok(node_mars, ld);
-    return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(total, 256)), dim3(256), 0,
-                                            pcb::as_stream(stream), 1u, data, data_ld, params, vids, s_pids, ncats,
-                                            node_offset, node_mars, ld, B, ngrp, total, vec), "pcb_input_cat_fwd");
+    const int64_t gy = pcb::cdiv(B, 1024);
+    if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: batch too large");
+    return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(num_nodes, kFwdNodes),
+                                                                       (unsigned)gy),
+                                            dim3(256), 0, pcb::as_stream(stream), 1u, data, data_ld, params, vids,
+                                            s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec),
+                              "pcb_input_cat_fwd");
 }
 
 extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,

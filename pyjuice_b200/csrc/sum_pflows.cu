@@ -7,7 +7,8 @@
 // with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b]: every
 // exponential is taken once per (row, sample), not once per (node, child, sample).
 //
-// The batch is split over a thread-block cluster of up to 8 CTAs. A CTA copies 64
+// The batch is split over a thread-block cluster of up to 8 CTAs (fewer when the layer's
+// tiles alone give about two CTAs per SM; a CTA then walks several chunks). A CTA copies 64
 // samples of its slice at a time (all node rows and child rows in one batch of
 // asynchronous copies), forms A and C, and contracts them either with FP32 FMA (prec 0)
 // or on the tensor cores (prec 1: bf16 operands; prec 2: both operands split into
@@ -360,9 +361,17 @@ extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, c
     if (num_tiles == 0) return PCB_OK;
     int rpb_log2 = 0;
     while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
-    // one CTA per 64-sample slice, up to 8 CTAs per cluster (a power of two)
+    // one CTA per 64-sample slice, up to 8 CTAs per cluster (a power of two); layers with many
+    // tiles take smaller clusters (each CTA then walks several 64-sample chunks) so that the
+    // launch stays within about two CTAs per SM instead of adding waves of short CTAs
     int cs = 1;
     while (cs < kMaxCluster && (int64_t)cs * KB < B) cs *= 2;
+    static int sms_of[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+        if (sms_of[dev] == 0) cudaDeviceGetAttribute(&sms_of[dev], cudaDevAttrMultiProcessorCount, dev);
+        while (cs > 1 && (int64_t)num_tiles * cs > 2 * (int64_t)sms_of[dev]) cs /= 2;
+    }
     if ((int64_t)num_tiles * cs > 2147483647) return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows: too many tiles");
     const bool vec = pcb::vec_ok(node_flows, ld) && pcb::vec_ok(node_mars, ld) && pcb::vec_ok(element_mars, ld);
     cudaStream_t s = pcb::as_stream(stream);
