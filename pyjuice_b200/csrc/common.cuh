@@ -91,13 +91,22 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Programmatic dependent launch. Every kernel starts with pdl_begin(): it lets the next
-// kernel of the stream be scheduled as soon as all of this grid's CTAs are running, then
-// waits until the previous grid has completed and its memory is visible. Kernels launched
-// without the attribute pass through both instructions at once.
+// Programmatic dependent launch. pdl_trigger() lets the next kernel of the stream be
+// scheduled as soon as every CTA of this grid has executed it; pdl_wait() blocks until the
+// previous grid has completed and its memory is visible. Kernels launched without the
+// attribute pass through both instructions at once. Most kernels start with both
+// (pdl_begin). A kernel may do work between the two, overlapping the previous kernel's
+// tail, only on memory that no early-triggering kernel writes: the compiled tables, data
+// written by other libraries' kernels (which never trigger early), and the parameters,
+// whose writers (the EM kernels) call pdl_wait() alone, so that their successors start
+// only after they have completed. Such reads bypass L1 (cp.async.cg, ld.global.cg).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 __device__ __forceinline__ void pdl_begin() {
-    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
-    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    pdl_trigger();
+    pdl_wait();
 }
 
 // Whether launches carry the programmatic-stream-serialization attribute (on unless the

@@ -15,7 +15,8 @@ __global__ void __launch_bounds__(256)
 sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int64_t* __restrict__ pbase,
               const int64_t* __restrict__ pfbase, const int* __restrict__ nchs, const int* __restrict__ bss,
               double step, double pc) {
-    pcb::pdl_begin();
+    // No early trigger: kernels after this one may read the parameters before their own wait.
+    pcb::pdl_wait();
     __shared__ double part[256];
     const int g = blockIdx.x;
     const int64_t pb = pbase[g];
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(256)
 input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int* __restrict__ s_pids,
                 const int* __restrict__ s_pfids, const int* __restrict__ ncats, const int* __restrict__ source_nids,
                 int num_src, double step, double pc) {
-    pcb::pdl_begin();
+    pcb::pdl_wait();  // no early trigger, as in sum_em_kernel
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= num_src) return;

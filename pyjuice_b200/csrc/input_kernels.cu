@@ -16,7 +16,9 @@ __global__ void __launch_bounds__(256)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
                      int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec) {
-    pcb::pdl_begin();
+    // The node tables and the parameter logs are read before the wait for the previous kernel
+    // (the parameters' writers do not trigger early); the samples and outputs after it.
+    pcb::pdl_trigger();
     __shared__ float slab[kFwdNodes][kFwdSlab];
     __shared__ int sV[kFwdNodes], sK[kFwdNodes], sP[kFwdNodes];
     const int n0 = blockIdx.x * kFwdNodes;
@@ -30,9 +32,10 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
     __syncthreads();
     for (int i = tid; i < kFwdNodes * kFwdSlab; i += blockDim.x) {
         const int j = i / kFwdSlab, k = i % kFwdSlab;
-        if (k < sK[j] && sK[j] <= kFwdSlab) slab[j][k] = __logf(__ldg(params + sP[j] + k));
+        if (k < sK[j] && sK[j] <= kFwdSlab) slab[j][k] = __logf(__ldcg(params + sP[j] + k));
     }
     __syncthreads();
+    pcb::pdl_wait();
     const int b = blockIdx.y * 1024 + tid * 4;
     if (b >= B) return;
     const int v0 = sV[0];
@@ -47,7 +50,7 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
             float r = 0.f;
             if (b + q < B) {
                 const int64_t x = (v == v0) ? x0[q] : __ldg(data + (int64_t)v * data_ld + b + q);
-                if (x >= 0 && x < K) r = (K <= kFwdSlab) ? slab[j][x] : __logf(__ldg(params + sP[j] + x));
+                if (x >= 0 && x < K) r = (K <= kFwdSlab) ? slab[j][x] : __logf(__ldcg(params + sP[j] + x));
                 else r = NAN;
             }
             pcb::set(o, q, r);

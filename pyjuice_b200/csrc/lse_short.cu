@@ -79,7 +79,9 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                  const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                  int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
                  const uint8_t* __restrict__ packed) {
-    pcb::pdl_begin();
+    // The term indices and the weights (compiled tables and parameters) are read before the
+    // wait for the previous kernel; only the source rows and the packed weights after it.
+    pcb::pdl_trigger();
     using S = Smem<RM, TB, MODE, PREC, WK>;
     constexpr int ES = S::ES, WS = S::WS, WROW = S::WROW;
     constexpr int PARTS = kThreads / TB;  // threads per sample column in the max / exp passes
@@ -111,6 +113,73 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
         sKw[tid] = __ldg(kw + t.k_off + tid);
     }
     __syncthreads();
+    constexpr int kPackHalf = RM * 256;
+    const bool pk = PREC > 0 && packed != nullptr;
+    auto wbase = [&](int r) -> int64_t {
+        const int rr = r0 + r;
+        return (int64_t)t.w_add + (int64_t)(rr >> rpb_log2) * t.g_stride + (int64_t)(rr & rpb_mask) * w_stride;
+    };
+    if (pk) {
+    } else if (WK) {
+        // sW[r][k]: each thread copies groups of 4 consecutive terms of one row
+        constexpr int IT = RM * (KMAX / 4) / kThreads;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * kThreads;
+            const int r = idx / (KMAX / 4);
+            const int k = (idx % (KMAX / 4)) * 4;
+            if (r < nrows && k < nk) {
+                const int64_t base = wbase(r);
+                if (wvec && k + 3 < nk) {
+                    pcb::cp_async16(&sW[r][k], params + base + sKw[k]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (k + j < nk) sW[r][k + j] = __ldcg(params + base + sKw[k + j]);
+                }
+            }
+        }
+    } else {
+        // sW[k][r]: each thread copies groups of 4 consecutive rows of one term
+        constexpr int IT = KMAX * (RM / 4) / kThreads;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * kThreads;
+            const int k = idx / (RM / 4);
+            const int r = (idx % (RM / 4)) * 4;
+            if (k < nk && r < nrows) {
+                const int64_t kb = sKw[k];
+                if (wvec && r + 3 < nrows) {
+                    pcb::cp_async16(&sW[k][r], params + kb + wbase(r));
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (r + j < nrows) sW[k][r + j] = __ldcg(params + kb + wbase(r + j));
+                }
+            }
+        }
+    }
+    pcb::cp_async_commit();
+    if constexpr (PREC > 0) {
+        // weights -> bf16 pairs along the terms (split: hi, then lo), still before the wait
+        if (!pk) {
+            pcb::cp_async_wait<0>();
+            __syncthreads();
+            for (int idx = tid; idx < (KMAX / 2) * RM; idx += kThreads) {
+                const int kk = idx / RM;
+                const int r = idx % RM;
+                float w0 = 0.f, w1 = 0.f;
+                if (r < nrows) {
+                    if (2 * kk < nk) w0 = WK ? sW[r][2 * kk] : sW[2 * kk][r];
+                    if (2 * kk + 1 < nk) w1 = WK ? sW[r][2 * kk + 1] : sW[2 * kk + 1][r];
+                }
+                if (PREC == 2) split_bf16(w0, w1, pW[kk * WS + r], pW[(KMAX / 2) * WS + kk * WS + r]);
+                else pW[kk * WS + r] = pack_bf16(w0, w1);
+            }
+        }
+    }
+
+    pcb::pdl_wait();
     {
         constexpr int NX = TB / 4;
         constexpr int IT = KMAX * NX / kThreads;
@@ -141,8 +210,6 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     }
     // packed bf16 weights (hi, then lo): rows r0 .. r0 + RM - 1 are RM / 8 core-matrix row
     // groups of 2048 bytes in each half of the tile's 64 KB block
-    constexpr int kPackHalf = RM * 256;
-    const bool pk = PREC > 0 && packed != nullptr;
     if (pk) {
         const uint8_t* srcp = packed + (size_t)(blockIdx.x / row_splits) * 65536 + (size_t)(r0 / 8) * 2048;
         uint8_t* dstp = reinterpret_cast<uint8_t*>(pW);
@@ -153,50 +220,6 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             const int i = tid + it * kThreads;
             const int h = i / CH, c = i % CH;
             pcb::cp_async16(dstp + h * kPackHalf + c * 16, srcp + (size_t)h * 32768 + c * 16);
-        }
-    }
-    auto wbase = [&](int r) -> int64_t {
-        const int rr = r0 + r;
-        return (int64_t)t.w_add + (int64_t)(rr >> rpb_log2) * t.g_stride + (int64_t)(rr & rpb_mask) * w_stride;
-    };
-    if (pk) {
-    } else if (WK) {
-        // sW[r][k]: each thread copies groups of 4 consecutive terms of one row
-        constexpr int IT = RM * (KMAX / 4) / kThreads;
-#pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            const int idx = tid + it * kThreads;
-            const int r = idx / (KMAX / 4);
-            const int k = (idx % (KMAX / 4)) * 4;
-            if (r < nrows && k < nk) {
-                const int64_t base = wbase(r);
-                if (wvec && k + 3 < nk) {
-                    pcb::cp_async16(&sW[r][k], params + base + sKw[k]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (k + j < nk) pcb::cp_async4(&sW[r][k + j], params + base + sKw[k + j]);
-                }
-            }
-        }
-    } else {
-        // sW[k][r]: each thread copies groups of 4 consecutive rows of one term
-        constexpr int IT = KMAX * (RM / 4) / kThreads;
-#pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            const int idx = tid + it * kThreads;
-            const int k = idx / (RM / 4);
-            const int r = (idx % (RM / 4)) * 4;
-            if (k < nk && r < nrows) {
-                const int64_t kb = sKw[k];
-                if (wvec && r + 3 < nrows) {
-                    pcb::cp_async16(&sW[k][r], params + kb + wbase(r));
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (r + j < nrows) pcb::cp_async4(&sW[k][r + j], params + kb + wbase(r + j));
-                }
-            }
         }
     }
     pcb::cp_async_commit();
@@ -297,17 +320,6 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             }
             if (SPLIT) split_bf16(e0, e1, pE[kk * ES + cb], pE[(KMAX / 2) * ES + kk * ES + cb]);
             else pE[kk * ES + cb] = pack_bf16(e0, e1);
-        }
-        for (int idx = tid; idx < (pk ? 0 : (KMAX / 2) * RM); idx += kThreads) {
-            const int kk = idx / RM;
-            const int r = idx % RM;
-            float w0 = 0.f, w1 = 0.f;
-            if (r < nrows) {
-                if (2 * kk < nk) w0 = WK ? sW[r][2 * kk] : sW[2 * kk][r];
-                if (2 * kk + 1 < nk) w1 = WK ? sW[r][2 * kk + 1] : sW[2 * kk + 1][r];
-            }
-            if (SPLIT) split_bf16(w0, w1, pW[kk * WS + r], pW[(KMAX / 2) * WS + kk * WS + r]);
-            else pW[kk * WS + r] = pack_bf16(w0, w1);
         }
         __syncthreads();
 

@@ -10,7 +10,9 @@ __global__ void __launch_bounds__(256)
 prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, int B, const int* __restrict__ blk_row,
             const int* __restrict__ blk_off, const int* __restrict__ blk_cnt, const int* __restrict__ chs,
             int blk_size, int ngrp, int64_t total, bool vec) {
-    pcb::pdl_begin();
+    // The block tables (and the first 8 child indices) are read before the wait for the
+    // previous kernel: they are compiled once and never written by a pass.
+    pcb::pdl_trigger();
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= total) return;
     const int grp = (int)(idx % ngrp);
@@ -20,14 +22,20 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
     const int b = grp * 4;
     const int off = __ldg(blk_off + g);
     const int cnt = __ldg(blk_cnt + g);
+    const int64_t row = (int64_t)__ldg(blk_row + g) + i;
+    int c[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c[j] = (j < cnt) ? __ldg(chs + off + j) : -1;
+    pcb::pdl_wait();
     float4 acc;
     if (!LSE) {
         acc = make_float4(0.f, 0.f, 0.f, 0.f);
         // 8 children at a time: all index loads, then all row loads, are independent
         for (int j0 = 0; j0 < cnt; j0 += 8) {
-            int c[8];
+            if (j0 > 0) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) c[j] = (j0 + j < cnt) ? __ldg(chs + off + j0 + j) : -1;
+                for (int j = 0; j < 8; ++j) c[j] = (j0 + j < cnt) ? __ldg(chs + off + j0 + j) : -1;
+            }
             float4 v[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j)
@@ -60,7 +68,6 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
             pcb::set(acc, q, mq == -INFINITY ? -INFINITY : logf(pcb::get(s, q)) + mq);
         }
     }
-    const int64_t row = (int64_t)__ldg(blk_row + g) + i;
     if (ACCUM) {
         const float4 old = pcb::load4(out, row, ld, b, B, vec, 0.f);
         if (!LSE) {
