@@ -7,11 +7,12 @@
 // with lf = log(node flow) - log(node mar) and M_b = max_r lf[nid + r, b]: every
 // exponential is taken once per (row, sample), not once per (node, child, sample).
 //
-// The batch is split over a thread-block cluster of up to 8 CTAs (fewer when the layer's
-// tiles alone give about two CTAs per SM; a CTA then walks several chunks). A CTA copies 64
-// samples of its slice at a time (all node rows and child rows in one batch of
-// asynchronous copies), forms A and C, and contracts them either with FP32 FMA (prec 0)
-// or on the tensor cores (prec 1: bf16 operands; prec 2: both operands split into
+// The batch is split over a thread-block cluster of up to 8 CTAs, one per 64-sample slice
+// (fewer when the layer's tiles alone give about two CTAs per SM; a CTA then walks a longer
+// slice). A CTA walks its slice in chunks of 32 samples, double-buffered: the copies of the
+// next chunk (all node rows and child rows in one batch of asynchronous copies) are in
+// flight while the current one is reduced. It forms A and C (4 samples per thread and
+// step), and contracts them either with FP32 FMA (prec 0) or on the tensor cores (prec 1: bf16 operands; prec 2: both operands split into
 // bf16 hi + lo, three MMAs, FP32 accumulators). At the end the CTAs exchange their
 // partial tiles through distributed shared memory and each adds the partials of its
 // share of the outputs in rank order: the result does not depend on timing (no float
@@ -29,9 +30,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int TMN = 128;      // nodes per tile
-constexpr int KB = 64;        // samples per staged chunk
+constexpr int KB = 32;        // samples per staged chunk (two chunks in flight)
+constexpr int kSliceUnit = 64;  // cluster sizing: one CTA per 64-sample slice
 constexpr int RS = KB + 4;    // fp32 staging row stride (16-byte rows)
 constexpr int PS = KB / 2 + 4;  // packed bf16-pair row stride (conflict-free fragment loads)
+constexpr int kParts = kThreads / KB;  // row parts of the max pass
+constexpr int RT = TMN + 4;   // partial-tile row stride (child-major; conflict-free fragment stores)
 constexpr int kMaxCluster = 8;
 
 __device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, uint32_t& l) {
@@ -55,20 +59,25 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// Shared-memory plan in 4-byte words (16-byte aligned arrays).
+// Shared-memory plan in 4-byte words (16-byte aligned arrays). Two staging buffers (chunk
+// c + 1 is copied while chunk c is reduced), each holding the node rows (flows, and mars
+// for unmodified flows) and the child rows of one chunk.
 template <int TKC, bool MODIFIED, int PREC>
 struct Plan {
     static constexpr int NB = PREC == 2 ? 2 : (PREC == 1 ? 1 : 0);
-    static constexpr int oA = 0;
-    static constexpr int oA2 = oA + TMN * RS;
-    static constexpr int oC = oA2 + (MODIFIED ? 0 : TMN * RS);
-    static constexpr int oPA = oC + TKC * RS;
+    static constexpr int sA = 0;
+    static constexpr int sA2 = sA + TMN * RS;
+    static constexpr int sC = sA2 + (MODIFIED ? 0 : TMN * RS);
+    static constexpr int kStage = sC + TKC * RS;
+    static constexpr int oPA = 2 * kStage;
     static constexpr int oPC = oPA + NB * TMN * PS;
     static constexpr int oPart = oPC + NB * TKC * PS;
     static constexpr int oM = oPart + kThreads;
     static constexpr int oCid = oM + KB;
-    static constexpr int words = oCid + TKC;
-    static_assert(words >= TMN * TKC, "the partial tile aliases the staging area");
+    static constexpr int oPid = oCid + TKC;
+    static constexpr int oPfid = oPid + TKC;
+    static constexpr int words = oPfid + TKC;
+    static_assert(2 * kStage >= TKC * RT, "the partial tile aliases the staging area");
     static constexpr size_t bytes() { return 4ull * words; }
 };
 
@@ -78,17 +87,18 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                   int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                   const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
                   const int* __restrict__ pids, const int* __restrict__ pfids, int slice, bool vec) {
-    pcb::pdl_begin();
+    // The tile and its child indices (compiled tables) are read before the wait for the
+    // previous kernel; the flows and values after it.
+    pcb::pdl_trigger();
     using P = Plan<TKC, MODIFIED, PREC>;
     extern __shared__ __align__(16) float dsm[];
-    float(*sA)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oA);
-    float(*sA2)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oA2);
-    float(*sC)[RS] = reinterpret_cast<float(*)[RS]>(dsm + P::oC);
     uint32_t* pA = reinterpret_cast<uint32_t*>(dsm + P::oPA);
     uint32_t* pC = reinterpret_cast<uint32_t*>(dsm + P::oPC);
     float* sPart = dsm + P::oPart;
     float* sM = dsm + P::oM;
     int* sCid = reinterpret_cast<int*>(dsm + P::oCid);
+    int* sPid = reinterpret_cast<int*>(dsm + P::oPid);
+    int* sPfid = reinterpret_cast<int*>(dsm + P::oPfid);
 
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
@@ -99,8 +109,14 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
     const int lane = tid & 31;
     const int rpb_mask = (1 << rpb_log2) - 1;
 
-    if (tid < TKC) sCid[tid] = (tid < t.k_cnt) ? __ldg(cids + t.k_off + tid) : -1;
+    if (tid < TKC) {
+        const bool in = tid < t.k_cnt;
+        sCid[tid] = in ? __ldg(cids + t.k_off + tid) : -1;
+        sPid[tid] = in ? __ldg(pids + t.k_off + tid) : 0;
+        sPfid[tid] = in ? __ldg(pfids + t.k_off + tid) : 0;
+    }
     __syncthreads();
+    pcb::pdl_wait();
 
     // FP32: thread (ty, tx) owns nodes ty * 8 .. + 8 and children tx + 16 * j.
     // Tensor cores: warp w owns nodes 16 w .. 16 w + 15 and all TKC children.
@@ -114,45 +130,23 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
 
     const int bs0 = crank * slice;
     const int bs1 = min(B, bs0 + slice);
-    for (int b0 = bs0; b0 < bs1; b0 += KB) {
-        // ---- one batch of asynchronous copies: node rows (flows, mars) and child rows ----
-        {
-            constexpr int NX = KB / 4;
+    const int nch = bs1 > bs0 ? (bs1 - bs0 + KB - 1) / KB : 0;
+
+    // one batch of asynchronous copies per chunk: node rows (flows, mars) and child rows
+    auto issue = [&](int b0, int st) {
+        float* stage = dsm + st * P::kStage;
+        constexpr int NX = KB / 4;
 #pragma unroll
-            for (int it = 0; it < TMN * NX / kThreads; ++it) {
-                const int idx = tid + it * kThreads;
-                const int r = idx / NX;
-                const int c4 = (idx % NX) * 4;
-                const int b = b0 + c4;
+        for (int it = 0; it < TMN * NX / kThreads; ++it) {
+            const int idx = tid + it * kThreads;
+            const int r = idx / NX;
+            const int c4 = (idx % NX) * 4;
+            const int b = b0 + c4;
 #pragma unroll
-                for (int h = 0; h < (MODIFIED ? 1 : 2); ++h) {
-                    float* d = h == 0 ? &sA[r][c4] : &sA2[r][c4];
-                    if (r < t.n_rows) {
-                        const float* g = (h == 0 ? nf : nm) + ((int64_t)t.nid + r) * ld + b;
-                        if (vec && b + 3 < bs1) {
-                            pcb::cp_async16(d, g);
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                if (b + j < bs1) pcb::cp_async4(d + j, g + j);
-                                else d[j] = -INFINITY;
-                            }
-                        }
-                    } else {
-                        *reinterpret_cast<float4*>(d) = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
-                    }
-                }
-            }
-#pragma unroll
-            for (int it = 0; it < TKC * NX / kThreads; ++it) {
-                const int idx = tid + it * kThreads;
-                const int k = idx / NX;
-                const int c4 = (idx % NX) * 4;
-                const int b = b0 + c4;
-                float* d = &sC[k][c4];
-                const int row = sCid[k];
-                if (row >= 0) {
-                    const float* g = em + (int64_t)row * ld + b;
+            for (int h = 0; h < (MODIFIED ? 1 : 2); ++h) {
+                float* d = stage + (h == 0 ? P::sA : P::sA2) + r * RS + c4;
+                if (r < t.n_rows) {
+                    const float* g = (h == 0 ? nf : nm) + ((int64_t)t.nid + r) * ld + b;
                     if (vec && b + 3 < bs1) {
                         pcb::cp_async16(d, g);
                     } else {
@@ -166,17 +160,55 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                     *reinterpret_cast<float4*>(d) = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
                 }
             }
-            pcb::cp_async_commit();
+        }
+#pragma unroll
+        for (int it = 0; it < TKC * NX / kThreads; ++it) {
+            const int idx = tid + it * kThreads;
+            const int k = idx / NX;
+            const int c4 = (idx % NX) * 4;
+            const int b = b0 + c4;
+            float* d = stage + P::sC + k * RS + c4;
+            const int row = sCid[k];
+            if (row >= 0) {
+                const float* g = em + (int64_t)row * ld + b;
+                if (vec && b + 3 < bs1) {
+                    pcb::cp_async16(d, g);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (b + j < bs1) pcb::cp_async4(d + j, g + j);
+                        else d[j] = -INFINITY;
+                    }
+                }
+            } else {
+                *reinterpret_cast<float4*>(d) = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+            }
+        }
+        pcb::cp_async_commit();
+    };
+
+    if (nch > 0) issue(bs0, 0);
+    for (int c = 0; c < nch; ++c) {
+        const int st = c & 1;
+        // the other buffer was last read before the previous chunk's contraction barrier
+        if (c + 1 < nch) {
+            issue(bs0 + (c + 1) * KB, st ^ 1);
+            pcb::cp_async_wait<1>();
+        } else {
             pcb::cp_async_wait<0>();
         }
         __syncthreads();
+        float(*sA)[RS] = reinterpret_cast<float(*)[RS]>(dsm + st * P::kStage + P::sA);
+        float(*sA2)[RS] = reinterpret_cast<float(*)[RS]>(dsm + st * P::kStage + P::sA2);
+        float(*sC)[RS] = reinterpret_cast<float(*)[RS]>(dsm + st * P::kStage + P::sC);
 
         // ---- lf = log f - log m (unmodified flows), then M_b = max over the tile's nodes ----
         {
             const int b = tid % KB;
-            const int part = tid / KB;  // 4 parts of 32 rows
+            const int part = tid / KB;
             float mx = -INFINITY;
-            for (int r = part * (TMN / 4); r < (part + 1) * (TMN / 4); ++r) {
+#pragma unroll 4
+            for (int r = part * (TMN / kParts); r < (part + 1) * (TMN / kParts); ++r) {
                 float v = sA[r][b];
                 if (!MODIFIED) {
                     const float m2 = sA2[r][b];
@@ -188,7 +220,12 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
             sPart[part * KB + b] = mx;
         }
         __syncthreads();
-        if (tid < KB) sM[tid] = fmaxf(fmaxf(sPart[tid], sPart[KB + tid]), fmaxf(sPart[2 * KB + tid], sPart[3 * KB + tid]));
+        if (tid < KB) {
+            float m = sPart[tid];
+#pragma unroll
+            for (int p = 1; p < kParts; ++p) m = fmaxf(m, sPart[p * KB + tid]);
+            sM[tid] = m;
+        }
         __syncthreads();
 
         if constexpr (PREC == 0) {
@@ -222,26 +259,48 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                     }
                 }
             }
+            __syncthreads();  // the next chunk's copies overwrite this buffer
         } else {
             constexpr bool SPLIT = PREC == 2;
-            // ---- exponentiate and pack sample pairs as bf16 (hi, lo) ----
-            for (int idx = tid; idx < TMN * (KB / 2); idx += kThreads) {
-                const int r = idx / (KB / 2), j = idx % (KB / 2);
-                const float2 v = *reinterpret_cast<const float2*>(&sA[r][2 * j]);
-                const float m0 = sM[2 * j], m1 = sM[2 * j + 1];
-                const float e0 = (m0 == -INFINITY) ? 0.f : __expf(v.x - m0);
-                const float e1 = (m1 == -INFINITY) ? 0.f : __expf(v.y - m1);
-                if (SPLIT) split_bf16(e0, e1, pA[r * PS + j], pA[TMN * PS + r * PS + j]);
-                else pA[r * PS + j] = pack_bf16(e0, e1);
+            // ---- exponentiate and pack sample pairs as bf16 (hi, lo), 4 samples per step ----
+            constexpr int NX = KB / 4;
+            for (int idx = tid; idx < TMN * NX; idx += kThreads) {
+                const int r = idx / NX, c4 = (idx % NX) * 4;
+                const float4 v = *reinterpret_cast<const float4*>(&sA[r][c4]);
+                const float4 m = *reinterpret_cast<const float4*>(&sM[c4]);
+                const float e0 = (m.x == -INFINITY) ? 0.f : __expf(v.x - m.x);
+                const float e1 = (m.y == -INFINITY) ? 0.f : __expf(v.y - m.y);
+                const float e2 = (m.z == -INFINITY) ? 0.f : __expf(v.z - m.z);
+                const float e3 = (m.w == -INFINITY) ? 0.f : __expf(v.w - m.w);
+                uint2 h, l;
+                if (SPLIT) {
+                    split_bf16(e0, e1, h.x, l.x);
+                    split_bf16(e2, e3, h.y, l.y);
+                    *reinterpret_cast<uint2*>(&pA[TMN * PS + r * PS + c4 / 2]) = l;
+                } else {
+                    h.x = pack_bf16(e0, e1);
+                    h.y = pack_bf16(e2, e3);
+                }
+                *reinterpret_cast<uint2*>(&pA[r * PS + c4 / 2]) = h;
             }
-            for (int idx = tid; idx < TKC * (KB / 2); idx += kThreads) {
-                const int k = idx / (KB / 2), j = idx % (KB / 2);
-                const float2 v = *reinterpret_cast<const float2*>(&sC[k][2 * j]);
-                const float m0 = sM[2 * j], m1 = sM[2 * j + 1];
-                const float e0 = (m0 == -INFINITY) ? 0.f : __expf(v.x + m0);
-                const float e1 = (m1 == -INFINITY) ? 0.f : __expf(v.y + m1);
-                if (SPLIT) split_bf16(e0, e1, pC[k * PS + j], pC[TKC * PS + k * PS + j]);
-                else pC[k * PS + j] = pack_bf16(e0, e1);
+            for (int idx = tid; idx < TKC * NX; idx += kThreads) {
+                const int k = idx / NX, c4 = (idx % NX) * 4;
+                const float4 v = *reinterpret_cast<const float4*>(&sC[k][c4]);
+                const float4 m = *reinterpret_cast<const float4*>(&sM[c4]);
+                const float e0 = (m.x == -INFINITY) ? 0.f : __expf(v.x + m.x);
+                const float e1 = (m.y == -INFINITY) ? 0.f : __expf(v.y + m.y);
+                const float e2 = (m.z == -INFINITY) ? 0.f : __expf(v.z + m.z);
+                const float e3 = (m.w == -INFINITY) ? 0.f : __expf(v.w + m.w);
+                uint2 h, l;
+                if (SPLIT) {
+                    split_bf16(e0, e1, h.x, l.x);
+                    split_bf16(e2, e3, h.y, l.y);
+                    *reinterpret_cast<uint2*>(&pC[TKC * PS + k * PS + c4 / 2]) = l;
+                } else {
+                    h.x = pack_bf16(e0, e1);
+                    h.y = pack_bf16(e2, e3);
+                }
+                *reinterpret_cast<uint2*>(&pC[k * PS + c4 / 2]) = h;
             }
             __syncthreads();
             const int g = lane >> 2, q = lane & 3;
@@ -269,45 +328,71 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                     }
                 }
             }
+            // The packed operands are rewritten only after the next chunk's first barrier, and
+            // this chunk's staging buffer was last read before the barrier above.
         }
-        __syncthreads();  // the next chunk (or the partial tile) overwrites the staging area
     }
+    __syncthreads();  // the partial tile overwrites the staging area
 
-    // ---- partial tile -> shared memory; cluster-wide fixed-order sum ----
-    float* red = dsm;  // [TMN][TKC]
+    // ---- partial tile -> shared memory (child-major); cluster-wide fixed-order sum ----
+    float* red = dsm;  // [TKC][RT]
     if constexpr (PREC == 0) {
         const int tx = tid % 16, ty = tid / 16;
 #pragma unroll
         for (int a = 0; a < 8; ++a)
 #pragma unroll
-            for (int j = 0; j < FJ; ++j) red[(ty * 8 + a) * TKC + tx + 16 * j] = acc[a][j];
+            for (int j = 0; j < FJ; ++j) red[(tx + 16 * j) * RT + ty * 8 + a] = acc[a][j];
     } else {
         const int g = lane >> 2, q = lane & 3;
         const int mr = warp * 16 + g;
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
             const int n = nt * 8 + 2 * q;
-            red[mr * TKC + n] = acc[nt][0];
-            red[mr * TKC + n + 1] = acc[nt][1];
-            red[(mr + 8) * TKC + n] = acc[nt][2];
-            red[(mr + 8) * TKC + n + 1] = acc[nt][3];
+            red[n * RT + mr] = acc[nt][0];
+            red[(n + 1) * RT + mr] = acc[nt][1];
+            red[n * RT + mr + 8] = acc[nt][2];
+            red[(n + 1) * RT + mr + 8] = acc[nt][3];
         }
     }
     cluster.sync();
+    // Outputs (child k, node i) with the node fastest, so that consecutive threads touch
+    // consecutive parameters and flow slots; U outputs per thread at a time, all loads of a
+    // round issued before any of its stores.
+    constexpr int U = 8;
     const int per = (TMN * TKC + csize - 1) / csize;
-    const int end = min(TMN * TKC, (crank + 1) * per);
-    for (int idx = crank * per + tid; idx < end; idx += kThreads) {
-        const int i = idx / TKC;
-        const int k = idx % TKC;
-        if (i >= t.n_rows || k >= t.k_cnt) continue;
-        float s = 0.f;
-        for (int r = 0; r < csize; ++r) s += cluster.map_shared_rank(red, r)[idx];
-        const int64_t roff = (int64_t)t.p_add + (int64_t)(i & rpb_mask);
-        const int blk = i >> rpb_log2;
-        const float w = __ldg(params + (int64_t)pids[t.k_off + k] + roff + (int64_t)blk * t.gs_p);
-        const int64_t slot = (int64_t)pfids[t.k_off + k] + roff + (int64_t)blk * t.gs_pf;
-        if (ATOMIC) atomicAdd(pf + slot, s * w);
-        else pf[slot] += s * w;
+    const int beg = crank * per;
+    const int end = min(TMN * TKC, beg + per);
+    for (int base = beg; base < end; base += kThreads * U) {
+        float sv[U], wv[U], old[U];
+        int64_t slot[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * kThreads + tid;
+            const int k = idx / TMN;
+            const int i = idx % TMN;
+            ok[u] = idx < end && i < t.n_rows && k < t.k_cnt;
+            sv[u] = 0.f;
+            wv[u] = 0.f;
+            slot[u] = 0;
+            if (ok[u]) {
+                for (int r = 0; r < csize; ++r) sv[u] += cluster.map_shared_rank(red, r)[k * RT + i];
+                const int64_t roff = (int64_t)t.p_add + (int64_t)(i & rpb_mask);
+                const int64_t blk = i >> rpb_log2;
+                wv[u] = __ldg(params + (int64_t)sPid[k] + roff + blk * t.gs_p);
+                slot[u] = (int64_t)sPfid[k] + roff + blk * t.gs_pf;
+            }
+        }
+        if (!ATOMIC) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) old[u] = ok[u] ? pf[slot[u]] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            if (ATOMIC) atomicAdd(pf + slot[u], sv[u] * wv[u]);
+            else pf[slot[u]] = old[u] + sv[u] * wv[u];
+        }
     }
     cluster.sync();  // keep every CTA's shared memory alive until all reads are done
 }
@@ -365,7 +450,7 @@ extern "C" int pcb_sum_pflows(const float* node_flows, const float* node_mars, c
     // tiles take smaller clusters (each CTA then walks several 64-sample chunks) so that the
     // launch stays within about two CTAs per SM instead of adding waves of short CTAs
     int cs = 1;
-    while (cs < kMaxCluster && (int64_t)cs * KB < B) cs *= 2;
+    while (cs < kMaxCluster && (int64_t)cs * kSliceUnit < B) cs *= 2;
     static int sms_of[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
