@@ -74,7 +74,9 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
     }
 }
 
-// One warp per source input node, categories strided over the lanes.
+// One warp per source input node, categories strided over the lanes. Nodes of up to 256
+// categories keep their flows and parameters in registers (all loads of a node issued at
+// once, one pass over memory); larger ones take two passes.
 template <bool KEEP_ZERO>
 __global__ void __launch_bounds__(256)
 input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int* __restrict__ s_pids,
@@ -89,6 +91,36 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
     const int64_t sp = s_pids[n];
     const int64_t sf = s_pfids[n];
     const double pcn = pc / (double)K;
+    auto update = [&](double p, double f, double s) -> float {
+        double np;
+        if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / s;
+        else np = (1.0 - step) * p + step * (f + pcn) / (s + pc);
+        return (float)np;
+    };
+    constexpr int R = 8;
+    if (K <= 32 * R) {
+        float f[R], p[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int k = lane + 32 * j;
+            f[j] = k < K ? pflows[sf + k] : 0.f;
+            p[j] = k < K ? params[sp + k] : 0.f;
+        }
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            if (lane + 32 * j >= K) continue;
+            if (KEEP_ZERO) s += (p[j] < 1e-12f) ? 0.0 : (double)f[j] + pcn;
+            else s += (double)f[j];
+        }
+        s = pcb::warp_sum(s);
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int k = lane + 32 * j;
+            if (k < K) params[sp + k] = update((double)p[j], (double)f[j], s);
+        }
+        return;
+    }
     double s = 0.0;
     for (int k = lane; k < K; k += 32) {
         const double f = (double)pflows[sf + k];
@@ -96,14 +128,7 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
         else s += f;
     }
     s = pcb::warp_sum(s);
-    for (int k = lane; k < K; k += 32) {
-        const double p = (double)params[sp + k];
-        const double f = (double)pflows[sf + k];
-        double np;
-        if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / s;
-        else np = (1.0 - step) * p + step * (f + pcn) / (s + pc);
-        params[sp + k] = (float)np;
-    }
+    for (int k = lane; k < K; k += 32) params[sp + k] = update((double)params[sp + k], (double)pflows[sf + k], s);
 }
 
 }  // namespace

@@ -28,7 +28,7 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int TMN = 128;      // nodes per tile
 constexpr int KB = 32;        // samples per staged chunk (two chunks in flight)
 constexpr int kSliceUnit = 64;  // cluster sizing: one CTA per 64-sample slice
@@ -37,6 +37,14 @@ constexpr int PS = KB / 2 + 4;  // packed bf16-pair row stride (conflict-free fr
 constexpr int kParts = kThreads / KB;  // row parts of the max pass
 constexpr int RT = TMN + 4;   // partial-tile row stride (child-major; conflict-free fragment stores)
 constexpr int kMaxCluster = 8;
+constexpr float kLog2e = 1.4426950408889634f;  // log2(e): exp(x) = 2^(x log2 e)
+
+// 2^x with the hardware approximation (flushes subnormal results to zero).
+__device__ __forceinline__ float ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 __device__ __forceinline__ void split_bf16(float lo_k, float hi_k, uint32_t& h, uint32_t& l) {
     __nv_bfloat162 hv = __floats2bfloat162_rn(lo_k, hi_k);
@@ -72,8 +80,8 @@ struct Plan {
     static constexpr int oPA = 2 * kStage;
     static constexpr int oPC = oPA + NB * TMN * PS;
     static constexpr int oPart = oPC + NB * TKC * PS;
-    static constexpr int oM = oPart + kThreads;
-    static constexpr int oCid = oM + KB;
+    static constexpr int oM = oPart + kThreads;   // [2][KB]: -M_b for A, +M_b for C
+    static constexpr int oCid = oM + 2 * KB;
     static constexpr int oPid = oCid + TKC;
     static constexpr int oPfid = oPid + TKC;
     static constexpr int words = oPfid + TKC;
@@ -82,7 +90,7 @@ struct Plan {
 };
 
 template <int TKC, bool MODIFIED, bool ATOMIC, int PREC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (PREC == 0 && TKC == 128) ? 1 : 2)
 sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, const float* __restrict__ em,
                   int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                   const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
@@ -118,13 +126,15 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
     __syncthreads();
     pcb::pdl_wait();
 
-    // FP32: thread (ty, tx) owns nodes ty * 8 .. + 8 and children tx + 16 * j.
-    // Tensor cores: warp w owns nodes 16 w .. 16 w + 15 and all TKC children.
+    // FP32: thread (ty, tx) owns nodes ty * FR .. + FR and children tx + 16 * j.
+    // Tensor cores: warp w owns nodes 16 (w % 8) .. + 15 and children half w / 8.
+    constexpr int FR = TMN * 16 / kThreads;
     constexpr int FJ = TKC / 16;
-    constexpr int NT = TKC / 8;
-    float acc[PREC == 0 ? 8 : NT][PREC == 0 ? FJ : 4];
+    constexpr int NT = TKC / 16;
+    static_assert(kThreads == 512 && FR >= 1 && NT >= 1, "thread layout");
+    float acc[PREC == 0 ? FR : NT][PREC == 0 ? FJ : 4];
 #pragma unroll
-    for (int a = 0; a < (PREC == 0 ? 8 : NT); ++a)
+    for (int a = 0; a < (PREC == 0 ? FR : NT); ++a)
 #pragma unroll
         for (int j = 0; j < (PREC == 0 ? FJ : 4); ++j) acc[a][j] = 0.f;
 
@@ -162,8 +172,9 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
             }
         }
 #pragma unroll
-        for (int it = 0; it < TKC * NX / kThreads; ++it) {
+        for (int it = 0; it < (TKC * NX + kThreads - 1) / kThreads; ++it) {
             const int idx = tid + it * kThreads;
+            if (idx >= TKC * NX) break;
             const int k = idx / NX;
             const int c4 = (idx % NX) * 4;
             const int b = b0 + c4;
@@ -224,32 +235,34 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
             float m = sPart[tid];
 #pragma unroll
             for (int p = 1; p < kParts; ++p) m = fmaxf(m, sPart[p * KB + tid]);
-            sM[tid] = m;
+            // A = 2^((lf - M) log2e), C = 2^((em + M) log2e); a sample whose rows are all -inf
+            // gets A = 0 (M taken as +inf there) and C = 0 (M as -inf). The sums are formed
+            // before scaling: lf and M (em and -M) are close, so the difference is exact.
+            sM[tid] = (m == -INFINITY) ? -INFINITY : -m;
+            sM[KB + tid] = m;
         }
         __syncthreads();
 
         if constexpr (PREC == 0) {
             for (int idx = tid; idx < TMN * KB; idx += kThreads) {
                 const int r = idx / KB, b = idx % KB;
-                const float m = sM[b];
-                sA[r][b] = (m == -INFINITY) ? 0.f : __expf(sA[r][b] - m);
+                sA[r][b] = ex2((sA[r][b] + sM[b]) * kLog2e);
             }
             for (int idx = tid; idx < TKC * KB; idx += kThreads) {
                 const int k = idx / KB, b = idx % KB;
-                const float m = sM[b];
-                sC[k][b] = (m == -INFINITY) ? 0.f : __expf(sC[k][b] + m);
+                sC[k][b] = ex2((sC[k][b] + sM[KB + b]) * kLog2e);
             }
             __syncthreads();
             const int tx = tid % 16;
             const int ty = tid / 16;
-#pragma unroll 2
+#pragma unroll 1
             for (int b = 0; b < KB; b += 4) {
                 float4 cv[FJ];
 #pragma unroll
                 for (int j = 0; j < FJ; ++j) cv[j] = *reinterpret_cast<const float4*>(&sC[tx + 16 * j][b]);
 #pragma unroll
-                for (int a = 0; a < 8; ++a) {
-                    const float4 av = *reinterpret_cast<const float4*>(&sA[ty * 8 + a][b]);
+                for (int a = 0; a < FR; ++a) {
+                    const float4 av = *reinterpret_cast<const float4*>(&sA[ty * FR + a][b]);
 #pragma unroll
                     for (int j = 0; j < FJ; ++j) {
                         acc[a][j] = fmaf(av.x, cv[j].x, acc[a][j]);
@@ -268,10 +281,10 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                 const int r = idx / NX, c4 = (idx % NX) * 4;
                 const float4 v = *reinterpret_cast<const float4*>(&sA[r][c4]);
                 const float4 m = *reinterpret_cast<const float4*>(&sM[c4]);
-                const float e0 = (m.x == -INFINITY) ? 0.f : __expf(v.x - m.x);
-                const float e1 = (m.y == -INFINITY) ? 0.f : __expf(v.y - m.y);
-                const float e2 = (m.z == -INFINITY) ? 0.f : __expf(v.z - m.z);
-                const float e3 = (m.w == -INFINITY) ? 0.f : __expf(v.w - m.w);
+                const float e0 = ex2((v.x + m.x) * kLog2e);
+                const float e1 = ex2((v.y + m.y) * kLog2e);
+                const float e2 = ex2((v.z + m.z) * kLog2e);
+                const float e3 = ex2((v.w + m.w) * kLog2e);
                 uint2 h, l;
                 if (SPLIT) {
                     split_bf16(e0, e1, h.x, l.x);
@@ -286,11 +299,11 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
             for (int idx = tid; idx < TKC * NX; idx += kThreads) {
                 const int k = idx / NX, c4 = (idx % NX) * 4;
                 const float4 v = *reinterpret_cast<const float4*>(&sC[k][c4]);
-                const float4 m = *reinterpret_cast<const float4*>(&sM[c4]);
-                const float e0 = (m.x == -INFINITY) ? 0.f : __expf(v.x + m.x);
-                const float e1 = (m.y == -INFINITY) ? 0.f : __expf(v.y + m.y);
-                const float e2 = (m.z == -INFINITY) ? 0.f : __expf(v.z + m.z);
-                const float e3 = (m.w == -INFINITY) ? 0.f : __expf(v.w + m.w);
+                const float4 m = *reinterpret_cast<const float4*>(&sM[KB + c4]);
+                const float e0 = ex2((v.x + m.x) * kLog2e);
+                const float e1 = ex2((v.y + m.y) * kLog2e);
+                const float e2 = ex2((v.z + m.z) * kLog2e);
+                const float e3 = ex2((v.w + m.w) * kLog2e);
                 uint2 h, l;
                 if (SPLIT) {
                     split_bf16(e0, e1, h.x, l.x);
@@ -304,7 +317,8 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
             }
             __syncthreads();
             const int g = lane >> 2, q = lane & 3;
-            const int mr = warp * 16 + g;
+            const int mr = (warp % 8) * 16 + g;
+            const int nw = (warp / 8) * (TKC / 2);
 #pragma unroll
             for (int kk = 0; kk < KB / 2; kk += 8) {
                 const uint32_t a0 = pA[mr * PS + kk + q], a1 = pA[(mr + 8) * PS + kk + q];
@@ -318,7 +332,7 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
                 }
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
-                    const int n = nt * 8 + g;
+                    const int n = nw + nt * 8 + g;
                     const uint32_t b0v = pC[n * PS + kk + q], b1v = pC[n * PS + kk + 4 + q];
                     mma_bf16(acc[nt], a0, a1, a2, a3, b0v, b1v);
                     if (SPLIT) {
@@ -339,15 +353,15 @@ sum_pflows_kernel(const float* __restrict__ nf, const float* __restrict__ nm, co
     if constexpr (PREC == 0) {
         const int tx = tid % 16, ty = tid / 16;
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
+        for (int a = 0; a < FR; ++a)
 #pragma unroll
-            for (int j = 0; j < FJ; ++j) red[(tx + 16 * j) * RT + ty * 8 + a] = acc[a][j];
+            for (int j = 0; j < FJ; ++j) red[(tx + 16 * j) * RT + ty * FR + a] = acc[a][j];
     } else {
         const int g = lane >> 2, q = lane & 3;
-        const int mr = warp * 16 + g;
+        const int mr = (warp % 8) * 16 + g;
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
-            const int n = nt * 8 + 2 * q;
+            const int n = (warp / 8) * (TKC / 2) + nt * 8 + 2 * q;
             red[n * RT + mr] = acc[nt][0];
             red[(n + 1) * RT + mr] = acc[nt][1];
             red[n * RT + mr + 8] = acc[nt][2];

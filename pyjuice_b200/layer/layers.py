@@ -502,6 +502,9 @@ class ProdLayer(Layer):
     """A layer of product node vectors."""
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_u_cids", "partitioned_parids")
+    # Backward: add the flows to the child rows (True) or overwrite them (False, set by the
+    # circuit for layers that are the first to write all of their child rows).
+    bk_accumulate = True
 
     def __init__(self, nodes: Sequence, global_nid_start: Optional[int] = None,
                  layer_sparsity_tol: Optional[float] = None, max_num_partitions: Optional[int] = None, **kwargs):
@@ -571,7 +574,7 @@ class ProdLayer(Layer):
             raise ValueError("node_flows and element_flows must share a row-major layout")
         nat.call("pcb_prod_gather_sum", nat.ptr(element_flows), nat.ptr(node_flows), ld, B, nat.ptr(d["bk_row"]),
                  nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]), d["bk_row"].size(0),
-                 self.block_size, 1, 1 if logspace_flows else 0, nat.stream())
+                 self.block_size, 1 if self.bk_accumulate else 0, 1 if logspace_flows else 0, nat.stream())
 
     def __repr__(self):
         return f"ProdLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
@@ -651,6 +654,8 @@ class InputLayer(Layer, torch.nn.Module):
     def init_param_flows(self, flows_memory: float = 1.0):
         if self.param_flows is None or self.param_flows.device != self.params.device:
             self.param_flows = torch.zeros([max(self.num_param_flows, 1)], device=self.params.device)
+        elif flows_memory == 0.0:
+            self.param_flows.zero_()  # write-only; same as multiplying finite flows by zero
         elif flows_memory < 1.0:
             self.param_flows.mul_(flows_memory)
 

@@ -205,7 +205,44 @@ class TensorCircuit(nn.Module):
         self._root_node_range = (self.num_nodes - self.num_root_nodes, self.num_nodes)
         self._node2tiednodes = node2tiednodes
         self._build_em_tables()
+        self._plan_node_flow_init()
         self._init_parameters()
+
+    def _plan_node_flow_init(self):
+        """Which node-flow rows the backward pass must initialise.
+
+        Product layers write the flows of their child nodes. Visited in backward order, a
+        layer none of whose target rows has been written yet overwrites them (no prior
+        zeroing needed); a layer that meets rows written before accumulates into them. Only
+        the rows that are accumulated into without an earlier writer, and the rows that no
+        product layer writes (dummy rows), are initialised by ``backward`` (the root rows
+        are set there explicitly). Results are the same as zeroing every row first.
+        """
+        written = np.zeros([self.num_nodes], dtype=bool)
+        need = np.zeros([self.num_nodes], dtype=bool)
+        for group in reversed(self.inner_layer_groups):
+            if not group.is_prod():
+                continue
+            for layer in group:
+                rows = layer._host_desc()["bk_row"].numpy().astype(np.int64)
+                tgt = (rows[:, None] + np.arange(layer.block_size)[None, :]).reshape(-1)
+                if written[tgt].any():
+                    layer.bk_accumulate = True
+                    need[tgt[~written[tgt]]] = True
+                else:
+                    layer.bk_accumulate = False
+                written[tgt] = True
+        r0, r1 = self._root_node_range
+        need |= ~written
+        need[r0:r1] = False
+        idx = np.flatnonzero(need)
+        ranges = []
+        if idx.size:
+            cuts = np.flatnonzero(np.diff(idx) != 1)
+            starts = np.concatenate([[idx[0]], idx[cuts + 1]])
+            ends = np.concatenate([idx[cuts] + 1, [idx[-1] + 1]])
+            ranges = [(int(a), int(b)) for a, b in zip(starts, ends)]
+        self._nf_init_ranges = ranges
 
     def _build_em_tables(self):
         """Per sum node block: parameter / flow base, #children, block size (untied vectors only).
@@ -483,7 +520,12 @@ class TensorCircuit(nn.Module):
             nf = self._buffer("node_flows", self.num_nodes, B, init)
             ef = self._buffer("element_flows", self.num_elements, B, init)
             if not _disable_buffer_init:
-                nf.fill_(init)
+                # only the rows that no product layer overwrites (see _plan_node_flow_init)
+                if len(self._nf_init_ranges) > 16:
+                    nf.fill_(init)
+                else:
+                    for a, b in self._nf_init_ranges:
+                        nat.call("pcb_fill_rows", nat.ptr(nf), B, a, b, init, nat.stream())
                 nat.call("pcb_fill_rows", nat.ptr(ef), B, 0, self.num_dummy_eles, init, nat.stream())
             r0, r1 = self._root_node_range
             if ll_weights is None:
@@ -585,6 +627,8 @@ class TensorCircuit(nn.Module):
         pf = self.param_flows
         if not isinstance(pf, torch.Tensor) or pf.shape != (self.num_param_flows,) or pf.device != self.device:
             self.param_flows = torch.zeros([self.num_param_flows], device=self.device)
+        elif flows_memory == 0.0:
+            self.param_flows.zero_()  # write-only; same as multiplying finite flows by zero
         elif flows_memory != 1.0:
             self.param_flows.mul_(flows_memory)
         for layer in self.input_layer_group:

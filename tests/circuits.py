@@ -39,6 +39,21 @@ def build_tiny_dag(juice, dists):
     return root
 
 
+def build_shared_child_dag(juice, dists):
+    """Inputs and sums that are children of product vectors in different product layers
+    (a sum over two decompositions of the same scope), so that the backward pass writes some
+    node flows from two layers: the first writer overwrites, the second accumulates."""
+    with juice.set_block_size(4):
+        i = [juice.inputs(v, num_node_blocks=2, dist=dists.Categorical(num_cats=4)) for v in range(4)]
+        s01 = juice.summate(juice.multiply(i[0], i[1]), num_node_blocks=2)
+        s23 = juice.summate(juice.multiply(i[2], i[3]), num_node_blocks=2)
+        s012 = juice.summate(juice.multiply(s01, i[2]), num_node_blocks=2)
+        a = juice.multiply(s012, i[3])
+        b = juice.multiply(s01, s23)
+        root = juice.summate(a, b, num_node_blocks=1, block_size=1)
+    return root
+
+
 def seeded_params(em_pbase, em_nch, em_bs, num_sum_params, in_num_nodes, in_ncats, seed: int):
     """Normalised random parameters for a compiled layout, regenerable from a seed.
 
