@@ -67,8 +67,10 @@ struct Smem {
     static constexpr int kW = WK ? RM * WROW : KMAX * WROW;
     static constexpr int kPE = NB * (KMAX / 2) * ES;
     static constexpr int kPW = NB * (KMAX / 2) * WS;
+    static constexpr int AS = TB + 4;            // epilogue rows (modes 1/2), 16-byte rows
+    static constexpr int kA = MODE >= 1 ? RM * AS : 0;
     static constexpr int oE = 0, oE2 = oE + kE, oW = oE2 + kE2, oPE = oW + kW, oPW = oPE + kPE;
-    static constexpr int oPart = oPW + kPW, oMax = oPart + kThreads, oIdx = oMax + TB;
+    static constexpr int oA = oPW + kPW, oPart = oA + kA, oMax = oPart + kThreads, oIdx = oMax + TB;
     static constexpr size_t bytes() { return 4ull * (oIdx + 2 * KMAX); }
 };
 
@@ -92,6 +94,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     float(*sW)[WROW] = reinterpret_cast<float(*)[WROW]>(sm + S::oW);
     uint32_t* pE = reinterpret_cast<uint32_t*>(sm + S::oPE);
     uint32_t* pW = reinterpret_cast<uint32_t*>(sm + S::oPW);
+    float(*sAux)[S::AS] = reinterpret_cast<float(*)[S::AS]>(sm + S::oA);
     float* sPart = sm + S::oPart;
     float* sMax = sm + S::oMax;
     int* sRow = reinterpret_cast<int*>(sm + S::oIdx);
@@ -222,6 +225,27 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             pcb::cp_async16(dstp + h * kPackHalf + c * 16, srcp + (size_t)h * 32768 + c * 16);
         }
     }
+    if constexpr (MODE >= 1) {
+        // the epilogue's element values: RM rows x TB samples, in the same batch of copies
+        constexpr int NX = TB / 4;
+        for (int idx = tid; idx < RM * NX; idx += kThreads) {
+            const int r = idx / NX;
+            const int c4 = (idx % NX) * 4;
+            const int b = b0 + c4;
+            if (r >= nrows) continue;
+            float* d = &sAux[r][c4];
+            const float* g = aux + ((int64_t)t.aux_row + r0 + r) * ld + b;
+            if (vec && b + 3 < B) {
+                pcb::cp_async16(d, g);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (b + j < B) pcb::cp_async4(d + j, g + j);
+                    else d[j] = 0.f;
+                }
+            }
+        }
+    }
     pcb::cp_async_commit();
     pcb::cp_async_wait<0>();
     __syncthreads();
@@ -295,7 +319,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                     pcb::set(o, j, (mm == -INFINITY) ? -INFINITY : logf(acc[r][j]) + mm);
                 }
             } else {
-                const float4 a = pcb::load4(aux, (int64_t)t.aux_row + row, ld, bb, B, vec, 0.f);
+                const float4 a = *reinterpret_cast<const float4*>(&sAux[rr][tx * 4]);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const float mm = sMax[tx * 4 + j];
@@ -404,7 +428,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                         } else if (MODE == 0) {
                             o[j] = (mm == -INFINITY) ? -INFINITY : __logf(v) + mm;
                         } else {
-                            const float x = (b + j < B) ? __ldg(aux + ((int64_t)t.aux_row + row) * ld + b + j) : 0.f;
+                            const float x = sAux[r][col + j];
                             o[j] = (mm == -INFINITY) ? 0.f : v * __expf(x + mm);
                         }
                     }
