@@ -189,6 +189,28 @@ int pcb_pack_weights(const float* params, const PcbLseTile* tiles, int32_t num_t
                      const int32_t* kw, int32_t w_stride, uint8_t* packed, void* stream);
 
 /*
+ * One tile table of a pcb_pack_weights_multi launch: the arguments of one
+ * pcb_pack_weights call (rows_per_block as its base-2 logarithm).
+ */
+typedef struct {
+    const PcbLseTile* tiles;
+    const int32_t* kw;
+    uint8_t* packed;             /* 16-byte aligned */
+    int32_t num_tiles;
+    int32_t rows_per_block_log2;
+    int32_t w_stride;
+    int32_t reserved;
+} PcbPackJob;
+
+/*
+ * pcb_pack_weights for several tile tables in one launch (device arrays): global tile g
+ * (g < total_tiles) is tile tile_index[g] of jobs[tile_job[g]]. The caller guarantees
+ * tile_index[g] < that job's num_tiles. Same output as one pcb_pack_weights per job.
+ */
+int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const int32_t* tile_job,
+                           const int32_t* tile_index, int32_t total_tiles, void* stream);
+
+/*
  * Same contraction and epilogues as pcb_lse_contract (BF16 forms, prec 1 or 2) on the
  * tcgen05 tensor cores with tensor-memory accumulators, for tiles of at most 128 terms,
  * using the weights packed by pcb_pack_weights from the same tile table. One CTA per

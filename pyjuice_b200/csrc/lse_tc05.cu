@@ -136,17 +136,13 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4& h, uint4& l) 
 // rows of the forward tables.
 constexpr int kPackSplit = (128 * (KT / 8)) / 256;
 
-__global__ void __launch_bounds__(256)
-pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
-                    const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
-    pcb::pdl_begin();
-    const int tile = blockIdx.x / kPackSplit;
-    const PcbLseTile t = tiles[tile];
-    uint8_t* dst = packed + (size_t)tile * kTileBytes;
+__device__ __forceinline__ void pack_tile_part(const float* __restrict__ params, const PcbLseTile& t, int rpb_log2,
+                                               const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ dst,
+                                               int part) {
     const int rpb_mask = (1 << rpb_log2) - 1;
     const int nk = min(t.k_cnt, KT);
     {
-        const int c = (blockIdx.x % kPackSplit) * 256 + threadIdx.x;
+        const int c = part * 256 + threadIdx.x;
         const int r = c % 128;
         const int kg = c / 128;
         float w[8];
@@ -162,6 +158,28 @@ pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restri
         *reinterpret_cast<uint4*>(dst + off) = h;
         *reinterpret_cast<uint4*>(dst + kHalfBytes + off) = l;
     }
+}
+
+__global__ void __launch_bounds__(256)
+pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
+                    const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
+    pcb::pdl_begin();
+    const int tile = blockIdx.x / kPackSplit;
+    pack_tile_part(params, tiles[tile], rpb_log2, kw, w_stride, packed + (size_t)tile * kTileBytes,
+                   blockIdx.x % kPackSplit);
+}
+
+// All tiles of several tile tables in one launch: global tile g is tile tile_index[g] of
+// job tile_job[g].
+__global__ void __launch_bounds__(256)
+pack_weights_multi_kernel(const float* __restrict__ params, const PcbPackJob* __restrict__ jobs,
+                          const int* __restrict__ tile_job, const int* __restrict__ tile_index) {
+    pcb::pdl_begin();
+    const int g = blockIdx.x / kPackSplit;
+    const PcbPackJob jb = jobs[tile_job[g]];
+    const int ti = tile_index[g];
+    pack_tile_part(params, jb.tiles[ti], jb.rows_per_block_log2, jb.kw, jb.w_stride,
+                   jb.packed + (size_t)ti * kTileBytes, blockIdx.x % kPackSplit);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -448,6 +466,18 @@ extern "C" int pcb_pack_weights(const float* params, const PcbLseTile* tiles, in
     return pcb::launch_status(pcb::launch_k(pack_weights_kernel, dim3((unsigned)(num_tiles * kPackSplit)), dim3(256),
                                             0, pcb::as_stream(stream), 1u, params, tiles, rpb_log2, kw, w_stride,
                                             packed), "pcb_pack_weights");
+}
+
+extern "C" int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const int32_t* tile_job,
+                                      const int32_t* tile_index, int32_t total_tiles, void* stream) {
+    if (!params || !jobs || !tile_job || !tile_index || total_tiles < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_pack_weights_multi: bad arguments");
+    if (total_tiles == 0) return PCB_OK;
+    if ((int64_t)total_tiles * kPackSplit > 2147483647)
+        return pcb::set_error(PCB_E_ARG, "pcb_pack_weights_multi: too many tiles");
+    return pcb::launch_status(pcb::launch_k(pack_weights_multi_kernel, dim3((unsigned)(total_tiles * kPackSplit)),
+                                            dim3(256), 0, pcb::as_stream(stream), 1u, params, jobs, tile_job,
+                                            tile_index), "pcb_pack_weights_multi");
 }
 
 extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld,

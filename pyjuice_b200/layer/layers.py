@@ -188,9 +188,9 @@ class SumLayer(Layer):
     bf16_form = 2
     short_kernels = True  # single-stage kernels for tiles of <= 128 terms
     tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
-    # The single-stage kernels of small layers can read pre-packed weights too; off by default:
-    # packing every layer in each pass costs more side-stream time than it saves.
-    pack_short_weights = False
+    # The single-stage kernels of small layers read pre-packed weights too (the circuit packs
+    # all layers' weights in one launch per pass, so the kernels skip their own conversion).
+    pack_short_weights = True
     # Children per parameter-flow tile (32, 64 or 128): with all children of a region in one
     # tile, its node rows are exponentiated once per sample slice instead of once per chunk.
     pflow_tile_children = 64
@@ -355,31 +355,48 @@ class SumLayer(Layer):
     def _el_tc05(self, eg, prec):
         return prec > 0 and eg["short"] and eg["tiles"].size(0) >= SumLayer.tc05_min_tiles
 
-    def pack_forward_weights(self, params: torch.Tensor, B: int, force_use_bf16: bool = False,
-                             force_use_fp32: bool = False) -> bool:
-        """Pack the weights the forward's tcgen05 kernel reads (on the current stream); returns
-        whether this layer uses them. ``forward(..., _weights_packed=True)`` then skips the pack."""
-        d = self._desc(params.device)
+    def forward_pack_job(self, device: torch.device, B: int, force_use_bf16: bool = False,
+                         force_use_fp32: bool = False):
+        """``(tiles, kw, packed, rows_per_block, w_stride)`` of the forward weights this layer
+        reads packed (tcgen05 layers; also the single-stage ones with ``pack_short_weights``),
+        or None."""
+        d = self._desc(device)
         prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
-        use = tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"])
-        if use:
-            t = d["fw_tiles"]
-            nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["kw"]), 1,
-                     nat.ptr(d["fw_pack"]), nat.stream())
-        return use
+        if tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"]):
+            return (d["fw_tiles"], d["kw"], d["fw_pack"], self.block_size, 1)
+        return None
 
-    def pack_flow_weights(self, params: torch.Tensor, B: int, force_use_fp32: bool = False) -> bool:
-        """Pack the weights of the element-flow tcgen05 kernels (see pack_forward_weights)."""
-        d = self._desc(params.device)
-        any_tc05 = False
+    def flow_pack_jobs(self, device: torch.device, B: int, force_use_fp32: bool = False):
+        """Pack jobs (see forward_pack_job) of the element-flow weights this layer reads packed."""
+        d = self._desc(device)
+        jobs = []
         for eg in d["el_groups"]:
             prec = self._el_prec(eg, B, force_use_fp32)
             if self._el_tc05(eg, prec) or (SumLayer.pack_short_weights and prec > 0 and eg["short"]):
-                et = eg["tiles"]
-                nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"], nat.ptr(eg["kw"]),
-                         self.block_size, nat.ptr(eg["pack"]), nat.stream())
-                any_tc05 = True
-        return any_tc05
+                jobs.append((eg["tiles"], eg["kw"], eg["pack"], eg["cbs"], self.block_size))
+        return jobs
+
+    @staticmethod
+    def _run_pack_job(params: torch.Tensor, job) -> None:
+        t, kw, packed, rpb, w_stride = job
+        nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), rpb, nat.ptr(kw), w_stride,
+                 nat.ptr(packed), nat.stream())
+
+    def pack_forward_weights(self, params: torch.Tensor, B: int, force_use_bf16: bool = False,
+                             force_use_fp32: bool = False) -> bool:
+        """Pack the weights the forward reads packed (on the current stream); returns whether
+        this layer uses them. ``forward(..., _weights_packed=True)`` then skips the pack."""
+        job = self.forward_pack_job(params.device, B, force_use_bf16, force_use_fp32)
+        if job is not None:
+            self._run_pack_job(params, job)
+        return job is not None
+
+    def pack_flow_weights(self, params: torch.Tensor, B: int, force_use_fp32: bool = False) -> bool:
+        """Pack the element-flow weights this layer reads packed (see pack_forward_weights)."""
+        jobs = self.flow_pack_jobs(params.device, B, force_use_fp32)
+        for job in jobs:
+            self._run_pack_job(params, job)
+        return bool(jobs)
 
     def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, params: torch.Tensor,
                 force_use_bf16: bool = False, force_use_fp32: bool = False, propagation_alg: str = "LL",

@@ -44,6 +44,11 @@ def _pc_model_backward_hook(grad, pc, inputs, record_cudagraph, apply_cudagraph,
     return None
 
 
+# One PcbPackJob record (include/pcb200.h): three pointers and four int32 fields.
+_PACK_JOB = np.dtype([("tiles", "<u8"), ("kw", "<u8"), ("packed", "<u8"), ("num_tiles", "<i4"),
+                      ("rpb_log2", "<i4"), ("w_stride", "<i4"), ("reserved", "<i4")])
+
+
 class TensorCircuit(nn.Module):
     # Side streams that the backward pass spreads the parameter-flow launches over.
     pflow_streams = 4
@@ -73,6 +78,9 @@ class TensorCircuit(nn.Module):
         self._cum_flow_dev = None
         self._side_streams = dict()
         self._dev_tables = {}
+        self._pack_tables = {}
+        self._param_epoch = 0      # bumped by every in-library write of the sum parameters
+        self._el_pack_state = None  # parameters and pass settings the element-flow packs were made for
         if device is not None:
             self.to(device)
 
@@ -349,31 +357,67 @@ class TensorCircuit(nn.Module):
             pool.append(torch.cuda.Stream(device=main.device))
         return pool[i]
 
-    def _prepack(self, side, pack_fn):
-        """Issue every sum group's weight packing on ``side`` (they only read the parameters);
-        returns {group id: event recorded after that group's packs}."""
-        events = dict()
-        with torch.cuda.stream(side):
-            for gi, group in enumerate(self.inner_layer_groups):
-                if group.is_sum() and any([pack_fn(layer) for layer in group]):
-                    ev = torch.cuda.Event()
-                    ev.record(side)
-                    events[gi] = ev
-        return events
+    def _multi_pack(self, jobs) -> bool:
+        """All given weight packs (``SumLayer.forward_pack_job`` tuples) in one launch on the
+        current stream; returns whether anything was launched."""
+        if not jobs:
+            return False
+        key = tuple(int(j[2].data_ptr()) for j in jobs)
+        tab = self._pack_tables.get(key)
+        if tab is None:
+            rec = np.zeros(len(jobs), dtype=_PACK_JOB)
+            tj, ti = [], []
+            for n, (t, kw, packed, rpb, w_stride) in enumerate(jobs):
+                if rpb <= 0 or rpb & (rpb - 1):
+                    raise ValueError("rows per block must be a power of two")
+                rec[n] = (t.data_ptr(), kw.data_ptr(), packed.data_ptr(), t.size(0), rpb.bit_length() - 1, w_stride, 0)
+                tj.append(np.full(t.size(0), n, np.int32))
+                ti.append(np.arange(t.size(0), dtype=np.int32))
+            dev = jobs[0][0].device
+            tab = (torch.from_numpy(rec.view(np.uint8).copy()).to(dev), torch.from_numpy(np.concatenate(tj)).to(dev),
+                   torch.from_numpy(np.concatenate(ti)).to(dev))
+            self._pack_tables[key] = tab
+        nat.call("pcb_pack_weights_multi", nat.ptr(self.params), nat.ptr(tab[0]), nat.ptr(tab[1]), nat.ptr(tab[2]),
+                 tab[1].size(0), nat.stream())
+        return True
+
+    def _pack_state_key(self, B: int, force_use_fp32: bool):
+        """What the element-flow packs depend on: the parameter values (storage, torch version
+        counter, in-library writes) and the settings that select the packed layers."""
+        return (self.params.data_ptr(), self.params._version, self._param_epoch, B, bool(force_use_fp32),
+                SumLayer.bf16_form, SumLayer.pack_short_weights, SumLayer.tc05_min_tiles)
 
     def _run_inner_forward(self, force_use_bf16, force_use_fp32, propagation_alg, **kwargs):
+        # The weights that the sum kernels read packed are packed on a side stream in two
+        # launches: the forward's (waited for before the first layer that reads them) and the
+        # element-flow weights of the backward pass that follows (joined at the end).
         main = torch.cuda.current_stream()
         side = self._side_stream(main)
         side.wait_stream(main)
         B = self.node_mars.size(1)
-        packed = self._prepack(side, lambda layer: layer.pack_forward_weights(self.params, B, force_use_bf16,
-                                                                              force_use_fp32))
+        fw_jobs, el_jobs, fw_groups = [], [], set()
+        for gi, group in enumerate(self.inner_layer_groups):
+            if group.is_sum():
+                for layer in group:
+                    job = layer.forward_pack_job(self.device, B, force_use_bf16, force_use_fp32)
+                    if job is not None:
+                        fw_jobs.append(job)
+                        fw_groups.add(gi)
+                    el_jobs += layer.flow_pack_jobs(self.device, B, force_use_fp32)
+        fw_ready = None
+        with torch.cuda.stream(side):
+            if self._multi_pack(fw_jobs):
+                fw_ready = torch.cuda.Event()
+                fw_ready.record(side)
+            self._multi_pack(el_jobs)
+        self._el_pack_state = self._pack_state_key(B, force_use_fp32)
         for gi, group in enumerate(self.inner_layer_groups):
             if group.is_prod():
                 group(self.node_mars, self._em_view(gi))
             else:
-                if gi in packed:
-                    main.wait_event(packed[gi])
+                if gi in fw_groups and fw_ready is not None:
+                    main.wait_event(fw_ready)
+                    fw_ready = None
                 group(self.node_mars, self._em_view(gi - 1), self.params, force_use_bf16=force_use_bf16,
                       force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, _weights_packed=True,
                       **kwargs)
@@ -464,7 +508,17 @@ class TensorCircuit(nn.Module):
         for side in sides:
             side.wait_stream(main)
         B = self.node_mars.size(1)
-        packed = self._prepack(sides[0], lambda layer: layer.pack_flow_weights(self.params, B, force_use_fp32))
+        # Element-flow weights: packed by the forward pass when the parameters have not changed
+        # since (the state is set by the forward only, so that every run of a captured backward
+        # makes the same choice); otherwise packed here in one launch.
+        el_ready = None
+        if self._el_pack_state != self._pack_state_key(B, force_use_fp32):
+            el_jobs = [job for group in self.inner_layer_groups if group.is_sum() for layer in group
+                       for job in layer.flow_pack_jobs(self.device, B, force_use_fp32)]
+            with torch.cuda.stream(sides[0]):
+                if self._multi_pack(el_jobs):
+                    el_ready = torch.cuda.Event()
+                    el_ready.record(sides[0])
         kwargs = dict(kwargs, _weights_packed=True)
         turn = 0
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
@@ -478,8 +532,9 @@ class TensorCircuit(nn.Module):
                 # the two flow kernels read one row per node instead of two.
                 modify = allow_modify_flows and any(
                     layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles for layer in group)
-                if layer_id in packed:
-                    main.wait_event(packed[layer_id])
+                if el_ready is not None:
+                    main.wait_event(el_ready)
+                    el_ready = None
                 group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
@@ -607,12 +662,14 @@ class TensorCircuit(nn.Module):
             nat.call("pcb_sum_em", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(t["pbase"]),
                      nat.ptr(t["pfbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0), float(step_size),
                      float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
+            self._param_epoch += 1
 
     def normalize_parameters(self, pseudocount: float = 0.0):
         """Renormalise the sum parameters in place on the device (FP64)."""
         t = self._tables()
         nat.call("pcb_sum_normalize", nat.ptr(self.params), nat.ptr(t["pbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]),
                  t["nch"].size(0), float(pseudocount), nat.stream())
+        self._param_epoch += 1
 
     def cumulate_flows(self, inputs: torch.Tensor):
         with torch.no_grad():

@@ -175,6 +175,72 @@ def test_recorded_backward_matches_eager(cuda_device):
     assert torch.equal(pf_e, pf_r)
 
 
+def test_multi_pack_equals_per_layer_packs(cuda_device):
+    """One pcb_pack_weights_multi launch writes the same bytes as one pcb_pack_weights per
+    tile table (forward and element-flow tables of every sum layer)."""
+    from pyjuice_b200.layer.layers import SumLayer
+    fx = load_fixture("hclt784")
+    pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    saved = SumLayer.pack_short_weights
+    try:
+        SumLayer.pack_short_weights = True
+        jobs = []
+        for group in pc.inner_layer_groups:
+            if group.is_sum():
+                for layer in group:
+                    job = layer.forward_pack_job(pc.device, 512, force_use_bf16=True)
+                    jobs += ([job] if job is not None else []) + layer.flow_pack_jobs(pc.device, 512)
+        assert len(jobs) > 20
+        ref = []
+        for job in jobs:
+            job[2].fill_(7)
+            SumLayer._run_pack_job(pc.params, job)
+            ref.append(job[2].clone())
+            job[2].zero_()
+        assert pc._multi_pack(jobs)
+        torch.cuda.synchronize()
+        for job, r in zip(jobs, ref):
+            assert torch.equal(job[2], r)
+    finally:
+        SumLayer.pack_short_weights = saved
+
+
+@pytest.mark.parametrize("change", ["torch_write", "em"])
+def test_backward_repacks_after_parameter_change(change, cuda_device):
+    """The element-flow weights packed by a forward pass are reused by the backward pass only
+    while the parameters are unchanged: after an in-place torch write or an EM step between
+    the two passes, the backward packs again (same flows as a forced repack)."""
+    from pyjuice_b200.layer.layers import SumLayer
+    fx = load_fixture("hclt784")
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    saved = SumLayer.pack_short_weights
+    try:
+        SumLayer.pack_short_weights = True
+        out = []
+        for force in (False, True):
+            pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+            load_fixture_params(pc, fx)
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                pc(x, force_use_bf16=True)
+            pc.backward(inputs=x, allow_modify_flows=True)
+            if change == "em":
+                pc.mini_batch_em(step_size=0.5, pseudocount=0.01)
+            else:
+                with torch.no_grad():
+                    pc.params.mul_(torch.linspace(0.5, 1.5, pc.params.numel(), device=cuda_device))
+            pc.init_param_flows(flows_memory=0.0)
+            if force:
+                pc._el_pack_state = None
+            pc.backward(inputs=x, allow_modify_flows=True)
+            torch.cuda.synchronize()
+            out.append(pc.param_flows.clone())
+        assert torch.equal(out[0], out[1])
+    finally:
+        SumLayer.pack_short_weights = saved
+
+
 def test_deterministic_flows(cuda_device):
     """Parameter flows carry no float atomics on untied circuits: two runs are bit-identical."""
     fx = load_fixture("hclt64")
