@@ -213,12 +213,14 @@ int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const in
 /*
  * Same contraction and epilogues as pcb_lse_contract (BF16 forms, prec 1 or 2) on the
  * tcgen05 tensor cores with tensor-memory accumulators, for tiles of at most 128 terms,
- * using the weights packed by pcb_pack_weights from the same tile table. One CTA per
- * tile and batch_tile (32 or 64) samples. A tile with more terms produces NaN rows.
+ * using the weights packed by pcb_pack_weights from the same tile table. One CTA per tile
+ * and run of slices_per_cta consecutive batch_tile-sample slices (batch_tile 32 or 64):
+ * the packed weights are copied once per CTA, and the next slice's source values are
+ * loaded while the current slice is processed. A tile with more terms produces NaN rows.
  */
 int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
                           const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles, const int32_t* krow,
-                          int32_t mode, int32_t prec, int32_t batch_tile, void* stream);
+                          int32_t mode, int32_t prec, int32_t batch_tile, int32_t slices_per_cta, void* stream);
 
 /*
  * In place on rows [row0, row1) of node_flows: f <- (m == -inf) ? -inf : log(f) - m.

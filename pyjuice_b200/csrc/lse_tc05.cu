@@ -11,21 +11,26 @@
 //    remainder (lo), written once per pass in the canonical no-swizzle K-major layout of a
 //    128 x 128 UMMA operand (8 x 8 core matrices of 128 contiguous bytes; adjacent core
 //    matrices 128 bytes apart along K and 2048 bytes apart along the rows).
-//  * contract: one CTA of 128 threads per (tile, N-sample slice). One thread starts a bulk
-//    copy of the packed weights into shared memory (mbarrier completion) while all threads
-//    load their source values straight into registers, reduce the per-sample max,
-//    exponentiate and write the B operand (bf16 hi and lo) in the canonical no-swizzle
-//    MN-major layout. One thread then issues the MMAs (M = 128 rows, N samples, K = 16 per
-//    instruction; three per step in the split form: hi*hi + lo*hi + hi*lo), commits them
-//    to an mbarrier, and every warp reads its 32 accumulator rows back from tensor memory
-//    for the epilogue. Every wait is bounded; a CTA whose wait runs out writes NaN rows.
+//  * contract: one CTA of 512 threads (256 for 32-sample slices) per tile and run of
+//    consecutive N-sample slices. One thread starts a bulk copy of the packed weights into
+//    shared memory (mbarrier completion, once per CTA). Per slice, all threads hold their
+//    source values in registers (the next slice's values are loaded while this one is
+//    processed), reduce the per-sample max, exponentiate and write the B operand (bf16 hi
+//    and lo) in the canonical no-swizzle MN-major layout. One thread then issues the MMAs
+//    (M = 128 rows, N samples, K = 16 per instruction; three per step in the split form:
+//    hi*hi + lo*hi + hi*lo) and commits them to an mbarrier. Every warp then reads its
+//    accumulator rows and columns back from tensor memory for the epilogue. Every wait is
+//    bounded; a CTA whose wait runs out writes NaN rows.
+//
+// These kernels serve the BF16 forms only: their logarithms use the hardware approximation
+// (__logf, absolute error ~1e-6, far below the bf16 operand rounding), which halves the
+// instruction count of the epilogue.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
 
 namespace {
 
-constexpr int kThreads = 128;
 constexpr int KT = 128;                      // terms per tile (zero padded)
 constexpr uint32_t kHalfBytes = 128 * KT * 2;  // one bf16 copy of a 128 x 128 operand
 constexpr uint32_t kTileBytes = 2 * kHalfBytes;  // hi + lo
@@ -183,30 +188,48 @@ pack_weights_multi_kernel(const float* __restrict__ params, const PcbPackJob* __
 }
 
 // ---------------------------------------------------------------------------------------
+// Threads of the contraction kernel: 16 warps for 64-sample slices, 8 for 32 (two CTAs per
+// SM by shared memory; each warp's epilogue reads 16 accumulator columns).
+template <int N>
+constexpr int tc05_threads() { return N == 64 ? 512 : 256; }
+
 template <int N>
 struct Tc05Smem {
+    static constexpr int W = tc05_threads<N>() / 32;
     static constexpr uint32_t oW = 0;                       // packed weights (hi, lo)
     static constexpr uint32_t oE = kTileBytes;              // B operand (hi, lo): N x 128 bf16 each
     static constexpr uint32_t kEHalf = (uint32_t)N * KT * 2;
-    static constexpr uint32_t oPart = oE + 2 * kEHalf;      // [4][N] partial maxima
-    static constexpr uint32_t oMax = oPart + 4 * N * 4;     // [N]
+    static constexpr uint32_t oPart = oE + 2 * kEHalf;      // [W][N] partial maxima
+    static constexpr uint32_t oMax = oPart + W * N * 4;     // [N]
     static constexpr uint32_t oRow = oMax + N * 4;          // [128] source rows
     static constexpr uint32_t oBar = oRow + KT * 4;         // two mbarriers
     static constexpr uint32_t oSlot = oBar + 16;            // tensor-memory address, failure flag
     static constexpr size_t bytes() { return oSlot + 16; }
 };
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
+// One CTA per tile and run of up to spc consecutive N-sample slices. The packed weights are
+// copied once per CTA; the source values (and epilogue element values) of slice s + 1 are
+// prefetched into L2 while slice s is reduced, exponentiated, contracted and written out.
 template <int N, int MODE, bool SPLIT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(tc05_threads<N>(), 2)
 lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const uint8_t* __restrict__ packed,
-                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, bool vec) {
-    pcb::pdl_begin();
+                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, int spc, bool vec) {
+    // tile and term indices (compiled tables) before the wait for the previous kernel
+    pcb::pdl_trigger();
     static_assert(N == 32 || N == 64, "sample slice");
     using S = Tc05Smem<N>;
+    constexpr int W = S::W;             // warps
     constexpr int NQ = N / 32;          // groups of 4 x 8 samples
-    constexpr int WPQ = 4 / NQ;         // warps per group
-    constexpr int ITER = N / 8;         // 16-byte chunks per thread
+    constexpr int WPQ = W / NQ;         // warps per group
+    constexpr int ITER = KT / (8 * WPQ);  // 8-term groups (16-byte chunks) per thread
+    constexpr int CW = N / (W / 4);     // accumulator columns per warp in the epilogue
+    constexpr int NH = MODE == 2 ? 2 : 1;  // source arrays (flows and mars in mode 2)
+    static_assert(ITER >= 1 && CW % 16 == 0, "thread layout");
     extern __shared__ __align__(1024) uint8_t sm[];
     float* sPart = reinterpret_cast<float*>(sm + S::oPart);
     float* sMax = reinterpret_cast<float*>(sm + S::oMax);
@@ -217,12 +240,15 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
 
     const int tile_id = blockIdx.x;
     const PcbLseTile t = tiles[tile_id];
-    const int b0 = blockIdx.y * N;
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const bool bad = t.k_cnt > KT;
     const int nk = bad ? 0 : t.k_cnt;
+    const int s0 = blockIdx.y * spc;
+    const int nsl = min(spc, (B + N - 1) / N - s0);
+    if (tid < nk) sRow[tid] = __ldg(krow + t.k_off + tid);
+    pcb::pdl_wait();
 
     if (warp == 0) {
         tmem_alloc(slot, N);
@@ -234,183 +260,223 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
         slot[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (tid < nk) sRow[tid] = __ldg(krow + t.k_off + tid);
-    __syncthreads();
-    if (tid == 0) {
-        const uint32_t wbytes = SPLIT ? kTileBytes : kHalfBytes;
-        mbar_expect_tx(barW, wbytes);
-        if (SPLIT) {
-            bulk_copy_g2s(sm + S::oW, packed + (size_t)tile_id * kTileBytes, kTileBytes, barW);
-        } else {
-            bulk_copy_g2s(sm + S::oW, packed + (size_t)tile_id * kTileBytes, kHalfBytes, barW);
-        }
-    }
-
-    // ---- source values: chunk (k, 8 samples) per thread and step ----
-    const int nq = warp % NQ;
-    const int n8 = nq * 4 + (lane >> 3);      // this thread's 8-sample group
-    const int kl = lane & 7;
-    const int bb = b0 + n8 * 8;
-    float v[ITER][8];
-#pragma unroll
-    for (int it = 0; it < ITER; ++it) {
-        const int k = ((warp / NQ) + it * WPQ) * 8 + kl;
-        if (k < nk) {
-            const int64_t off = (int64_t)sRow[k] * ld + bb;
-#pragma unroll
-            for (int h = 0; h < (MODE == 2 ? 2 : 1); ++h) {
-                const float* g = (h == 0 ? src : src2) + off;
-                float x[8];
-                if (vec && bb + 7 < B) {
-                    const float4 a = __ldg(reinterpret_cast<const float4*>(g));
-                    const float4 c = __ldg(reinterpret_cast<const float4*>(g + 4));
-                    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = c.x; x[5] = c.y; x[6] = c.z; x[7] = c.w;
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) x[j] = (bb + j < B) ? __ldg(g + j) : -INFINITY;
-                }
-                if (h == 0) {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) v[it][j] = x[j];
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) v[it][j] = (x[j] == -INFINITY) ? -INFINITY : logf(v[it][j]) - x[j];
-                }
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) v[it][j] = -INFINITY;
-        }
-    }
-    // per-sample max: over this thread's terms, the 8 lanes of the group, then the warps
-    float m[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float x = v[0][j];
-#pragma unroll
-        for (int it = 1; it < ITER; ++it) x = fmaxf(x, v[it][j]);
-        x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 1));
-        x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 2));
-        x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 4));
-        m[j] = x;
-    }
-    if (kl == 0) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) sPart[(warp / NQ) * N + n8 * 8 + j] = m[j];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float x = sPart[n8 * 8 + j];
-#pragma unroll
-        for (int w = 1; w < WPQ; ++w) x = fmaxf(x, sPart[w * N + n8 * 8 + j]);
-        m[j] = x;
-    }
-    if (warp / NQ == 0 && kl == 0) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) sMax[n8 * 8 + j] = m[j];
-    }
-    // ---- exponentiate; B operand in the MN-major core-matrix layout ----
-    uint8_t* eh = sm + S::oE;
-    uint8_t* el = eh + S::kEHalf;
-#pragma unroll
-    for (int it = 0; it < ITER; ++it) {
-        const int k = ((warp / NQ) + it * WPQ) * 8 + kl;
-        float e[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) e[j] = (m[j] == -INFINITY) ? 0.f : __expf(v[it][j] - m[j]);
-        const uint32_t off = (uint32_t)n8 * kSBO + (uint32_t)(k >> 3) * kLBO + (uint32_t)(k & 7) * 16;
-        if (SPLIT) {
-            uint4 h, l;
-            split8(e, h, l);
-            *reinterpret_cast<uint4*>(eh + off) = h;
-            *reinterpret_cast<uint4*>(el + off) = l;
-        } else {
-            *reinterpret_cast<uint4*>(eh + off) =
-                make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
-        }
-    }
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t taddr = slot[0];
-
-    // ---- one thread issues the MMAs ----
     if (tid == 0) {
-        const bool wok = mbar_wait_bounded(barW, 0);
-        if (wok) {
-            constexpr uint32_t idesc = make_idesc<N>();
-            const uint32_t aw = smem_u32(sm + S::oW);
-            const uint32_t ae = smem_u32(eh);
-            const int ks = (nk + 15) / 16;
-            for (int s = 0; s < ks; ++s) {
-                const uint32_t o = (uint32_t)s * 2 * kLBO;
-                mma_bf16_ss(taddr, make_desc(aw + o), make_desc(ae + o), idesc, s > 0 ? 1u : 0u);
-                if (SPLIT) {
-                    mma_bf16_ss(taddr, make_desc(aw + kHalfBytes + o), make_desc(ae + o), idesc, 1u);
-                    mma_bf16_ss(taddr, make_desc(aw + o), make_desc(ae + S::kEHalf + o), idesc, 1u);
-                }
-            }
-        } else {
-            slot[1] = 1;
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         smem_u32(barM))
-                     : "memory");
+        const uint32_t wbytes = SPLIT ? kTileBytes : kHalfBytes;
+        mbar_expect_tx(barW, wbytes);
+        bulk_copy_g2s(sm + S::oW, packed + (size_t)tile_id * kTileBytes, wbytes, barW);
     }
-    const bool mok = mbar_wait_bounded(barM, 0);
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const bool fail = !mok || slot[1] != 0 || bad;
 
-    // ---- epilogue: warp w owns accumulator rows 32 w .. 32 w + 31 ----
-    const int r = warp * 32 + lane;
-    float acc[N];
+    // thread layout of the source values: term chunk (k, 8 samples) per thread and step
+    const int nq = warp % NQ;
+    const int n8 = nq * 4 + (lane >> 3);      // this thread's 8-sample group
+    const int kl = lane & 7;
+    // epilogue: warp w owns accumulator rows 32 (w % 4) .. + 31 (its lane quarter) and
+    // columns (w / 4) CW .. + CW
+    const int q = warp & 3;
+    const int cb = (warp >> 2) * CW;
+    const int r = q * 32 + lane;
+
+    auto load_slice = [&](int sl, float (&v)[NH][ITER][8]) {
+        const int bb = (s0 + sl) * N + n8 * 8;
 #pragma unroll
-    for (int c = 0; c < N / 16; ++c) {
-        float x[16];
-        tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 16), x);
+        for (int it = 0; it < ITER; ++it) {
+            const int k = ((warp / NQ) + it * WPQ) * 8 + kl;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[c * 16 + i] = x[i];
-    }
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    if (r < t.n_rows) {
-        const int row = r;
-        float* dst = out + ((int64_t)t.out_row + row) * ld + b0;
-        const float* ax = (MODE == 0) ? nullptr : aux + ((int64_t)t.aux_row + row) * ld + b0;
+            for (int h = 0; h < NH; ++h) {
+                if (k < nk) {
+                    const float* g = (h == 0 ? src : src2) + (int64_t)sRow[k] * ld + bb;
+                    if (vec && bb + 7 < B) {
+                        const float4 a = __ldg(reinterpret_cast<const float4*>(g));
+                        const float4 c = __ldg(reinterpret_cast<const float4*>(g + 4));
+                        v[h][it][0] = a.x; v[h][it][1] = a.y; v[h][it][2] = a.z; v[h][it][3] = a.w;
+                        v[h][it][4] = c.x; v[h][it][5] = c.y; v[h][it][6] = c.z; v[h][it][7] = c.w;
+                    } else {
 #pragma unroll
-        for (int c4 = 0; c4 < N / 4; ++c4) {
-            float o[4];
-            float a[4] = {0.f, 0.f, 0.f, 0.f};
-            const int b = b0 + c4 * 4;
-            if (MODE != 0) {
-                if (vec && b + 3 < B) {
-                    const float4 av = __ldg(reinterpret_cast<const float4*>(ax + c4 * 4));
-                    a[0] = av.x; a[1] = av.y; a[2] = av.z; a[3] = av.w;
+                        for (int j = 0; j < 8; ++j) v[h][it][j] = (bb + j < B) ? __ldg(g + j) : -INFINITY;
+                    }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) a[j] = (b + j < B) ? __ldg(ax + c4 * 4 + j) : 0.f;
+                    for (int j = 0; j < 8; ++j) v[h][it][j] = -INFINITY;
                 }
             }
+        }
+    };
+
+    // the next slice's rows into L2 (one prefetch per 32-byte sector this thread will read)
+    auto prefetch_slice = [&](int sl) {
+        const int bb = (s0 + sl) * N + n8 * 8;
+        if (bb < B) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float mm = sMax[c4 * 4 + j];
-                const float val = acc[c4 * 4 + j];
-                if (fail) o[j] = __int_as_float(0x7fc00000);
-                else if (MODE == 0) o[j] = (mm == -INFINITY) ? -INFINITY : logf(val) + mm;
-                else o[j] = (mm == -INFINITY) ? 0.f : val * __expf(a[j] + mm);
-            }
-            if (vec && b + 3 < B) {
-                *reinterpret_cast<float4*>(dst + c4 * 4) = make_float4(o[0], o[1], o[2], o[3]);
-            } else {
+            for (int it = 0; it < ITER; ++it) {
+                const int k = ((warp / NQ) + it * WPQ) * 8 + kl;
+                if (k < nk) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (b + j < B) dst[c4 * 4 + j] = o[j];
+                    for (int h = 0; h < NH; ++h) prefetch_l2((h == 0 ? src : src2) + (int64_t)sRow[k] * ld + bb);
+                }
             }
         }
+        if (MODE != 0 && r < t.n_rows) {
+            const int b = (s0 + sl) * N + cb;
+#pragma unroll
+            for (int c8 = 0; c8 < CW / 8; ++c8)
+                if (b + c8 * 8 < B) prefetch_l2(aux + ((int64_t)t.aux_row + r) * ld + b + c8 * 8);
+        }
+    };
+
+    float cur[NH][ITER][8];
+    bool fail = bad;
+    for (int sl = 0; sl < nsl; ++sl) {
+        const int b0 = (s0 + sl) * N;
+        if (sl == 0) prefetch_slice(0);
+        load_slice(sl, cur);
+        if (sl + 1 < nsl) prefetch_slice(sl + 1);
+        // mode 2: node flows -> log f - log m
+        float v[ITER][8];
+#pragma unroll
+        for (int it = 0; it < ITER; ++it)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (MODE == 2) {
+                    const float m2 = cur[NH - 1][it][j];
+                    v[it][j] = (m2 == -INFINITY) ? -INFINITY : __logf(cur[0][it][j]) - m2;
+                } else {
+                    v[it][j] = cur[0][it][j];
+                }
+            }
+        // per-sample max: over this thread's terms, the 8 lanes of the group, then the warps
+        float m[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float x = v[0][j];
+#pragma unroll
+            for (int it = 1; it < ITER; ++it) x = fmaxf(x, v[it][j]);
+            x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 1));
+            x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 2));
+            x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, 4));
+            m[j] = x;
+        }
+        if (kl == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) sPart[(warp / NQ) * N + n8 * 8 + j] = m[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float x = sPart[n8 * 8 + j];
+#pragma unroll
+            for (int w = 1; w < WPQ; ++w) x = fmaxf(x, sPart[w * N + n8 * 8 + j]);
+            m[j] = x;
+        }
+        if (warp / NQ == 0 && kl == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) sMax[n8 * 8 + j] = m[j];
+        }
+        // exponentiate; B operand in the MN-major core-matrix layout (the previous slice's
+        // MMAs have completed: its epilogue waited for them)
+        uint8_t* eh = sm + S::oE;
+        uint8_t* el = eh + S::kEHalf;
+#pragma unroll
+        for (int it = 0; it < ITER; ++it) {
+            const int k = ((warp / NQ) + it * WPQ) * 8 + kl;
+            float e[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) e[j] = (m[j] == -INFINITY) ? 0.f : __expf(v[it][j] - m[j]);
+            const uint32_t off = (uint32_t)n8 * kSBO + (uint32_t)(k >> 3) * kLBO + (uint32_t)(k & 7) * 16;
+            if (SPLIT) {
+                uint4 h, l;
+                split8(e, h, l);
+                *reinterpret_cast<uint4*>(eh + off) = h;
+                *reinterpret_cast<uint4*>(el + off) = l;
+            } else {
+                *reinterpret_cast<uint4*>(eh + off) =
+                    make_uint4(pack2(e[0], e[1]), pack2(e[2], e[3]), pack2(e[4], e[5]), pack2(e[6], e[7]));
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+        // ---- one thread issues the MMAs ----
+        if (tid == 0) {
+            if (sl == 0 && !mbar_wait_bounded(barW, 0)) slot[1] = 1;
+            if (slot[1] == 0) {
+                constexpr uint32_t idesc = make_idesc<N>();
+                const uint32_t aw = smem_u32(sm + S::oW);
+                const uint32_t ae = smem_u32(eh);
+                const int ks = (nk + 15) / 16;
+                for (int s = 0; s < ks; ++s) {
+                    const uint32_t o = (uint32_t)s * 2 * kLBO;
+                    mma_bf16_ss(taddr, make_desc(aw + o), make_desc(ae + o), idesc, s > 0 ? 1u : 0u);
+                    if (SPLIT) {
+                        mma_bf16_ss(taddr, make_desc(aw + kHalfBytes + o), make_desc(ae + o), idesc, 1u);
+                        mma_bf16_ss(taddr, make_desc(aw + o), make_desc(ae + S::kEHalf + o), idesc, 1u);
+                    }
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(barM))
+                         : "memory");
+        }
+        const bool mok = mbar_wait_bounded(barM, (uint32_t)(sl & 1));
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        fail = fail || !mok || slot[1] != 0;
+
+        // ---- epilogue ----
+        float a[CW];  // element values of this slice (modes 1/2; in L2 by the prefetch)
+        if (MODE != 0) {
+            const float* ax = aux + ((int64_t)t.aux_row + (r < t.n_rows ? r : 0)) * ld + b0 + cb;
+#pragma unroll
+            for (int c4 = 0; c4 < CW / 4; ++c4) {
+                const int b = b0 + cb + c4 * 4;
+                if (vec && b + 3 < B) {
+                    const float4 av = __ldg(reinterpret_cast<const float4*>(ax + c4 * 4));
+                    a[c4 * 4] = av.x; a[c4 * 4 + 1] = av.y; a[c4 * 4 + 2] = av.z; a[c4 * 4 + 3] = av.w;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) a[c4 * 4 + j] = (b + j < B) ? __ldg(ax + c4 * 4 + j) : 0.f;
+                }
+            }
+        }
+        float acc[CW];
+#pragma unroll
+        for (int c = 0; c < CW / 16; ++c) {
+            float x[16];
+            tmem_ld16(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(cb + c * 16), x);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[c * 16 + i] = x[i];
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (r < t.n_rows) {
+            float* dst = out + ((int64_t)t.out_row + r) * ld + b0 + cb;
+#pragma unroll
+            for (int c4 = 0; c4 < CW / 4; ++c4) {
+                float o[4];
+                const int b = b0 + cb + c4 * 4;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float mm = sMax[cb + c4 * 4 + j];
+                    const float val = acc[c4 * 4 + j];
+                    if (fail) o[j] = __int_as_float(0x7fc00000);
+                    else if (MODE == 0) o[j] = (mm == -INFINITY) ? -INFINITY : __logf(val) + mm;
+                    else o[j] = (mm == -INFINITY) ? 0.f : val * __expf(a[c4 * 4 + j] + mm);
+                }
+                if (vec && b + 3 < B) {
+                    *reinterpret_cast<float4*>(dst + c4 * 4) = make_float4(o[0], o[1], o[2], o[3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (b + j < B) dst[c4 * 4 + j] = o[j];
+                }
+            }
+        }
+        // the next slice rewrites the partial maxima, the B operand and the accumulators
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
     }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
     if (warp == 0) tmem_dealloc(taddr, N);
 }
 
@@ -421,8 +487,8 @@ int current_device() {
 }
 
 template <int N, int MODE, bool SPLIT>
-int launch(int num_tiles, const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
-           const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s, bool vec) {
+int launch(int num_tiles, int spc, const float* src, const float* src2, const float* aux, float* out, int64_t ld,
+           int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s, bool vec) {
     constexpr size_t smem = Tc05Smem<N>::bytes();
     static_assert(smem <= 227 * 1024, "shared memory");
     static bool configured[64] = {false};
@@ -433,19 +499,19 @@ int launch(int num_tiles, const float* src, const float* src2, const float* aux,
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract_tc05: %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
-    const int64_t gy = pcb::cdiv(B, N);
+    const int64_t gy = pcb::cdiv(pcb::cdiv(B, N), spc);
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: batch too large");
     return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, SPLIT>,
-                                            dim3((unsigned)num_tiles, (unsigned)gy), dim3(kThreads), smem, s,
-                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, vec),
+                                            dim3((unsigned)num_tiles, (unsigned)gy), dim3(tc05_threads<N>()), smem, s,
+                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec),
                               "pcb_lse_contract_tc05");
 }
 
 template <int N>
-int launch_n(int mode, bool split, int num_tiles, const float* src, const float* src2, const float* aux, float* out,
-             int64_t ld, int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s,
-             bool vec) {
-#define PCB_TC(M, SP) launch<N, M, SP>(num_tiles, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec)
+int launch_n(int mode, bool split, int num_tiles, int spc, const float* src, const float* src2, const float* aux,
+             float* out, int64_t ld, int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow,
+             cudaStream_t s, bool vec) {
+#define PCB_TC(M, SP) launch<N, M, SP>(num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec)
     if (split) return mode == 0 ? PCB_TC(0, true) : (mode == 1 ? PCB_TC(1, true) : PCB_TC(2, true));
     return mode == 0 ? PCB_TC(0, false) : (mode == 1 ? PCB_TC(1, false) : PCB_TC(2, false));
 #undef PCB_TC
@@ -483,16 +549,18 @@ extern "C" int pcb_pack_weights_multi(const float* params, const PcbPackJob* job
 extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
                                      int32_t B, const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles,
                                      const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
-                                     void* stream) {
+                                     int32_t slices_per_cta, void* stream) {
     if (!src || !out || !packed || !tiles || !krow || B <= 0 || ld < B || num_tiles < 0 || mode < 0 || mode > 2 ||
         (mode == 2 && !src2) || (mode >= 1 && !aux) || prec < 1 || prec > 2 ||
-        (batch_tile != 32 && batch_tile != 64) || (reinterpret_cast<uintptr_t>(packed) & 15) != 0)
+        (batch_tile != 32 && batch_tile != 64) || slices_per_cta < 1 || (reinterpret_cast<uintptr_t>(packed) & 15) != 0)
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: bad arguments");
     if (num_tiles == 0) return PCB_OK;
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!src2 || pcb::vec_ok(src2, ld)) &&
                      (!aux || pcb::vec_ok(aux, ld));
     cudaStream_t s = pcb::as_stream(stream);
     const bool split = prec == 2;
-    if (batch_tile == 32) return launch_n<32>(mode, split, num_tiles, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
-    return launch_n<64>(mode, split, num_tiles, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
+    const int spc = slices_per_cta;
+    if (batch_tile == 32)
+        return launch_n<32>(mode, split, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
+    return launch_n<64>(mode, split, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
 }

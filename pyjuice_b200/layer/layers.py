@@ -68,6 +68,22 @@ def _tc05_batch_tile(num_tiles: int, B: int) -> int:
     return 64 if num_tiles * -(-B // 64) >= 2 * _num_sms() else 32
 
 
+def _tc05_slices_per_cta(num_tiles: int, B: int, batch_tile: int) -> int:
+    """Sample slices per CTA for pcb_lse_contract_tc05. One, unless SumLayer.tc05_slices_per_cta
+    says otherwise: on HCLT-784 (B = 512) runs of 4 slices per CTA (weights copied once, the
+    next slice prefetched into L2) measured no faster than one CTA per slice."""
+    return SumLayer.tc05_slices_per_cta or 1
+
+
+def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream):
+    """One tcgen05 contraction (pcb_lse_contract_tc05) with the batch tile and slices per CTA
+    chosen for the layer's tile count."""
+    bt = _tc05_batch_tile(tiles.size(0), B)
+    nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B, nat.ptr(pack),
+             nat.ptr(tiles), tiles.size(0), nat.ptr(krow), mode, prec, bt, _tc05_slices_per_cta(tiles.size(0), B, bt),
+             stream)
+
+
 def _rows_vec4(tiles: np.ndarray, kw: np.ndarray, rpb: int, w_stride: int) -> bool:
     """Weights of 4 consecutive rows are consecutive and 16-byte aligned (forward tables)."""
     return (w_stride == 1 and rpb % 4 == 0 and bool(np.all(kw % 4 == 0)) and bool(np.all(tiles[:, 4] % 4 == 0))
@@ -188,6 +204,7 @@ class SumLayer(Layer):
     bf16_form = 2
     short_kernels = True  # single-stage kernels for tiles of <= 128 terms
     tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
+    tc05_slices_per_cta = None  # sample slices per tcgen05 CTA (None: one)
     # The single-stage kernels of small layers read pre-packed weights too (the circuit packs
     # all layers' weights in one launch per pass, so the kernels skip their own conversion).
     pack_short_weights = True
@@ -417,9 +434,7 @@ class SumLayer(Layer):
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
                 _weights_packed = True
-            nat.call("pcb_lse_contract_tc05", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
-                     nat.ptr(node_mars), ld, B, nat.ptr(d["fw_pack"]), nat.ptr(t), t.size(0), nat.ptr(d["krow"]), 0,
-                     prec, _tc05_batch_tile(t.size(0), B), st)
+            _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st)
             return
         if d["fw_short"] and SumLayer.short_kernels:
             packed = d["fw_pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
@@ -470,11 +485,8 @@ class SumLayer(Layer):
             prec = self._el_prec(eg, B, force_use_fp32)
             if self._el_tc05(eg, prec):
                 st = nat.stream()
-                nat.call("pcb_lse_contract_tc05", nat.ptr(node_flows),
-                         nat.ptr(None if allow_modify_flows else node_mars), nat.ptr(element_mars),
-                         nat.ptr(element_flows), ld, B, nat.ptr(eg["pack"]), nat.ptr(et), et.size(0),
-                         nat.ptr(eg["krow"]), 1 if allow_modify_flows else 2, prec,
-                         _tc05_batch_tile(et.size(0), B), st)
+                _tc05_call(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld, B,
+                           eg["pack"], et, eg["krow"], 1 if allow_modify_flows else 2, prec, st)
                 continue
             if eg["short"] and SumLayer.short_kernels:
                 packed = eg["pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None

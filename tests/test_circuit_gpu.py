@@ -175,6 +175,38 @@ def test_recorded_backward_matches_eager(cuda_device):
     assert torch.equal(pf_e, pf_r)
 
 
+def test_tc05_multi_slice_equals_per_slice(cuda_device):
+    """On HCLT-784 at batch 128 (two 64-sample slices per tile), tcgen05 CTAs that walk both
+    slices (loading the second while the first is processed) give the same node values,
+    node flows and parameter flows as one CTA per slice, and the log-likelihoods stay within
+    1e-3 nats of the FP64 oracle."""
+    from pyjuice_b200.layer.layers import SumLayer
+    fx = load_fixture("hclt784")
+    rng = np.random.default_rng(11)
+    xn = rng.integers(0, 256, size=(128, 784))
+    x = torch.from_numpy(xn).to(cuda_device)
+    saved = SumLayer.tc05_slices_per_cta
+    out = []
+    try:
+        for spc in (1, 2):
+            SumLayer.tc05_slices_per_cta = spc
+            pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+            load_fixture_params(pc, fx)
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                lls = pc(x, force_use_bf16=True)
+            pc.backward(inputs=x, allow_modify_flows=True)
+            torch.cuda.synchronize()
+            out.append((lls.clone(), pc.node_mars.clone(), pc.node_flows.clone(), pc.param_flows.clone()))
+    finally:
+        SumLayer.tc05_slices_per_cta = saved
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)
+    p0, q0 = fixture_params(pc, fx)
+    _, _, lls_o = orc.forward(orc.layout_from_circuit(pc), p0, q0, xn[:16])
+    assert abs(out[1][0][:16].double().cpu().numpy().mean() - lls_o.mean()) < 1e-3
+
+
 def test_multi_pack_equals_per_layer_packs(cuda_device):
     """One pcb_pack_weights_multi launch writes the same bytes as one pcb_pack_weights per
     tile table (forward and element-flow tables of every sum layer)."""

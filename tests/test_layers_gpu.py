@@ -108,7 +108,7 @@ def test_prod_layer_forward_backward(B, cuda_device):
                 assert torch.allclose(nf[u[g] + i], ref, atol=1e-6)
 
 
-@pytest.mark.parametrize("path", ["short", "short_packed", "tc05"])
+@pytest.mark.parametrize("path", ["short", "short_packed", "tc05", "tc05_multi"])
 @pytest.mark.parametrize("bs,B,form", [(8, 7, 2), (16, 130, 2), (32, 256, 2), (32, 512, 1), (64, 33, 2)])
 def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
     """The single-stage contractions (<= 128 terms: mma.sync or tcgen05) agree with the chunked ones."""
@@ -123,13 +123,16 @@ def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
     params = torch.rand([bs ** 2 + 3 * 4 * bs * bs], device=cuda_device)
     nf0 = torch.rand([n_nd, B], device=cuda_device)
     outs = {}
-    saved = (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights)
+    saved = (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights,
+             SumLayer.tc05_slices_per_cta)
     try:
         SumLayer.bf16_form = form
         SumLayer.pack_short_weights = path == "short_packed"
         for short in (False, True):
             SumLayer.short_kernels = short
-            SumLayer.tc05_min_tiles = 1 if (short and path == "tc05") else 1 << 30
+            SumLayer.tc05_min_tiles = 1 if (short and path in ("tc05", "tc05_multi")) else 1 << 30
+            # "tc05": one CTA per sample slice; "tc05_multi": two slices per CTA
+            SumLayer.tc05_slices_per_cta = 2 if path == "tc05_multi" else 1
             packed = short and path == "short_packed"
             if packed:  # weights packed ahead of the contractions, as the circuit passes do
                 layer.pack_forward_weights(params, B, force_use_bf16=True)
@@ -145,7 +148,8 @@ def test_short_kernels_match_chunked(bs, B, form, path, cuda_device):
             layer.backward(nf2, ef2, nm, em, params, None, allow_modify_flows=True, _weights_packed=packed)
             outs[short] = (nm[bs:], ef[bs:], ef2[bs:], pf)
     finally:
-        SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights = saved
+        (SumLayer.short_kernels, SumLayer.bf16_form, SumLayer.tc05_min_tiles, SumLayer.pack_short_weights,
+         SumLayer.tc05_slices_per_cta) = saved
     tol = 2e-5 if form == 2 else 2e-2
     for a, b in zip(outs[False], outs[True]):
         assert torch.isfinite(b).all()
