@@ -159,6 +159,23 @@ int pcb_lse_contract(const float* src, const float* src2, const float* aux, floa
                      int32_t prec, void* stream);
 
 /*
+ * Product layer fused into a pcb_lse_contract_short launch (replaces the
+ * pcb_prod_gather_sum launch of the product layer below / above the sum layer):
+ *  - forward (mode 0): term_children[4 k + j], j < 4, are the node rows whose sum is term
+ *    k's element value (-1: no such child). src is then node_mars; the kernel also writes
+ *    the element values to element_out row krow[k] (the product layer's output).
+ *  - element flows (mode 2): out_children[4 e + j], j < 4, are the node rows that receive
+ *    output row e's flow (-1: none); out is then node_flows. Valid when those children
+ *    have no other parent and nothing else writes their rows.
+ * Fused launches need batch_tile <= 32. NULL (or null members) leaves the kernel unfused.
+ */
+typedef struct {
+    const int32_t* term_children;
+    float* element_out;
+    const int32_t* out_children;
+} PcbShortFusion;
+
+/*
  * Same contraction, epilogues and precision forms (prec 0 FP32, 1 bf16, 2 split bf16) as
  * pcb_lse_contract for tiles of at most 128 terms, built for latency: each CTA stages all
  * its terms at once and computes a slice of RM rows (32 when tile_rows <= 32, else 64) by
@@ -175,7 +192,7 @@ int pcb_lse_contract_short(const float* src, const float* src2, const float* aux
                            const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t tile_rows,
                            int32_t rows_per_block, const int32_t* krow, const int32_t* kw, int32_t w_stride,
                            int32_t mode, int32_t prec, const uint8_t* packed, int32_t wlayout, int32_t batch_tile,
-                           void* stream);
+                           const PcbShortFusion* fusion, void* stream);
 
 /*
  * Weights of LSE-contraction tiles (at most 128 rows x 128 terms each, same tile table,

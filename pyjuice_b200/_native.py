@@ -72,7 +72,7 @@ _SIGS = {
                           c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_short": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
                                 c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
-                                c_int32, c_int32, c_void_p], c_int32),
+                                c_int32, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_pack_weights": ([c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_pack_weights_multi": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_tc05": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
@@ -126,6 +126,18 @@ def call(name: str, *args):
         msg = lib.pcb_last_error().decode(errors="replace")
         raise RuntimeError(f"{name} failed ({rc}): {msg}")
     return rc
+
+
+class ShortFusion(ctypes.Structure):
+    """PcbShortFusion (include/pcb200.h): a product layer fused into pcb_lse_contract_short."""
+    _fields_ = [("term_children", c_void_p), ("element_out", c_void_p), ("out_children", c_void_p)]
+
+
+def short_fusion(term_children=None, element_out=None, out_children=None):
+    """Pointer to a PcbShortFusion built from device tensors (None when nothing is fused)."""
+    if term_children is None and out_children is None:
+        return c_void_p(0)
+    return ctypes.pointer(ShortFusion(ptr(term_children), ptr(element_out), ptr(out_children)))
 
 
 def ptr(t) -> c_void_p:

@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int KMAX = 128;
+constexpr int kFuse = 4;  // children per element of a fused product layer (table stride)
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -56,14 +57,15 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
 
 // Shared-memory plan (offsets in 4-byte words; every array starts 16-byte aligned).
 // PREC: 0 = FP32, 1 = bf16, 2 = split bf16.
-template <int RM, int TB, int MODE, int PREC, bool WK>
+template <int RM, int TB, int MODE, int PREC, bool WK, bool FUSE = false>
 struct Smem {
     static constexpr int ES = TB + 8;            // packed row strides: conflict-free fragment loads
     static constexpr int WS = RM + 8;
     static constexpr int NB = PREC == 2 ? 2 : (PREC == 1 ? 1 : 0);
     static constexpr int WROW = WK ? KMAX + 4 : RM + 4;   // fp32 weight staging row
     static constexpr int kE = KMAX * TB;
-    static constexpr int kE2 = MODE == 2 ? KMAX * TB : 0;
+    // second staging set: node mars (mode 2) or children 1 .. kFuse - 1 (fused forward)
+    static constexpr int kE2 = MODE == 2 ? KMAX * TB : ((MODE == 0 && FUSE) ? (kFuse - 1) * KMAX * TB : 0);
     static constexpr int kW = WK ? RM * WROW : KMAX * WROW;
     static constexpr int kPE = NB * (KMAX / 2) * ES;
     static constexpr int kPW = NB * (KMAX / 2) * WS;
@@ -71,20 +73,20 @@ struct Smem {
     static constexpr int kA = MODE >= 1 ? RM * AS : 0;
     static constexpr int oE = 0, oE2 = oE + kE, oW = oE2 + kE2, oPE = oW + kW, oPW = oPE + kPE;
     static constexpr int oA = oPW + kPW, oPart = oA + kA, oMax = oPart + kThreads, oIdx = oMax + TB;
-    static constexpr size_t bytes() { return 4ull * (oIdx + 2 * KMAX); }
+    static constexpr size_t bytes() { return 4ull * (oIdx + (2 + kFuse) * KMAX); }
 };
 
-template <int RM, int TB, int MODE, int PREC, bool WK>
+template <int RM, int TB, int MODE, int PREC, bool WK, bool FUSE>
 __global__ void __launch_bounds__(kThreads)
 lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                  float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                  const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                  int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
-                 const uint8_t* __restrict__ packed) {
+                 const uint8_t* __restrict__ packed, PcbShortFusion fu) {
     // The term indices and the weights (compiled tables and parameters) are read before the
     // wait for the previous kernel; only the source rows and the packed weights after it.
     pcb::pdl_trigger();
-    using S = Smem<RM, TB, MODE, PREC, WK>;
+    using S = Smem<RM, TB, MODE, PREC, WK, FUSE>;
     constexpr int ES = S::ES, WS = S::WS, WROW = S::WROW;
     constexpr int PARTS = kThreads / TB;  // threads per sample column in the max / exp passes
     static_assert(kThreads % TB == 0 && RM % 16 == 0 && TB % 8 == 0, "tile shape");
@@ -111,9 +113,15 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     const int rpb_mask = (1 << rpb_log2) - 1;
 
     // ---- term indices, then one batch of asynchronous copies ----
+    int* sCh = sKw + KMAX;  // fused forward: [KMAX][kFuse] child node rows of each term
     if (tid < nk) {
         sRow[tid] = __ldg(krow + t.k_off + tid);
         sKw[tid] = __ldg(kw + t.k_off + tid);
+        if (MODE == 0 && FUSE) {
+#pragma unroll
+            for (int j = 0; j < kFuse; ++j)
+                sCh[kFuse * tid + j] = __ldg(fu.term_children + (int64_t)kFuse * (t.k_off + tid) + j);
+        }
     }
     __syncthreads();
     constexpr int kPackHalf = RM * 256;
@@ -193,11 +201,18 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
             const int c4 = idx % NX;
             const int b = b0 + c4 * 4;
             if (k < nk) {
-                const int64_t off = (int64_t)sRow[k] * ld + b;
+                constexpr bool F0 = MODE == 0 && FUSE;
 #pragma unroll
-                for (int h = 0; h < (MODE == 2 ? 2 : 1); ++h) {
-                    float* d = h == 0 ? &sE[k][c4 * 4] : &sE2[k][c4 * 4];
-                    const float* g = (h == 0 ? src : src2) + off;
+                for (int h = 0; h < (MODE == 2 ? 2 : (F0 ? kFuse : 1)); ++h) {
+                    // fused forward: the term's element value is the sum of its child node
+                    // rows (staged in set h = child h; a missing child reads as 0)
+                    float* d = h == 0 ? &sE[k][c4 * 4] : &sE2[(h - 1) * KMAX + k][c4 * 4];
+                    const int row = F0 ? sCh[kFuse * k + h] : sRow[k];
+                    if (F0 && row < 0) {
+                        *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
+                        continue;
+                    }
+                    const float* g = (h == 0 || F0 ? src : src2) + (int64_t)row * ld + b;
                     if (vec && b + 3 < B) {
                         pcb::cp_async16(d, g);
                     } else {
@@ -255,12 +270,19 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     const int part = tid / TB;
     {
         float mx = -INFINITY;
+        const bool write_em = MODE == 0 && FUSE && r0 == 0 && b0 + cb < B;
         for (int k = part; k < nk; k += PARTS) {
             float v = sE[k][cb];
             if (MODE == 2) {
                 const float m2 = sE2[k][cb];
                 v = (m2 == -INFINITY) ? -INFINITY : logf(v) - m2;
                 sE[k][cb] = v;
+            }
+            if (MODE == 0 && FUSE) {
+#pragma unroll
+                for (int j = 1; j < kFuse; ++j) v = v + sE2[(j - 1) * KMAX + k][cb];
+                sE[k][cb] = v;
+                if (write_em) fu.element_out[(int64_t)sRow[k] * ld + b0 + cb] = v;
             }
             mx = fmaxf(mx, v);
         }
@@ -326,7 +348,16 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                     pcb::set(o, j, (mm == -INFINITY) ? 0.f : acc[r][j] * __expf(pcb::get(a, j) + mm));
                 }
             }
-            pcb::store4(out, (int64_t)t.out_row + row, ld, bb, B, vec, o);
+            if (MODE != 0 && FUSE) {
+                const int64_t e = (int64_t)t.out_row + row;
+#pragma unroll
+                for (int h = 0; h < kFuse; ++h) {
+                    const int c = __ldg(fu.out_children + kFuse * e + h);
+                    if (c >= 0) pcb::store4(out, c, ld, bb, B, vec, o);
+                }
+            } else {
+                pcb::store4(out, (int64_t)t.out_row + row, ld, bb, B, vec, o);
+            }
         }
     } else {
         constexpr bool SPLIT = PREC == 2;
@@ -432,12 +463,22 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                             o[j] = (mm == -INFINITY) ? 0.f : v * __expf(x + mm);
                         }
                     }
-                    float* dst = out + ((int64_t)t.out_row + row) * ld + b;
-                    if (vec && b + 1 < B) {
-                        *reinterpret_cast<float2*>(dst) = make_float2(o[0], o[1]);
-                    } else {
-                        if (b < B) dst[0] = o[0];
-                        if (b + 1 < B) dst[1] = o[1];
+#pragma unroll
+                    for (int hh = 0; hh < ((MODE != 0 && FUSE) ? kFuse : 1); ++hh) {
+                        int64_t orow = (int64_t)t.out_row + row;
+                        if (MODE != 0 && FUSE) {
+                            // fused backward: the element's flow is the flow of its child rows
+                            const int c = __ldg(fu.out_children + kFuse * orow + hh);
+                            if (c < 0) continue;
+                            orow = c;
+                        }
+                        float* dst = out + orow * ld + b;
+                        if (vec && b + 1 < B) {
+                            *reinterpret_cast<float2*>(dst) = make_float2(o[0], o[1]);
+                        } else {
+                            if (b < B) dst[0] = o[0];
+                            if (b + 1 < B) dst[1] = o[1];
+                        }
                     }
                 }
             }
@@ -451,16 +492,17 @@ int current_device() {
     return d < 0 ? 0 : (d > 63 ? 63 : d);
 }
 
-template <int RM, int TB, int MODE, int PREC, bool WK>
+template <int RM, int TB, int MODE, int PREC, bool WK, bool FUSE>
 int launch_one(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
-               int w_stride, int rpb_log2, cudaStream_t s, bool vec, bool wvec, const uint8_t* packed) {
-    constexpr size_t smem = Smem<RM, TB, MODE, PREC, WK>::bytes();
+               int w_stride, int rpb_log2, cudaStream_t s, bool vec, bool wvec, const uint8_t* packed,
+               const PcbShortFusion& fu) {
+    constexpr size_t smem = Smem<RM, TB, MODE, PREC, WK, FUSE>::bytes();
     static_assert(smem <= 227 * 1024, "shared memory");
     static bool configured[64] = {false};
     const int dev = current_device();
     if (!configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(lse_short_kernel<RM, TB, MODE, PREC, WK>,
+        cudaError_t e = cudaFuncSetAttribute(lse_short_kernel<RM, TB, MODE, PREC, WK, FUSE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract_short: %s", cudaGetErrorString(e));
         configured[dev] = true;
@@ -468,21 +510,32 @@ int launch_one(int num_tiles, int row_splits, const float* src, const float* src
     const int64_t gx = (int64_t)num_tiles * row_splits;
     const int64_t gy = pcb::cdiv(B, TB);
     if (gx > 2147483647 || gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: grid too large");
-    return pcb::launch_status(pcb::launch_k(lse_short_kernel<RM, TB, MODE, PREC, WK>,
+    return pcb::launch_status(pcb::launch_k(lse_short_kernel<RM, TB, MODE, PREC, WK, FUSE>,
                                             dim3((unsigned)gx, (unsigned)gy), dim3(kThreads), smem, s, 1u, src,
                                             src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2,
-                                            row_splits, vec, wvec, packed), "pcb_lse_contract_short");
+                                            row_splits, vec, wvec, packed, fu), "pcb_lse_contract_short");
 }
 
 template <int RM, int TB, int PREC>
 int launch_prec(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                 int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
                 int w_stride, int rpb_log2, int mode, bool wk, cudaStream_t s, bool vec, bool wvec,
-                const uint8_t* packed) {
-#define PCB_LS(M, W) \
-    launch_one<RM, TB, M, PREC, W>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec, wvec, packed)
-    if (wk) return mode == 0 ? PCB_LS(0, true) : (mode == 1 ? PCB_LS(1, true) : PCB_LS(2, true));
-    return mode == 0 ? PCB_LS(0, false) : (mode == 1 ? PCB_LS(1, false) : PCB_LS(2, false));
+                const uint8_t* packed, const PcbShortFusion& fu) {
+    // fusion: forward (mode 0) with term_children, element flows (mode 2) with out_children
+    const bool f = mode == 0 ? fu.term_children != nullptr : (mode == 2 && fu.out_children != nullptr);
+#define PCB_LS(M, W, F) \
+    launch_one<RM, TB, M, PREC, W, F>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, s, vec, wvec, packed, fu)
+    if (f) {
+        // fused forms stage up to four child rows per term: batch tiles of at most 32 samples
+        if constexpr (TB <= 32) {
+            if (wk) return mode == 0 ? PCB_LS(0, true, true) : PCB_LS(2, true, true);
+            return mode == 0 ? PCB_LS(0, false, true) : PCB_LS(2, false, true);
+        } else {
+            return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: product fusion needs batch_tile <= 32");
+        }
+    }
+    if (wk) return mode == 0 ? PCB_LS(0, true, false) : (mode == 1 ? PCB_LS(1, true, false) : PCB_LS(2, true, false));
+    return mode == 0 ? PCB_LS(0, false, false) : (mode == 1 ? PCB_LS(1, false, false) : PCB_LS(2, false, false));
 #undef PCB_LS
 }
 
@@ -490,9 +543,9 @@ template <int RM, int TB>
 int launch_shape(int num_tiles, int row_splits, const float* src, const float* src2, const float* aux, float* out,
                  int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow, const int* kw,
                  int w_stride, int rpb_log2, int mode, int prec, bool wk, cudaStream_t s, bool vec, bool wvec,
-                 const uint8_t* packed) {
+                 const uint8_t* packed, const PcbShortFusion& fu) {
 #define PCB_LP(P) \
-    launch_prec<RM, TB, P>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, wk, s, vec, wvec, packed)
+    launch_prec<RM, TB, P>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, wk, s, vec, wvec, packed, fu)
     if (prec == 0) return PCB_LP(0);
     if (prec == 1) return PCB_LP(1);
     return PCB_LP(2);
@@ -505,7 +558,8 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
                                       int32_t B, const float* params, const PcbLseTile* tiles, int32_t num_tiles,
                                       int32_t tile_rows, int32_t rows_per_block, const int32_t* krow,
                                       const int32_t* kw, int32_t w_stride, int32_t mode, int32_t prec,
-                                      const uint8_t* packed, int32_t wlayout, int32_t batch_tile, void* stream) {
+                                      const uint8_t* packed, int32_t wlayout, int32_t batch_tile,
+                                      const PcbShortFusion* fusion, void* stream) {
     if (!src || !out || !params || !tiles || !krow || !kw || B <= 0 || ld < B || num_tiles < 0 || mode < 0 ||
         mode > 2 || (mode == 2 && !src2) || (mode >= 1 && !aux) || rows_per_block <= 0 ||
         (rows_per_block & (rows_per_block - 1)) || tile_rows < 1 || tile_rows > 128 || prec < 0 || prec > 2 ||
@@ -516,6 +570,12 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: packed weights need a BF16 form and 16-byte alignment");
     if (wlayout != 0 && (reinterpret_cast<uintptr_t>(params) & 15) != 0)
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: 16-byte weight copies need an aligned params base");
+    PcbShortFusion fu = {nullptr, nullptr, nullptr};
+    if (fusion) fu = *fusion;
+    if ((fu.term_children && (mode != 0 || !fu.element_out)) || (fu.out_children && mode != 2))
+        return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_short: product fusion needs mode 0 (with element_out) or mode 2");
+    if (mode != 0) fu.term_children = nullptr;
+    if (mode != 2) fu.out_children = nullptr;
     int rpb_log2 = 0;
     while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!src2 || pcb::vec_ok(src2, ld)) &&
@@ -526,7 +586,7 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
     const int rm = tile_rows <= 32 ? 32 : 64;
     const int row_splits = (tile_rows + rm - 1) / rm;
 #define PCB_SH(RM, TB) \
-    launch_shape<RM, TB>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, prec, wk, s, vec, wvec, packed)
+    launch_shape<RM, TB>(num_tiles, row_splits, src, src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2, mode, prec, wk, s, vec, wvec, packed, fu)
     if (rm == 32) {
         if (batch_tile == 16) return PCB_SH(32, 16);
         if (batch_tile == 32) return PCB_SH(32, 32);

@@ -53,11 +53,12 @@ def _num_sms() -> int:
     return _NUM_SMS
 
 
-def _short_batch_tile(num_tiles: int, tile_rows: int, B: int) -> int:
+def _short_batch_tile(num_tiles: int, tile_rows: int, B: int, fused: bool = False) -> int:
     """Samples per CTA for pcb_lse_contract_short: the widest slice that still launches two
-    CTAs per SM (small layers get narrow slices and therefore more CTAs)."""
+    CTAs per SM (small layers get narrow slices and therefore more CTAs); at most 32 when a
+    product layer is fused in."""
     splits = 1 if tile_rows <= 32 else -(-tile_rows // 64)
-    for tb in (64, 32):
+    for tb in ((32,) if fused else (64, 32)):
         if num_tiles * splits * -(-B // tb) >= 2 * _num_sms():
             return tb
     return 16
@@ -372,6 +373,18 @@ class SumLayer(Layer):
     def _el_tc05(self, eg, prec):
         return prec > 0 and eg["short"] and eg["tiles"].size(0) >= SumLayer.tc05_min_tiles
 
+    def runs_single_stage(self, device: torch.device, B: int, force_use_bf16: bool = False,
+                          force_use_fp32: bool = False, backward: bool = False) -> bool:
+        """Whether the forward (or every element-flow launch) runs pcb_lse_contract_short with
+        these settings, so that a product layer can be fused into it."""
+        d = self._desc(device)
+        if not SumLayer.short_kernels:
+            return False
+        if not backward:
+            return d["fw_short"] and not self._fw_tc05(d, B, force_use_bf16, force_use_fp32)[1]
+        return all(eg["short"] and not self._el_tc05(eg, self._el_prec(eg, B, force_use_fp32))
+                   for eg in d["el_groups"])
+
     def forward_pack_job(self, device: torch.device, B: int, force_use_bf16: bool = False,
                          force_use_fp32: bool = False):
         """``(tiles, kw, packed, rows_per_block, w_stride)`` of the forward weights this layer
@@ -436,13 +449,20 @@ class SumLayer(Layer):
                 _weights_packed = True
             _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st)
             return
+        # _fuse_fw = (term_children, element values out): the product layer below is fused in
+        # (the terms are sums of node rows; the element values are written as a side output)
+        fuse = kwargs.get("_fuse_fw")
         if d["fw_short"] and SumLayer.short_kernels:
             packed = d["fw_pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
-            nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
-                     ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
-                     nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(packed), d["fw_wlayout"],
-                     _short_batch_tile(t.size(0), d["fw_tm"], B), nat.stream())
+            fusion = nat.short_fusion(fuse[0], fuse[1]) if fuse is not None else nat.ptr(None)
+            nat.call("pcb_lse_contract_short", nat.ptr(element_mars if fuse is None else node_mars), nat.ptr(None),
+                     nat.ptr(None), nat.ptr(node_mars), ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"],
+                     self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(packed),
+                     d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B, fuse is not None), fusion,
+                     nat.stream())
             return
+        if fuse is not None:
+            raise RuntimeError("a fused product layer needs the single-stage sum kernel")
         nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B,
                  nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]),
                  nat.ptr(d["kw"]), 1, 0, prec, nat.stream())
@@ -490,12 +510,20 @@ class SumLayer(Layer):
                 continue
             if eg["short"] and SumLayer.short_kernels:
                 packed = eg["pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
+                # _fuse_bw = out_children: the product layer below is fused in (each element's
+                # flow goes straight to the node-flow rows of its children)
+                fuse = kwargs.get("_fuse_bw")
+                if fuse is not None and allow_modify_flows:
+                    raise RuntimeError("a fused product layer needs unmodified node flows")
                 nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
-                         nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et),
-                         et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
-                         1 if allow_modify_flows else 2, prec, nat.ptr(packed), eg["wlayout"],
-                         _short_batch_tile(et.size(0), eg["tm"], B), nat.stream())
+                         nat.ptr(element_mars), nat.ptr(element_flows if fuse is None else node_flows), ld, B,
+                         nat.ptr(params), nat.ptr(et), et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]),
+                         nat.ptr(eg["kw"]), self.block_size, 1 if allow_modify_flows else 2, prec, nat.ptr(packed),
+                         eg["wlayout"], _short_batch_tile(et.size(0), eg["tm"], B, fuse is not None),
+                         nat.short_fusion(out_children=fuse) if fuse is not None else nat.ptr(None), nat.stream())
                 continue
+            if kwargs.get("_fuse_bw") is not None:
+                raise RuntimeError("a fused product layer needs the single-stage element-flow kernel")
             nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
                      nat.ptr(element_mars), nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0),
                      eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size,
