@@ -50,7 +50,7 @@ STEP_SIZE = 0.1
 PSEUDOCOUNT = 0.1
 # DRAM bytes (read + written) of the roofline launch, the largest layer's parameter flows,
 # from one ncu capture of `bench.py --profile-step` (-k regex:sum_pflows -s 63 -c 1).
-PFLOW_TRAFFIC_BYTES = 81_506_816
+PFLOW_TRAFFIC_BYTES = 81_879_552
 METRIC = "EM samples/s (fwd+bwd+update) 1xB200, BF16-TC vs FP32 plain; dLL vs FP64 oracle"
 WORKLOAD = "HCLT 28x28 vars x 256 cats, 128 latents, block 32, EM step (fwd+bwd+mini_batch_em)"
 
