@@ -5,14 +5,17 @@ namespace {
 
 // node_mars[node_offset + n, b] = log(params[s_pids[n] + x]) with x = data[vids[n], b].
 // A category outside [0, ncats) yields NaN (no out-of-range read).
-// A CTA covers kFwdNodes consecutive nodes over 1024 samples (4 per thread): the logs of
+// A CTA covers kFwdNodes consecutive nodes over 512 samples (4 per thread): the logs of
 // the nodes' parameter slabs (up to kFwdSlab categories) are taken once into shared
 // memory, each thread loads its 4 category values once and reuses them for every node of
 // the same variable, and each node row is written with 16-byte stores.
 constexpr int kFwdNodes = 8;
 constexpr int kFwdSlab = 256;
 
-__global__ void __launch_bounds__(256)
+constexpr int kFwdThreads = 128;
+constexpr int kFwdSamples = 4 * kFwdThreads;
+
+__global__ void __launch_bounds__(kFwdThreads)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
                      int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec) {
@@ -36,7 +39,7 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
     }
     __syncthreads();
     pcb::pdl_wait();
-    const int b = blockIdx.y * 1024 + tid * 4;
+    const int b = blockIdx.y * kFwdSamples + tid * 4;
     if (b >= B) return;
     const int v0 = sV[0];
     int64_t x0[4];
@@ -145,16 +148,30 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                 for (int i = lane; i < nb; i += 32) wrow[i] = __ldg(frow + i);
             }
             __syncwarp();
-            for (int k = lane; k < K; k += 32) {
-                const int s = (k == 0) ? 0 : seg[k - 1];
-                const int e = seg[k];
-                if (e == s) continue;
-                float acc = 0.f;
-                for (int p = s; p < e; ++p) {
-                    const float f = wrow[perm[p]];
-                    acc += logspace ? __expf(f) : f;
+            // categories lane, lane + 32, ...: the slots' old values are loaded for a batch of
+            // kR categories at once (one round trip), then summed and stored
+            constexpr int kR = 8;
+            for (int k0 = 0; k0 < K; k0 += 32 * kR) {
+                float old[kR];
+#pragma unroll
+                for (int j = 0; j < kR; ++j) {
+                    const int k = k0 + lane + 32 * j;
+                    old[j] = (k < K) ? pf[sf + k] : 0.f;
                 }
-                pf[sf + k] += acc;
+#pragma unroll
+                for (int j = 0; j < kR; ++j) {
+                    const int k = k0 + lane + 32 * j;
+                    if (k >= K) continue;
+                    const int s = (k == 0) ? 0 : seg[k - 1];
+                    const int e = seg[k];
+                    if (e == s) continue;
+                    float acc = 0.f;
+                    for (int p = s; p < e; ++p) {
+                        const float f = wrow[perm[p]];
+                        acc += logspace ? __expf(f) : f;
+                    }
+                    pf[sf + k] = old[j] + acc;
+                }
             }
             __syncwarp();  // the next node overwrites this warp's row
         }
@@ -171,11 +188,11 @@ extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const flo
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: bad arguments");
     if (num_nodes == 0) return PCB_OK;
     const bool vec = pcb::vec_ok(node_mars, ld);
-    const int64_t gy = pcb::cdiv(B, 1024);
+    const int64_t gy = pcb::cdiv(B, kFwdSamples);
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: batch too large");
     return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(num_nodes, kFwdNodes),
                                                                        (unsigned)gy),
-                                            dim3(256), 0, pcb::as_stream(stream), 1u, data, data_ld, params, vids,
+                                            dim3(kFwdThreads), 0, pcb::as_stream(stream), 1u, data, data_ld, params, vids,
                                             s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec),
                               "pcb_input_cat_fwd");
 }
