@@ -29,22 +29,57 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
     const int rg = threadIdx.x / cols;
     const double pcn = pc / (double)nch;
 
+    // Update of one entry with the column's scale: inv = step / (tot + pc) (EM), 1 / (tot + pc)
+    // (normalisation); one FP64 reciprocal per column instead of a division per entry.
+    auto update = [&](double p, double f, double inv) -> float {
+        double np;
+        if (EM) {
+            if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + (f + pcn) * inv;
+            else np = (1.0 - step) * p + (f + pcn) * inv;
+        } else {
+            np = (p + pcn) * inv;
+        }
+        return (float)np;
+    };
+    constexpr int R = 16;  // entries per thread held in registers (nch <= rgs * R)
     for (int c0 = 0; c0 < bs; c0 += cols) {
         const int col = c0 + c;
+        const bool reg = nch <= rgs * R;
+        float pv[R], fv[R];
         double s = 0.0;
         if (rg < rgs) {
-            for (int k = rg; k < nch; k += rgs) {
-                const int64_t off = (int64_t)k * bs + col;
-                if (EM) {
-                    const double f = (double)pflows[fb + off];
-                    if (KEEP_ZERO) {
-                        const float p = params[pb + off];
-                        s += (p < 1e-12f) ? 0.0 : (f + pcn);
+            if (reg) {
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const int k = rg + j * rgs;
+                    const int64_t off = (int64_t)k * bs + col;
+                    pv[j] = (k < nch) ? params[pb + off] : 0.f;
+                    fv[j] = (EM && k < nch) ? pflows[fb + off] : 0.f;
+                }
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    if (rg + j * rgs >= nch) continue;
+                    if (EM) {
+                        if (KEEP_ZERO) s += (pv[j] < 1e-12f) ? 0.0 : ((double)fv[j] + pcn);
+                        else s += (double)fv[j];
                     } else {
-                        s += f;
+                        s += (double)pv[j];
                     }
-                } else {
-                    s += (double)params[pb + off];
+                }
+            } else {
+                for (int k = rg; k < nch; k += rgs) {
+                    const int64_t off = (int64_t)k * bs + col;
+                    if (EM) {
+                        const double f = (double)pflows[fb + off];
+                        if (KEEP_ZERO) {
+                            const float p = params[pb + off];
+                            s += (p < 1e-12f) ? 0.0 : (f + pcn);
+                        } else {
+                            s += f;
+                        }
+                    } else {
+                        s += (double)params[pb + off];
+                    }
                 }
             }
         }
@@ -53,22 +88,19 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
         double tot = 0.0;
         for (int r = 0; r < rgs; ++r) tot += part[r * cols + c];
         __syncthreads();
+        const double inv = EM ? (KEEP_ZERO ? step / tot : step / (tot + pc)) : 1.0 / (tot + pc);
         if (rg < rgs) {
-            for (int k = rg; k < nch; k += rgs) {
-                const int64_t off = (int64_t)k * bs + col;
-                const double p = (double)params[pb + off];
-                double np;
-                if (EM) {
-                    const double f = (double)pflows[fb + off];
-                    if (KEEP_ZERO) {
-                        np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / tot;
-                    } else {
-                        np = (1.0 - step) * p + step * (f + pcn) / (tot + pc);
-                    }
-                } else {
-                    np = (p + pcn) / (tot + pc);
+            if (reg) {
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const int k = rg + j * rgs;
+                    if (k < nch) params[pb + (int64_t)k * bs + col] = update((double)pv[j], (double)fv[j], inv);
                 }
-                params[pb + off] = (float)np;
+            } else {
+                for (int k = rg; k < nch; k += rgs) {
+                    const int64_t off = (int64_t)k * bs + col;
+                    params[pb + off] = update((double)params[pb + off], EM ? (double)pflows[fb + off] : 0.0, inv);
+                }
             }
         }
     }
@@ -91,10 +123,12 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
     const int64_t sp = s_pids[n];
     const int64_t sf = s_pfids[n];
     const double pcn = pc / (double)K;
-    auto update = [&](double p, double f, double s) -> float {
+    // one FP64 reciprocal per node: inv = step / s (keep-zero form) or step / (s + pc)
+    auto scale = [&](double s) -> double { return KEEP_ZERO ? step / s : step / (s + pc); };
+    auto update = [&](double p, double f, double inv) -> float {
         double np;
-        if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + step * (f + pcn) / s;
-        else np = (1.0 - step) * p + step * (f + pcn) / (s + pc);
+        if (KEEP_ZERO) np = (p < 1e-12) ? 0.0 : (1.0 - step) * p + (f + pcn) * inv;
+        else np = (1.0 - step) * p + (f + pcn) * inv;
         return (float)np;
     };
     constexpr int R = 8;
@@ -114,10 +148,11 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
             else s += (double)f[j];
         }
         s = pcb::warp_sum(s);
+        const double inv = scale(s);
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int k = lane + 32 * j;
-            if (k < K) params[sp + k] = update((double)p[j], (double)f[j], s);
+            if (k < K) params[sp + k] = update((double)p[j], (double)f[j], inv);
         }
         return;
     }
@@ -128,7 +163,8 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
         else s += f;
     }
     s = pcb::warp_sum(s);
-    for (int k = lane; k < K; k += 32) params[sp + k] = update((double)params[sp + k], (double)pflows[sf + k], s);
+    const double inv = scale(s);
+    for (int k = lane; k < K; k += 32) params[sp + k] = update((double)params[sp + k], (double)pflows[sf + k], inv);
 }
 
 }  // namespace
