@@ -141,6 +141,18 @@ int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int32_t B,
                         int32_t num_blocks, int32_t blk_size, int32_t accum, int32_t logsumexp, void* stream);
 
 /*
+ * pcb_prod_gather_sum backward in overwrite mode (accum = 0, linear flows) fused with
+ * pcb_modify_flows: rows r in [modify_row0, modify_row1) receive log(sum) - node_mars[r]
+ * (-inf where node_mars is -inf) instead of the sum, other rows the sum. Valid when this
+ * launch is the only writer of those rows (their flows are complete when written).
+ * Replaces the same reference kernels as the two launches it combines.
+ */
+int pcb_prod_gather_sum_modify(const float* in, float* out, int64_t ld, int32_t B, const int32_t* blk_row,
+                               const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs, int32_t num_blocks,
+                               int32_t blk_size, const float* node_mars, int64_t modify_row0, int64_t modify_row1,
+                               void* stream);
+
+/*
  * Log-sum-exp contraction over tiles, FP32 FMA (plain) or BF16 tensor-core (prec=1):
  *   acc[r, b] = sum_k W(k, r) * exp(src[krow[k], b] - m_b),  m_b = max_k src[krow[k], b]
  *   W(k, r)   = params[kw[k] + w_add + (r / rows_per_block) * g_stride + (r % rows_per_block) * w_stride]

@@ -484,7 +484,7 @@ class SumLayer(Layer):
         for t in (node_flows, element_flows, element_mars):
             if t.stride(0) != ld or t.stride(1) != 1:
                 raise ValueError("node/element mars/flows must share a row-major layout")
-        if allow_modify_flows:
+        if allow_modify_flows and not kwargs.get("_flows_modified"):
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
                      self._layer_nid_range[1], nat.stream())
         # The parameter flows only read this layer's node flows / mars and its children's element
@@ -629,6 +629,16 @@ class ProdLayer(Layer):
         ld = node_flows.stride(0)
         if element_flows.stride(0) != ld:
             raise ValueError("node_flows and element_flows must share a row-major layout")
+        # _modify = (node_mars, row0, row1): the flows of rows [row0, row1) are written as
+        # log f - log m (what the sum layer below would rewrite them to); overwrite mode only
+        mod = kwargs.get("_modify")
+        if mod is not None:
+            if self.bk_accumulate or logspace_flows:
+                raise RuntimeError("fused flow rewriting needs an overwriting product layer and linear flows")
+            nat.call("pcb_prod_gather_sum_modify", nat.ptr(element_flows), nat.ptr(node_flows), ld, B,
+                     nat.ptr(d["bk_row"]), nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]),
+                     d["bk_row"].size(0), self.block_size, nat.ptr(mod[0]), mod[1], mod[2], nat.stream())
+            return
         nat.call("pcb_prod_gather_sum", nat.ptr(element_flows), nat.ptr(node_flows), ld, B, nat.ptr(d["bk_row"]),
                  nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]), d["bk_row"].size(0),
                  self.block_size, 1 if self.bk_accumulate else 0, 1 if logspace_flows else 0, nat.stream())

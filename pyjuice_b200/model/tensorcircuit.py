@@ -61,6 +61,9 @@ class TensorCircuit(nn.Module):
     # 0.07 ms.
     fuse_products = True
     fuse_products_forward = False
+    # Let the product layer that alone writes a large sum layer's node flows write them as
+    # log f - log m directly (the rewrite that layer's backward would otherwise launch).
+    fuse_flow_rewrite = True
 
     def __init__(self, root_ns: CircuitNodes, layer_sparsity_tol: float = 0.5,
                  max_num_partitions: Optional[int] = None, disable_gpu_compilation: bool = False,
@@ -301,7 +304,10 @@ class TensorCircuit(nn.Module):
         """
         written = np.zeros([self.num_nodes], dtype=bool)
         need = np.zeros([self.num_nodes], dtype=bool)
-        for group in reversed(self.inner_layer_groups):
+        nwriters = np.zeros([self.num_nodes], dtype=np.int64)
+        writer = np.full([self.num_nodes], -1, dtype=np.int64)
+        for gi in range(len(self.inner_layer_groups) - 1, -1, -1):
+            group = self.inner_layer_groups[gi]
             if not group.is_prod():
                 continue
             for layer in group:
@@ -313,6 +319,19 @@ class TensorCircuit(nn.Module):
                 else:
                     layer.bk_accumulate = False
                 written[tgt] = True
+                nwriters[tgt] += 1
+                writer[tgt] = gi if len(group) == 1 else -2
+        # Sum layers whose node flows come complete from one overwriting product layer: that
+        # product layer can write them already rewritten as log f - log m.
+        self._rewrite_fusion = dict()
+        for gs, group in enumerate(self.inner_layer_groups):
+            if not group.is_sum() or len(group) != 1:
+                continue
+            lo, hi = group[0]._layer_nid_range
+            gp = int(writer[lo]) if hi > lo else -1
+            if gp >= 0 and np.all(nwriters[lo:hi] == 1) and np.all(writer[lo:hi] == gp) and \
+                    not self.inner_layer_groups[gp][0].bk_accumulate:
+                self._rewrite_fusion[gp] = (gs, int(lo), int(hi))
         r0, r1 = self._root_node_range
         need |= ~written
         need[r0:r1] = False
@@ -601,19 +620,31 @@ class TensorCircuit(nn.Module):
                     el_ready.record(sides[0])
         kwargs = dict(kwargs, _weights_packed=True)
         turn = 0
-        fused_prod = set()
+        fused_prod, rewritten = set(), set()
+
+        def rewrites(g):  # large layers rewrite their node flows as log f - log m
+            return allow_modify_flows and any(
+                layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles
+                for layer in self.inner_layer_groups[g])
+
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
             group = self.inner_layer_groups[layer_id]
             if group.is_prod():
-                if layer_id not in fused_prod:  # else the sum layer above wrote these flows
+                if layer_id in fused_prod:  # the sum layer above wrote these flows
+                    continue
+                rf = self._rewrite_fusion.get(layer_id) if TensorCircuit.fuse_flow_rewrite else None
+                if rf is not None and not logspace_flows and rewrites(rf[0]):
+                    group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows,
+                                   _modify=(self.node_mars, rf[1], rf[2]))
+                    rewritten.add(rf[0])
+                else:
                     group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows)
             else:
                 # The element values of the forward pass are still resident (no recomputation). Small
                 # layers form log f - log m inside the flow kernels instead of rewriting the node flows
                 # in place (one launch fewer); large ones rewrite them once (allow_modify_flows) so that
                 # the two flow kernels read one row per node instead of two.
-                modify = allow_modify_flows and any(
-                    layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles for layer in group)
+                modify = rewrites(layer_id)
                 if el_ready is not None:
                     main.wait_event(el_ready)
                     el_ready = None
@@ -628,7 +659,7 @@ class TensorCircuit(nn.Module):
                                param_flows=self.param_flows if compute_param_flows else None,
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
                                force_use_fp32=force_use_fp32, _pflow_stream=sides[turn % len(sides)], _fuse_bw=fz,
-                               **kwargs)
+                               _flows_modified=layer_id in rewritten, **kwargs)
                 turn += 1
         for side in sides:
             main.wait_stream(side)

@@ -210,18 +210,20 @@ def test_tc05_multi_slice_equals_per_slice(cuda_device):
 @pytest.mark.parametrize("name,B,fw", [("hclt64", 37, dict(force_use_fp32=True)), ("hclt784", 64, dict(force_use_bf16=True)),
                                        ("tiny", 19, dict(force_use_fp32=True))])
 def test_fused_products_equal_unfused(name, B, fw, cuda_device):
-    """Product layers fused into the single-stage sum kernels give bit-identical node values,
-    element values, node flows and parameter flows."""
+    """Product layers fused into the single-stage sum kernels, and product layers that write
+    a large layer's node flows already rewritten as log f - log m, give bit-identical node
+    values, element values, node flows and parameter flows."""
     from pyjuice_b200.model.tensorcircuit import TensorCircuit
     fx = load_fixture(name)
     rng = np.random.default_rng(5)
     ncat = 4 if name != "hclt784" else 256
     x = torch.from_numpy(rng.integers(0, ncat, size=(B, fx["x"].shape[1]))).to(cuda_device)
-    saved = (TensorCircuit.fuse_products, TensorCircuit.fuse_products_forward)
+    saved = (TensorCircuit.fuse_products, TensorCircuit.fuse_products_forward, TensorCircuit.fuse_flow_rewrite)
     out = []
     try:
         for fuse in (False, True):
             TensorCircuit.fuse_products = TensorCircuit.fuse_products_forward = fuse
+            TensorCircuit.fuse_flow_rewrite = fuse
             pc = build_fixture_circuit(name, fx).to(cuda_device)
             load_fixture_params(pc, fx)
             if fuse:
@@ -234,7 +236,7 @@ def test_fused_products_equal_unfused(name, B, fw, cuda_device):
             em = torch.cat([pc._em_view(gi) for gi in pc._fusion_host])
             out.append((pc.node_mars.clone(), em.clone(), pc.node_flows.clone(), pc.param_flows.clone()))
     finally:
-        TensorCircuit.fuse_products, TensorCircuit.fuse_products_forward = saved
+        TensorCircuit.fuse_products, TensorCircuit.fuse_products_forward, TensorCircuit.fuse_flow_rewrite = saved
     for a, b in zip(out[0], out[1]):
         assert torch.equal(a, b)
 
