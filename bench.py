@@ -9,8 +9,10 @@ forward -> backward -> ``mini_batch_em(step_size=0.1, pseudocount=0.1)``.
   graph, inputs resident in HBM, device time (CUDA events), max over ranks;
 * ``fp32_plain``: the same for the plain FP32 form;
 * ``e2e``: the BF16 form through the public API (``lls = pc(x, record_cudagraph=True)``,
-  ``lls.mean().backward()``, ``pc.mini_batch_em``) with the batch copied from pinned
-  host memory and the log-likelihoods read back every step;
+  ``lls.mean().backward()``, ``pc.mini_batch_em``) with every step's batch copied from
+  pinned host memory (on a copy stream, while the previous step computes, as an input
+  pipeline does; the first copy starts after the timer) and the log-likelihoods read back
+  every step;
 * ``roofline``: the parameter-flow launch of the largest sum layer (the kernel with the
   largest share of the step), timed per launch with CUDA events;
 * ``cpu_baseline``: the FP64 CPU restatement (oracle port) on a bounded sample.
@@ -407,8 +409,29 @@ def main():
     ll_host = torch.empty([B, 1], dtype=torch.float32).pin_memory()
     e2e_steps = max(3, args.steps // 2)
 
-    def e2e_step(i):
-        x = host[(i % 8) * B:(i % 8 + 1) * B].to(device, non_blocking=True)
+    # Input pipeline: batch i + 1 is copied (pinned host -> one of two device buffers) on a
+    # copy stream while step i computes; a buffer is refilled only after the step that read
+    # it has finished.
+    copy_stream = torch.cuda.Stream(device=device)
+    xbuf = [torch.empty([B, SIDE * SIDE], dtype=host.dtype, device=device) for _ in range(2)]
+    copied = [torch.cuda.Event() for _ in range(2)]
+    free = [torch.cuda.Event() for _ in range(2)]
+
+    def prefetch(i, after=None):
+        k = i % 2
+        with torch.cuda.stream(copy_stream):
+            if after is not None:
+                copy_stream.wait_event(after)
+            copy_stream.wait_event(free[k])
+            xbuf[k].copy_(host[(i % 8) * B:(i % 8 + 1) * B], non_blocking=True)
+            copied[k].record(copy_stream)
+
+    def e2e_step(i, last):
+        k = i % 2
+        torch.cuda.current_stream().wait_event(copied[k])
+        if i + 1 < last:
+            prefetch(i + 1)
+        x = xbuf[k]
         pc.init_param_flows(flows_memory=0.0)
         # the public API's own CUDA-graph option: the inner passes are recorded once, then replayed
         lls = pc(x, force_use_bf16=True, record_cudagraph=True)
@@ -416,14 +439,17 @@ def main():
         allreduce_flows()
         pc.mini_batch_em(step_size=STEP_SIZE, pseudocount=PSEUDOCOUNT)
         ll_host.copy_(lls.detach(), non_blocking=True)
+        free[k].record()
 
+    prefetch(0)
     for i in range(2):
-        e2e_step(i)
+        e2e_step(i, 2)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
+    prefetch(0, after=e0)
     for i in range(e2e_steps):
-        e2e_step(i)
+        e2e_step(i, e2e_steps)
     e1.record()
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
