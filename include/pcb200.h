@@ -142,15 +142,15 @@ int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int32_t B,
 
 /*
  * pcb_prod_gather_sum backward in overwrite mode (accum = 0, linear flows) fused with
- * pcb_modify_flows: rows r in [modify_row0, modify_row1) receive log(sum) - node_mars[r]
- * (-inf where node_mars is -inf) instead of the sum, other rows the sum. Valid when this
- * launch is the only writer of those rows (their flows are complete when written).
- * Replaces the same reference kernels as the two launches it combines.
+ * pcb_modify_flows: the rows of blocks g with block_rewrite[g] != 0 (device array, one entry
+ * per block) receive log(sum) - node_mars (-inf where node_mars is -inf) instead of the sum,
+ * other rows the sum. Valid when this launch is the only writer of the flagged rows (their
+ * flows are complete when written). Replaces the same reference kernels as the two
+ * launches it combines.
  */
 int pcb_prod_gather_sum_modify(const float* in, float* out, int64_t ld, int32_t B, const int32_t* blk_row,
                                const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs, int32_t num_blocks,
-                               int32_t blk_size, const float* node_mars, int64_t modify_row0, int64_t modify_row1,
-                               void* stream);
+                               int32_t blk_size, const float* node_mars, const int32_t* block_rewrite, void* stream);
 
 /*
  * Log-sum-exp contraction over tiles, FP32 FMA (plain) or BF16 tensor-core (prec=1):

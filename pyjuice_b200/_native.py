@@ -69,7 +69,7 @@ _SIGS = {
     "pcb_prod_gather_sum": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_prod_gather_sum_modify": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
-                                    c_int32, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
+                                    c_int32, c_int32, c_void_p, c_void_p, c_void_p], c_int32),
     "pcb_lse_contract": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                           c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_short": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,

@@ -5,14 +5,14 @@
 
 namespace {
 
-// MOD (overwrite, linear flows only): rows in [mod0, mod1) are written as log(sum) - nm, the
-// sum layer's "modified" node flows (log f - log m), instead of the sum itself.
+// MOD (overwrite, linear flows only): the rows of blocks g with mod_blk[g] != 0 are written as
+// log(sum) - nm, the sum layer's "modified" node flows (log f - log m), instead of the sum.
 template <bool ACCUM, bool LSE, bool MOD = false>
 __global__ void __launch_bounds__(256)
 prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, int B, const int* __restrict__ blk_row,
             const int* __restrict__ blk_off, const int* __restrict__ blk_cnt, const int* __restrict__ chs,
-            int blk_size, int ngrp, int64_t total, bool vec, const float* __restrict__ nm, int64_t mod0,
-            int64_t mod1) {
+            int blk_size, int ngrp, int64_t total, bool vec, const float* __restrict__ nm,
+            const int* __restrict__ mod_blk) {
     // The block tables (and the first 8 child indices) are read before the wait for the
     // previous kernel: they are compiled once and never written by a pass.
     pcb::pdl_trigger();
@@ -26,6 +26,7 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
     const int off = __ldg(blk_off + g);
     const int cnt = __ldg(blk_cnt + g);
     const int64_t row = (int64_t)__ldg(blk_row + g) + i;
+    const bool rewrite = MOD && __ldg(mod_blk + g) != 0;
     int c[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) c[j] = (j < cnt) ? __ldg(chs + off + j) : -1;
@@ -71,7 +72,7 @@ prod_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t ld, i
             pcb::set(acc, q, mq == -INFINITY ? -INFINITY : logf(pcb::get(s, q)) + mq);
         }
     }
-    if (MOD && row >= mod0 && row < mod1) {
+    if (rewrite) {
         const float4 m = pcb::load4(nm, row, ld, b, B, vec, 0.f);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -126,22 +127,22 @@ extern "C" int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int3
     if (!accum && !logsumexp) {
         return pcb::launch_status(pcb::launch_k(prod_kernel<false, false>, dim3(grid), dim3(256), 0, s, 1u, in, out,
                                                 ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec,
-                                                static_cast<const float*>(nullptr), (int64_t)0, (int64_t)0),
+                                                static_cast<const float*>(nullptr), static_cast<const int*>(nullptr)),
                                   "pcb_prod_gather_sum");
     } else if (accum && !logsumexp) {
         return pcb::launch_status(pcb::launch_k(prod_kernel<true, false>, dim3(grid), dim3(256), 0, s, 1u, in, out,
                                                 ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec,
-                                                static_cast<const float*>(nullptr), (int64_t)0, (int64_t)0),
+                                                static_cast<const float*>(nullptr), static_cast<const int*>(nullptr)),
                                   "pcb_prod_gather_sum");
     } else if (!accum && logsumexp) {
         return pcb::launch_status(pcb::launch_k(prod_kernel<false, true>, dim3(grid), dim3(256), 0, s, 1u, in, out,
                                                 ld, B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec,
-                                                static_cast<const float*>(nullptr), (int64_t)0, (int64_t)0),
+                                                static_cast<const float*>(nullptr), static_cast<const int*>(nullptr)),
                                   "pcb_prod_gather_sum");
     } else {
         return pcb::launch_status(pcb::launch_k(prod_kernel<true, true>, dim3(grid), dim3(256), 0, s, 1u, in, out, ld,
                                                 B, blk_row, blk_off, blk_cnt, chs, blk_size, ngrp, total, vec,
-                                                static_cast<const float*>(nullptr), (int64_t)0, (int64_t)0),
+                                                static_cast<const float*>(nullptr), static_cast<const int*>(nullptr)),
                                   "pcb_prod_gather_sum");
     }
 }
@@ -149,9 +150,9 @@ extern "C" int pcb_prod_gather_sum(const float* in, float* out, int64_t ld, int3
 extern "C" int pcb_prod_gather_sum_modify(const float* in, float* out, int64_t ld, int32_t B, const int32_t* blk_row,
                                           const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs,
                                           int32_t num_blocks, int32_t blk_size, const float* node_mars,
-                                          int64_t modify_row0, int64_t modify_row1, void* stream) {
-    if (!in || !out || !blk_row || !blk_off || !blk_cnt || !chs || !node_mars || B <= 0 || ld < B || num_blocks < 0 ||
-        blk_size <= 0 || modify_row0 < 0 || modify_row1 < modify_row0)
+                                          const int32_t* block_rewrite, void* stream) {
+    if (!in || !out || !blk_row || !blk_off || !blk_cnt || !chs || !node_mars || !block_rewrite || B <= 0 || ld < B ||
+        num_blocks < 0 || blk_size <= 0)
         return pcb::set_error(PCB_E_ARG, "pcb_prod_gather_sum_modify: bad arguments");
     if (num_blocks == 0) return PCB_OK;
     const int ngrp = (int)pcb::cdiv(B, 4);
@@ -159,8 +160,7 @@ extern "C" int pcb_prod_gather_sum_modify(const float* in, float* out, int64_t l
     const bool vec = pcb::vec_ok(in, ld) && pcb::vec_ok(out, ld) && pcb::vec_ok(node_mars, ld);
     return pcb::launch_status(pcb::launch_k(prod_kernel<false, false, true>, dim3((unsigned)pcb::cdiv(total, 256)),
                                             dim3(256), 0, pcb::as_stream(stream), 1u, in, out, ld, B, blk_row, blk_off,
-                                            blk_cnt, chs, blk_size, ngrp, total, vec, node_mars, modify_row0,
-                                            modify_row1),
+                                            blk_cnt, chs, blk_size, ngrp, total, vec, node_mars, block_rewrite),
                               "pcb_prod_gather_sum_modify");
 }
 

@@ -629,15 +629,15 @@ class ProdLayer(Layer):
         ld = node_flows.stride(0)
         if element_flows.stride(0) != ld:
             raise ValueError("node_flows and element_flows must share a row-major layout")
-        # _modify = (node_mars, row0, row1): the flows of rows [row0, row1) are written as
-        # log f - log m (what the sum layer below would rewrite them to); overwrite mode only
+        # _modify = (node_mars, block flags): the flows of the flagged child blocks are written
+        # as log f - log m (what the sum layer below would rewrite them to); overwrite mode only
         mod = kwargs.get("_modify")
         if mod is not None:
             if self.bk_accumulate or logspace_flows:
                 raise RuntimeError("fused flow rewriting needs an overwriting product layer and linear flows")
             nat.call("pcb_prod_gather_sum_modify", nat.ptr(element_flows), nat.ptr(node_flows), ld, B,
                      nat.ptr(d["bk_row"]), nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]),
-                     d["bk_row"].size(0), self.block_size, nat.ptr(mod[0]), mod[1], mod[2], nat.stream())
+                     d["bk_row"].size(0), self.block_size, nat.ptr(mod[0]), nat.ptr(mod[1]), nat.stream())
             return
         nat.call("pcb_prod_gather_sum", nat.ptr(element_flows), nat.ptr(node_flows), ld, B, nat.ptr(d["bk_row"]),
                  nat.ptr(d["bk_off"]), nat.ptr(d["bk_cnt"]), nat.ptr(d["bk_chs"]), d["bk_row"].size(0),

@@ -278,6 +278,50 @@ class TensorCircuit(nn.Module):
                     bw = ech.astype(np.int32).reshape(-1)
             self._fusion_host[gi] = dict(fw=fw, bw=bw)
 
+    def _rewrite_plan(self, fused_prod=frozenset()):
+        """Large sum layers whose node flows the product layers write already rewritten as
+        log f - log m: every row written by exactly one overwriting single-layer product
+        group that is not fused into an element-flow kernel in this pass (``fused_prod``).
+        Returns ({product group: device flags per child block}, {rewritten sum groups});
+        cached per device, large-layer threshold and fused set."""
+        fused_prod = frozenset(fused_prod)
+        key = (self.device.type, self.device.index, SumLayer.tc05_min_tiles, fused_prod)
+        plan = self._rewrite_plans.get(key)
+        if plan is not None:
+            return plan
+        groups = self.inner_layer_groups
+        nw, wr = self._row_nwriters, self._row_writer
+        ranges, done = [], set()
+        for gs, group in enumerate(groups):
+            if not group.is_sum() or len(group) != 1:
+                continue
+            layer = group[0]
+            if layer._host_desc()["fw_tiles"].size(0) < SumLayer.tc05_min_tiles:
+                continue
+            lo, hi = layer._layer_nid_range
+            if hi <= lo or not np.all(nw[lo:hi] == 1):
+                continue
+            gps = np.unique(wr[lo:hi])
+            if np.any(gps < 0) or any(groups[int(g)][0].bk_accumulate or int(g) in fused_prod for g in gps):
+                continue
+            ranges.append((int(lo), int(hi)))
+            done.add(gs)
+        flags = dict()
+        if ranges:
+            for gp, group in enumerate(groups):
+                if not group.is_prod() or len(group) != 1 or gp in fused_prod:
+                    continue
+                layer = group[0]
+                rows = layer._host_desc()["bk_row"].numpy().astype(np.int64)
+                inside = np.zeros(rows.shape[0], dtype=bool)
+                for lo, hi in ranges:
+                    inside |= (rows >= lo) & (rows + layer.block_size <= hi)
+                if inside.any():
+                    flags[gp] = torch.from_numpy(inside.astype(np.int32)).to(self.device)
+        plan = (flags, done)
+        self._rewrite_plans[key] = plan
+        return plan
+
     def _fusion_tables(self, gi: int, kind: str):
         """Device table ``kind`` ("fw" or "bw") of product group ``gi`` (None if not fusable)."""
         h = self._fusion_host.get(gi)
@@ -321,17 +365,10 @@ class TensorCircuit(nn.Module):
                 written[tgt] = True
                 nwriters[tgt] += 1
                 writer[tgt] = gi if len(group) == 1 else -2
-        # Sum layers whose node flows come complete from one overwriting product layer: that
-        # product layer can write them already rewritten as log f - log m.
-        self._rewrite_fusion = dict()
-        for gs, group in enumerate(self.inner_layer_groups):
-            if not group.is_sum() or len(group) != 1:
-                continue
-            lo, hi = group[0]._layer_nid_range
-            gp = int(writer[lo]) if hi > lo else -1
-            if gp >= 0 and np.all(nwriters[lo:hi] == 1) and np.all(writer[lo:hi] == gp) and \
-                    not self.inner_layer_groups[gp][0].bk_accumulate:
-                self._rewrite_fusion[gp] = (gs, int(lo), int(hi))
+        # kept for _rewrite_plan: how many product layers write each row, and which group
+        # (-2: a group of several layers)
+        self._row_nwriters, self._row_writer = nwriters, writer
+        self._rewrite_plans = dict()
         r0, r1 = self._root_node_range
         need |= ~written
         need[r0:r1] = False
@@ -620,25 +657,33 @@ class TensorCircuit(nn.Module):
                     el_ready.record(sides[0])
         kwargs = dict(kwargs, _weights_packed=True)
         turn = 0
-        fused_prod, rewritten = set(), set()
-
         def rewrites(g):  # large layers rewrite their node flows as log f - log m
             return allow_modify_flows and any(
                 layer._desc(self.device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles
                 for layer in self.inner_layer_groups[g])
+
+        # product layers fused into the element-flow kernel above them in this pass
+        fuse_bw = dict()
+        for g, group in enumerate(self.inner_layer_groups):
+            if not group.is_sum() or rewrites(g) or logspace_flows:
+                continue
+            fz = self._fusion_tables(g - 1, "bw")
+            if fz is not None and group[0].runs_single_stage(self.device, B, force_use_fp32=force_use_fp32,
+                                                             backward=True):
+                fuse_bw[g] = fz
+        fused_prod = set(g - 1 for g in fuse_bw)
+        rw_flags, rewritten = (self._rewrite_plan(fused_prod) if (TensorCircuit.fuse_flow_rewrite and
+                                                                  allow_modify_flows and not logspace_flows)
+                               else (dict(), set()))
 
         for layer_id in range(len(self.inner_layer_groups) - 1, -1, -1):
             group = self.inner_layer_groups[layer_id]
             if group.is_prod():
                 if layer_id in fused_prod:  # the sum layer above wrote these flows
                     continue
-                rf = self._rewrite_fusion.get(layer_id) if TensorCircuit.fuse_flow_rewrite else None
-                if rf is not None and not logspace_flows and rewrites(rf[0]):
-                    group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows,
-                                   _modify=(self.node_mars, rf[1], rf[2]))
-                    rewritten.add(rf[0])
-                else:
-                    group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows)
+                rf = rw_flags.get(layer_id)
+                group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows,
+                               _modify=None if rf is None else (self.node_mars, rf))
             else:
                 # The element values of the forward pass are still resident (no recomputation). Small
                 # layers form log f - log m inside the flow kernels instead of rewriting the node flows
@@ -648,12 +693,7 @@ class TensorCircuit(nn.Module):
                 if el_ready is not None:
                     main.wait_event(el_ready)
                     el_ready = None
-                fz = None if (modify or logspace_flows) else self._fusion_tables(layer_id - 1, "bw")
-                if fz is not None and not group[0].runs_single_stage(self.device, B, force_use_fp32=force_use_fp32,
-                                                                     backward=True):
-                    fz = None
-                if fz is not None:
-                    fused_prod.add(layer_id - 1)
+                fz = fuse_bw.get(layer_id)
                 group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
