@@ -63,13 +63,13 @@ typedef struct {
     int32_t reserved;
 } PcbPflowTile;
 
-/* Version of the library ABI (currently 1). */
+/* Version of the library ABI (currently 1). No counterpart in the reference (library utility). */
 int pcb_version(void);
 
-/* Last error message of the calling host thread ("" if none). */
+/* Last error message of the calling host thread ("" if none). No counterpart in the reference (library utility). */
 const char* pcb_last_error(void);
 
-/* Number of SMs of the current device (for grid sizing on the host). */
+/* Number of SMs of the current device (for grid sizing on the host). No counterpart in the reference (library utility). */
 int pcb_num_sms(void);
 
 /*
@@ -213,6 +213,8 @@ int pcb_lse_contract_short(const float* src, const float* src2, const float* aux
  * rounded to bf16 (first 32 KB) and the bf16 rounding of the remainder (next 32 KB), in
  * the canonical no-swizzle K-major layout of a 128 x 128 tensor-core operand; rows and
  * terms beyond the tile are zero. packed must be 16-byte aligned.
+ * No counterpart in the reference: its Triton kernels convert the weights inside each
+ * contraction (sum_layer.py:534-541).
  */
 int pcb_pack_weights(const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t rows_per_block,
                      const int32_t* kw, int32_t w_stride, uint8_t* packed, void* stream);
@@ -220,6 +222,7 @@ int pcb_pack_weights(const float* params, const PcbLseTile* tiles, int32_t num_t
 /*
  * One tile table of a pcb_pack_weights_multi launch: the arguments of one
  * pcb_pack_weights call (rows_per_block as its base-2 logarithm).
+ * No counterpart in the reference (see pcb_pack_weights).
  */
 typedef struct {
     const PcbLseTile* tiles;
@@ -235,6 +238,7 @@ typedef struct {
  * pcb_pack_weights for several tile tables in one launch (device arrays): global tile g
  * (g < total_tiles) is tile tile_index[g] of jobs[tile_job[g]]. The caller guarantees
  * tile_index[g] < that job's num_tiles. Same output as one pcb_pack_weights per job.
+ * No counterpart in the reference (see pcb_pack_weights).
  */
 int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const int32_t* tile_job,
                            const int32_t* tile_index, int32_t total_tiles, void* stream);
@@ -246,6 +250,7 @@ int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const in
  * and run of slices_per_cta consecutive batch_tile-sample slices (batch_tile 32 or 64):
  * the packed weights are copied once per CTA, and the next slice's source values are
  * loaded while the current slice is processed. A tile with more terms produces NaN rows.
+ * Replaces the same reference kernels as pcb_lse_contract.
  */
 int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
                           const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles, const int32_t* krow,
@@ -300,6 +305,7 @@ int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const int32_t* bl
 /*
  * Log-likelihood reduction in FP64: out[0] += sum_b lls[row * ld + b] for b < B.
  * Dataset-level LL accumulation.
+ * No kernel counterpart in the reference (its callers sum log-likelihoods with torch).
  */
 int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double* out, void* stream);
 
