@@ -364,7 +364,7 @@ def main():
             print(json.dumps({"profile_step": True, "kernels_per_step": kernels_per_step}), flush=True)
         return
 
-    def timed(kw, use_graph):
+    def timed(kw, use_graph, sample_clocks=False):
         x_static = data_dev[:B].clone()
         g = None
         if use_graph:
@@ -377,6 +377,9 @@ def main():
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 step(x_static, kw)
+        # nvidia-smi needs a moment to start: the sampler runs from before the warm-up steps
+        # to the end of the timed region
+        clocks = Clocks(local) if sample_clocks else None
         for i in range(args.warmup):
             x_static.copy_(data_dev[(i % 8) * B:(i % 8 + 1) * B])
             g.replay() if g is not None else step(x_static, kw)
@@ -385,7 +388,6 @@ def main():
             import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize()
-        clocks = Clocks(local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for i in range(args.steps):
@@ -393,7 +395,7 @@ def main():
             g.replay() if g is not None else step(x_static, kw)
         e1.record()
         torch.cuda.synchronize()
-        ck = clocks.stop()
+        ck = clocks.stop() if clocks is not None else None
         ms = e0.elapsed_time(e1)
         if group is not None:
             import torch.distributed as dist
@@ -408,7 +410,7 @@ def main():
     SumLayer.bf16_form = 1
     ms_bf16p, _ = timed({"force_use_bf16": True}, use_graph)
     SumLayer.bf16_form = 2
-    ms_bf16, clocks = timed({"force_use_bf16": True}, use_graph)
+    ms_bf16, clocks = timed({"force_use_bf16": True}, use_graph, sample_clocks=True)
     ms_fp32, _ = timed({"force_use_fp32": True}, use_graph)
     value = ws * B * args.steps / (ms_bf16 / 1e3)
     value_fp32 = ws * B * args.steps / (ms_fp32 / 1e3)
@@ -484,6 +486,23 @@ def main():
             SumLayer.bf16_form = 2
             l_bf = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
             l_32 = pc(xs.to(device), force_use_fp32=True).double().cpu().numpy()
+        # parameter-flow error of each form against the FP64 oracle (16 samples, unit root flows)
+        xp = xs[:16]
+        nm_o, ems_o, _ = orc.forward(lay, params, in_params, xp.numpy())
+        _, pf_o, ipf_o = orc.backward(lay, params, xp.numpy(), nm_o, ems_o)
+        pf_err = {}
+        for name, bform, kw in (("bf16_split", 2, {"force_use_bf16": True}), ("bf16_single", 1, {"force_use_bf16": True}),
+                                ("fp32", 2, {"force_use_fp32": True})):
+            SumLayer.bf16_form = bform
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                pc(xp.to(device), **kw)
+            pc.backward(inputs=xp.to(device), allow_modify_flows=True, force_use_fp32="force_use_fp32" in kw)
+            got = pc.param_flows.double().cpu().numpy()
+            gin = pc.input_layer_group[0].param_flows.double().cpu().numpy()[:ipf_o.shape[0]]
+            pf_err[name] = {"sum_max_rel": float(np.abs(got - pf_o).max() / np.abs(pf_o).max()),
+                            "input_max_rel": float(np.abs(gin - ipf_o).max() / np.abs(ipf_o).max())}
+        SumLayer.bf16_form = 2
         ll_err = {"bf16_dmean_ll_nats": float(abs(l_bf.mean() - lls_o.mean())),
                   "bf16_mean_abs_dll_nats": float(np.abs(l_bf - lls_o).mean()),
                   "bf16_single_dmean_ll_nats": float(abs(l_bp.mean() - lls_o.mean())),
@@ -528,6 +547,7 @@ def main():
             "fp32_plain": {"value": value_fp32, "unit": "samples/s", "ms_per_step": ms_fp32 / args.steps},
             "bf16_single": {"value": value_bf16p, "unit": "samples/s", "ms_per_step": ms_bf16p / args.steps},
             "ll_error_vs_fp64": ll_err,
+            "param_flow_rel_err_vs_fp64": {"samples": 16, "measure": "max |pf - pf_fp64| / max |pf_fp64|", **pf_err},
             "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": B * SIDE * SIDE * 8,
                     "d2h_bytes_per_step": B * 4},
             "gpu_launches": kernels_per_step * args.steps,

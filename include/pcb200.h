@@ -28,6 +28,12 @@ extern "C" {
 #define PCB_E_LAUNCH -2    /* CUDA launch error */
 #define PCB_E_CUDA -3      /* other CUDA runtime error */
 
+/* Bits of the device status word (pcb_device_status): faults that kernels detect on the
+ * device, where they cannot return an error code. The affected outputs are NaN. */
+#define PCB_STATUS_WAIT_TIMEOUT 1   /* a bounded wait (mbarrier: bulk copy or MMA completion) ran out */
+#define PCB_STATUS_TILE_TOO_LONG 2  /* a contraction tile had more terms than the kernel handles */
+#define PCB_STATUS_BAD_CATEGORY 4   /* an input value outside [0, num_cats) */
+
 /*
  * One tile of an LSE contraction (sum forward / element flows). A tile covers n_rows
  * consecutive output rows made of consecutive blocks of `rows_per_block` rows (the
@@ -73,6 +79,24 @@ const char* pcb_last_error(void);
 int pcb_num_sms(void);
 
 /*
+ * Device status word of the current device: waits for `stream`, writes the OR of all
+ * PCB_STATUS_* bits reported by kernels since the last clear to *out (host memory) and,
+ * if clear != 0, resets it (on `stream`). Synchronises the stream. The word is per device
+ * and shared by all streams and callers on it.
+ * No counterpart in the reference (its Triton kernels have no device-side error channel;
+ * the host asserts before launch, e.g. src/pyjuice/layer/sum_layer.py:819, 842-844).
+ */
+int pcb_device_status(int32_t* out, int32_t clear, void* stream);
+
+/*
+ * Test of the device error channel: one CTA polls an mbarrier that nothing completes at
+ * most spin_limit times (the bounded wait of pcb_lse_contract_tc05), then reports
+ * PCB_STATUS_WAIT_TIMEOUT and returns; the context stays usable.
+ * No counterpart in the reference (library self-test).
+ */
+int pcb_status_selftest(int32_t spin_limit, void* stream);
+
+/*
  * Fill rows [row0, row1) of a rows x ld matrix with `value` (all ld columns).
  * Replaces the buffer initialisations of TensorCircuit.forward / backward
  * (src/pyjuice/model/tensorcircuit.py:240-241, 394-395) for the rows that are read
@@ -83,7 +107,8 @@ int pcb_fill_rows(float* mat, int64_t ld, int64_t row0, int64_t row1, float valu
 /*
  * Categorical input layer forward: node_mars[node_offset + n, b] =
  *   log(params[s_pids[n] + data[vids[n] * data_ld + b]]) for n < num_nodes, b < B
- * (NaN where the category is outside [0, ncats[n])). data is int64 [num_vars, data_ld].
+ * (NaN where the category is outside [0, ncats[n]), reported as PCB_STATUS_BAD_CATEGORY).
+ * data is int64 [num_vars, data_ld].
  * Replaces InputLayer._mars_kernel_template + Categorical.fw_mar_fn
  * (src/pyjuice/layer/input_layer.py:1016-1054, src/pyjuice/nodes/distributions/categorical.py:83-91).
  */
@@ -197,7 +222,7 @@ typedef struct {
  * do (element-flow tables). packed (BF16 forms only, may be NULL): the same tiles' weights
  * as written by pcb_pack_weights; the kernel then copies them instead of reading params.
  * The caller guarantees k_cnt <= 128 and the wlayout property; a tile with more terms
- * produces NaN rows.
+ * produces NaN rows and reports PCB_STATUS_TILE_TOO_LONG.
  * Replaces the same sum-layer kernels as pcb_lse_contract (small-K case).
  */
 int pcb_lse_contract_short(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
@@ -249,7 +274,9 @@ int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const in
  * using the weights packed by pcb_pack_weights from the same tile table. One CTA per tile
  * and run of slices_per_cta consecutive batch_tile-sample slices (batch_tile 32 or 64):
  * the packed weights are copied once per CTA, and the next slice's source values are
- * loaded while the current slice is processed. A tile with more terms produces NaN rows.
+ * loaded while the current slice is processed. A tile with more terms produces NaN rows
+ * (PCB_STATUS_TILE_TOO_LONG); a bounded wait that runs out NaN rows and
+ * PCB_STATUS_WAIT_TIMEOUT.
  * Replaces the same reference kernels as pcb_lse_contract.
  */
 int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld, int32_t B,
@@ -295,6 +322,26 @@ int pcb_sum_em(float* params, const float* param_flows, const int64_t* blk_pbase
                double step_size, double pseudocount, int32_t keep_zero_params, void* stream);
 
 /*
+ * FP64 epoch-level parameter flows. pcb_flows_accumulate_f64: acc[i] += flows[i] (i < n),
+ * after each batch's FP32 parameter flows; pcb_pflow_accum_f64: pcb_pflow_accum on FP64
+ * flows (tied slots summed into the source slot); pcb_sum_em_f64flows /
+ * pcb_input_cat_em_f64flows: pcb_sum_em / pcb_input_cat_em reading FP64 flows.
+ * The reference accumulates parameter flows over batches in FP32 with atomics
+ * (src/pyjuice/layer/sum_layer.py:2167-2169, TensorCircuit.cumulate_flows
+ * src/pyjuice/model/tensorcircuit.py:592-595) and runs the same EM update
+ * (par_update.py:174-256, categorical.py:164-244); these keep the epoch's sum in FP64.
+ */
+int pcb_flows_accumulate_f64(double* acc, const float* flows, int64_t n, void* stream);
+int pcb_pflow_accum_f64(double* param_flows, int64_t dst, int64_t n, const int64_t* srcs, int32_t nsrc, void* stream);
+int pcb_sum_em_f64flows(float* params, const double* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
+                        const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks, double step_size,
+                        double pseudocount, int32_t keep_zero_params, void* stream);
+int pcb_input_cat_em_f64flows(float* params, const double* param_flows, const int32_t* s_pids,
+                              const int32_t* s_pfids, const int32_t* ncats, const int32_t* source_nids,
+                              int32_t num_source_nodes, double step_size, double pseudocount,
+                              int32_t keep_zero_params, void* stream);
+
+/*
  * Sum-parameter normalisation (FP64), same block table as pcb_sum_em:
  *   theta' = (p + pc / nch) / (sum_k p + pc)
  * Replaces cum_par_kernel + par_update_kernel (src/pyjuice/model/backend/normalize.py:13-68).
@@ -315,7 +362,10 @@ int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double*
  * src/pyjuice/layer/input_layer.py:1222-1249, categorical.py:137-161).
  * Per sample s, nlist[s * cap_n + j] (j < ncnt[s]) are its active node ids and
  * elist[s * cap_e + j] (j < ecnt[s]) its active element ids. Uniform draws are
- * u(seed, id, s) = top 24 bits of SplitMix64(seed + ((id << 32) | s + 1) * 0x9E3779B97F4A7C15) / 2^24.
+ * u(seed, id, s) = top 24 bits of SplitMix64(seed + ((id << 32) | s + 1) * 0x9E3779B97F4A7C15) / 2^24,
+ * or, when `uniforms` is not NULL, uniforms[id * u_ld + s] (a [num_nodes, u_ld >= S] FP32
+ * table, so that the draws of another sampler, e.g. the reference's tl.rand draws as
+ * recorded per node and sample, are replayed exactly; seed is then unused).
  * *err is set to 1 on list overflow, 2 on an element outside the product group.
  *
  * pcb_sample_sum: nodes of the sum layer [lo, hi) (block size bs) choose the first child
@@ -330,13 +380,14 @@ int pcb_ll_sum_f64(const float* lls, int64_t ld, int32_t B, int64_t row, double*
 int pcb_sample_sum(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt, int32_t S, int32_t cap_n,
                    int32_t cap_e, int32_t lo, int32_t hi, int32_t bs, const int32_t* node2blk, const int32_t* blk_nid,
                    const int32_t* blk_koff, const int32_t* blk_kcnt, const int32_t* krow, const int32_t* kw,
-                   const float* params, uint64_t seed, int32_t* err, void* stream);
+                   const float* params, const float* uniforms, int64_t u_ld, uint64_t seed, int32_t* err,
+                   void* stream);
 int pcb_sample_prod(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt, int32_t S, int32_t cap_n,
                     int32_t cap_e, int32_t elo, int32_t ehi, const int32_t* elem2blk, const int32_t* blk_row,
                     const int32_t* blk_off, const int32_t* blk_cnt, const int32_t* chs, int32_t* err, void* stream);
 int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
                      const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, const float* params,
-                     int64_t* samples, int64_t sld, uint64_t seed, void* stream);
+                     int64_t* samples, int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream);
 
 /*
  * Whole-circuit sampling that allocates nothing. No counterpart in the reference: the
@@ -365,8 +416,11 @@ int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32
  * (cudaGetSymbolAddress; with lazy module loading the runtime loads the module and
  * reserves the array at that point); make that first call before any stream capture.
  * *err is set to zero by the call (cudaMemsetAsync on `stream`), then to 1 on list
- * overflow, 2 on an element outside its product layer. samples[s * sld + v] is written
- * for every variable v that sample s draws; other entries are left as they are.
+ * overflow, 2 on an element outside its product layer, 3 on a malformed step (kind not
+ * 0, 1 or 2, or a sum step with bs <= 0; that sample stops there). samples[s * sld + v]
+ * is written for every variable v that sample s draws; other entries are left as they are.
+ * The kernel runs on the current device, which must be the device that holds the step
+ * table, the tables it points to and the buffers.
  */
 #define PCB_SAMPLE_NOALLOC_MAX_INTS (1 << 21)
 typedef struct {

@@ -250,8 +250,12 @@ def _sum_block_table(layout: dict):
 
 
 def em_update(layout: dict, params: np.ndarray, pf: np.ndarray, in_params: np.ndarray, in_pf: np.ndarray,
-              step_size: float, pseudocount: float):
-    """One EM step (keep_zero_params=False); returns new (params, in_params) as float64."""
+              step_size: float, pseudocount: float, keep_zero_params: bool = False):
+    """One EM step; returns new (params, in_params) as float64.
+
+    keep_zero_params (par_update.py:199-203, 238-248; categorical.py:180-198): parameters
+    below 1e-12 stay zero, and the normaliser is the sum of ``flow + pc / n`` over the
+    other entries (no extra pseudocount)."""
     newp = params.astype(np.float64).copy()
     for p0, (nch, bs, f0s) in _sum_block_table(layout).items():
         n = nch * bs
@@ -259,8 +263,14 @@ def em_update(layout: dict, params: np.ndarray, pf: np.ndarray, in_params: np.nd
         for f0 in f0s:
             f += pf[f0:f0 + n]
         f = f.reshape(nch, bs)
-        tot = f.sum(axis=0)                                    # per node of the block
         old = newp[p0:p0 + n].reshape(nch, bs)
+        if keep_zero_params:
+            nz = old >= 1e-12
+            tot = np.where(nz, f + pseudocount / nch, 0.0).sum(axis=0)
+            upd = (1 - step_size) * old + step_size * (f + pseudocount / nch) / tot
+            newp[p0:p0 + n] = np.where(nz, upd, 0.0).reshape(-1)
+            continue
+        tot = f.sum(axis=0)                                    # per node of the block
         newp[p0:p0 + n] = ((1 - step_size) * old + step_size * (f + pseudocount / nch) / (tot + pseudocount)).reshape(-1)
     inp = layout["input"]
     new_in = in_params.astype(np.float64).copy()
@@ -273,9 +283,25 @@ def em_update(layout: dict, params: np.ndarray, pf: np.ndarray, in_params: np.nd
         sp = np.unique(sel[:, 0])
         rows = sp[:, None] + ar                                # [n, K]
         f = acc[rows]
+        if keep_zero_params:
+            old = new_in[rows]
+            nz = old >= 1e-12
+            tot = np.where(nz, f + pseudocount / K, 0.0).sum(axis=1, keepdims=True)
+            new_in[rows] = np.where(nz, (1 - step_size) * old + step_size * (f + pseudocount / K) / tot, 0.0)
+            continue
         new_in[rows] = (1 - step_size) * new_in[rows] + step_size * (f + pseudocount / K) / (
             f.sum(axis=1, keepdims=True) + pseudocount)
     return newp, new_in
+
+
+def normalize(layout: dict, params: np.ndarray, pseudocount: float) -> np.ndarray:
+    """Sum-to-one normalisation of every node's weights, ``(p + pc / n) / (sum p + pc)``
+    (nodes/backend/normalize.py:13-68, model/tensorcircuit.py:1118-1120)."""
+    newp = params.astype(np.float64).copy()
+    for p0, (nch, bs, _) in _sum_block_table(layout).items():
+        w = newp[p0:p0 + nch * bs].reshape(nch, bs)
+        newp[p0:p0 + nch * bs] = ((w + pseudocount / nch) / (w.sum(axis=0) + pseudocount)).reshape(-1)
+    return newp
 
 
 # ----------------------------------------------------------------------------- sampling
@@ -288,6 +314,19 @@ def uniform(seed: int, node: int, sample: int) -> np.float32:
     z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
     z = z ^ (z >> 31)
     return np.float32((z >> 40) * (1.0 / 16777216.0))
+
+
+def uniform_table(seed: int, num_nodes: int, num_samples: int) -> np.ndarray:
+    """``[num_nodes, num_samples]`` float32 table of :func:`uniform` (vectorised)."""
+    g = np.uint64(0x9E3779B97F4A7C15)
+    with np.errstate(over="ignore"):
+        ctr = (np.arange(num_nodes, dtype=np.uint64)[:, None] << np.uint64(32)) | \
+            np.arange(num_samples, dtype=np.uint64)[None, :]
+        z = np.uint64(seed) + (ctr + np.uint64(1)) * g
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return ((z >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0)).astype(np.float32)
 
 
 def sample(layout: dict, params: np.ndarray, in_params: np.ndarray, num_samples: int, seed: int,

@@ -35,21 +35,50 @@ def _nvcc():
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile ``libpcb200.so`` for sm_100a if it is missing or older than its sources."""
+    """Compile ``libpcb200.so`` for sm_100a if it is missing or older than its sources.
+
+    Each source is compiled to its own object (in parallel, under ``_build/``; an object is
+    rebuilt when it is older than its source or a shared header), then the objects are
+    linked. The kernels of different files share no device symbols, so no relocatable
+    device code is needed.
+    """
+    from concurrent.futures import ThreadPoolExecutor
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "lse_stage.cuh"),
-                   os.path.join(_HERE, "..", "include", "pcb200.h")]
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(_HERE, "..", "include", "pcb200.h"))
+    newest_header = max(os.path.getmtime(h) for h in headers if os.path.exists(h))
     if not force and os.path.exists(LIB_PATH):
         lib_m = os.path.getmtime(LIB_PATH)
-        if all(os.path.getmtime(d) <= lib_m for d in deps if os.path.exists(d)):
+        if all(os.path.getmtime(d) <= lib_m for d in srcs) and newest_header <= lib_m:
             return LIB_PATH
-    tmp = LIB_PATH + ".tmp"
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + srcs
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("building libpcb200.so failed:\n" + res.stdout + res.stderr)
+    bdir = os.path.join(_HERE, "_build")
+    os.makedirs(bdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src):
+        obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), newest_header):
+            return obj, None
+        res = subprocess.run([_nvcc()] + compile_flags + ["-c", "-o", obj + ".tmp", src], capture_output=True, text=True)
+        if res.returncode != 0:
+            return obj, res.stdout + res.stderr
+        os.replace(obj + ".tmp", obj)
+        return obj, (res.stdout + res.stderr) if verbose else None
+
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, srcs))
+    errors = [msg for obj, msg in results if msg and not os.path.exists(obj)]
+    if errors:
+        raise RuntimeError("building libpcb200.so failed:\n" + "\n".join(errors))
     if verbose:
-        print(res.stdout + res.stderr)
+        for _, msg in results:
+            if msg:
+                print(msg)
+    tmp = LIB_PATH + ".tmp"
+    res = subprocess.run([_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp]
+                         + [obj for obj, _ in results], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("linking libpcb200.so failed:\n" + res.stdout + res.stderr)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 
@@ -58,6 +87,8 @@ _SIGS = {
     "pcb_version": ([], c_int32),
     "pcb_last_error": ([], ctypes.c_char_p),
     "pcb_num_sms": ([], c_int32),
+    "pcb_device_status": ([c_void_p, c_int32, c_void_p], c_int32),
+    "pcb_status_selftest": ([c_int32, c_void_p], c_int32),
     "pcb_fill_rows": ([c_void_p, c_int64, c_int64, c_int64, c_float, c_void_p], c_int32),
     "pcb_input_cat_fwd": ([c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
                            c_int64, c_int32, c_void_p], c_int32),
@@ -84,15 +115,21 @@ _SIGS = {
                         c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_sum_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double, c_int32,
                     c_void_p], c_int32),
+    "pcb_sum_em_f64flows": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
+                             c_double, c_int32, c_void_p], c_int32),
+    "pcb_input_cat_em_f64flows": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
+                                   c_double, c_int32, c_void_p], c_int32),
+    "pcb_flows_accumulate_f64": ([c_void_p, c_void_p, c_int64, c_void_p], c_int32),
+    "pcb_pflow_accum_f64": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_sum_normalize": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_void_p], c_int32),
     "pcb_ll_sum_f64": ([c_void_p, c_int64, c_int32, c_int64, c_void_p, c_void_p], c_int32),
     "pcb_sample_sum": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
-                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p,
-                        c_void_p], c_int32),
+                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                        c_uint64, c_void_p, c_void_p], c_int32),
     "pcb_sample_prod": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32,
                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
     "pcb_sample_input": ([c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
-                          c_void_p, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
+                          c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
     "pcb_sample_circuit_noalloc": ([c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p, c_int64, c_uint64,
                                     c_void_p, c_void_p], c_int32),
 }
@@ -153,3 +190,23 @@ def ptr(t) -> c_void_p:
 
 def stream() -> c_void_p:
     return c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+STATUS_BITS = {1: "a bounded device wait ran out", 2: "a contraction tile had more terms than the kernel handles",
+               4: "an input value outside [0, num_cats)"}
+
+
+def device_status(clear: bool = True) -> int:
+    """OR of the fault bits the kernels reported on the current device since the last clear
+    (``pcb_device_status``; waits for the current stream)."""
+    out = c_int32(0)
+    call("pcb_device_status", ctypes.byref(out), 1 if clear else 0, stream())
+    return int(out.value)
+
+
+def check_device_status(clear: bool = True) -> None:
+    """Raise ``RuntimeError`` naming every fault bit that is set (see :func:`device_status`)."""
+    st = device_status(clear)
+    if st:
+        what = "; ".join(msg for bit, msg in STATUS_BITS.items() if st & bit) or "unknown"
+        raise RuntimeError(f"device status {st:#x}: {what}")

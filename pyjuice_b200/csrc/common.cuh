@@ -145,6 +145,15 @@ inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
 // Status of a launch_k call: PCB_OK, or PCB_E_LAUNCH with the message recorded.
 int launch_status(cudaError_t e, const char* what);
 
+// Device address of the library's status word on the current device (a __device__ int32 in
+// capi_common.cu, looked up once per device; nullptr if the look-up failed). Kernels OR
+// PCB_STATUS_* bits into it when they detect a fault; pcb_device_status reads it.
+int32_t* status_word();
+
+__device__ __forceinline__ void report_status(int32_t* status, int32_t bits) {
+    if (status) atomicOr(status, bits);
+}
+
 // Vectorised access needs ld % 4 == 0 and a 16-byte aligned base.
 inline bool vec_ok(const void* p, int64_t ld) {
     return (ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);

@@ -10,9 +10,9 @@ namespace {
 
 // Column sums of a [nch x bs] slab for columns [c0, c0 + 256/ROWS...]: thread layout
 // (row group rg, column c); partial sums in shared memory.
-template <bool EM, bool KEEP_ZERO>
+template <bool EM, bool KEEP_ZERO, typename FT>
 __global__ void __launch_bounds__(256)
-sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int64_t* __restrict__ pbase,
+sum_em_kernel(float* __restrict__ params, const FT* __restrict__ pflows, const int64_t* __restrict__ pbase,
               const int64_t* __restrict__ pfbase, const int* __restrict__ nchs, const int* __restrict__ bss,
               double step, double pc) {
     // No early trigger: kernels after this one may read the parameters before their own wait.
@@ -45,7 +45,8 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
     for (int c0 = 0; c0 < bs; c0 += cols) {
         const int col = c0 + c;
         const bool reg = nch <= rgs * R;
-        float pv[R], fv[R];
+        float pv[R];
+        FT fv[R];
         double s = 0.0;
         if (rg < rgs) {
             if (reg) {
@@ -54,7 +55,7 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
                     const int k = rg + j * rgs;
                     const int64_t off = (int64_t)k * bs + col;
                     pv[j] = (k < nch) ? params[pb + off] : 0.f;
-                    fv[j] = (EM && k < nch) ? pflows[fb + off] : 0.f;
+                    fv[j] = (EM && k < nch) ? pflows[fb + off] : FT(0);
                 }
 #pragma unroll
                 for (int j = 0; j < R; ++j) {
@@ -109,9 +110,9 @@ sum_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, cons
 // One warp per source input node, categories strided over the lanes. Nodes of up to 256
 // categories keep their flows and parameters in registers (all loads of a node issued at
 // once, one pass over memory); larger ones take two passes.
-template <bool KEEP_ZERO>
+template <bool KEEP_ZERO, typename FT>
 __global__ void __launch_bounds__(256)
-input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, const int* __restrict__ s_pids,
+input_em_kernel(float* __restrict__ params, const FT* __restrict__ pflows, const int* __restrict__ s_pids,
                 const int* __restrict__ s_pfids, const int* __restrict__ ncats, const int* __restrict__ source_nids,
                 int num_src, double step, double pc) {
     pcb::pdl_wait();  // no early trigger, as in sum_em_kernel
@@ -133,11 +134,12 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
     };
     constexpr int R = 8;
     if (K <= 32 * R) {
-        float f[R], p[R];
+        FT f[R];
+        float p[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int k = lane + 32 * j;
-            f[j] = k < K ? pflows[sf + k] : 0.f;
+            f[j] = k < K ? pflows[sf + k] : FT(0);
             p[j] = k < K ? params[sp + k] : 0.f;
         }
         double s = 0.0;
@@ -167,25 +169,77 @@ input_em_kernel(float* __restrict__ params, const float* __restrict__ pflows, co
     for (int k = lane; k < K; k += 32) params[sp + k] = update((double)params[sp + k], (double)pflows[sf + k], inv);
 }
 
+template <typename FT>
+int sum_em_launch(float* params, const FT* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
+                  const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks, double step_size,
+                  double pseudocount, int32_t keep_zero_params, void* stream, const char* name) {
+    if (!params || !param_flows || !blk_pbase || !blk_pfbase || !blk_nch || !blk_bs || num_blocks < 0)
+        return pcb::set_error(PCB_E_ARG, "%s: bad arguments", name);
+    if (!(step_size > 0.0 && step_size <= 1.0)) return pcb::set_error(PCB_E_ARG, "%s: step_size must be in (0, 1]", name);
+    if (num_blocks == 0) return PCB_OK;
+    cudaStream_t s = pcb::as_stream(stream);
+    if (keep_zero_params) {
+        return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, true, FT>, dim3(num_blocks), dim3(256), 0, s, 1u,
+                                                params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs,
+                                                step_size, pseudocount), name);
+    }
+    return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, false, FT>, dim3(num_blocks), dim3(256), 0, s, 1u,
+                                            params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, step_size,
+                                            pseudocount), name);
+}
+
+template <typename FT>
+int input_em_launch(float* params, const FT* param_flows, const int32_t* s_pids, const int32_t* s_pfids,
+                    const int32_t* ncats, const int32_t* source_nids, int32_t num_source_nodes, double step_size,
+                    double pseudocount, int32_t keep_zero_params, void* stream, const char* name) {
+    if (!params || !param_flows || !s_pids || !s_pfids || !ncats || !source_nids || num_source_nodes < 0)
+        return pcb::set_error(PCB_E_ARG, "%s: bad arguments", name);
+    if (!(step_size > 0.0 && step_size <= 1.0)) return pcb::set_error(PCB_E_ARG, "%s: step_size must be in (0, 1]", name);
+    if (num_source_nodes == 0) return PCB_OK;
+    const unsigned grid = (unsigned)pcb::cdiv((int64_t)num_source_nodes * 32, 256);
+    cudaStream_t s = pcb::as_stream(stream);
+    if (keep_zero_params) {
+        return pcb::launch_status(pcb::launch_k(input_em_kernel<true, FT>, dim3(grid), dim3(256), 0, s, 1u, params,
+                                                param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                                step_size, pseudocount), name);
+    }
+    return pcb::launch_status(pcb::launch_k(input_em_kernel<false, FT>, dim3(grid), dim3(256), 0, s, 1u, params,
+                                            param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                            step_size, pseudocount), name);
+}
+
+// acc[i] += flows[i]: 4 elements per thread, grid-stride.
+__global__ void flows_accumulate_f64_kernel(double* __restrict__ acc, const float* __restrict__ flows, int64_t n) {
+    pcb::pdl_begin();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) acc[i] += (double)flows[i];
+}
+
+__global__ void pflow_accum_f64_kernel(double* __restrict__ pf, int64_t dst, int64_t n,
+                                       const int64_t* __restrict__ srcs, int nsrc) {
+    pcb::pdl_begin();
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int j = 0; j < nsrc; ++j) s += pf[srcs[j] + i];
+    pf[dst + i] = s;
+}
+
 }  // namespace
 
 extern "C" int pcb_sum_em(float* params, const float* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
                           const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks, double step_size,
                           double pseudocount, int32_t keep_zero_params, void* stream) {
-    if (!params || !param_flows || !blk_pbase || !blk_pfbase || !blk_nch || !blk_bs || num_blocks < 0)
-        return pcb::set_error(PCB_E_ARG, "pcb_sum_em: bad arguments");
-    if (!(step_size > 0.0 && step_size <= 1.0)) return pcb::set_error(PCB_E_ARG, "pcb_sum_em: step_size must be in (0, 1]");
-    if (num_blocks == 0) return PCB_OK;
-    cudaStream_t s = pcb::as_stream(stream);
-    if (keep_zero_params) {
-        return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, true>, dim3(num_blocks), dim3(256), 0, s, 1u,
-                                                params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs,
-                                                step_size, pseudocount), "pcb_sum_em");
-    } else {
-        return pcb::launch_status(pcb::launch_k(sum_em_kernel<true, false>, dim3(num_blocks), dim3(256), 0, s, 1u,
-                                                params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs,
-                                                step_size, pseudocount), "pcb_sum_em");
-    }
+    return sum_em_launch<float>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, num_blocks, step_size,
+                                pseudocount, keep_zero_params, stream, "pcb_sum_em");
+}
+
+extern "C" int pcb_sum_em_f64flows(float* params, const double* param_flows, const int64_t* blk_pbase,
+                                   const int64_t* blk_pfbase, const int32_t* blk_nch, const int32_t* blk_bs,
+                                   int32_t num_blocks, double step_size, double pseudocount, int32_t keep_zero_params,
+                                   void* stream) {
+    return sum_em_launch<double>(params, param_flows, blk_pbase, blk_pfbase, blk_nch, blk_bs, num_blocks, step_size,
+                                 pseudocount, keep_zero_params, stream, "pcb_sum_em_f64flows");
 }
 
 extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const int32_t* blk_nch, const int32_t* blk_bs,
@@ -193,7 +247,7 @@ extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const 
     if (!params || !blk_pbase || !blk_nch || !blk_bs || num_blocks < 0)
         return pcb::set_error(PCB_E_ARG, "pcb_sum_normalize: bad arguments");
     if (num_blocks == 0) return PCB_OK;
-    return pcb::launch_status(pcb::launch_k(sum_em_kernel<false, false>, dim3(num_blocks), dim3(256), 0,
+    return pcb::launch_status(pcb::launch_k(sum_em_kernel<false, false, float>, dim3(num_blocks), dim3(256), 0,
                                             pcb::as_stream(stream), 1u, params, nullptr, blk_pbase, nullptr, blk_nch,
                                             blk_bs, 1.0, pseudocount), "pcb_sum_normalize");
 }
@@ -201,20 +255,32 @@ extern "C" int pcb_sum_normalize(float* params, const int64_t* blk_pbase, const 
 extern "C" int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_pids, const int32_t* s_pfids,
                                 const int32_t* ncats, const int32_t* source_nids, int32_t num_source_nodes,
                                 double step_size, double pseudocount, int32_t keep_zero_params, void* stream) {
-    if (!params || !param_flows || !s_pids || !s_pfids || !ncats || !source_nids || num_source_nodes < 0)
-        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_em: bad arguments");
-    if (!(step_size > 0.0 && step_size <= 1.0))
-        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_em: step_size must be in (0, 1]");
-    if (num_source_nodes == 0) return PCB_OK;
-    const unsigned grid = (unsigned)pcb::cdiv((int64_t)num_source_nodes * 32, 256);
-    cudaStream_t s = pcb::as_stream(stream);
-    if (keep_zero_params) {
-        return pcb::launch_status(pcb::launch_k(input_em_kernel<true>, dim3(grid), dim3(256), 0, s, 1u, params,
-                                                param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
-                                                step_size, pseudocount), "pcb_input_cat_em");
-    } else {
-        return pcb::launch_status(pcb::launch_k(input_em_kernel<false>, dim3(grid), dim3(256), 0, s, 1u, params,
-                                                param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
-                                                step_size, pseudocount), "pcb_input_cat_em");
-    }
+    return input_em_launch<float>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                  step_size, pseudocount, keep_zero_params, stream, "pcb_input_cat_em");
+}
+
+extern "C" int pcb_input_cat_em_f64flows(float* params, const double* param_flows, const int32_t* s_pids,
+                                         const int32_t* s_pfids, const int32_t* ncats, const int32_t* source_nids,
+                                         int32_t num_source_nodes, double step_size, double pseudocount,
+                                         int32_t keep_zero_params, void* stream) {
+    return input_em_launch<double>(params, param_flows, s_pids, s_pfids, ncats, source_nids, num_source_nodes,
+                                   step_size, pseudocount, keep_zero_params, stream, "pcb_input_cat_em_f64flows");
+}
+
+extern "C" int pcb_flows_accumulate_f64(double* acc, const float* flows, int64_t n, void* stream) {
+    if (!acc || !flows || n < 0) return pcb::set_error(PCB_E_ARG, "pcb_flows_accumulate_f64: bad arguments");
+    if (n == 0) return PCB_OK;
+    int64_t blocks = pcb::cdiv(n, 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    return pcb::launch_status(pcb::launch_k(flows_accumulate_f64_kernel, dim3((unsigned)blocks), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, acc, flows, n), "pcb_flows_accumulate_f64");
+}
+
+extern "C" int pcb_pflow_accum_f64(double* param_flows, int64_t dst, int64_t n, const int64_t* srcs, int32_t nsrc,
+                                   void* stream) {
+    if (!param_flows || !srcs || n < 0 || nsrc <= 0) return pcb::set_error(PCB_E_ARG, "pcb_pflow_accum_f64: bad arguments");
+    if (n == 0) return PCB_OK;
+    return pcb::launch_status(pcb::launch_k(pflow_accum_f64_kernel, dim3((unsigned)pcb::cdiv(n, 256)), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, param_flows, dst, n, srcs, nsrc),
+                              "pcb_pflow_accum_f64");
 }

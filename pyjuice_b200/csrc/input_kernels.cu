@@ -18,7 +18,8 @@ constexpr int kFwdSamples = 4 * kFwdThreads;
 __global__ void __launch_bounds__(kFwdThreads)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
-                     int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec) {
+                     int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec,
+                     int32_t* __restrict__ status) {
     // The node tables and the parameter logs are read before the wait for the previous kernel
     // (the parameters' writers do not trigger early); the samples and outputs after it.
     pcb::pdl_trigger();
@@ -54,7 +55,10 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
             if (b + q < B) {
                 const int64_t x = (v == v0) ? x0[q] : __ldg(data + (int64_t)v * data_ld + b + q);
                 if (x >= 0 && x < K) r = (K <= kFwdSlab) ? slab[j][x] : __logf(__ldcg(params + sP[j] + x));
-                else r = NAN;
+                else {
+                    r = NAN;
+                    pcb::report_status(status, PCB_STATUS_BAD_CATEGORY);
+                }
             }
             pcb::set(o, q, r);
         }
@@ -193,7 +197,8 @@ extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const flo
     return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(num_nodes, kFwdNodes),
                                                                        (unsigned)gy),
                                             dim3(kFwdThreads), 0, pcb::as_stream(stream), 1u, data, data_ld, params, vids,
-                                            s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec),
+                                            s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec,
+                                            pcb::status_word()),
                               "pcb_input_cat_fwd");
 }
 

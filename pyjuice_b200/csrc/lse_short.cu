@@ -82,7 +82,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
                  float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
                  const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
                  int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
-                 const uint8_t* __restrict__ packed, PcbShortFusion fu) {
+                 const uint8_t* __restrict__ packed, PcbShortFusion fu, int32_t* __restrict__ status) {
     // The term indices and the weights (compiled tables and parameters) are read before the
     // wait for the previous kernel; only the source rows and the packed weights after it.
     pcb::pdl_trigger();
@@ -110,6 +110,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     if (nrows <= 0) return;
     const bool bad = t.k_cnt > KMAX;  // the host only sends tiles of <= 128 terms; never read past them
     const int nk = bad ? 0 : t.k_cnt;
+    if (bad && tid == 0) pcb::report_status(status, PCB_STATUS_TILE_TOO_LONG);
     const int rpb_mask = (1 << rpb_log2) - 1;
 
     // ---- term indices, then one batch of asynchronous copies ----
@@ -513,7 +514,8 @@ int launch_one(int num_tiles, int row_splits, const float* src, const float* src
     return pcb::launch_status(pcb::launch_k(lse_short_kernel<RM, TB, MODE, PREC, WK, FUSE>,
                                             dim3((unsigned)gx, (unsigned)gy), dim3(kThreads), smem, s, 1u, src,
                                             src2, aux, out, ld, B, params, tiles, krow, kw, w_stride, rpb_log2,
-                                            row_splits, vec, wvec, packed, fu), "pcb_lse_contract_short");
+                                            row_splits, vec, wvec, packed, fu, pcb::status_word()),
+                              "pcb_lse_contract_short");
 }
 
 template <int RM, int TB, int PREC>

@@ -20,7 +20,8 @@
 //    (M = 128 rows, N samples, K = 16 per instruction; three per step in the split form:
 //    hi*hi + lo*hi + hi*lo) and commits them to an mbarrier. Every warp then reads its
 //    accumulator rows and columns back from tensor memory for the epilogue. Every wait is
-//    bounded; a CTA whose wait runs out writes NaN rows.
+//    bounded; a CTA whose wait runs out writes NaN rows and reports PCB_STATUS_WAIT_TIMEOUT in
+//    the device status word.
 //
 // These kernels serve the BF16 forms only: their logarithms use the hardware approximation
 // (__logf, absolute error ~1e-6, far below the bf16 operand rounding), which halves the
@@ -218,7 +219,8 @@ template <int N, int MODE, bool SPLIT>
 __global__ void __launch_bounds__(tc05_threads<N>(), 2)
 lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const uint8_t* __restrict__ packed,
-                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, int spc, bool vec) {
+                const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, int spc, bool vec,
+                int32_t* __restrict__ status) {
     // tile and term indices (compiled tables) before the wait for the previous kernel
     pcb::pdl_trigger();
     static_assert(N == 32 || N == 64, "sample slice");
@@ -477,6 +479,7 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         __syncthreads();
     }
+    if (fail) pcb::report_status(status, bad ? PCB_STATUS_TILE_TOO_LONG : PCB_STATUS_WAIT_TIMEOUT);
     if (warp == 0) tmem_dealloc(taddr, N);
 }
 
@@ -503,7 +506,8 @@ int launch(int num_tiles, int spc, const float* src, const float* src2, const fl
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: batch too large");
     return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, SPLIT>,
                                             dim3((unsigned)num_tiles, (unsigned)gy), dim3(tc05_threads<N>()), smem, s,
-                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec),
+                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec,
+                                            pcb::status_word()),
                               "pcb_lse_contract_tc05");
 }
 

@@ -9,7 +9,9 @@
 //   inputs:     each remaining input node draws a category (first k with u <= cumsum_k,
 //               0 if none) into samples[s, var].
 // Uniforms come from pcb_uniform(seed, node_id, sample) (SplitMix64 of a counter), so a
-// CPU restatement with the same seed reproduces every draw bit for bit.
+// CPU restatement with the same seed reproduces every draw bit for bit, or from a caller
+// table uniforms[node_id * u_ld + sample] (the draws of another sampler, e.g. the
+// reference's, replayed exactly).
 #include "common.cuh"
 
 namespace {
@@ -28,7 +30,8 @@ __global__ void sample_sum_kernel(int* __restrict__ nlist, int* __restrict__ ncn
                                   const int* __restrict__ node2blk, const int* __restrict__ blk_nid,
                                   const int* __restrict__ blk_koff, const int* __restrict__ blk_kcnt,
                                   const int* __restrict__ krow, const int* __restrict__ kw,
-                                  const float* __restrict__ params, uint64_t seed, int* __restrict__ err) {
+                                  const float* __restrict__ params, const float* __restrict__ uniforms, int64_t u_ld,
+                                  uint64_t seed, int* __restrict__ err) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     int* nl = nlist + (int64_t)s * cap_n;
@@ -46,7 +49,7 @@ __global__ void sample_sum_kernel(int* __restrict__ nlist, int* __restrict__ ncn
         const int i = id - blk_nid[g];
         const int off = blk_koff[g];
         const int cnt = blk_kcnt[g];
-        const float u = uniform(seed, (uint32_t)id, (uint32_t)s);
+        const float u = uniforms ? uniforms[(int64_t)id * u_ld + s] : uniform(seed, (uint32_t)id, (uint32_t)s);
         float cum = 0.f;
         int pick = -1, last_nz = 0;
         for (int k = 0; k < cnt; ++k) {
@@ -98,7 +101,8 @@ __global__ void sample_prod_kernel(int* __restrict__ nlist, int* __restrict__ nc
 __global__ void sample_input_kernel(const int* __restrict__ nlist, const int* __restrict__ ncnt, int S, int cap_n,
                                     int lo, int hi, const int* __restrict__ vids, const int* __restrict__ s_pids,
                                     const int* __restrict__ ncats, const float* __restrict__ params,
-                                    int64_t* __restrict__ samples, int64_t sld, uint64_t seed) {
+                                    int64_t* __restrict__ samples, int64_t sld, const float* __restrict__ uniforms,
+                                    int64_t u_ld, uint64_t seed) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= (int64_t)S * cap_n) return;
     const int s = (int)(idx / cap_n);
@@ -109,7 +113,7 @@ __global__ void sample_input_kernel(const int* __restrict__ nlist, const int* __
     const int n = id - lo;
     const int K = ncats[n];
     const int64_t sp = s_pids[n];
-    const float u = uniform(seed, (uint32_t)id, (uint32_t)s);
+    const float u = uniforms ? uniforms[(int64_t)id * u_ld + s] : uniform(seed, (uint32_t)id, (uint32_t)s);
     float cum = 0.f;
     int pick = -1;
     for (int k = 0; k < K; ++k) {
@@ -127,14 +131,15 @@ extern "C" {
 int pcb_sample_sum(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt, int32_t S, int32_t cap_n,
                    int32_t cap_e, int32_t lo, int32_t hi, int32_t bs, const int32_t* node2blk, const int32_t* blk_nid,
                    const int32_t* blk_koff, const int32_t* blk_kcnt, const int32_t* krow, const int32_t* kw,
-                   const float* params, uint64_t seed, int32_t* err, void* stream) {
+                   const float* params, const float* uniforms, int64_t u_ld, uint64_t seed, int32_t* err,
+                   void* stream) {
     if (!nlist || !ncnt || !elist || !ecnt || !node2blk || !blk_nid || !blk_koff || !blk_kcnt || !krow || !kw ||
-        !params || !err || S < 0 || cap_n <= 0 || cap_e <= 0 || hi < lo || bs <= 0)
+        !params || !err || S < 0 || cap_n <= 0 || cap_e <= 0 || hi < lo || bs <= 0 || (uniforms && u_ld < S))
         return pcb::set_error(PCB_E_ARG, "pcb_sample_sum: bad arguments");
     if (S == 0) return PCB_OK;
     sample_sum_kernel<<<(unsigned)pcb::cdiv(S, 128), 128, 0, pcb::as_stream(stream)>>>(
         nlist, ncnt, elist, ecnt, S, cap_n, cap_e, lo, hi, bs, node2blk, blk_nid, blk_koff, blk_kcnt, krow, kw, params,
-        seed, err);
+        uniforms, u_ld, seed, err);
     return pcb::check_launch("pcb_sample_sum");
 }
 
@@ -152,13 +157,14 @@ int pcb_sample_prod(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt
 
 int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
                      const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, const float* params,
-                     int64_t* samples, int64_t sld, uint64_t seed, void* stream) {
-    if (!nlist || !ncnt || !vids || !s_pids || !ncats || !params || !samples || S < 0 || cap_n <= 0 || hi < lo)
+                     int64_t* samples, int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream) {
+    if (!nlist || !ncnt || !vids || !s_pids || !ncats || !params || !samples || S < 0 || cap_n <= 0 || hi < lo ||
+        (uniforms && u_ld < S))
         return pcb::set_error(PCB_E_ARG, "pcb_sample_input: bad arguments");
     if (S == 0) return PCB_OK;
     const int64_t total = (int64_t)S * cap_n;
     sample_input_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
-        nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, ncats, params, samples, sld, seed);
+        nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, ncats, params, samples, sld, uniforms, u_ld, seed);
     return pcb::check_launch("pcb_sample_input");
 }
 

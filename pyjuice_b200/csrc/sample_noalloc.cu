@@ -45,6 +45,12 @@ __global__ void sample_circuit_kernel(int32_t* __restrict__ scratch, const PcbSa
     nl[0] = root_id;
     for (int si = 0; si < num_steps; ++si) {
         const PcbSampleStep st = steps[si];
+        // The table lives in device memory, so the host cannot check it: a step of unknown
+        // kind, or a sum step without a positive block size, stops this sample with code 3.
+        if ((st.kind != 0 && st.kind != 1 && st.kind != 2) || (st.kind == 0 && st.bs <= 0)) {
+            atomicExch(err, 3);
+            return;
+        }
         if (st.kind == 0) {  // sum layer: each active node of the layer picks one child element
             int keep = 0;
             for (int j = 0; j < n; ++j) {
@@ -84,7 +90,7 @@ __global__ void sample_circuit_kernel(int32_t* __restrict__ scratch, const PcbSa
                 }
             }
             ne = keep;
-        } else {  // input layer: each active input node draws its category
+        } else {  // kind 2, input layer: each active input node draws its category
             for (int j = 0; j < n; ++j) {
                 const int id = nl[j];
                 if (id < st.lo || id >= st.hi) continue;

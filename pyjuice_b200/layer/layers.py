@@ -674,6 +674,7 @@ class InputLayer(Layer, torch.nn.Module):
         self.params = torch.nn.Parameter(torch.empty([max(self.num_parameters, 1)], dtype=torch.float32),
                                          requires_grad=False)
         self.param_flows = None
+        self.param_flows_f64 = None
 
     def is_input(self):
         return True
@@ -757,13 +758,32 @@ class InputLayer(Layer, torch.nn.Module):
                  d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
                  nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.stream())
 
-    def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False):
+    def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
+                      use_f64_flows: bool = False):
         d = self._desc(self.params.device)
+        pf = self.param_flows_f64 if use_f64_flows else self.param_flows
+        if pf is None:
+            raise RuntimeError("no parameter flows for the input layer")
         for dst, n, ch in d["tied"]:
-            nat.call("pcb_pflow_accum", nat.ptr(self.param_flows), dst, n, nat.ptr(ch), ch.size(0), nat.stream())
-        nat.call("pcb_input_cat_em", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(d["s_pids"]),
-                 nat.ptr(d["s_pfids"]), nat.ptr(d["ncats"]), nat.ptr(d["source_nids"]), d["source_nids"].size(0),
-                 float(step_size), float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
+            nat.call("pcb_pflow_accum_f64" if use_f64_flows else "pcb_pflow_accum", nat.ptr(pf), dst, n, nat.ptr(ch),
+                     ch.size(0), nat.stream())
+        nat.call("pcb_input_cat_em_f64flows" if use_f64_flows else "pcb_input_cat_em", nat.ptr(self.params),
+                 nat.ptr(pf), nat.ptr(d["s_pids"]), nat.ptr(d["s_pfids"]), nat.ptr(d["ncats"]),
+                 nat.ptr(d["source_nids"]), d["source_nids"].size(0), float(step_size), float(pseudocount),
+                 1 if keep_zero_params else 0, nat.stream())
+
+    def init_param_flows_f64(self):
+        n = max(self.num_param_flows, 1)
+        if self.param_flows_f64 is None or self.param_flows_f64.device != self.params.device:
+            self.param_flows_f64 = torch.zeros([n], dtype=torch.float64, device=self.params.device)
+        else:
+            self.param_flows_f64.zero_()
+
+    def accumulate_param_flows_f64(self):
+        if self.param_flows_f64 is None or self.param_flows_f64.device != self.params.device:
+            self.init_param_flows_f64()
+        nat.call("pcb_flows_accumulate_f64", nat.ptr(self.param_flows_f64), nat.ptr(self.param_flows),
+                 self.param_flows.numel(), nat.stream())
 
     def update_parameters(self):
         for ns in self.nodes:

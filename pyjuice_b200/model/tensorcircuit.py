@@ -80,6 +80,7 @@ class TensorCircuit(nn.Module):
         self.node_flows = None
         self.element_flows = None
         self.param_flows = None
+        self.param_flows_f64 = None
         self._init_layers(layer_sparsity_tol=layer_sparsity_tol, max_num_partitions=max_num_partitions,
                           max_tied_ns_per_parflow_block=max_tied_ns_per_parflow_block)
         self._optim_hyperparams = {"compute_param_flows": True, "flows_memory": 1.0}
@@ -805,24 +806,62 @@ class TensorCircuit(nn.Module):
         return 0.0 if self._cum_flow_dev is None else float(self._cum_flow_dev.item())
 
     def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
-                      step_size_rescaling: bool = False, use_cudagraph: bool = True):
-        """EM update from the accumulated parameter flows (tensorcircuit.py:549-590)."""
+                      step_size_rescaling: bool = False, use_cudagraph: bool = True, use_f64_flows: bool = False):
+        """EM update from the accumulated parameter flows (tensorcircuit.py:549-590).
+
+        ``use_f64_flows``: update from the FP64 epoch flows (``param_flows_f64``, see
+        :meth:`accumulate_param_flows_f64`) instead of the FP32 ``param_flows``.
+        """
         if step_size_rescaling:
             raise NotImplementedError("step_size_rescaling needs top-down probabilities, which have no CUDA path yet")
         if not (0.0 < step_size <= 1.0):
             raise ValueError("`step_size` should be between 0 and 1.")
-        if self.param_flows is None:
+        if self.param_flows is None and not use_f64_flows:
             raise RuntimeError("run a backward pass before mini_batch_em")
+        if use_f64_flows and self.param_flows_f64 is None:
+            raise RuntimeError("no FP64 flows: call init_param_flows_f64 / accumulate_param_flows_f64 first")
         with torch.no_grad():
             for layer in self.input_layer_group:
-                layer.mini_batch_em(step_size=step_size, pseudocount=pseudocount, keep_zero_params=keep_zero_params)
+                layer.mini_batch_em(step_size=step_size, pseudocount=pseudocount, keep_zero_params=keep_zero_params,
+                                    use_f64_flows=use_f64_flows)
             t = self._tables()
+            pf = self.param_flows_f64 if use_f64_flows else self.param_flows
             for dst, n, srcs in t["fusing"]:
-                nat.call("pcb_pflow_accum", nat.ptr(self.param_flows), dst, n, nat.ptr(srcs), srcs.size(0), nat.stream())
-            nat.call("pcb_sum_em", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(t["pbase"]),
-                     nat.ptr(t["pfbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0), float(step_size),
-                     float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
+                nat.call("pcb_pflow_accum_f64" if use_f64_flows else "pcb_pflow_accum", nat.ptr(pf), dst, n,
+                         nat.ptr(srcs), srcs.size(0), nat.stream())
+            nat.call("pcb_sum_em_f64flows" if use_f64_flows else "pcb_sum_em", nat.ptr(self.params), nat.ptr(pf),
+                     nat.ptr(t["pbase"]), nat.ptr(t["pfbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0),
+                     float(step_size), float(pseudocount), 1 if keep_zero_params else 0, nat.stream())
             self._param_epoch += 1
+
+    def init_param_flows_f64(self):
+        """Zero the FP64 epoch-level parameter flows (sum and input layers)."""
+        n = max(self.num_param_flows, 1)
+        if self.param_flows_f64 is None or self.param_flows_f64.device != self.device or self.param_flows_f64.numel() != n:
+            self.param_flows_f64 = torch.zeros([n], dtype=torch.float64, device=self.device)
+        else:
+            self.param_flows_f64.zero_()
+        for layer in self.input_layer_group:
+            layer.init_param_flows_f64()
+
+    def accumulate_param_flows_f64(self):
+        """Add the FP32 parameter flows of the last backward pass(es) to the FP64 epoch flows.
+
+        An epoch of full-batch EM then reads: per batch ``init_param_flows(0)``, forward,
+        backward, ``accumulate_param_flows_f64()``; at the end
+        ``mini_batch_em(1.0, pseudocount, use_f64_flows=True)``. The reference sums the
+        batches' flows in FP32 (``cumulate_flows``, tensorcircuit.py:592-595); here each
+        batch's FP32 flows are added into FP64 on the device (``pcb_flows_accumulate_f64``).
+        """
+        if self.param_flows is None:
+            raise RuntimeError("run a backward pass first")
+        if self.param_flows_f64 is None or self.param_flows_f64.device != self.device:
+            self.init_param_flows_f64()
+        with torch.no_grad():
+            nat.call("pcb_flows_accumulate_f64", nat.ptr(self.param_flows_f64), nat.ptr(self.param_flows),
+                     self.num_param_flows, nat.stream())
+            for layer in self.input_layer_group:
+                layer.accumulate_param_flows_f64()
 
     def normalize_parameters(self, pseudocount: float = 0.0):
         """Renormalise the sum parameters in place on the device (FP64)."""
@@ -831,10 +870,17 @@ class TensorCircuit(nn.Module):
                  t["nch"].size(0), float(pseudocount), nat.stream())
         self._param_epoch += 1
 
-    def cumulate_flows(self, inputs: torch.Tensor):
+    def cumulate_flows(self, inputs: torch.Tensor, params: Optional[torch.Tensor] = None, fp64: bool = False):
+        """Forward + backward adding this batch's parameter flows to the kept ones
+        (tensorcircuit.py:592-595). ``fp64``: the batch's flows go to the FP64 epoch flows
+        instead (``param_flows`` then holds this batch's flows only)."""
+        if params is not None:
+            raise NotImplementedError("external parameters have no CUDA path")
         with torch.no_grad():
             self.forward(inputs)
-            self.backward(inputs=inputs, compute_param_flows=True, flows_memory=1.0)
+            self.backward(inputs=inputs, compute_param_flows=True, flows_memory=0.0 if fp64 else 1.0)
+            if fp64:
+                self.accumulate_param_flows_f64()
 
     def init_param_flows(self, flows_memory: float = 1.0, batch_size: Optional[int] = None):
         if not (0.0 <= flows_memory <= 1.0):

@@ -7,7 +7,10 @@ draws its category. Unlike the reference there is no host round trip per layer: 
 sample carries its active node / element lists on the device
 (``csrc/sample_kernels.cu``), and the uniforms are a counter-based hash of
 ``(seed, node id, sample index)``, so a given seed reproduces the samples bit for bit
-(the CPU oracle restates the same draws).
+(the CPU oracle restates the same draws), or come from a caller's table indexed by
+(node id, sample index): given the uniform each of the reference's ``tl.rand`` draws
+produced for a (node, sample) (sample.py:77 for sums, categorical.py:144 for inputs),
+the device sampler returns the reference's samples exactly.
 """
 
 from __future__ import annotations
@@ -37,8 +40,14 @@ def _scope_bounds(pc):
 
 
 def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, seed: Optional[int] = None,
-           _sample_input_ns: bool = True, **kwargs) -> torch.Tensor:
-    """Draw ``num_samples`` joint samples ``[num_samples, num_vars]`` (int64)."""
+           _sample_input_ns: bool = True, uniforms: Optional[torch.Tensor] = None, **kwargs) -> torch.Tensor:
+    """Draw ``num_samples`` joint samples ``[num_samples, num_vars]`` (int64).
+
+    ``uniforms``: optional ``[num_nodes, >= num_samples]`` FP32 table on the circuit's
+    device; node ``n`` of sample ``s`` then draws with ``uniforms[n, s]`` instead of the
+    seeded hash. With the draws the reference's ``tl.rand`` made for each (node, sample),
+    the samples equal the reference's bit for bit.
+    """
     if conditional:
         raise NotImplementedError("conditional sampling has no CUDA path yet")
     if num_samples is None or num_samples <= 0:
@@ -51,6 +60,19 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
         seed = random.randint(0, 2 ** 62)
     dev = pc.device
     S = int(num_samples)
+    u_ld = 0
+    if uniforms is not None:
+        if (uniforms.dtype != torch.float32 or uniforms.dim() != 2 or uniforms.size(0) < pc.num_nodes
+                or uniforms.size(1) < S or uniforms.stride(1) != 1 or uniforms.device != dev):
+            raise ValueError("`uniforms` must be a row-major float32 [num_nodes, >= num_samples] tensor on "
+                             f"the circuit's device {dev}")
+        u_ld = uniforms.stride(0)
+    with torch.cuda.device(dev):
+        return _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns)
+
+
+def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns):
+    dev = pc.device
     cap_n, cap_e = _scope_bounds(pc)
     cap_n = max(cap_n, 1)
     cap_e = max(cap_e, 1)
@@ -70,7 +92,7 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
                 nat.call("pcb_sample_sum", nat.ptr(nlist), nat.ptr(ncnt), nat.ptr(elist), nat.ptr(ecnt), S, cap_n,
                          cap_e, lo, hi, layer.block_size, nat.ptr(d["node2blk"]), nat.ptr(d["blk_nid"]),
                          nat.ptr(d["blk_koff"]), nat.ptr(d["blk_kcnt"]), nat.ptr(d["krow"]), nat.ptr(d["kw"]),
-                         nat.ptr(pc.params), seed, nat.ptr(err), st)
+                         nat.ptr(pc.params), nat.ptr(uniforms), u_ld, seed, nat.ptr(err), st)
             else:
                 lo, hi = layer._layer_nid_range
                 nat.call("pcb_sample_prod", nat.ptr(nlist), nat.ptr(ncnt), nat.ptr(elist), nat.ptr(ecnt), S, cap_n,
@@ -84,7 +106,7 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
         lo, hi = layer._output_ind_range
         nat.call("pcb_sample_input", nat.ptr(nlist), nat.ptr(ncnt), S, cap_n, lo, hi, nat.ptr(d["vids"]),
                  nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), nat.ptr(layer.params), nat.ptr(samples), pc.num_vars,
-                 seed, st)
+                 nat.ptr(uniforms), u_ld, seed, st)
     e = int(err.item())
     if e != 0:
         raise RuntimeError(f"sampling failed on the device (code {e}: "
@@ -150,8 +172,8 @@ def sample_noalloc(pc, samples: torch.Tensor, err: torch.Tensor, seed: int, plan
     """Fill ``samples`` ([S, num_vars] int64, caller-allocated) without any device allocation.
 
     Same draws as :func:`sample` with the same ``seed``. ``err`` (one int32 on the device)
-    receives 0, or 1 on list overflow, 2 on an element outside its product layer; the
-    call does not synchronise, so read it when the stream reaches that point. Variables a
+    receives 0, or 1 on list overflow, 2 on an element outside its product layer, 3 on a
+    malformed step table; the call does not synchronise, so read it when the stream reaches that point. Variables a
     sample does not draw keep their value in ``samples``. At most
     ``PCB_SAMPLE_NOALLOC_MAX_INTS // (cap_n + cap_e)`` samples per call; calls that
     overlap in time on one device share the library's working lists and must be
@@ -163,7 +185,15 @@ def sample_noalloc(pc, samples: torch.Tensor, err: torch.Tensor, seed: int, plan
     table, num_steps, root_id, cap_n, cap_e = plan
     if samples.dtype != torch.long or samples.dim() != 2 or samples.stride(1) != 1:
         raise ValueError("`samples` must be a row-major int64 tensor [S, num_vars]")
+    if samples.size(1) < pc.num_vars or samples.stride(0) < pc.num_vars:
+        raise ValueError(f"`samples` must have at least num_vars = {pc.num_vars} columns")
+    if samples.size(0) >= 2 ** 31:
+        raise ValueError("at most 2^31 - 1 samples per call")
     if err.dtype != torch.int32 or err.numel() < 1:
         raise ValueError("`err` must hold one int32")
-    nat.call("pcb_sample_circuit_noalloc", nat.ptr(table), num_steps, root_id, samples.size(0), cap_n, cap_e,
-             nat.ptr(samples), samples.stride(0), int(seed), nat.ptr(err), nat.stream())
+    if samples.device != pc.device or err.device != pc.device:
+        raise ValueError(f"`samples` and `err` must be on the circuit's device {pc.device}")
+    # the kernel runs on the current device: make it the one that holds the tables
+    with torch.cuda.device(pc.device):
+        nat.call("pcb_sample_circuit_noalloc", nat.ptr(table), num_steps, root_id, samples.size(0), cap_n, cap_e,
+                 nat.ptr(samples), samples.stride(0), int(seed), nat.ptr(err), nat.stream())

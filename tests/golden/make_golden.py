@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory by running the reference PyJuice.
 
-Run from the repository root in a container that holds the reference sources
-(``PYJUICE_REF_SRC``, default ``/root/reference/src``):
+Run from the repository root in a container that holds the reference sources, with
+``PYJUICE_REF_SRC`` set to the reference's ``src`` directory:
 
     python tests/golden/make_golden.py [tiny] [hclt64] [hclt784]
 
@@ -15,7 +15,14 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``hclt64.npz``    HCLT, 64 variables x 4 categories, 16 latents, block size 16, B = 512,
                     data from a seeded random tree Bayesian network;
 * ``hclt784.npz``   HCLT, 28x28 variables x 256 categories, 128 latents, block size 32:
-                    structure, index digests and the log-likelihoods of 8 samples.
+                    structure, index digests and the log-likelihoods of 8 samples;
+* ``em_tiny.npz``    the tiny circuit with a tenth of its parameters zeroed: one step with
+                    ``keep_zero_params=True``, and the reference's normalisation of a seeded
+                    parameter vector with pseudocount 0.3;
+* ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
+                    circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
+                    ``tl.rand`` draw replaced by a table lookup by (node, sample)
+                    (``ref_shim.install_uniform_table``).
 """
 
 from __future__ import annotations
@@ -194,9 +201,85 @@ def make_hclt784():
     np.savez_compressed(os.path.join(HERE, "hclt784.npz"), **out)
 
 
+def make_em_variants():
+    """The tiny circuit with some sum and input parameters set to zero: one forward /
+    backward, then ``mini_batch_em(0.1, 0.1, keep_zero_params=True)``; and the reference's
+    sum-to-one normalisation (``TensorCircuit._normalize_parameters``, pseudocount 0.3) of a
+    seeded positive parameter vector."""
+    fx = dict(np.load(os.path.join(HERE, "tiny.npz")))
+    torch.manual_seed(1)
+    pc = juice.compile(build_tiny_dag(juice, dists), max_tied_ns_per_parflow_block=1, verbose=False)
+    p0 = fx["params0"].copy()
+    q0 = fx["in_params0"].copy()
+    rng = np.random.default_rng(5)
+    nd = pc.num_dummy_params
+    zs = nd + rng.choice(p0.shape[0] - nd, size=(p0.shape[0] - nd) // 10, replace=False)
+    p0[zs] = 0.0
+    q0[rng.choice(q0.shape[0], size=q0.shape[0] // 10, replace=False)] = 0.0
+    out = dict(params0=p0, in_params0=q0, x=fx["x"])
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(p0))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(q0))
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(torch.from_numpy(fx["x"]), force_use_fp32=True)
+    lls.mean().backward()
+    out["param_flows"] = pc.param_flows.detach().cpu().numpy().copy()
+    out["in_param_flows"] = pc.input_layer_group[0].param_flows.detach().cpu().numpy().copy()
+    pc.mini_batch_em(step_size=0.1, pseudocount=0.1, keep_zero_params=True)
+    out["params1_keep_zero"] = pc.params.detach().cpu().numpy().copy()
+    out["in_params1_keep_zero"] = pc.input_layer_group[0].params.detach().cpu().numpy().copy()
+    raw = np.exp(-4.0 * rng.random(p0.shape[0])).astype(np.float32)
+    raw[:nd] = 0.0
+    t = torch.from_numpy(raw.copy())
+    pc._normalize_parameters(t, pseudocount=0.3)
+    out["norm_in"] = raw
+    out["norm_out"] = t.numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "em_tiny.npz"), **out)
+
+
+SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
+SAMPLE_S = 256
+
+
+def make_samples(name: str):
+    """Samples the reference draws when every ``tl.rand`` draw of node n in sample s is
+    ``uniform_table(SAMPLE_SEED)[n, s]``: the circuit and parameters of fixture ``name``,
+    ``juice.queries.sample(pc, SAMPLE_S)``."""
+    from ref_shim import install_uniform_table
+    from oracle import pc_oracle as orc
+    fx = dict(np.load(os.path.join(HERE, name + ".npz")))
+    if name == "tiny":
+        torch.manual_seed(1)
+        root = build_tiny_dag(juice, dists)
+        pc = juice.compile(root, max_tied_ns_per_parflow_block=1, verbose=False)
+    else:
+        seq = [int(v) for v in fx["tree_seq"]]
+        off, flat = fx["tree_children_off"], fx["tree_children"]
+        T = nx.Graph()
+        T.add_nodes_from(range(len(seq)))
+        for v in range(len(seq)):
+            for c in flat[off[v]:off[v + 1]]:
+                T.add_edge(v, int(c))
+        with juice.set_block_size(16):
+            r = BayesianTreeToHiddenRegionGraph(T, int(fx["tree_root"]), 16, dists.Categorical, {"num_cats": 4},
+                                                num_root_ns=1, block_size=16)
+        pc = juice.compile(r, verbose=False)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+    table = orc.uniform_table(SAMPLE_SEED, pc.num_nodes, SAMPLE_S)
+    install_uniform_table(juice, table)
+    samples = juice.queries.sample(pc, SAMPLE_S)
+    out = dict(uniform_seed=np.array(SAMPLE_SEED), num_samples=np.array(SAMPLE_S),
+               samples=samples.detach().cpu().numpy().astype(np.int64), num_nodes=np.array(pc.num_nodes))
+    np.savez_compressed(os.path.join(HERE, f"samples_{name}.npz"), **out)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny"]
     for w in which:
         t = time.time()
-        {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784}[w]()
+        {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
+         "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
+         "em_tiny": make_em_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

@@ -16,7 +16,14 @@ import sys
 import tempfile
 import types
 
-REF_SRC = os.environ.get("PYJUICE_REF_SRC", "/root/reference/src")
+
+
+def _ref_src() -> str:
+    """Source directory of the reference package (``PYJUICE_REF_SRC``, required)."""
+    src = os.environ.get("PYJUICE_REF_SRC")
+    if not src or not os.path.isdir(os.path.join(src, "pyjuice")):
+        raise RuntimeError("set PYJUICE_REF_SRC to the reference's `src` directory (the one holding `pyjuice/`)")
+    return src
 
 
 def load_reference():
@@ -28,7 +35,7 @@ def load_reference():
     with open(os.path.join(stub, "matplotlib", "pyplot.py"), "w") as f:
         f.write("")
     sys.path.insert(0, stub)
-    sys.path.insert(0, REF_SRC)
+    sys.path.insert(0, _ref_src())
 
     import torch
 
@@ -89,3 +96,58 @@ def load_reference():
     for name in ("forward", "backward", "mini_batch_em", "sample"):
         _wrap_method(name)
     return juice
+
+
+def install_uniform_table(juice, table):
+    """Make the reference's sampler draw ``table[node id, sample]`` (a float32 numpy array
+    ``[num_nodes, S]``) wherever it calls ``tl.rand``.
+
+    The reference draws ``tl.rand(seed, offset)`` where ``offset`` indexes the list of
+    (node, sample) pairs a launch processes: for sum layers the pairs of
+    ``torch.where`` over ``node_samples`` (queries/sample.py:77, list built at 418), for
+    input layers the pairs of ``torch.where(node_flows > 1e-8)`` (input_layer.py:592,
+    categorical.py:144). The launchers are wrapped to record each launch's pair list, and
+    ``triton.language.rand`` is replaced by a lookup of the table through that list, so
+    every draw is a known function of the node and the sample.
+    """
+    import numpy as np
+    import torch
+    import triton.language as tl
+    from triton.runtime.interpreter import TensorHandle
+    import pyjuice.queries  # noqa: F401  (the package re-exports the function `sample`)
+    from pyjuice.layer import input_layer as il
+    qs = sys.modules["pyjuice.queries.sample"]
+
+    ctx = {"nodes": None, "samples": None}
+
+    def rand(seed, offset, *a, **k):
+        off = np.asarray(offset.handle.data).astype(np.int64).reshape(-1)
+        nodes, samples = ctx["nodes"], ctx["samples"]
+        ok = off < nodes.shape[0]
+        o = np.where(ok, off, 0)
+        vals = np.where(ok, table[nodes[o], samples[o]], 0.0).astype(np.float32)
+        shape = list(offset.type.shape) if offset.type.is_block() else []
+        ty = tl.core.block_type(tl.float32, shape) if shape else tl.float32
+        return tl.core.tensor(TensorHandle(vals.reshape(shape) if shape else vals.reshape(()), tl.float32), ty)
+
+    tl.rand = rand
+    orig_sum = qs.sample_sum_layer
+
+    def sample_sum_layer(pc, layer, nids, cids, pids, node_mars, element_mars, params, node_samples,
+                         element_samples, ind_target, ind_n, ind_b, *a, **k):
+        ctx["nodes"] = node_samples[ind_n, ind_b].numpy().astype(np.int64)
+        ctx["samples"] = ind_b.numpy().astype(np.int64)
+        return orig_sum(pc, layer, nids, cids, pids, node_mars, element_mars, params, node_samples,
+                        element_samples, ind_target, ind_n, ind_b, *a, **k)
+
+    qs.sample_sum_layer = sample_sum_layer
+    orig_in = il.InputLayer.sample
+
+    def in_sample(self, samples, node_flows, *a, **k):
+        sid, eid = self._output_ind_range
+        xs, ys = torch.where(node_flows[sid:eid, :] > 1e-8)
+        ctx["nodes"] = (xs.numpy() + sid).astype(np.int64)
+        ctx["samples"] = ys.numpy().astype(np.int64)
+        return orig_in(self, samples, node_flows, *a, **k)
+
+    il.InputLayer.sample = in_sample

@@ -372,3 +372,24 @@ def test_errors_are_raised(cuda_device):
         pc.mini_batch_em(step_size=0.1)  # no flows yet
     with pytest.raises(ValueError):
         pc.mini_batch_em(step_size=0.0)
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_sampling_matches_reference_draws(name, cuda_device):
+    """Bit-exact against the reference's own samples: the reference's queries.sample was run
+    with every tl.rand draw of node n in sample s replaced by table[n, s]; the device sampler
+    given the same table (``uniforms=``) returns the same 256 samples. The table is the
+    SplitMix64 hash of the seeded sampler, so the seeded path must agree too."""
+    fx = load_fixture(name)
+    sf = load_fixture("samples_" + name)
+    pc = build_fixture_circuit(name, fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    S, seed = int(sf["num_samples"]), int(sf["uniform_seed"])
+    table = torch.from_numpy(orc.uniform_table(seed, pc.num_nodes, S)).to(cuda_device)
+    got = juice.queries.sample(pc, S, uniforms=table).cpu().numpy()
+    assert np.array_equal(got, sf["samples"])
+    assert np.array_equal(juice.queries.sample(pc, S, seed=seed).cpu().numpy(), sf["samples"])
+    # a table wider than S (leading dimension > S) reads the same draws
+    wide = torch.zeros([pc.num_nodes, S + 13], dtype=torch.float32, device=cuda_device)
+    wide[:, :S] = table
+    assert np.array_equal(juice.queries.sample(pc, S, uniforms=wide).cpu().numpy(), sf["samples"])

@@ -55,3 +55,36 @@ def test_uniform_hash_known_values():
     assert all(0.0 <= v < 1.0 for v in u)
     assert len(set(u)) == 3
     assert orc.uniform(1, 2, 3) == orc.uniform(1, 2, 3)
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_oracle_sampler_matches_reference_draws(name):
+    """The oracle's sampler reproduces the samples the reference's own queries.sample drew
+    when each of its tl.rand draws for node n in sample s was uniform_table(seed)[n, s]
+    (fixtures samples_*.npz, made by running the reference): pins the draw rules (sum: first
+    child whose running weight sum exceeds u; categorical: first category whose running sum
+    reaches u) to the reference's."""
+    fx = load_fixture(name)
+    sf = load_fixture("samples_" + name)
+    lay = orc.layout_from_fixture(fx, ncats=NCATS[name])
+    assert lay["num_nodes"] == int(sf["num_nodes"])
+    got = orc.sample(lay, fx["params0"], fx["in_params0"], int(sf["num_samples"]), int(sf["uniform_seed"]),
+                     sf["samples"].shape[1])
+    assert np.array_equal(got, sf["samples"])
+
+
+def test_oracle_keep_zero_em_and_normalisation():
+    """keep_zero_params EM and the sum-to-one normalisation of the oracle against the
+    reference's own outputs (fixture em_tiny.npz)."""
+    fx = load_fixture("em_tiny")
+    lay = orc.layout_from_fixture(load_fixture("tiny"), ncats=4)
+    nm, ems, _ = orc.forward(lay, fx["params0"], fx["in_params0"], fx["x"])
+    _, pf, in_pf = orc.backward(lay, fx["params0"], fx["x"], nm, ems)
+    assert np.abs(pf - fx["param_flows"]).max() <= 1e-5 * np.abs(fx["param_flows"]).max()
+    p1, ip1 = orc.em_update(lay, fx["params0"], fx["param_flows"].astype(np.float64), fx["in_params0"],
+                            fx["in_param_flows"].astype(np.float64), 0.1, 0.1, keep_zero_params=True)
+    assert np.abs(p1 - fx["params1_keep_zero"]).max() <= 1e-6
+    assert np.all(p1[fx["params0"] == 0] == 0)
+    assert np.abs(ip1 - fx["in_params1_keep_zero"]).max() <= 1e-6
+    got = orc.normalize(lay, fx["norm_in"], 0.3)
+    assert np.abs(got - fx["norm_out"]).max() <= 1e-6

@@ -1,0 +1,219 @@
+"""Parity of the backward pass and the EM update against the FP64 oracle and the reference's
+own outputs, in every precision form the EM step runs in:
+
+* HCLT over 28x28 variables, 256 categories, 128 latents, block size 32 (the benchmarked
+  circuit) at batch 32: node flows, parameter flows, input flows and the EM update, for
+  plain FP32 and the two BF16 tensor-core forms (split hi + lo operands, single operands),
+  through the tcgen05 kernels of the large layers in both element-flow modes;
+* keep_zero_params EM and the device normalisation against the reference's outputs;
+* non-uniform root weights (``ll_weights``), the FP64 dataset log-likelihood reducer and
+  FP64 epoch-level parameter flows against the oracle.
+
+Error bounds, relative to the largest magnitude of the compared quantity: FP32 1e-4; split
+BF16 2e-3; single BF16 5e-2 (its operands keep 8 mantissa bits).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_fixture
+from helpers import build_fixture_circuit, fixture_params, load_fixture_params
+from oracle import pc_oracle as orc
+
+import pyjuice_b200 as juice
+from pyjuice_b200.layer.layers import SumLayer
+from pyjuice_b200.synthetic import gaussian_field_data
+
+pytestmark = pytest.mark.gpu
+
+FORMS = {"fp32": (0, 1e-4), "bf16_split": (2, 2e-3), "bf16_single": (1, 5e-2)}
+_CACHE = {}
+
+
+def _hclt784(device):
+    """The benchmarked circuit with the fixture's seeded parameters, its oracle layout and a
+    batch of 32 quantised random fields (compiled once per module)."""
+    if "pc" not in _CACHE:
+        fx = load_fixture("hclt784")
+        pc = build_fixture_circuit("hclt784", fx)
+        p0, q0 = fixture_params(pc, fx)
+        x = gaussian_field_data(32, side=28, num_cats=256, length_scale=3.0, seed=1).numpy()
+        lay = orc.layout_from_circuit(pc)
+        nm, ems, lls = orc.forward(lay, p0, q0, x)
+        nf, pf, ipf = orc.backward(lay, p0, x, nm, ems)
+        _CACHE.update(pc=pc, fx=fx, p0=p0, q0=q0, x=x, lay=lay, lls=lls, nf=nf, pf=pf, ipf=ipf)
+    c = _CACHE
+    pc = c["pc"].to(device)
+    load_fixture_params(pc, c["fx"])
+    return pc, c
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("form", list(FORMS))
+@pytest.mark.parametrize("modify", [True, False])
+def test_hclt784_flows_and_em_vs_fp64(form, modify, cuda_device):
+    bf16_form, tol = FORMS[form]
+    pc, c = _hclt784(cuda_device)
+    x = torch.from_numpy(c["x"]).to(cuda_device)
+    kw = {"force_use_fp32": True} if bf16_form == 0 else {"force_use_bf16": True}
+    saved = SumLayer.bf16_form
+    try:
+        if bf16_form:
+            SumLayer.bf16_form = bf16_form
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            lls = pc(x, **kw)
+        pc.backward(inputs=x, allow_modify_flows=modify, force_use_fp32=bf16_form == 0)
+        torch.cuda.synchronize()
+    finally:
+        SumLayer.bf16_form = saved
+    # the large layers ran on the tcgen05 kernels in the BF16 forms (element-flow mode 1 when
+    # the node flows are rewritten in place, mode 2 when they are not)
+    if bf16_form:
+        assert any(l._fw_tc05(l._desc(cuda_device), 32, True, False)[1]
+                   for g in pc.inner_layer_groups if g.is_sum() for l in g)
+    dll = np.abs(lls.cpu().numpy() - c["lls"])
+    if bf16_form == 0:
+        assert np.all(dll <= 1e-5 * np.abs(c["lls"]))
+    else:  # mean absolute LL error in nats
+        assert dll.mean() <= (1e-3 if bf16_form == 2 else 5e-2)
+    assert _rel(pc.param_flows.cpu().numpy(), c["pf"]) <= tol
+    il = pc.input_layer_group[0]
+    ipf = c["ipf"]
+    assert _rel(il.param_flows.cpu().numpy()[:ipf.shape[0]], ipf) <= tol
+    lo, hi = il._output_ind_range
+    assert _rel(pc.node_flows[lo:hi].cpu().numpy(), c["nf"][lo:hi]) <= tol
+    if not modify:  # no row was rewritten: every node flow is comparable
+        assert _rel(pc.node_flows.cpu().numpy(), c["nf"]) <= tol
+    # EM from the device flows equals the oracle's EM from the same flows (FP64 update), and
+    # stays within the flow bound of the EM from the oracle's own flows
+    gpf = pc.param_flows.cpu().numpy().astype(np.float64)
+    gipf = il.param_flows.cpu().numpy()[:ipf.shape[0]].astype(np.float64)
+    pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+    p1, q1 = orc.em_update(c["lay"], c["p0"], gpf, c["q0"], gipf, 0.1, 0.1)
+    assert np.abs(pc.params.cpu().numpy() - p1).max() <= 1e-6
+    assert np.abs(il.params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-6
+    p1o, _ = orc.em_update(c["lay"], c["p0"], c["pf"], c["q0"], c["ipf"], 0.1, 0.1)
+    assert np.abs(pc.params.cpu().numpy() - p1o).max() <= max(tol, 1e-5)
+
+
+def test_keep_zero_em_matches_reference(cuda_device):
+    fx = load_fixture("em_tiny")
+    pc = build_fixture_circuit("tiny", load_fixture("tiny")).to(cuda_device)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]).to(cuda_device))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]).to(cuda_device))
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    lls.mean().backward()
+    assert _rel(pc.param_flows.cpu().numpy(), fx["param_flows"]) <= 1e-4
+    pc.mini_batch_em(step_size=0.1, pseudocount=0.1, keep_zero_params=True)
+    got = pc.params.cpu().numpy()
+    assert np.abs(got - fx["params1_keep_zero"]).max() <= 1e-5
+    assert np.all(got[fx["params0"] == 0] == 0)
+    ip = pc.input_layer_group[0].params.cpu().numpy()[:fx["in_params1_keep_zero"].shape[0]]
+    assert np.abs(ip - fx["in_params1_keep_zero"]).max() <= 1e-5
+    assert np.all(ip[fx["in_params0"] == 0] == 0)
+
+
+def test_normalize_parameters_matches_reference(cuda_device):
+    fx = load_fixture("em_tiny")
+    pc = build_fixture_circuit("tiny", load_fixture("tiny")).to(cuda_device)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["norm_in"]).to(cuda_device))
+    pc.normalize_parameters(pseudocount=0.3)
+    assert np.abs(pc.params.cpu().numpy() - fx["norm_out"]).max() <= 1e-6
+
+
+def test_nonuniform_ll_weights(cuda_device):
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    B = 200
+    xn = fx["x"][:B]
+    x = torch.from_numpy(xn).to(cuda_device)
+    w = np.random.default_rng(3).uniform(0.1, 3.0, size=(1, B))
+    lay = orc.layout_from_circuit(pc)
+    nm, ems, _ = orc.forward(lay, fx["params0"], fx["in_params0"], xn)
+    _, pf, ipf = orc.backward(lay, fx["params0"], xn, nm, ems, ll_weights=w)
+    pc.init_param_flows(flows_memory=0.0)
+    with torch.no_grad():
+        pc(x, force_use_fp32=True)
+    pc.backward(inputs=x, ll_weights=torch.from_numpy(w).float().to(cuda_device), force_use_fp32=True)
+    assert _rel(pc.param_flows.cpu().numpy(), pf) <= 1e-4
+    assert _rel(pc.input_layer_group[0].param_flows.cpu().numpy()[:ipf.shape[0]], ipf) <= 1e-4
+    # lls.mean().backward() normalises the weights to sum to the batch size (all ones here)
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    (lls * torch.from_numpy(w.T).float().to(cuda_device)).sum().backward()
+    _, pf_n, _ = orc.backward(lay, fx["params0"], xn, nm, ems, ll_weights=w / w.sum() * B)
+    assert _rel(pc.param_flows.cpu().numpy(), pf_n) <= 1e-4
+
+
+def test_dataset_ll_accumulate_fp64(cuda_device):
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    acc = torch.zeros([], dtype=torch.float64, device=cuda_device)
+    total = 0.0
+    for b0 in range(0, 512, 128):
+        x = torch.from_numpy(fx["x"][b0:b0 + 128]).to(cuda_device)
+        with torch.no_grad():
+            lls = pc(x, force_use_fp32=True)
+        pc.dataset_ll_accumulate(lls, acc)
+        total += lls.double().sum().item()
+    assert abs(acc.item() - total) <= 1e-9 * abs(total)
+
+
+def test_fp64_epoch_flows_and_em(cuda_device):
+    """Three batches: the FP64 epoch flows equal the sum of each batch's flows (oracle), and
+    EM from them equals the oracle's EM from the summed flows."""
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    lay = orc.layout_from_circuit(pc)
+    pc.init_param_flows_f64()
+    pf_sum, ipf_sum = 0.0, 0.0
+    for b0 in (0, 100, 300):
+        xn = fx["x"][b0:b0 + 100]
+        nm, ems, _ = orc.forward(lay, fx["params0"], fx["in_params0"], xn)
+        _, pf, ipf = orc.backward(lay, fx["params0"], xn, nm, ems)
+        pf_sum, ipf_sum = pf_sum + pf, ipf_sum + ipf
+        x = torch.from_numpy(xn).to(cuda_device)
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            pc(x, force_use_fp32=True)
+        pc.backward(inputs=x, force_use_fp32=True)
+        pc.accumulate_param_flows_f64()
+    assert pc.param_flows_f64.dtype == torch.float64
+    assert _rel(pc.param_flows_f64.cpu().numpy(), pf_sum) <= 1e-4
+    il = pc.input_layer_group[0]
+    assert _rel(il.param_flows_f64.cpu().numpy()[:ipf_sum.shape[0]], ipf_sum) <= 1e-4
+    gpf = pc.param_flows_f64.cpu().numpy()
+    gipf = il.param_flows_f64.cpu().numpy()[:ipf_sum.shape[0]]
+    pc.mini_batch_em(step_size=1.0, pseudocount=0.1, use_f64_flows=True)
+    p1, q1 = orc.em_update(lay, fx["params0"], gpf, fx["in_params0"], gipf, 1.0, 0.1)
+    assert np.abs(pc.params.cpu().numpy() - p1).max() <= 1e-6
+    assert np.abs(il.params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-6
+
+
+def test_cumulate_flows_fp64_matches_fp32_accumulation(cuda_device):
+    """cumulate_flows(fp64=True) over batches gives the same epoch flows as the reference's
+    FP32 accumulation (flows_memory=1), up to FP32 rounding of the latter."""
+    fx = load_fixture("hclt64")
+    out = []
+    for fp64 in (False, True):
+        pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+        load_fixture_params(pc, fx)
+        pc.init_param_flows(flows_memory=0.0)
+        if fp64:
+            pc.init_param_flows_f64()
+        for b0 in (0, 128, 256, 384):
+            pc.cumulate_flows(torch.from_numpy(fx["x"][b0:b0 + 128]).to(cuda_device), fp64=fp64)
+        out.append((pc.param_flows_f64 if fp64 else pc.param_flows).double().cpu().numpy())
+    assert _rel(out[1], out[0]) <= 1e-5

@@ -35,16 +35,17 @@ def test_noalloc_matches_per_layer_sampling(name, cuda_device):
     assert S * (plan[3] + plan[4]) <= MAX_INTS
     seeds = [1234567, 99]
     outs = [torch.zeros([S, pc.num_vars], dtype=torch.long, device=cuda_device) for _ in seeds]
-    err = torch.full([1], 7, dtype=torch.int32, device=cuda_device)
-    _call(plan, outs[0], err, 5)  # first call on the device: address look-up
+    errs = [torch.full([1], 7, dtype=torch.int32, device=cuda_device) for _ in seeds]
+    _call(plan, outs[0], errs[0], 5)  # first call on the device: address look-up
     torch.cuda.synchronize()
     outs[0].zero_()
+    errs[0].fill_(7)
     before = torch.cuda.memory_allocated(cuda_device)
-    for out, seed in zip(outs, seeds):  # two calls in a row, no synchronisation between them
+    for out, err, seed in zip(outs, errs, seeds):  # two calls in a row, no synchronisation between them
         _call(plan, out, err, seed)
     torch.cuda.synchronize()
     assert torch.cuda.memory_allocated(cuda_device) == before
-    assert int(err.item()) == 0
+    assert [int(e.item()) for e in errs] == [0, 0]  # each call cleared and kept its own error word
     for out, seed in zip(outs, seeds):
         ref = juice.queries.sample(pc, S, seed=seed)
         assert torch.equal(out, ref)
@@ -68,3 +69,36 @@ def test_noalloc_rejects_oversize(cuda_device):
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     assert torch.equal(big[:64], juice.queries.sample(pc, 64, seed=3))
+
+
+def test_noalloc_reports_list_overflow(cuda_device):
+    """Element lists one slot too short: the kernel skips the writes past the cap and reports
+    code 1 (the working area is sized from the caps the caller passes, so nothing is written
+    out of bounds)."""
+    fx = load_fixture("hclt64")
+    pc = build_fixture_circuit("hclt64", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    table, num_steps, root_id, cap_n, cap_e = noalloc_sample_plan(pc)
+    samples = torch.zeros([64, pc.num_vars], dtype=torch.long, device=cuda_device)
+    err = torch.zeros([1], dtype=torch.int32, device=cuda_device)
+    _call((table, num_steps, root_id, cap_n, cap_e - 1), samples, err, 1)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1
+
+
+def test_noalloc_python_wrapper(cuda_device):
+    """queries.sample_noalloc (argument checks, then the same entry point) equals queries.sample;
+    a samples tensor narrower than num_vars is refused before anything is launched."""
+    from pyjuice_b200.queries.sample import sample_noalloc
+    fx = load_fixture("tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    out = torch.zeros([100, pc.num_vars], dtype=torch.long, device=cuda_device)
+    err = torch.full([1], 9, dtype=torch.int32, device=cuda_device)
+    sample_noalloc(pc, out, err, seed=42)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(out, juice.queries.sample(pc, 100, seed=42))
+    narrow = torch.zeros([100, pc.num_vars - 1], dtype=torch.long, device=cuda_device)
+    with pytest.raises(ValueError, match="num_vars"):
+        sample_noalloc(pc, narrow, err, seed=42)
