@@ -284,6 +284,43 @@ int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux,
                           int32_t mode, int32_t prec, int32_t batch_tile, int32_t slices_per_cta, void* stream);
 
 /*
+ * Sum layers under the MPE / GeneralLL propagation algorithms and the backward pass in
+ * log space, with negated parameter flows or accumulated child flows (plain FP32; these
+ * serve queries, not the EM step). alg: 0 LL, 1 MPE, 2 GeneralLL (alpha > 0).
+ * pcb_sum_fwd_generic: forward over the forward tile table (same tiles, kw, rows_per_block
+ *   and w_stride as pcb_lse_contract mode 0):
+ *   LL log sum w exp(e); MPE max (log w + e);
+ *   GeneralLL (log(sum w^alpha exp(alpha (e - m)) + 1e-24) + alpha m) / alpha, m = max e.
+ *   Replaces the propagation_alg_id 1/2 branches of _fw_triton_block_sparse_*_kernel and
+ *   _fw_triton_sparse_kernel (src/pyjuice/layer/sum_layer.py:454-568, 970-1037).
+ * pcb_sum_ele_generic: element flows over an element-flow tile table (rows = child rows,
+ *   krow = parent node rows, aux_row = the child's element_mars row):
+ *   LL sum f w exp(e - m); MPE sum over parents with |log w + e - m| < 1e-6 of f;
+ *   GeneralLL sum f w^alpha exp(alpha (e - m)); logspace = 1: flows are log flows and the
+ *   sums are log-sum-exps; accumulate = 1 adds to (log-adds to) the existing flows.
+ *   Replaces _bk_triton_block_sparse_ele_kernel / _bk_triton_sparse_ele_kernel in those
+ *   modes (sum_layer.py:1572-1889, 2466-2666).
+ * pcb_sum_par_generic: parameter flows over a parameter-flow tile table, summed over the
+ *   batch and added (negate = 1: subtracted) with float atomics:
+ *   LL / GeneralLL w sum_b f exp(e - m) (logspace: w sum_b exp(f + e - m), exp(f) where
+ *   m = -inf); MPE sum_b [|log w + e - m| < 1e-6] f (logspace: exp(f)).
+ *   Replaces _bk_triton_block_sparse_par_kernel / _bk_triton_sparse_par_kernel in those
+ *   modes (sum_layer.py:2052-2169, 2795-2902).
+ */
+int pcb_sum_fwd_generic(const float* element_mars, float* node_mars, int64_t ld, int32_t B, const float* params,
+                        const PcbLseTile* tiles, int32_t num_tiles, int32_t rows_per_block, const int32_t* krow,
+                        const int32_t* kw, int32_t w_stride, int32_t alg, float alpha, void* stream);
+int pcb_sum_ele_generic(const float* node_flows, const float* node_mars, const float* element_mars,
+                        float* element_flows, int64_t ld, int32_t B, const float* params, const PcbLseTile* tiles,
+                        int32_t num_tiles, int32_t rows_per_block, const int32_t* krow, const int32_t* kw,
+                        int32_t w_stride, int32_t alg, float alpha, int32_t logspace, int32_t accumulate,
+                        void* stream);
+int pcb_sum_par_generic(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld,
+                        int32_t B, const float* params, float* param_flows, const PcbPflowTile* tiles,
+                        int32_t num_tiles, int32_t rows_per_block, const int32_t* cids, const int32_t* pids,
+                        const int32_t* pfids, int32_t alg, int32_t logspace, int32_t negate, void* stream);
+
+/*
  * In place on rows [row0, row1) of node_flows: f <- (m == -inf) ? -inf : log(f) - m.
  * Replaces SumLayer._bk_triton_modify_flow_kernel (src/pyjuice/layer/sum_layer.py:1355-1515).
  */

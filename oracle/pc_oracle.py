@@ -228,6 +228,157 @@ def backward(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, em
     return nf, pf, in_pf
 
 
+def forward_alg(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarray, alg: str = "LL",
+                alpha: float = 1.0):
+    """Forward pass under a propagation algorithm (layer/sum_layer.py:500-563): "LL"
+    (``forward``), "MPE" ``max_c (log w + e_c)``, "GeneralLL"
+    ``(log(sum_c w^a exp(a (e_c - m)) + 1e-24) + a m) / a``. Returns (node_mars, ems, lls)."""
+    if alg == "LL":
+        return forward(layout, params, in_params, x)
+    x = np.asarray(x, dtype=np.int64)
+    B = x.shape[0]
+    nm = np.zeros([layout["num_nodes"], B])
+    inp = layout["input"]
+    n_in = inp["vids"].shape[0]
+    with np.errstate(divide="ignore"):
+        nm[inp["nid_start"]:inp["nid_start"] + n_in] = np.log(in_params.astype(np.float64))[
+            inp["s_pids"][:, None] + x[:, inp["vids"]].T]
+        logw = np.log(params.astype(np.float64))
+    ems, em = {}, None
+    for gi, g in enumerate(layout["groups"]):
+        if g["kind"] == "prod":
+            em = np.full([layout["num_elements"], B], -np.inf)
+            for l in g["layers"]:
+                bs = l["block_size"]
+                for nids, cids in zip(l["nids"], l["cids"]):
+                    acc = np.zeros([nids.shape[0] * bs, B])
+                    for j in range(cids.shape[1]):
+                        acc += nm[_rows(cids[:, j], bs)]
+                    em[_rows(nids, bs)] = acc
+            ems[gi] = em
+            continue
+        for l in g["layers"]:
+            bs = l["block_size"]
+            for nids, cids, pids in zip(l["nids"], l["cids"], l["pids"]):
+                G, C = cids.shape
+                e = np.where(cids[:, :, None] == 0, -np.inf, em[cids.reshape(-1)].reshape(G, C, B))
+                lw = np.where(cids[:, :, None] == 0, -np.inf, logw[pids[:, :, None] + np.arange(bs)[None, None, :]])
+                if alg == "MPE":
+                    s = np.max(lw[:, :, :, None] + e[:, :, None, :], axis=1)         # [G, bs, B]
+                else:
+                    m = np.max(e, axis=1)
+                    fin = np.isfinite(m)
+                    m0 = np.where(fin, m, 0.0)
+                    t = np.exp(alpha * lw)[:, :, :, None] * np.exp(alpha * (e - m0[:, None, :]))[:, :, None, :]
+                    with np.errstate(divide="ignore"):
+                        s = np.where(fin[:, None, :], (np.log(t.sum(axis=1) + 1e-24) + alpha * m0[:, None, :]) / alpha,
+                                     -np.inf)
+                nm[_rows(nids, bs)] = s.reshape(G * bs, B)
+    r0, r1 = layout["root_range"]
+    return nm, ems, nm[r0:r1].T.copy()
+
+
+def _lse(a, axis):
+    m = np.max(a, axis=axis, keepdims=True)
+    m0 = np.where(np.isfinite(m), m, 0.0)
+    with np.errstate(divide="ignore"):
+        out = np.log(np.exp(a - m0).sum(axis=axis, keepdims=True)) + m0
+    return np.squeeze(np.where(np.isfinite(m), out, -np.inf), axis=axis)
+
+
+def backward_alg(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, ems: dict, alg: str = "LL",
+                 alpha: float = 1.0, logspace: bool = False, negate: bool = False, ll_weights: np.ndarray = None):
+    """Backward pass under a propagation algorithm, in linear or log-space flows, with
+    optionally negated parameter flows (sum_layer.py:1572-1730, 2052-2169, 3068-3127;
+    prod_layer.py:432-466; categorical.py:94-100). Small circuits only (dense per-edge
+    arrays). Returns (node_flows, param_flows, input param_flows).
+
+    Element flows of child c with parents n (weight w, flow f, value m):
+      LL  f w exp(e - m);  GeneralLL  f w^a exp(a (e - m));  MPE  f where |log w + e - m| < 1e-6
+    summed (log space: log-sum-exp of the logs). Parameter flows of edge (n, c):
+      LL / GeneralLL  w sum_b f exp(e - m) (log space: w sum_b exp(f + e - m), exp(f) where
+      m = -inf);  MPE  sum_b [|log w + e - m| < 1e-6] f (log space: exp(f)).
+    """
+    x = np.asarray(x, dtype=np.int64)
+    B = x.shape[0]
+    N = layout["num_nodes"]
+    nf = np.full([N, B], -np.inf if logspace else 0.0)
+    r0, r1 = layout["root_range"]
+    w_root = np.ones([r1 - r0, B]) if ll_weights is None else np.broadcast_to(ll_weights, (r1 - r0, B))
+    with np.errstate(divide="ignore"):
+        nf[r0:r1] = np.log(w_root) if logspace else w_root
+    pf = np.zeros([layout["num_param_flows"]])
+    w = params.astype(np.float64)
+    with np.errstate(divide="ignore"):
+        lw_all = np.log(w)
+    groups = layout["groups"]
+    ef = None
+    sign = -1.0 if negate else 1.0
+    for gi in range(len(groups) - 1, -1, -1):
+        g = groups[gi]
+        if g["kind"] == "prod":
+            for l in g["layers"]:
+                bs = l["block_size"]
+                for u, par in zip(l["u_cids"], l["parids"]):
+                    tgt = _rows(u, bs)
+                    cols = [np.where(np.repeat(par[:, q] != 0, bs)[:, None], ef[_rows(par[:, q], bs)],
+                                     -np.inf if logspace else 0.0) for q in range(par.shape[1])]
+                    if logspace:
+                        nf[tgt] = _lse(np.stack([nf[tgt]] + cols), axis=0)
+                    else:
+                        nf[tgt] += np.sum(cols, axis=0)
+            continue
+        em = ems[gi - 1]
+        ef = np.full([layout["num_elements"], B], -np.inf if logspace else 0.0)
+        for l in g["layers"]:
+            bs = l["block_size"]
+            ar = np.arange(bs)
+            for chids, parids, parpids, cbs in zip(l["chids"], l["parids"], l["parpids"], l["cs_block_sizes"]):
+                for r in range(chids.shape[0]):
+                    pr = parids[r][parids[r] != 0]
+                    pp = parpids[r][:pr.shape[0]]
+                    nrow = (pr[:, None] + ar).reshape(-1)                        # parents [K]
+                    for j in range(cbs):
+                        c = int(chids[r]) + j
+                        lw = lw_all[(pp[:, None] + j * bs + ar).reshape(-1)]     # [K]
+                        f, m, e = nf[nrow], nm[nrow], em[c][None, :]
+                        with np.errstate(invalid="ignore", over="ignore"):
+                            d = lw[:, None] + e - m
+                            if alg == "MPE":
+                                hit = np.isfinite(m) & (np.abs(d) < 1e-6)
+                                v = _lse(np.where(hit, f, -np.inf), 0) if logspace else np.where(hit, f, 0.0).sum(0)
+                            else:
+                                xx = np.where(np.isfinite(m), alpha * d if alg == "GeneralLL" else d, -np.inf)
+                                v = _lse(f + xx, 0) if logspace else np.where(np.isfinite(xx), f * np.exp(xx), 0.0).sum(0)
+                        ef[c] = v
+            for nids, cids, pids, pfids in zip(l["nids"], l["cids"], l["pids"], l["pfids"]):
+                for r in range(nids.shape[0]):
+                    real = cids[r] != 0
+                    for i in range(bs):
+                        n = int(nids[r]) + i
+                        f, m = nf[n][None, :], nm[n][None, :]
+                        wv = w[pids[r][real] + i][:, None]
+                        e = em[cids[r][real]]
+                        with np.errstate(invalid="ignore", over="ignore", divide="ignore"):
+                            if alg == "MPE":
+                                hit = np.abs(np.log(wv) + e - m) < 1e-6
+                                v = np.where(hit, np.exp(f) if logspace else f, 0.0).sum(1)
+                            elif logspace:
+                                v = wv[:, 0] * np.where(np.isfinite(m), np.exp(f + e - m), np.exp(f)).sum(1)
+                            else:
+                                v = wv[:, 0] * np.where(np.isfinite(m), f * np.exp(e - m), 0.0).sum(1)
+                        np.add.at(pf, pfids[r][real] + i, sign * v)
+    inp = layout["input"]
+    n_in = inp["vids"].shape[0]
+    npf = inp["num_param_flows"] if inp.get("num_param_flows") else int(inp["s_pfids"].max() + inp["ncats"].max())
+    in_pf = np.zeros([npf])
+    rows = inp["nid_start"] + np.arange(n_in)
+    slots = inp["s_pfids"][:, None] + x[:, inp["vids"]].T
+    vals = np.exp(nf[rows]) if logspace else nf[rows]
+    np.add.at(in_pf, slots.reshape(-1), vals.reshape(-1))
+    return nf, pf, in_pf
+
+
 def _sum_block_table(layout: dict):
     """Per distinct parameter slab: (first param id, #children, block size, set of first flow ids).
 

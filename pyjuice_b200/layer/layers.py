@@ -428,11 +428,23 @@ class SumLayer(Layer):
             self._run_pack_job(params, job)
         return bool(jobs)
 
+    @staticmethod
+    def _alg(propagation_alg: str, kwargs) -> tuple:
+        """(algorithm id, alpha) of a propagation algorithm (layer.py:11-15, 89-97)."""
+        if propagation_alg not in Layer.propagation_alg_mapping:
+            raise ValueError(f"Unknown propagation algorithm {propagation_alg}.")
+        alpha = 0.0
+        if propagation_alg == "GeneralLL":
+            if "alpha" not in kwargs:
+                raise ValueError("Argument `alpha` should be provided for the `GeneralLL` propagation algorithm.")
+            alpha = float(kwargs["alpha"])
+            if not alpha > 0.0:
+                raise ValueError("`alpha` must be positive")
+        return Layer.propagation_alg_mapping[propagation_alg], alpha
+
     def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, params: torch.Tensor,
                 force_use_bf16: bool = False, force_use_fp32: bool = False, propagation_alg: str = "LL",
                 _weights_packed: bool = False, **kwargs) -> None:
-        if propagation_alg != "LL":
-            raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
         if params.dim() != 1:
             raise ValueError("Expecting a 1D `params`.")
         d = self._desc(node_mars.device)
@@ -440,6 +452,14 @@ class SumLayer(Layer):
         ld = node_mars.stride(0)
         if element_mars.stride(0) != ld or node_mars.stride(1) != 1 or element_mars.stride(1) != 1:
             raise ValueError("node_mars and element_mars must share a row-major layout")
+        if propagation_alg != "LL":
+            # MPE / GeneralLL: the FP32 kernel of these modes (pcb_sum_fwd_generic)
+            alg, alpha = self._alg(propagation_alg, kwargs)
+            t = d["fw_tiles"]
+            nat.call("pcb_sum_fwd_generic", nat.ptr(element_mars), nat.ptr(node_mars), ld, B, nat.ptr(params),
+                     nat.ptr(t), t.size(0), self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, alg, alpha,
+                     nat.stream())
+            return
         prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
         t = d["fw_tiles"]
         st = nat.stream()
@@ -474,16 +494,24 @@ class SumLayer(Layer):
                  allow_modify_flows: bool = False, propagation_alg: str = "LL", logspace_flows: bool = False,
                  negate_pflows: bool = False, accumulate_ch_flows: bool = False, allow_neg_flows: bool = False,
                  force_use_fp32: bool = False, _weights_packed: bool = False, **kwargs) -> None:
-        if propagation_alg != "LL":
-            raise NotImplementedError(f"propagation algorithm {propagation_alg} is not supported by the CUDA path")
-        if logspace_flows or negate_pflows or accumulate_ch_flows or allow_neg_flows:
-            raise NotImplementedError("logspace / negated / accumulated / negative flows are not supported by the CUDA path")
+        if allow_modify_flows and logspace_flows:
+            raise ValueError("`allow_modify_flows` should be set to `False` when using `logspace_flows`.")
+        if accumulate_ch_flows and logspace_flows:
+            raise ValueError("`accumulate_ch_flows` should be set to `False` when using `logspace_flows`.")
+        if allow_neg_flows and (logspace_flows or propagation_alg != "LL"):
+            raise ValueError("`allow_neg_flows` needs linear LL flows")
         d = self._desc(node_mars.device)
         B = node_mars.size(1)
         ld = node_mars.stride(0)
         for t in (node_flows, element_flows, element_mars):
             if t.stride(0) != ld or t.stride(1) != 1:
                 raise ValueError("node/element mars/flows must share a row-major layout")
+        if propagation_alg != "LL" or logspace_flows or negate_pflows or accumulate_ch_flows or allow_neg_flows:
+            if allow_modify_flows:
+                raise ValueError("these flow modes read unmodified node flows: pass allow_modify_flows=False")
+            self._backward_generic(node_flows, element_flows, node_mars, element_mars, params, param_flows,
+                                   propagation_alg, logspace_flows, negate_pflows, accumulate_ch_flows, kwargs)
+            return
         if allow_modify_flows and not kwargs.get("_flows_modified"):
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
                      self._layer_nid_range[1], nat.stream())
@@ -535,6 +563,29 @@ class SumLayer(Layer):
             with torch.cuda.stream(pflow_stream if ready is not None else torch.cuda.current_stream()):
                 self.param_flows_only(node_flows, node_mars, element_mars, params, param_flows,
                                       allow_modify_flows=allow_modify_flows, force_use_fp32=force_use_fp32)
+
+    def _backward_generic(self, node_flows, element_flows, node_mars, element_mars, params, param_flows,
+                          propagation_alg, logspace_flows, negate_pflows, accumulate_ch_flows, kwargs):
+        """Element and parameter flows of the MPE / GeneralLL algorithms, of log-space flows, of
+        negated parameter flows and of accumulated child flows (pcb_sum_ele_generic,
+        pcb_sum_par_generic; FP32)."""
+        alg, alpha = self._alg(propagation_alg, kwargs)
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        st = nat.stream()
+        for eg in d["el_groups"]:
+            et = eg["tiles"]
+            nat.call("pcb_sum_ele_generic", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
+                     nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0), eg["cbs"],
+                     nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size, alg, alpha, 1 if logspace_flows else 0,
+                     1 if accumulate_ch_flows else 0, st)
+        if param_flows is not None:
+            pt = d["pf_tiles"]
+            nat.call("pcb_sum_par_generic", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
+                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size,
+                     nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]), alg, 1 if logspace_flows else 0,
+                     1 if negate_pflows else 0, st)
 
     def param_flows_only(self, node_flows: torch.Tensor, node_mars: torch.Tensor, element_mars: torch.Tensor,
                          params: torch.Tensor, param_flows: torch.Tensor, allow_modify_flows: bool = False,

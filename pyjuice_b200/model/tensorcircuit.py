@@ -470,10 +470,28 @@ class TensorCircuit(nn.Module):
 
     # ------------------------------------------------------------------ passes
     def set_propagation_alg(self, propagation_alg: str, **kwargs):
-        if propagation_alg != "LL":
-            raise NotImplementedError("only the LL propagation algorithm runs on the CUDA path")
-        self.default_propagation_alg = "LL"
-        self.propagation_alg_kwargs.clear()
+        """Default propagation algorithm of ``forward`` (tensorcircuit.py:192-205): "LL",
+        "MPE" or "GeneralLL" (with ``alpha``)."""
+        if propagation_alg in ("LL", "MPE"):
+            self.default_propagation_alg = propagation_alg
+            self.propagation_alg_kwargs.clear()
+        elif propagation_alg == "GeneralLL":
+            if "alpha" not in kwargs:
+                raise ValueError("Argument `alpha` should be provided for the `GeneralLL` propagation algorithm.")
+            self.default_propagation_alg = "GeneralLL"
+            self.propagation_alg_kwargs.clear()
+            self.propagation_alg_kwargs["alpha"] = kwargs["alpha"]
+        else:
+            raise NotImplementedError(f"Unknown propagation algorithm {propagation_alg}.")
+
+    def forward_ll(self, *args, **kwargs):
+        return self.forward(*args, propagation_alg="LL", **kwargs)
+
+    def forward_mpe(self, *args, **kwargs):
+        return self.forward(*args, propagation_alg="MPE", **kwargs)
+
+    def forward_general_ll(self, *args, alpha: float = 1.0, **kwargs):
+        return self.forward(*args, propagation_alg="GeneralLL", alpha=alpha, **kwargs)
 
     def _em_view(self, group_id: int) -> torch.Tensor:
         """Element values of product layer group ``group_id`` (rows indexed like ``element_mars``)."""
@@ -543,6 +561,7 @@ class TensorCircuit(nn.Module):
         self._el_pack_state = self._pack_state_key(B, force_use_fp32)
         groups = self.inner_layer_groups
         for gi, group in enumerate(groups):
+            alg = propagation_alg if isinstance(propagation_alg, str) else propagation_alg[gi]
             if group.is_prod():
                 fused = (gi + 1 < len(groups) and self._fusion_tables(gi, "fw") is not None and
                          groups[gi + 1][0].runs_single_stage(self.device, B, force_use_bf16, force_use_fp32))
@@ -555,8 +574,10 @@ class TensorCircuit(nn.Module):
                 fz = self._fusion_tables(gi - 1, "fw")
                 if fz is not None and not group[0].runs_single_stage(self.device, B, force_use_bf16, force_use_fp32):
                     fz = None
+                if alg != "LL" and fz is not None:  # the fused kernels run LL only
+                    raise RuntimeError("forward product fusion runs the LL algorithm only")
                 group(self.node_mars, self._em_view(gi - 1), self.params, force_use_bf16=force_use_bf16,
-                      force_use_fp32=force_use_fp32, propagation_alg=propagation_alg, _weights_packed=True,
+                      force_use_fp32=force_use_fp32, propagation_alg=alg, _weights_packed=True,
                       _fuse_fw=None if fz is None else (fz, self._em_view(gi - 1)), **kwargs)
         main.wait_stream(side)
 
@@ -570,6 +591,11 @@ class TensorCircuit(nn.Module):
             raise RuntimeError("TensorCircuit runs on CUDA only: call pc.to('cuda') first")
         if propagation_alg is None:
             propagation_alg = self.default_propagation_alg
+            kwargs.update(self.propagation_alg_kwargs)
+        if not isinstance(propagation_alg, str):
+            propagation_alg = tuple(propagation_alg)
+            if len(propagation_alg) != len(self.inner_layer_groups):
+                raise ValueError("a per-layer propagation_alg needs one entry per inner layer group")
         with torch.no_grad():
             B = inputs.size(0)
             origin_inputs = inputs
@@ -596,7 +622,8 @@ class TensorCircuit(nn.Module):
                         ret = input_layer_fn(layer, inputs, nm, **kwargs)
                         if not ret and ret is not None:
                             layer(data, nm, **kwargs)
-            sig = (0, id(nm), id(em), id(self._em_resident), id(self.params), B, force_use_bf16, force_use_fp32)
+            sig = (0, id(nm), id(em), id(self._em_resident), id(self.params), B, force_use_bf16, force_use_fp32,
+                   propagation_alg, kwargs.get("alpha"))
             run = partial(self._run_inner_forward, force_use_bf16, force_use_fp32, propagation_alg, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
                 self._recorded_cuda_graphs[sig] = self._capture(run)
@@ -635,7 +662,8 @@ class TensorCircuit(nn.Module):
             fn()
         return g
 
-    def _run_inner_backward(self, compute_param_flows, allow_modify_flows, logspace_flows, force_use_fp32, **kwargs):
+    def _run_inner_backward(self, compute_param_flows, allow_modify_flows, logspace_flows, force_use_fp32,
+                            propagation_alg="LL", negate_pflows=False, **kwargs):
         # Parameter flows go to side streams: nothing later in the pass reads them, so they run
         # alongside the element-flow / product chain and join before the pass ends. The
         # parameter-flow launches of the small levels are latency-bound, so consecutive levels
@@ -657,6 +685,8 @@ class TensorCircuit(nn.Module):
                     el_ready = torch.cuda.Event()
                     el_ready.record(sides[0])
         kwargs = dict(kwargs, _weights_packed=True)
+        plain = (propagation_alg == "LL" if isinstance(propagation_alg, str) else
+                 all(a == "LL" for a in propagation_alg)) and not negate_pflows and not logspace_flows
         turn = 0
         def rewrites(g):  # large layers rewrite their node flows as log f - log m
             return allow_modify_flows and any(
@@ -666,7 +696,7 @@ class TensorCircuit(nn.Module):
         # product layers fused into the element-flow kernel above them in this pass
         fuse_bw = dict()
         for g, group in enumerate(self.inner_layer_groups):
-            if not group.is_sum() or rewrites(g) or logspace_flows:
+            if not group.is_sum() or rewrites(g) or not plain:
                 continue
             fz = self._fusion_tables(g - 1, "bw")
             if fz is not None and group[0].runs_single_stage(self.device, B, force_use_fp32=force_use_fp32,
@@ -695,12 +725,14 @@ class TensorCircuit(nn.Module):
                     main.wait_event(el_ready)
                     el_ready = None
                 fz = fuse_bw.get(layer_id)
+                alg = propagation_alg if isinstance(propagation_alg, str) else propagation_alg[layer_id]
                 group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
                                force_use_fp32=force_use_fp32, _pflow_stream=sides[turn % len(sides)], _fuse_bw=fz,
-                               _flows_modified=layer_id in rewritten, **kwargs)
+                               _flows_modified=layer_id in rewritten, propagation_alg=alg,
+                               negate_pflows=negate_pflows, **kwargs)
                 turn += 1
         for side in sides:
             main.wait_stream(side)
@@ -717,10 +749,13 @@ class TensorCircuit(nn.Module):
         """Node flows, element flows and (accumulated) parameter flows of the last forward batch."""
         if self.node_mars is None or self.element_mars is None:
             raise RuntimeError("Should run forward path first.")
-        if propagation_alg != "LL" or negate_pflows:
-            raise NotImplementedError("only LL flows run on the CUDA path")
         if allow_modify_flows and logspace_flows:
             raise ValueError("`allow_modify_flows` should be set to `False` when using `logspace_flows`.")
+        if not isinstance(propagation_alg, str):
+            propagation_alg = tuple(propagation_alg)
+        if propagation_alg != "LL" or negate_pflows:
+            # the kernels of these modes read unmodified node flows (the results are the same)
+            allow_modify_flows = False
         if sum_layer_pre_backward_callback is not None or sum_layer_post_backward_callback is not None:
             raise NotImplementedError("sum-layer callbacks are not supported")
         self._run_params.update(allow_modify_flows=allow_modify_flows, propagation_alg=propagation_alg,
@@ -763,9 +798,10 @@ class TensorCircuit(nn.Module):
             if compute_param_flows:
                 self.init_param_flows(flows_memory=flows_memory)
             sig = (1, id(nf), id(ef), id(self.node_mars), id(self._em_resident), id(self.params),
-                   id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows)
+                   id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows,
+                   propagation_alg, negate_pflows, kwargs.get("alpha"))
             run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,
-                          force_use_fp32, **kwargs)
+                          force_use_fp32, propagation_alg=propagation_alg, negate_pflows=negate_pflows, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
                 # The pass rewrites node flows in place and accumulates parameter flows, so each
                 # warm-up run starts from the state of this call and the state is put back after

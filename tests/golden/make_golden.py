@@ -19,6 +19,8 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``em_tiny.npz``    the tiny circuit with a tenth of its parameters zeroed: one step with
                     ``keep_zero_params=True``, and the reference's normalisation of a seeded
                     parameter vector with pseudocount 0.3;
+* ``alg_tiny.npz``   the tiny circuit under MPE, GeneralLL(0.5), log-space flows and negated
+                    parameter flows: log-likelihoods, node values, node flows, parameter flows;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -237,6 +239,35 @@ def make_em_variants():
     np.savez_compressed(os.path.join(HERE, "em_tiny.npz"), **out)
 
 
+def make_alg_variants():
+    """The tiny circuit under the other propagation algorithms and flow modes (FP32 forms):
+    MPE forward + backward, GeneralLL(alpha = 0.5) forward + backward, log-space LL flows and
+    negated LL parameter flows (``allow_modify_flows=False`` throughout)."""
+    fx = dict(np.load(os.path.join(HERE, "tiny.npz")))
+    torch.manual_seed(1)
+    pc = juice.compile(build_tiny_dag(juice, dists), max_tied_ns_per_parflow_block=1, verbose=False)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+    x = torch.from_numpy(fx["x"])
+    out = {}
+    cases = {"mpe": (dict(propagation_alg="MPE"), dict()),
+             "gll": (dict(propagation_alg="GeneralLL", alpha=0.5), dict()),
+             "logspace": (dict(), dict(logspace_flows=True)),
+             "negate": (dict(), dict(negate_pflows=True))}
+    for name, (fw_kw, bw_kw) in cases.items():
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            lls = pc(x, force_use_fp32=True, **fw_kw)
+        pc.backward(inputs=x, allow_modify_flows=False, force_use_fp32=True, **fw_kw, **bw_kw)
+        out[name + "_lls"] = lls.detach().cpu().numpy().copy()
+        out[name + "_node_mars"] = pc.node_mars.detach().cpu().numpy().copy()
+        out[name + "_node_flows"] = pc.node_flows.detach().cpu().numpy().copy()
+        out[name + "_param_flows"] = pc.param_flows.detach().cpu().numpy().copy()
+        out[name + "_in_param_flows"] = pc.input_layer_group[0].param_flows.detach().cpu().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "alg_tiny.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -276,10 +307,10 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
-         "em_tiny": make_em_variants}[w]()
+         "em_tiny": make_em_variants, "alg_tiny": make_alg_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

@@ -88,3 +88,29 @@ def test_oracle_keep_zero_em_and_normalisation():
     assert np.abs(ip1 - fx["in_params1_keep_zero"]).max() <= 1e-6
     got = orc.normalize(lay, fx["norm_in"], 0.3)
     assert np.abs(got - fx["norm_out"]).max() <= 1e-6
+
+
+ALG_CASES = [("mpe", "MPE", 1.0, False, False), ("gll", "GeneralLL", 0.5, False, False),
+             ("logspace", "LL", 1.0, True, False), ("negate", "LL", 1.0, False, True)]
+
+
+@pytest.mark.parametrize("case", ALG_CASES, ids=[c[0] for c in ALG_CASES])
+def test_oracle_propagation_algorithms_match_reference(case):
+    """MPE and GeneralLL(0.5) passes, log-space flows and negated parameter flows of the
+    oracle against the reference's own outputs on the tiny circuit (fixture alg_tiny.npz)."""
+    name, alg, alpha, logspace, negate = case
+    fx = load_fixture("tiny")
+    ref = load_fixture("alg_tiny")
+    lay = orc.layout_from_fixture(fx, ncats=4)
+    nm, ems, lls = orc.forward_alg(lay, fx["params0"], fx["in_params0"], fx["x"], alg, alpha)
+    assert np.allclose(lls, ref[name + "_lls"], rtol=1e-6, atol=1e-5)
+    nf, pf, ipf = orc.backward_alg(lay, fx["params0"], fx["x"], nm, ems, alg=alg, alpha=alpha, logspace=logspace,
+                                   negate=negate)
+    rpf = ref[name + "_param_flows"]
+    assert np.abs(pf - rpf).max() <= 1e-5 * np.abs(rpf).max()
+    ripf = ref[name + "_in_param_flows"][:ipf.shape[0]]
+    assert np.abs(ipf - ripf).max() <= 1e-5 * np.abs(ripf).max()
+    rnf = ref[name + "_node_flows"]
+    fin = np.isfinite(rnf)
+    assert np.array_equal(fin, np.isfinite(nf))
+    assert np.abs(nf[fin] - rnf[fin]).max() <= 1e-5

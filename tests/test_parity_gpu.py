@@ -9,7 +9,8 @@ own outputs, in every precision form the EM step runs in:
 * non-uniform root weights (``ll_weights``), the FP64 dataset log-likelihood reducer and
   FP64 epoch-level parameter flows against the oracle.
 
-Error bounds, relative to the largest magnitude of the compared quantity: FP32 1e-4; split
+Error bounds, relative to the largest magnitude of the compared quantity: FP32 3e-4 (59 levels
+of FP32 rounding between the root and the inputs); split
 BF16 2e-3; single BF16 5e-2 (its operands keep 8 mantissa bits).
 """
 
@@ -27,7 +28,7 @@ from pyjuice_b200.synthetic import gaussian_field_data
 
 pytestmark = pytest.mark.gpu
 
-FORMS = {"fp32": (0, 1e-4), "bf16_split": (2, 2e-3), "bf16_single": (1, 5e-2)}
+FORMS = {"fp32": (0, 3e-4), "bf16_split": (2, 2e-3), "bf16_single": (1, 5e-2)}
 _CACHE = {}
 
 
@@ -217,3 +218,53 @@ def test_cumulate_flows_fp64_matches_fp32_accumulation(cuda_device):
             pc.cumulate_flows(torch.from_numpy(fx["x"][b0:b0 + 128]).to(cuda_device), fp64=fp64)
         out.append((pc.param_flows_f64 if fp64 else pc.param_flows).double().cpu().numpy())
     assert _rel(out[1], out[0]) <= 1e-5
+
+
+ALG_CASES = [("mpe", "MPE", 1.0, False, False), ("gll", "GeneralLL", 0.5, False, False),
+             ("logspace", "LL", 1.0, True, False), ("negate", "LL", 1.0, False, True)]
+
+
+@pytest.mark.parametrize("case", ALG_CASES, ids=[c[0] for c in ALG_CASES])
+def test_propagation_algorithms_match_reference(case, cuda_device):
+    """MPE / GeneralLL forward and backward, log-space flows and negated parameter flows on
+    the tiny circuit (partitions, sparse edges, ties, pass-through) against the reference's
+    own outputs (alg_tiny.npz), through the public API."""
+    name, alg, alpha, logspace, negate = case
+    fx = load_fixture("tiny")
+    ref = load_fixture("alg_tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    fw = dict(propagation_alg=alg) if alg == "MPE" else (dict(propagation_alg=alg, alpha=alpha) if alg != "LL" else {})
+    pc.init_param_flows(flows_memory=0.0)
+    with torch.no_grad():
+        lls = pc(x, force_use_fp32=True, **fw)
+    pc.backward(inputs=x, allow_modify_flows=False, force_use_fp32=True, logspace_flows=logspace,
+                negate_pflows=negate, **fw)
+    rl = ref[name + "_lls"]
+    assert np.all(np.abs(lls.cpu().numpy() - rl) <= 1e-5 * np.abs(rl) + 1e-6)
+    assert _rel(pc.param_flows.cpu().numpy(), ref[name + "_param_flows"]) <= 1e-4
+    ripf = ref[name + "_in_param_flows"]
+    assert _rel(pc.input_layer_group[0].param_flows.cpu().numpy()[:ripf.shape[0]], ripf) <= 1e-4
+    rnf = ref[name + "_node_flows"]
+    nf = pc.node_flows.cpu().numpy()
+    fin = np.isfinite(rnf)
+    assert np.array_equal(fin, np.isfinite(nf))
+    assert np.abs(nf[fin] - rnf[fin]).max() <= 1e-4 * max(1.0, np.abs(rnf[fin]).max())
+
+
+def test_set_propagation_alg_and_forward_mpe(cuda_device):
+    fx = load_fixture("tiny")
+    ref = load_fixture("alg_tiny")
+    pc = build_fixture_circuit("tiny", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"]).to(cuda_device)
+    with torch.no_grad():
+        a = pc.forward_mpe(x, force_use_fp32=True).cpu().numpy()
+        pc.set_propagation_alg("GeneralLL", alpha=0.5)
+        b = pc(x, force_use_fp32=True).cpu().numpy()
+        pc.set_propagation_alg("LL")
+    assert np.abs(a - ref["mpe_lls"]).max() <= 1e-4
+    assert np.abs(b - ref["gll_lls"]).max() <= 1e-4
+    with pytest.raises(ValueError):
+        pc.set_propagation_alg("GeneralLL")
