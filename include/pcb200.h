@@ -107,14 +107,18 @@ int pcb_fill_rows(float* mat, int64_t ld, int64_t row0, int64_t row1, float valu
 /*
  * Categorical input layer forward: node_mars[node_offset + n, b] =
  *   log(params[s_pids[n] + data[vids[n] * data_ld + b]]) for n < num_nodes, b < B
- * (NaN where the category is outside [0, ncats[n]), reported as PCB_STATUS_BAD_CATEGORY).
- * data is int64 [num_vars, data_ld].
+ * (NaN where the category is outside [0, ncats[n]), reported as PCB_STATUS_BAD_CATEGORY),
+ * or 0 where `missing` (may be NULL) marks the variable as missing in that sample:
+ * missing[b * miss_sb + vids[n] * miss_sv] != 0 (miss_sb = 0 for a per-variable mask).
+ * data is int64 [num_vars, data_ld]. The missing-mask form replaces
+ * InputLayer._fw_missing_mask_kernel (src/pyjuice/layer/input_layer.py:1059-1095).
  * Replaces InputLayer._mars_kernel_template + Categorical.fw_mar_fn
  * (src/pyjuice/layer/input_layer.py:1016-1054, src/pyjuice/nodes/distributions/categorical.py:83-91).
  */
 int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params,
                       const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, int32_t num_nodes,
-                      int32_t node_offset, float* node_mars, int64_t ld, int32_t B, void* stream);
+                      int32_t node_offset, float* node_mars, int64_t ld, int32_t B, const uint8_t* missing,
+                      int64_t miss_sb, int64_t miss_sv, void* stream);
 
 /*
  * Categorical input layer backward (parameter flows), deterministic:
@@ -122,7 +126,10 @@ int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params,
  * for every node n of every variable group. Groups are runs of nodes over the same
  * variable: group g covers nodes [grp_node0[g], grp_node0[g] + grp_count[g]) of
  * variable grp_var[g], with grp_ncats[g] categories; samples whose category is outside
- * [0, ncats) are skipped. logspace_flows: node flows hold log flows.
+ * [0, ncats) are skipped. logspace_flows: node flows hold log flows. Where `missing`
+ * (may be NULL; same indexing as pcb_input_cat_fwd) marks the variable as missing, the
+ * node's flow f goes to every category k as f * params[s_pids[n] + k] (s_pids and params
+ * are read only then; categorical.py:102-134).
  * Replaces InputLayer._flows_kernel_template + Categorical.bk_flow_fn
  * (src/pyjuice/layer/input_layer.py:1098-1155, categorical.py:94-100), whose atomic
  * scatter this replaces with a per-variable counting sort of the batch.
@@ -131,7 +138,8 @@ int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_fl
                       const int32_t* grp_var, const int32_t* grp_node0, const int32_t* grp_count,
                       const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
                       const int32_t* s_pfids, int32_t node_offset, float* param_flows,
-                      int32_t logspace_flows, void* stream);
+                      int32_t logspace_flows, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
+                      const int32_t* s_pids, const float* params, void* stream);
 
 /*
  * Categorical EM update of the source nodes (in FP64):
@@ -377,6 +385,61 @@ int pcb_input_cat_em_f64flows(float* params, const double* param_flows, const in
                               const int32_t* s_pfids, const int32_t* ncats, const int32_t* source_nids,
                               int32_t num_source_nodes, double step_size, double pseudocount,
                               int32_t keep_zero_params, void* stream);
+
+/*
+ * Gradients with respect to softmax logits of the parameters (one softmax per node over
+ * its children / categories), from parameter flows pf (theta times dLL/dtheta, as the
+ * backward pass accumulates them with root weights dLoss/dLL):
+ *   grad = scale * (pf - theta * sum_children pf)
+ * written in the parameters' layout. pcb_sum_logit_grad uses the pcb_sum_em block table
+ * (tied flow slots must be summed into the source slot first, pcb_pflow_accum);
+ * pcb_input_cat_logit_grad the pcb_input_cat_em node table.
+ * No counterpart in the reference (its parameters carry no autograd; the formula is the
+ * softmax chain rule applied to its parameter flows, sum_layer.py:2052-2169).
+ */
+int pcb_sum_logit_grad(const float* params, const float* param_flows, const int64_t* blk_pbase,
+                       const int64_t* blk_pfbase, const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks,
+                       double scale, float* grad, void* stream);
+/* Sum weights from logits: softmax over each node's children (pcb_sum_em block table; FP64
+ * normaliser). No counterpart in the reference (its weights are not parameterised by logits). */
+int pcb_sum_softmax(const float* logits, float* params, const int64_t* blk_pbase, const int32_t* blk_nch,
+                    const int32_t* blk_bs, int32_t num_blocks, void* stream);
+int pcb_input_cat_logit_grad(const float* params, const float* param_flows, const int32_t* s_pids,
+                             const int32_t* s_pfids, const int32_t* ncats, const int32_t* source_nids,
+                             int32_t num_source_nodes, double scale, float* grad, void* stream);
+
+/*
+ * Categorical input layer with soft evidence E (FP32, element (b, v, k) at
+ * evidence[b * e_sb + v * e_sv + k * e_sk]):
+ *   node_mars[node_offset + n, b] = min(log sum_{k < ncats} E[b, vids[n], k] params[s_pids[n] + k], 0)
+ * (0 where `missing`, indexed as in pcb_input_cat_fwd, is set), over the variable-run
+ * table of pcb_input_cat_bwd (max_group_nodes = the largest grp_count).
+ * Replaces _soft_evi_categorical_fw_kernel and the clip that follows it
+ * (src/pyjuice/queries/conditional.py:25-68, 108-111).
+ */
+int pcb_input_cat_soft_fwd(const float* evidence, int64_t e_sb, int64_t e_sv, int64_t e_sk, const float* params,
+                           const int32_t* grp_var, const int32_t* grp_node0, const int32_t* grp_count,
+                           const int32_t* grp_ncats, int32_t num_groups, int32_t max_group_nodes,
+                           const int32_t* s_pids, int32_t node_offset, float* node_mars, int64_t ld, int32_t B,
+                           const uint8_t* missing, int64_t miss_sb, int64_t miss_sv, void* stream);
+
+/*
+ * Per-category evidence quantities from the node flows of an input layer, for target
+ * variable t (its nodes: tgt_nodes[tgt_ptr[t] .. tgt_ptr[t + 1]), layer-local ids):
+ *   out[(b * num_targets + t) * max_ncats + k] = sum_n W[n, b] params[s_pids[n] + k]
+ * mode 0: W = node flows (the conditional query's category weights before their
+ * normalisation over k; replaces _categorical_backward_kernel, conditional.py:241-336,
+ * which adds the same terms with float atomics);
+ * mode 1: W = node flows / exp(node_mars) (0 where node_mars = -inf): the derivative of the
+ * weighted log-likelihood with respect to the soft evidence E[b, v, k] of the
+ * soft-evidence forward (no reference counterpart).
+ * Deterministic (every output is one sum in node order); entries k >= a node's ncats
+ * receive no term.
+ */
+int pcb_input_cat_evidence_bwd(const float* node_flows, const float* node_mars, int64_t ld, int32_t B,
+                               const float* params, const int32_t* tgt_ptr, const int32_t* tgt_nodes,
+                               int32_t num_targets, const int32_t* s_pids, const int32_t* ncats, int32_t node_offset,
+                               int32_t max_ncats, int32_t mode, float* out, void* stream);
 
 /*
  * Sum-parameter normalisation (FP64), same block table as pcb_sum_em:

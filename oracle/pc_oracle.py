@@ -106,17 +106,49 @@ def _rows(start: np.ndarray, bs: int) -> np.ndarray:
     return (start[:, None] + np.arange(bs)[None, :]).reshape(-1)
 
 
-def forward(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarray):
-    """Returns (node_mars [N, B], element_mars per inner group index, lls [B])."""
-    x = np.asarray(x, dtype=np.int64)
-    B = x.shape[0]
+def _mask_rows(layout: dict, missing_mask, B: int) -> np.ndarray:
+    """[n_in, B] bool: input node n is summed out in sample b (mask [V] or [B, V])."""
+    vids = layout["input"]["vids"]
+    m = np.asarray(missing_mask, dtype=bool)
+    return np.broadcast_to(m[vids][:, None], (vids.shape[0], B)) if m.ndim == 1 else m[:, vids].T
+
+
+def input_values(layout: dict, in_params: np.ndarray, x: np.ndarray = None, evidence: np.ndarray = None,
+                 missing_mask=None) -> np.ndarray:
+    """[n_in, B] log values of the Categorical input nodes: hard evidence ``log theta[x]``
+    (categorical.py:83-91), soft evidence ``min(log sum_k E[b, v, k] theta[k], 0)``
+    (queries/conditional.py:25-68, 108-111); 0 where ``missing_mask`` marks the variable
+    (input_layer.py:1059-1095)."""
+    inp = layout["input"]
+    theta = in_params.astype(np.float64)
+    with np.errstate(divide="ignore"):
+        if evidence is None:
+            x = np.asarray(x, dtype=np.int64)
+            vals = np.log(theta)[inp["s_pids"][:, None] + x[:, inp["vids"]].T]
+        else:
+            ev = np.asarray(evidence, dtype=np.float64)                            # [B, V, K]
+            K = int(inp["ncats"].max())
+            th = theta[np.minimum(inp["s_pids"][:, None] + np.arange(K)[None, :], theta.shape[0] - 1)]
+            th = np.where(np.arange(K)[None, :] < inp["ncats"][:, None], th, 0.0)  # [n_in, K]
+            vals = np.minimum(np.log(np.einsum("nk,bnk->nb", th, ev[:, inp["vids"], :K])), 0.0)
+    if missing_mask is not None:
+        vals = np.where(_mask_rows(layout, missing_mask, vals.shape[1]), 0.0, vals)
+    return vals
+
+
+def forward(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarray = None, missing_mask=None,
+            evidence: np.ndarray = None):
+    """Returns (node_mars [N, B], element_mars per inner group index, lls [B]). Hard
+    evidence ``x`` [B, V] or soft evidence ``evidence`` [B, V, K]; variables marked in
+    ``missing_mask`` are summed out."""
+    vals = input_values(layout, in_params, x, evidence, missing_mask)
+    B = vals.shape[1]
     N = layout["num_nodes"]
     nm = np.zeros([N, B], dtype=np.float64)
     inp = layout["input"]
     n_in = inp["vids"].shape[0]
+    nm[inp["nid_start"]:inp["nid_start"] + n_in] = vals
     with np.errstate(divide="ignore"):
-        logp = np.log(in_params.astype(np.float64))
-        nm[inp["nid_start"]:inp["nid_start"] + n_in] = logp[inp["s_pids"][:, None] + x[:, inp["vids"]].T]
         logw = np.log(params.astype(np.float64))
     ems = {}
     em = None
@@ -153,10 +185,13 @@ def forward(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarr
 
 
 def backward(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, ems: dict,
-             ll_weights: np.ndarray = None):
-    """Returns (node_flows [N, B] (unmodified), param_flows, input param_flows) of one batch."""
-    x = np.asarray(x, dtype=np.int64)
-    B = x.shape[0]
+             ll_weights: np.ndarray = None, missing_mask=None, in_params: np.ndarray = None):
+    """Returns (node_flows [N, B] (unmodified), param_flows, input param_flows) of one batch.
+    Where ``missing_mask`` marks a variable, an input node's flow goes to every category k
+    as ``flow * theta[k]`` (categorical.py:102-134; needs ``in_params``). ``x`` None: no
+    input flows from observed values (soft evidence)."""
+    x = None if x is None else np.asarray(x, dtype=np.int64)
+    B = nm.shape[1]
     N = layout["num_nodes"]
     nf = np.zeros([N, B], dtype=np.float64)
     r0, r1 = layout["root_range"]
@@ -223,9 +258,40 @@ def backward(layout: dict, params: np.ndarray, x: np.ndarray, nm: np.ndarray, em
     npf = inp["num_param_flows"] if inp.get("num_param_flows") else int(inp["s_pfids"].max() + inp["ncats"].max())
     in_pf = np.zeros([npf], dtype=np.float64)
     rows = inp["nid_start"] + np.arange(n_in)
-    slots = inp["s_pfids"][:, None] + x[:, inp["vids"]].T
-    np.add.at(in_pf, slots.reshape(-1), nf[rows].reshape(-1))
+    flows = nf[rows]
+    if missing_mask is not None:
+        miss = _mask_rows(layout, missing_mask, B)
+        theta = in_params.astype(np.float64)
+        msum = np.where(miss, flows, 0.0).sum(axis=1)
+        for k in range(int(inp["ncats"].max())):
+            ok = k < inp["ncats"]
+            np.add.at(in_pf, inp["s_pfids"][ok] + k, msum[ok] * theta[inp["s_pids"][ok] + k])
+        flows = np.where(miss, 0.0, flows)
+    if x is not None:
+        slots = inp["s_pfids"][:, None] + x[:, inp["vids"]].T
+        np.add.at(in_pf, slots.reshape(-1), flows.reshape(-1))
     return nf, pf, in_pf
+
+
+def conditional(layout: dict, in_params: np.ndarray, nf: np.ndarray, target_vars=None, scale=None) -> np.ndarray:
+    """The conditional query's category distributions ``[B, T, K]``: per target variable,
+    ``sum_n nf[n, b] theta[n, k]`` over its input nodes, normalised over k with + 1e-12
+    (queries/conditional.py:241-336). ``scale`` ([n_in, B], optional) multiplies the flows
+    first and skips the normalisation (the soft-evidence adjoint uses 1 / exp(node_mars))."""
+    inp = layout["input"]
+    n_in = inp["vids"].shape[0]
+    K = int(inp["ncats"].max())
+    f = nf[inp["nid_start"]:inp["nid_start"] + n_in]
+    if scale is not None:
+        f = f * scale
+    theta = in_params.astype(np.float64)
+    th = theta[np.minimum(inp["s_pids"][:, None] + np.arange(K)[None, :], theta.shape[0] - 1)]
+    th = np.where(np.arange(K)[None, :] < inp["ncats"][:, None], th, 0.0)
+    tv = range(int(inp["vids"].max()) + 1) if target_vars is None else target_vars
+    out = np.stack([np.einsum("nb,nk->bk", f[inp["vids"] == v], th[inp["vids"] == v]) for v in tv], axis=1)
+    if scale is None:
+        out = out / (out.sum(axis=2, keepdims=True) + 1e-12)
+    return out
 
 
 def forward_alg(layout: dict, params: np.ndarray, in_params: np.ndarray, x: np.ndarray, alg: str = "LL",

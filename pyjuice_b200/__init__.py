@@ -2,14 +2,15 @@
 
 Same public API as the reference package for the circuit passes:
 ``compile`` / ``TensorCircuit``, ``inputs`` / ``multiply`` / ``summate`` /
-``set_block_size``, ``distributions.Categorical``, ``structures.HCLT`` and
-``queries.sample``.
+``set_block_size``, ``distributions.Categorical``, ``structures.HCLT``,
+``queries.sample`` / ``marginal`` / ``conditional``, and ``autograd.circuit_ll`` (a
+differentiable soft-evidence log-likelihood).
 """
 
-from . import nodes, layer, model, structures, queries
+from . import nodes, layer, model, structures, queries, autograd
 from .nodes import inputs, multiply, summate, set_block_size, distributions
 from .model import TensorCircuit, compile
 from .layer import InputLayer, ProdLayer, SumLayer
 
 __all__ = ["compile", "TensorCircuit", "inputs", "multiply", "summate", "set_block_size", "distributions",
-           "structures", "queries", "InputLayer", "ProdLayer", "SumLayer"]
+           "structures", "queries", "autograd", "InputLayer", "ProdLayer", "SumLayer"]

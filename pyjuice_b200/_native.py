@@ -20,7 +20,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpcb200.so")
 CSRC = os.path.join(_HERE, "csrc")
 SOURCES = ["capi_common.cu", "lse_contract.cu", "lse_contract_tc.cu", "lse_short.cu", "lse_tc05.cu", "prod_kernels.cu", "sum_pflows.cu",
-           "sum_generic.cu", "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu"]
+           "sum_generic.cu", "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu",
+           "input_soft.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-shared",
               "-Xcompiler", "-fPIC"]
 
@@ -91,9 +92,10 @@ _SIGS = {
     "pcb_status_selftest": ([c_int32, c_void_p], c_int32),
     "pcb_fill_rows": ([c_void_p, c_int64, c_int64, c_int64, c_float, c_void_p], c_int32),
     "pcb_input_cat_fwd": ([c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
-                           c_int64, c_int32, c_void_p], c_int32),
+                           c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
     "pcb_input_cat_bwd": ([c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
-                           c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_void_p], c_int32),
+                           c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int64,
+                           c_void_p, c_void_p, c_void_p], c_int32),
     "pcb_input_cat_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double,
                           c_int32, c_void_p], c_int32),
     "pcb_pflow_accum": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),
@@ -128,6 +130,16 @@ _SIGS = {
                                    c_double, c_int32, c_void_p], c_int32),
     "pcb_flows_accumulate_f64": ([c_void_p, c_void_p, c_int64, c_void_p], c_int32),
     "pcb_pflow_accum_f64": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),
+    "pcb_sum_logit_grad": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_void_p,
+                            c_void_p], c_int32),
+    "pcb_sum_softmax": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p], c_int32),
+    "pcb_input_cat_logit_grad": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
+                                  c_void_p, c_void_p], c_int32),
+    "pcb_input_cat_soft_fwd": ([c_void_p, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32, c_void_p, c_int64,
+                                c_int64, c_void_p], c_int32),
+    "pcb_input_cat_evidence_bwd": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
+                                    c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_sum_normalize": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_void_p], c_int32),
     "pcb_ll_sum_f64": ([c_void_p, c_int64, c_int32, c_int64, c_void_p, c_void_p], c_int32),
     "pcb_sample_sum": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,

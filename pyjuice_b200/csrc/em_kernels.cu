@@ -225,7 +225,102 @@ __global__ void pflow_accum_f64_kernel(double* __restrict__ pf, int64_t dst, int
     pf[dst + i] = s;
 }
 
+// Gradient of the scaled log-likelihood with respect to softmax logits of the weights:
+// per node i of a block, grad[k, i] = scale * (pf[k, i] - theta[k, i] * sum_k' pf[k', i]),
+// where pf are the parameter flows (theta times the derivative with respect to theta).
+__global__ void __launch_bounds__(256)
+sum_logit_grad_kernel(const float* __restrict__ params, const float* __restrict__ pflows,
+                      const int64_t* __restrict__ pbase, const int64_t* __restrict__ pfbase,
+                      const int* __restrict__ nchs, const int* __restrict__ bss, double scale,
+                      float* __restrict__ grad) {
+    pcb::pdl_begin();
+    const int g = blockIdx.x;
+    const int64_t pb = pbase[g], fb = pfbase[g];
+    const int nch = nchs[g], bs = bss[g];
+    for (int i = threadIdx.x; i < bs; i += blockDim.x) {
+        double tot = 0.0;
+        for (int k = 0; k < nch; ++k) tot += (double)pflows[fb + (int64_t)k * bs + i];
+        for (int k = 0; k < nch; ++k) {
+            const int64_t o = (int64_t)k * bs + i;
+            grad[pb + o] = (float)(scale * ((double)pflows[fb + o] - (double)params[pb + o] * tot));
+        }
+    }
+}
+
+// Weights from softmax logits: per node i of a block, theta[k, i] = exp(z[k, i] - m) / sum_k' exp(z[k', i] - m),
+// m = max_k z[k, i] (FP64 sum).
+__global__ void __launch_bounds__(128)
+sum_softmax_kernel(const float* __restrict__ logits, float* __restrict__ params, const int64_t* __restrict__ pbase,
+                   const int* __restrict__ nchs, const int* __restrict__ bss) {
+    pcb::pdl_begin();
+    const int g = blockIdx.x;
+    const int64_t pb = pbase[g];
+    const int nch = nchs[g], bs = bss[g];
+    for (int i = threadIdx.x; i < bs; i += blockDim.x) {
+        float m = -INFINITY;
+        for (int k = 0; k < nch; ++k) m = fmaxf(m, logits[pb + (int64_t)k * bs + i]);
+        double tot = 0.0;
+        for (int k = 0; k < nch; ++k) tot += exp((double)logits[pb + (int64_t)k * bs + i] - (double)m);
+        const double inv = 1.0 / tot;
+        for (int k = 0; k < nch; ++k) {
+            const int64_t o = pb + (int64_t)k * bs + i;
+            params[o] = (float)(exp((double)logits[o] - (double)m) * inv);
+        }
+    }
+}
+
+// The same for Categorical input nodes: one warp per source node.
+__global__ void __launch_bounds__(256)
+input_logit_grad_kernel(const float* __restrict__ params, const float* __restrict__ pflows,
+                        const int* __restrict__ s_pids, const int* __restrict__ s_pfids, const int* __restrict__ ncats,
+                        const int* __restrict__ source_nids, int num_src, double scale, float* __restrict__ grad) {
+    pcb::pdl_begin();
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= num_src) return;
+    const int n = source_nids[w];
+    const int K = ncats[n];
+    const int64_t sp = s_pids[n], sf = s_pfids[n];
+    double tot = 0.0;
+    for (int k = lane; k < K; k += 32) tot += (double)pflows[sf + k];
+    tot = pcb::warp_sum(tot);
+    for (int k = lane; k < K; k += 32)
+        grad[sp + k] = (float)(scale * ((double)pflows[sf + k] - (double)params[sp + k] * tot));
+}
+
 }  // namespace
+
+extern "C" int pcb_sum_logit_grad(const float* params, const float* param_flows, const int64_t* blk_pbase,
+                                  const int64_t* blk_pfbase, const int32_t* blk_nch, const int32_t* blk_bs,
+                                  int32_t num_blocks, double scale, float* grad, void* stream) {
+    if (!params || !param_flows || !blk_pbase || !blk_pfbase || !blk_nch || !blk_bs || !grad || num_blocks < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_sum_logit_grad: bad arguments");
+    if (num_blocks == 0) return PCB_OK;
+    return pcb::launch_status(pcb::launch_k(sum_logit_grad_kernel, dim3(num_blocks), dim3(128), 0,
+                                            pcb::as_stream(stream), 1u, params, param_flows, blk_pbase, blk_pfbase,
+                                            blk_nch, blk_bs, scale, grad), "pcb_sum_logit_grad");
+}
+
+extern "C" int pcb_sum_softmax(const float* logits, float* params, const int64_t* blk_pbase, const int32_t* blk_nch,
+                               const int32_t* blk_bs, int32_t num_blocks, void* stream) {
+    if (!logits || !params || !blk_pbase || !blk_nch || !blk_bs || num_blocks < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_sum_softmax: bad arguments");
+    if (num_blocks == 0) return PCB_OK;
+    return pcb::launch_status(pcb::launch_k(sum_softmax_kernel, dim3(num_blocks), dim3(128), 0, pcb::as_stream(stream),
+                                            1u, logits, params, blk_pbase, blk_nch, blk_bs), "pcb_sum_softmax");
+}
+
+extern "C" int pcb_input_cat_logit_grad(const float* params, const float* param_flows, const int32_t* s_pids,
+                                        const int32_t* s_pfids, const int32_t* ncats, const int32_t* source_nids,
+                                        int32_t num_source_nodes, double scale, float* grad, void* stream) {
+    if (!params || !param_flows || !s_pids || !s_pfids || !ncats || !source_nids || !grad || num_source_nodes < 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_input_cat_logit_grad: bad arguments");
+    if (num_source_nodes == 0) return PCB_OK;
+    return pcb::launch_status(pcb::launch_k(input_logit_grad_kernel,
+                                            dim3((unsigned)pcb::cdiv((int64_t)num_source_nodes * 32, 256)), dim3(256),
+                                            0, pcb::as_stream(stream), 1u, params, param_flows, s_pids, s_pfids, ncats,
+                                            source_nids, num_source_nodes, scale, grad), "pcb_input_cat_logit_grad");
+}
 
 extern "C" int pcb_sum_em(float* params, const float* param_flows, const int64_t* blk_pbase, const int64_t* blk_pfbase,
                           const int32_t* blk_nch, const int32_t* blk_bs, int32_t num_blocks, double step_size,

@@ -3,8 +3,10 @@
 
 namespace {
 
-// node_mars[node_offset + n, b] = log(params[s_pids[n] + x]) with x = data[vids[n], b].
-// A category outside [0, ncats) yields NaN (no out-of-range read).
+// node_mars[node_offset + n, b] = log(params[s_pids[n] + x]) with x = data[vids[n], b], or
+// 0 (log 1: the variable is summed out) where the missing mask is set,
+// miss[b * m_sb + vids[n] * m_sv] != 0. A category outside [0, ncats) yields NaN (no
+// out-of-range read).
 // A CTA covers kFwdNodes consecutive nodes over 512 samples (4 per thread): the logs of
 // the nodes' parameter slabs (up to kFwdSlab categories) are taken once into shared
 // memory, each thread loads its 4 category values once and reuses them for every node of
@@ -19,7 +21,7 @@ __global__ void __launch_bounds__(kFwdThreads)
 input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ params,
                      const int* __restrict__ vids, const int* __restrict__ s_pids, const int* __restrict__ ncats,
                      int num_nodes, int node_offset, float* __restrict__ nm, int64_t ld, int B, bool vec,
-                     int32_t* __restrict__ status) {
+                     const uint8_t* __restrict__ miss, int64_t m_sb, int64_t m_sv, int32_t* __restrict__ status) {
     // The node tables and the parameter logs are read before the wait for the previous kernel
     // (the parameters' writers do not trigger early); the samples and outputs after it.
     pcb::pdl_trigger();
@@ -52,7 +54,9 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             float r = 0.f;
-            if (b + q < B) {
+            if (b + q < B && miss && miss[(int64_t)(b + q) * m_sb + (int64_t)v * m_sv]) {
+                r = 0.f;
+            } else if (b + q < B) {
                 const int64_t x = (v == v0) ? x0[q] : __ldg(data + (int64_t)v * data_ld + b + q);
                 if (x >= 0 && x < K) r = (K <= kFwdSlab) ? slab[j][x] : __logf(__ldcg(params + sP[j] + x));
                 else {
@@ -70,12 +74,16 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 // up to CB samples; warp-parallel prefix sum of the category counts), then one warp per
 // node copies the node's flow row into shared memory with coalesced loads and sums it per
 // category in sample order, adding the sums to the node's flow slots. Deterministic: no
-// float atomics.
+// float atomics. Samples whose variable is missing (miss[b * m_sb + v * m_sv] != 0) form
+// their own segment: their flow sum M is spread over the categories as M * params[k]
+// (input_layer.py:537-571, categorical.py:102-134).
 __global__ void __launch_bounds__(256)
 input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const float* __restrict__ nf, int64_t ld,
                      int B, const int* __restrict__ grp_var, const int* __restrict__ grp_node0,
                      const int* __restrict__ grp_count, const int* __restrict__ grp_ncats,
-                     const int* __restrict__ s_pfids, int node_offset, float* __restrict__ pf, bool logspace, int CB) {
+                     const int* __restrict__ s_pfids, int node_offset, float* __restrict__ pf, bool logspace, int CB,
+                     const uint8_t* __restrict__ miss, int64_t m_sb, int64_t m_sv, const int* __restrict__ s_pids,
+                     const float* __restrict__ params) {
     pcb::pdl_begin();
     extern __shared__ int smem[];
     const int g = blockIdx.x;
@@ -86,34 +94,39 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
     int* keys = smem;              // [CB]
     int* perm = keys + CB;         // [CB]
     float* rows = reinterpret_cast<float*>(perm + CB);  // [warps][CB]
-    int* seg = perm + CB + (blockDim.x >> 5) * CB;      // [K + 2]
+    int* seg = perm + CB + (blockDim.x >> 5) * CB;      // [K + 3]: categories, dropped, missing
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
 
     for (int c0 = 0; c0 < B; c0 += CB) {
         const int nb = min(CB, B - c0);
-        for (int i = tid; i < K + 2; i += blockDim.x) seg[i] = 0;
+        for (int i = tid; i < K + 3; i += blockDim.x) seg[i] = 0;
         __syncthreads();
         for (int i = tid; i < nb; i += blockDim.x) {
-            const int64_t x = data[v * data_ld + c0 + i];
-            const int key = (x >= 0 && x < K) ? (int)x : K;  // out-of-range samples are dropped
+            int key;
+            if (miss && miss[(int64_t)(c0 + i) * m_sb + v * m_sv]) {
+                key = K + 1;  // missing: spread over the categories below
+            } else {
+                const int64_t x = data[v * data_ld + c0 + i];
+                key = (x >= 0 && x < K) ? (int)x : K;  // out-of-range samples are dropped
+            }
             keys[i] = key;
             atomicAdd(&seg[key + 1], 1);
         }
         __syncthreads();
         if (warp == 0) {
             int carry = 0;
-            for (int base = 0; base < K + 2; base += 32) {
+            for (int base = 0; base < K + 3; base += 32) {
                 const int i = base + lane;
-                int v = (i < K + 2) ? seg[i] : 0;
+                int v = (i < K + 3) ? seg[i] : 0;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     const int t = __shfl_up_sync(0xffffffffu, v, o);
                     if (lane >= o) v += t;
                 }
                 v += carry;
-                if (i < K + 2) seg[i] = v;
+                if (i < K + 3) seg[i] = v;
                 carry = __shfl_sync(0xffffffffu, v, 31);
             }
         }
@@ -152,6 +165,17 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                 for (int i = lane; i < nb; i += 32) wrow[i] = __ldg(frow + i);
             }
             __syncwarp();
+            // flow of the samples with this variable missing (segment K + 1)
+            float msum = 0.f;
+            if (miss) {
+                for (int p = seg[K] + lane; p < seg[K + 1]; p += 32) {
+                    const float f = wrow[perm[p]];
+                    msum += logspace ? __expf(f) : f;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
+            }
+            const int64_t sp = miss ? s_pids[node0 + n] : 0;
             // categories lane, lane + 32, ...: the slots' old values are loaded for a batch of
             // kR categories at once (one round trip), then summed and stored
             constexpr int kR = 8;
@@ -168,8 +192,8 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                     if (k >= K) continue;
                     const int s = (k == 0) ? 0 : seg[k - 1];
                     const int e = seg[k];
-                    if (e == s) continue;
-                    float acc = 0.f;
+                    if (e == s && msum == 0.f) continue;
+                    float acc = (msum != 0.f) ? msum * params[sp + k] : 0.f;
                     for (int p = s; p < e; ++p) {
                         const float f = wrow[perm[p]];
                         acc += logspace ? __expf(f) : f;
@@ -187,7 +211,8 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 
 extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params, const int32_t* vids,
                                  const int32_t* s_pids, const int32_t* ncats, int32_t num_nodes, int32_t node_offset,
-                                 float* node_mars, int64_t ld, int32_t B, void* stream) {
+                                 float* node_mars, int64_t ld, int32_t B, const uint8_t* missing, int64_t miss_sb,
+                                 int64_t miss_sv, void* stream) {
     if (!data || !params || !vids || !s_pids || !ncats || !node_mars || B <= 0 || ld < B || data_ld < B || num_nodes < 0)
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_fwd: bad arguments");
     if (num_nodes == 0) return PCB_OK;
@@ -197,8 +222,8 @@ extern "C" int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const flo
     return pcb::launch_status(pcb::launch_k(input_cat_fwd_kernel, dim3((unsigned)pcb::cdiv(num_nodes, kFwdNodes),
                                                                        (unsigned)gy),
                                             dim3(kFwdThreads), 0, pcb::as_stream(stream), 1u, data, data_ld, params, vids,
-                                            s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec,
-                                            pcb::status_word()),
+                                            s_pids, ncats, num_nodes, node_offset, node_mars, ld, B, vec, missing,
+                                            miss_sb, miss_sv, pcb::status_word()),
                               "pcb_input_cat_fwd");
 }
 
@@ -206,13 +231,14 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
                                  const int32_t* grp_var, const int32_t* grp_node0, const int32_t* grp_count,
                                  const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
                                  const int32_t* s_pfids, int32_t node_offset, float* param_flows,
-                                 int32_t logspace_flows, void* stream) {
+                                 int32_t logspace_flows, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
+                                 const int32_t* s_pids, const float* params, void* stream) {
     if (!data || !node_flows || !grp_var || !grp_node0 || !grp_count || !grp_ncats || !s_pfids || !param_flows ||
-        B <= 0 || ld < B || data_ld < B || num_groups < 0 || max_ncats <= 0)
+        B <= 0 || ld < B || data_ld < B || num_groups < 0 || max_ncats <= 0 || (missing && (!s_pids || !params)))
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: bad arguments");
     if (num_groups == 0) return PCB_OK;
     const int CB = B < 1024 ? B : 1024;
-    const size_t smem = (size_t)(2 * CB + 8 * CB + max_ncats + 2) * sizeof(int);
+    const size_t smem = (size_t)(2 * CB + 8 * CB + max_ncats + 3) * sizeof(int);
     if (smem > 200 * 1024) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: too many categories (%d)", max_ncats);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(input_cat_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -221,5 +247,6 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
     return pcb::launch_status(pcb::launch_k(input_cat_bwd_kernel, dim3(num_groups), dim3(256), smem,
                                             pcb::as_stream(stream), 1u, data, data_ld, node_flows, ld, B, grp_var,
                                             grp_node0, grp_count, grp_ncats, s_pfids, node_offset, param_flows,
-                                            logspace_flows != 0, CB), "pcb_input_cat_bwd");
+                                            logspace_flows != 0, CB, missing, miss_sb, miss_sv, s_pids, params),
+                              "pcb_input_cat_bwd");
 }

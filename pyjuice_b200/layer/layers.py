@@ -754,10 +754,17 @@ class InputLayer(Layer, torch.nn.Module):
         tied = []
         for dst, n, ch in self.tied2source_nids:
             tied.append((int(dst), int(n), ch.clone().long()))
+        # nodes of every variable (CSR over the variable ids 0 .. max vid), for the evidence
+        # backward contractions
+        order = np.argsort(vids, kind="stable")
+        var_ptr = np.zeros(int(vids.max()) + 2, np.int64)
+        np.add.at(var_ptr, vids + 1, 1)
+        var_ptr = np.cumsum(var_ptr)
         return dict(vids=_i32(vids), s_pids=_i32(self.s_pids.cpu()), s_pfids=_i32(self.s_pfids.cpu()),
                     ncats=_i32(ncats), source_nids=_i32(self.source_nids.cpu()),
                     grp_var=_i32(vids[starts]), grp_node0=_i32(starts), grp_count=_i32(counts),
-                    grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), tied=tied)
+                    grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), max_grp=int(counts.max()),
+                    tied=tied, var_ptr=var_ptr, var_nodes=order.astype(np.int64))
 
     def _init_parameters(self, perturbation: float = 2.0):
         p0 = 0
@@ -778,25 +785,86 @@ class InputLayer(Layer, torch.nn.Module):
         elif flows_memory < 1.0:
             self.param_flows.mul_(flows_memory)
 
-    def forward(self, data: torch.Tensor, node_mars: torch.Tensor, params=None, missing_mask=None, **kwargs):
-        """``data`` is ``[num_vars, B]`` (int64), as passed by ``TensorCircuit.forward``."""
-        if params is not None or missing_mask is not None:
-            raise NotImplementedError("external input parameters / missing masks have no CUDA path")
+    def _mask_args(self, missing_mask, B: int, device, batch_first: bool = True):
+        """(uint8 tensor or None, sample stride, variable stride) of a missing mask: ``[num_vars]``,
+        ``[B, num_vars]`` or, with ``batch_first=False`` and ambiguous sizes, ``[num_vars, B]``
+        (input_layer.py:378-385, 439-451)."""
+        if missing_mask is None:
+            return None, 0, 0
+        m = missing_mask.to(device=device, dtype=torch.bool)
+        if m.dim() == 1:
+            return m.view(torch.uint8), 0, m.stride(0)
+        if m.dim() != 2:
+            raise ValueError("`missing_mask` must be [num_vars], [B, num_vars] or [num_vars, B]")
+        if batch_first or m.size(1) == self.pc_num_vars:
+            return m.view(torch.uint8), m.stride(0), m.stride(1)
+        return m.view(torch.uint8), m.stride(1), m.stride(0)
+
+    def forward(self, data: torch.Tensor, node_mars: torch.Tensor, params=None, missing_mask=None,
+                _batch_first: bool = True, **kwargs):
+        """``data`` is ``[num_vars, B]`` (int64), as passed by ``TensorCircuit.forward``;
+        variables set in ``missing_mask`` are summed out (their nodes' values are log 1)."""
+        if params is not None:
+            raise NotImplementedError("external input parameters have no CUDA path")
         d = self._desc(node_mars.device)
         data = data.to(torch.long)
         if data.stride(1) != 1:
             data = data.contiguous()
         B = node_mars.size(1)
+        m, sb, sv = self._mask_args(missing_mask, B, node_mars.device, _batch_first)
         nat.call("pcb_input_cat_fwd", nat.ptr(data), data.stride(0), nat.ptr(self.params), nat.ptr(d["vids"]),
                  nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), self.num_nodes, self._output_ind_range[0],
-                 nat.ptr(node_mars), node_mars.stride(0), B, nat.stream())
+                 nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+
+    def forward_soft(self, evidence: torch.Tensor, node_mars: torch.Tensor, missing_mask=None,
+                     _batch_first: bool = True, **kwargs):
+        """Soft evidence ``[B, num_vars, num_cats]`` (FP32, entries in [0, 1]):
+        ``node_mars = min(log sum_k E[b, v, k] theta[n, k], 0)`` (conditional.py:25-68, 108-111)."""
+        if evidence.dim() != 3 or evidence.dtype != torch.float32:
+            raise ValueError("soft evidence must be a float32 [B, num_vars, num_cats] tensor")
+        d = self._desc(node_mars.device)
+        ev = evidence.to(node_mars.device)
+        B = node_mars.size(1)
+        if ev.size(0) != B or ev.size(2) < d["max_ncats"]:
+            raise ValueError("soft evidence must be [B, num_vars, >= num_cats]")
+        m, sb, sv = self._mask_args(missing_mask, B, node_mars.device, _batch_first)
+        nat.call("pcb_input_cat_soft_fwd", nat.ptr(ev), ev.stride(0), ev.stride(1), ev.stride(2), nat.ptr(self.params),
+                 nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
+                 d["grp_var"].size(0), d["max_grp"], nat.ptr(d["s_pids"]), self._output_ind_range[0],
+                 nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+
+    def evidence_backward(self, node_flows: torch.Tensor, node_mars: Optional[torch.Tensor] = None,
+                          target_vars=None, mode: int = 0) -> torch.Tensor:
+        """``[B, T, max_ncats]``: per target variable and category, ``sum_n W[n, b] theta[n, k]``
+        over the variable's nodes, W = node flows (mode 0) or node flows / exp(node_mars)
+        (mode 1, the derivative of the weighted log-likelihood with respect to soft evidence)."""
+        d = self._desc(node_flows.device)
+        B = node_flows.size(1)
+        nv = d["var_ptr"].shape[0] - 1
+        tv = list(range(nv)) if target_vars is None else [int(v) for v in target_vars]
+        key = ("tgt", tuple(tv) if target_vars is not None else None)
+        tab = d.get(key)
+        if tab is None:
+            ptr, nodes = [0], []
+            for v in tv:
+                a, b = (int(d["var_ptr"][v]), int(d["var_ptr"][v + 1])) if 0 <= v < nv else (0, 0)
+                nodes.append(d["var_nodes"][a:b])
+                ptr.append(ptr[-1] + b - a)
+            tab = (_i32(ptr).to(node_flows.device),
+                   _i32(np.concatenate(nodes) if nodes else np.zeros([0], np.int64)).to(node_flows.device))
+            d[key] = tab
+        out = torch.empty([B, len(tv), d["max_ncats"]], dtype=torch.float32, device=node_flows.device)
+        nat.call("pcb_input_cat_evidence_bwd", nat.ptr(node_flows), nat.ptr(node_mars), node_flows.stride(0), B,
+                 nat.ptr(self.params), nat.ptr(tab[0]), nat.ptr(tab[1]), len(tv), nat.ptr(d["s_pids"]),
+                 nat.ptr(d["ncats"]), self._output_ind_range[0], d["max_ncats"], mode, nat.ptr(out), nat.stream())
+        return out
 
     __call__ = forward
 
     def backward(self, data: torch.Tensor, node_flows: torch.Tensor, node_mars: torch.Tensor, params=None,
-                 logspace_flows: bool = False, missing_mask=None, **kwargs):
-        if params is not None or missing_mask is not None:
-            raise NotImplementedError("external input parameters / missing masks have no CUDA path")
+                 logspace_flows: bool = False, missing_mask=None, _batch_first: bool = True, **kwargs):
+        if params is not None:
+            raise NotImplementedError("external input parameters have no CUDA path")
         d = self._desc(node_flows.device)
         if self.param_flows is None:
             self.init_param_flows(0.0)
@@ -804,10 +872,12 @@ class InputLayer(Layer, torch.nn.Module):
         if data.stride(1) != 1:
             data = data.contiguous()
         B = node_flows.size(1)
+        m, sb, sv = self._mask_args(missing_mask, B, node_flows.device, _batch_first)
         nat.call("pcb_input_cat_bwd", nat.ptr(data), data.stride(0), nat.ptr(node_flows), node_flows.stride(0), B,
                  nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
                  d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
-                 nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.stream())
+                 nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.ptr(m), sb, sv, nat.ptr(d["s_pids"]),
+                 nat.ptr(self.params), nat.stream())
 
     def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
                       use_f64_flows: bool = False):

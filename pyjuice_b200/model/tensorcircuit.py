@@ -686,7 +686,8 @@ class TensorCircuit(nn.Module):
                     el_ready.record(sides[0])
         kwargs = dict(kwargs, _weights_packed=True)
         plain = (propagation_alg == "LL" if isinstance(propagation_alg, str) else
-                 all(a == "LL" for a in propagation_alg)) and not negate_pflows and not logspace_flows
+                 all(a == "LL" for a in propagation_alg)) and not negate_pflows and not logspace_flows and \
+            not kwargs.get("allow_neg_flows")
         turn = 0
         def rewrites(g):  # large layers rewrite their node flows as log f - log m
             return allow_modify_flows and any(
@@ -753,7 +754,7 @@ class TensorCircuit(nn.Module):
             raise ValueError("`allow_modify_flows` should be set to `False` when using `logspace_flows`.")
         if not isinstance(propagation_alg, str):
             propagation_alg = tuple(propagation_alg)
-        if propagation_alg != "LL" or negate_pflows:
+        if propagation_alg != "LL" or negate_pflows or kwargs.get("allow_neg_flows"):
             # the kernels of these modes read unmodified node flows (the results are the same)
             allow_modify_flows = False
         if sum_layer_pre_backward_callback is not None or sum_layer_post_backward_callback is not None:
@@ -898,6 +899,34 @@ class TensorCircuit(nn.Module):
                      self.num_param_flows, nat.stream())
             for layer in self.input_layer_group:
                 layer.accumulate_param_flows_f64()
+
+    def set_params_from_logits(self, logits: torch.Tensor):
+        """Sum weights = softmax of ``logits`` over each node's children (``logits`` in the
+        layout of ``params``; entries outside the nodes' weights are ignored)."""
+        if logits.shape != self.params.shape or logits.dtype != torch.float32 or logits.device != self.device:
+            raise ValueError("logits must be a float32 tensor shaped like `params` on the circuit's device")
+        t = self._tables()
+        with torch.no_grad():
+            nat.call("pcb_sum_softmax", nat.ptr(logits.contiguous()), nat.ptr(self.params), nat.ptr(t["pbase"]),
+                     nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0), nat.stream())
+        self._param_epoch += 1
+
+    def sum_logit_grad(self, scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Gradient with respect to softmax logits of the sum weights from the current parameter
+        flows: ``scale * (pf - theta * sum_children pf)`` in the layout of ``params`` (tied flow
+        slots are summed into their source slots first)."""
+        if self.param_flows is None:
+            raise RuntimeError("run a backward pass first")
+        t = self._tables()
+        out = torch.zeros_like(self.params) if out is None else out
+        with torch.no_grad():
+            for dst, n, srcs in t["fusing"]:
+                nat.call("pcb_pflow_accum", nat.ptr(self.param_flows), dst, n, nat.ptr(srcs), srcs.size(0),
+                         nat.stream())
+            nat.call("pcb_sum_logit_grad", nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(t["pbase"]),
+                     nat.ptr(t["pfbase"]), nat.ptr(t["nch"]), nat.ptr(t["bs"]), t["nch"].size(0), float(scale),
+                     nat.ptr(out), nat.stream())
+        return out
 
     def normalize_parameters(self, pseudocount: float = 0.0):
         """Renormalise the sum parameters in place on the device (FP64)."""

@@ -21,6 +21,9 @@ the results of one forward / backward / ``mini_batch_em`` step:
                     parameter vector with pseudocount 0.3;
 * ``alg_tiny.npz``   the tiny circuit under MPE, GeneralLL(0.5), log-space flows and negated
                     parameter flows: log-likelihoods, node values, node flows, parameter flows;
+* ``query_tiny.npz`` the tiny circuit's queries: marginals and the hard-evidence conditional
+                    with a per-sample missing mask, the soft-evidence conditional, and
+                    input-layer flows with a per-variable missing mask;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -268,6 +271,42 @@ def make_alg_variants():
     np.savez_compressed(os.path.join(HERE, "alg_tiny.npz"), **out)
 
 
+def make_query_variants():
+    """Queries on the tiny circuit: marginals with a per-sample missing mask, the conditional
+    query with hard evidence (missing mask, target variables) and with soft evidence (rows of
+    a seeded Dirichlet(1)), and the input-layer parameter flows of a backward pass with a
+    per-variable missing mask."""
+    fx = dict(np.load(os.path.join(HERE, "tiny.npz")))
+    torch.manual_seed(1)
+    pc = juice.compile(build_tiny_dag(juice, dists), max_tied_ns_per_parflow_block=1, verbose=False)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+    x = torch.from_numpy(fx["x"])
+    rng = np.random.default_rng(9)
+    B, V = x.shape
+    mask = rng.random((B, V)) < 0.3
+    out = dict(mask=mask)
+    out["marginal_lls"] = juice.queries.marginal(pc, data=x, missing_mask=torch.from_numpy(mask)).detach().numpy().copy()
+    out["cond_hard"] = juice.queries.conditional(pc, data=x, missing_mask=torch.from_numpy(mask),
+                                                 target_vars=[0, 2, 5]).detach().numpy().copy()
+    out["cond_hard_full"] = juice.queries.conditional(pc, data=x, missing_mask=torch.from_numpy(mask)).detach().numpy().copy()
+    soft = rng.dirichlet(np.ones(4), size=(B, V)).astype(np.float32)
+    out["soft"] = soft
+    out["cond_soft"] = juice.queries.conditional(pc, data=torch.from_numpy(soft.copy())).detach().numpy().copy()
+    out["soft_lls"] = pc.node_mars[pc._root_node_range[0]:pc._root_node_range[1]].detach().numpy().T.copy()
+    vmask = np.zeros(V, dtype=bool)
+    vmask[[1, 4]] = True
+    out["vmask"] = vmask
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, missing_mask=torch.from_numpy(vmask), force_use_fp32=True)
+    out["vmask_lls"] = lls.detach().numpy().copy()
+    lls.mean().backward()
+    out["vmask_param_flows"] = pc.param_flows.detach().numpy().copy()
+    out["vmask_in_param_flows"] = pc.input_layer_group[0].param_flows.detach().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "query_tiny.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -307,10 +346,10 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
-         "em_tiny": make_em_variants, "alg_tiny": make_alg_variants}[w]()
+         "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

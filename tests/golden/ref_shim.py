@@ -48,12 +48,14 @@ def load_reference():
 
     torch.cuda.device = _nodev
 
-    # libdevice calls have no interpreter implementation: log1p(x) becomes log(1 + x)
+    # libdevice calls have no interpreter implementation: log1p(x) becomes log(1 + x), ceil
+    # the language's ceil
     # (the log-space flow kernels use it; the difference is within FP32 rounding)
     import triton.language as tl
     libdev = getattr(tl.extra.cuda, "libdevice", None)
     if libdev is not None:
         libdev.log1p = lambda x, *a, **k: tl.log(x + 1.0)
+        libdev.ceil = lambda x, *a, **k: tl.ceil(x)
 
     import pyjuice as juice
     from pyjuice.layer import input_layer as il

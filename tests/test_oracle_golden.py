@@ -114,3 +114,27 @@ def test_oracle_propagation_algorithms_match_reference(case):
     fin = np.isfinite(rnf)
     assert np.array_equal(fin, np.isfinite(nf))
     assert np.abs(nf[fin] - rnf[fin]).max() <= 1e-5
+
+
+def test_oracle_queries_match_reference():
+    """Marginals with a per-sample missing mask, the conditional query with hard evidence
+    (missing mask) and with soft evidence, and input flows with a per-variable missing mask,
+    against the reference's own outputs (fixture query_tiny.npz)."""
+    fx = load_fixture("tiny")
+    q = load_fixture("query_tiny")
+    lay = orc.layout_from_fixture(fx, ncats=4)
+    p0, q0, x = fx["params0"], fx["in_params0"], fx["x"]
+    nm, ems, lls = orc.forward(lay, p0, q0, x, missing_mask=q["mask"])
+    assert np.allclose(lls, q["marginal_lls"], rtol=1e-6, atol=1e-5)
+    nf, _, _ = orc.backward(lay, p0, x, nm, ems)
+    assert np.abs(orc.conditional(lay, q0, nf) - q["cond_hard_full"]).max() <= 1e-6
+    nm, ems, lls = orc.forward(lay, p0, q0, evidence=q["soft"])
+    assert np.allclose(lls, q["soft_lls"], rtol=1e-6, atol=1e-5)
+    nf, _, _ = orc.backward(lay, p0, None, nm, ems)
+    assert np.abs(orc.conditional(lay, q0, nf) - q["cond_soft"]).max() <= 1e-6
+    nm, ems, lls = orc.forward(lay, p0, q0, x, missing_mask=q["vmask"])
+    assert np.allclose(lls, q["vmask_lls"], rtol=1e-6, atol=1e-5)
+    _, pf, ipf = orc.backward(lay, p0, x, nm, ems, missing_mask=q["vmask"], in_params=q0)
+    assert np.abs(pf - q["vmask_param_flows"]).max() <= 1e-5 * np.abs(pf).max()
+    ref_ipf = q["vmask_in_param_flows"][:ipf.shape[0]]
+    assert np.abs(ipf - ref_ipf).max() <= 1e-5 * np.abs(ref_ipf).max()
