@@ -354,6 +354,21 @@ int pcb_sum_pflows(const float* node_flows, const float* node_mars, const float*
                    int32_t modified, int32_t atomic, int32_t tile_children, int32_t prec, void* stream);
 
 /*
+ * pcb_sum_pflows on the tcgen05 tensor cores (prec 1: bf16 operands, 2: split bf16 hi + lo,
+ * three MMAs; tile_children 64 or 128): the [128 x tile_children] accumulator of a tile stays
+ * in tensor memory over the CTA's batch slice; each 32-sample chunk is exponentiated into
+ * K-major bf16 operands (K = samples) while the previous chunk's MMAs run. Same tiles,
+ * results (up to the FP32 summation order), cluster reduction and flow-slot update as
+ * pcb_sum_pflows. A bounded wait that runs out reports PCB_STATUS_WAIT_TIMEOUT (NaN flows).
+ * Replaces the same reference kernels as pcb_sum_pflows.
+ */
+int pcb_sum_pflows_tc05(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld,
+                        int32_t B, const float* params, float* param_flows, const PcbPflowTile* tiles,
+                        int32_t num_tiles, int32_t rows_per_block, const int32_t* cids, const int32_t* pids,
+                        const int32_t* pfids, int32_t modified, int32_t atomic, int32_t tile_children, int32_t prec,
+                        void* stream);
+
+/*
  * Sum-parameter EM update, per node block (FP64 normalisation):
  *   for node i < bs, child k < nch:   p = params[pbase + k * bs + i], f = pflows[pfbase + k * bs + i]
  *   theta' = (1 - s) * p + s * (f + pc / nch) / (sum_k f + pc)

@@ -20,7 +20,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpcb200.so")
 CSRC = os.path.join(_HERE, "csrc")
 SOURCES = ["capi_common.cu", "lse_contract.cu", "lse_contract_tc.cu", "lse_short.cu", "lse_tc05.cu", "prod_kernels.cu", "sum_pflows.cu",
-           "sum_generic.cu", "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu",
+           "sum_pflows_tc05.cu", "sum_generic.cu", "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu",
            "input_soft.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-shared",
               "-Xcompiler", "-fPIC"]
@@ -122,6 +122,9 @@ _SIGS = {
     "pcb_modify_flows": ([c_void_p, c_void_p, c_int64, c_int32, c_int64, c_int64, c_void_p], c_int32),
     "pcb_sum_pflows": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                         c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_sum_pflows_tc05": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
+                             c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p],
+                            c_int32),
     "pcb_sum_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double, c_int32,
                     c_void_p], c_int32),
     "pcb_sum_em_f64flows": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,

@@ -212,6 +212,9 @@ class SumLayer(Layer):
     # Children per parameter-flow tile (32, 64 or 128): with all children of a region in one
     # tile, its node rows are exponentiated once per sample slice instead of once per chunk.
     pflow_tile_children = 64
+    # BF16 parameter flows on the tcgen05 tensor cores (accumulators in tensor memory);
+    # False: the warp-level mma.sync kernel.
+    pflow_tc05 = True
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -597,7 +600,8 @@ class SumLayer(Layer):
         kc = SumLayer.pflow_tile_children
         pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
         prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
-        nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
+        entry = "pcb_sum_pflows_tc05" if (prec > 0 and SumLayer.pflow_tc05 and kc in (64, 128)) else "pcb_sum_pflows"
+        nat.call(entry, nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
                  node_mars.stride(0), B, nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0),
                  self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]),
                  1 if allow_modify_flows else 0, 1 if self._has_tied else 0, kc, prec, nat.stream())

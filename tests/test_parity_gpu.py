@@ -9,8 +9,9 @@ own outputs, in every precision form the EM step runs in:
 * non-uniform root weights (``ll_weights``), the FP64 dataset log-likelihood reducer and
   FP64 epoch-level parameter flows against the oracle.
 
-Error bounds, relative to the largest magnitude of the compared quantity: FP32 3e-4 (59 levels
-of FP32 rounding between the root and the inputs); split
+Error bounds, relative to the largest magnitude of the compared quantity: FP32 1e-3 (node
+values of this circuit are log-likelihoods near -3000 nats, where one FP32 ulp is 2.4e-4, so
+every exp(element value - node value) carries that relative error); split
 BF16 2e-3; single BF16 5e-2 (its operands keep 8 mantissa bits).
 """
 
@@ -28,7 +29,7 @@ from pyjuice_b200.synthetic import gaussian_field_data
 
 pytestmark = pytest.mark.gpu
 
-FORMS = {"fp32": (0, 3e-4), "bf16_split": (2, 2e-3), "bf16_single": (1, 5e-2)}
+FORMS = {"fp32": (0, 1e-3), "bf16_split": (2, 2e-3), "bf16_single": (1, 5e-2)}
 _CACHE = {}
 
 
@@ -268,3 +269,44 @@ def test_set_propagation_alg_and_forward_mpe(cuda_device):
     assert np.abs(b - ref["gll_lls"]).max() <= 1e-4
     with pytest.raises(ValueError):
         pc.set_propagation_alg("GeneralLL")
+
+
+@pytest.mark.parametrize("tkc", [64, 128])
+@pytest.mark.parametrize("modified", [True, False])
+@pytest.mark.parametrize("form", [2, 1])
+def test_pflows_tc05_matches_mma_sync(tkc, modified, form, cuda_device):
+    """The tcgen05 parameter-flow kernel (accumulators in tensor memory) against the warp-level
+    mma.sync kernel on every sum layer of the 28x28 circuit at batch 96 (a partial last
+    chunk), for 64- and 128-child tiles, rewritten and raw node flows, both BF16 forms."""
+    pc, c = _hclt784(cuda_device)
+    rng = np.random.default_rng(5)
+    x = torch.from_numpy(rng.integers(0, 256, size=(96, 784))).to(cuda_device)
+    saved = (SumLayer.pflow_tc05, SumLayer.pflow_tile_children, SumLayer.bf16_form)
+    try:
+        SumLayer.bf16_form = form
+        SumLayer.pflow_tile_children = tkc
+        with torch.no_grad():
+            pc(x, force_use_bf16=True)
+        pc.init_param_flows(flows_memory=0.0)
+        pc.backward(inputs=x, allow_modify_flows=False, compute_param_flows=False)
+        nfl = pc.node_flows
+        if modified:  # the kernels' other input form: log f - log m
+            nfl = torch.where(torch.isinf(pc.node_mars), torch.full_like(nfl, -float("inf")),
+                              torch.log(pc.node_flows) - pc.node_mars)
+        torch.cuda.synchronize()
+        out = []
+        for tc05 in (False, True):
+            SumLayer.pflow_tc05 = tc05
+            pf = torch.zeros_like(pc.param_flows)
+            for gi, g in enumerate(pc.inner_layer_groups):
+                if g.is_sum():
+                    for layer in g:
+                        layer.param_flows_only(nfl, pc.node_mars, pc._em_view(gi - 1), pc.params, pf,
+                                               allow_modify_flows=modified)
+            torch.cuda.synchronize()
+            out.append(pf.double().cpu().numpy())
+    finally:
+        SumLayer.pflow_tc05, SumLayer.pflow_tile_children, SumLayer.bf16_form = saved
+    ref, got = out
+    assert np.isfinite(got).all()
+    assert np.abs(got - ref).max() <= (1e-5 if form == 2 else 1e-2) * np.abs(ref).max()
