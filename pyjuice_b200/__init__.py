@@ -7,10 +7,11 @@ Same public API as the reference package for the circuit passes:
 differentiable soft-evidence log-likelihood).
 """
 
-from . import nodes, layer, model, structures, queries, autograd
+from . import nodes, layer, model, structures, queries, autograd, io
 from .nodes import inputs, multiply, summate, set_block_size, distributions
 from .model import TensorCircuit, compile
 from .layer import InputLayer, ProdLayer, SumLayer
+from .io import load, save
 
 __all__ = ["compile", "TensorCircuit", "inputs", "multiply", "summate", "set_block_size", "distributions",
-           "structures", "queries", "autograd", "InputLayer", "ProdLayer", "SumLayer"]
+           "structures", "queries", "autograd", "io", "load", "save", "InputLayer", "ProdLayer", "SumLayer"]

@@ -24,6 +24,9 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``query_tiny.npz`` the tiny circuit's queries: marginals and the hard-evidence conditional
                     with a per-sample missing mask, the soft-evidence conditional, and
                     input-layer flows with a per-variable missing mask;
+* ``io_tiny.npz``    ``.jpc`` files both ways: the bytes of the reference's file of the tiny
+                    circuit, and the reference's parameters and log-likelihoods after loading
+                    a file saved by pyjuice_b200;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -307,6 +310,35 @@ def make_query_variants():
     np.savez_compressed(os.path.join(HERE, "query_tiny.npz"), **out)
 
 
+def make_io_variants():
+    """.jpc files in both directions on the tiny circuit: the reference saves its circuit
+    (parameters of tiny.npz; the file bytes are stored), and the reference loads a file that
+    pyjuice_b200 saved from its own build of the same circuit and evaluates it (FP32)."""
+    import tempfile
+    import pyjuice_b200 as mine
+    from pyjuice_b200.nodes import distributions as mdists
+    fx = dict(np.load(os.path.join(HERE, "tiny.npz")))
+    torch.manual_seed(1)
+    pc = juice.compile(build_tiny_dag(juice, dists), max_tied_ns_per_parflow_block=1, verbose=False)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        juice.save(os.path.join(d, "ref.jpc"), pc)
+        with open(os.path.join(d, "ref.jpc"), "rb") as f:
+            out["ref_jpc"] = np.frombuffer(f.read(), dtype=np.uint8).copy()
+        mpc = mine.compile(build_tiny_dag(mine, mdists), max_tied_ns_per_parflow_block=1)
+        with torch.no_grad():
+            mpc.params.copy_(torch.from_numpy(fx["params0"]))
+            mpc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+        mine.save(os.path.join(d, "ours.jpc"), mpc)
+        rpc = juice.compile(juice.load(os.path.join(d, "ours.jpc")), max_tied_ns_per_parflow_block=1, verbose=False)
+        out["ref_loads_ours_params"] = rpc.params.detach().cpu().numpy().copy()
+        out["ref_loads_ours_lls"] = rpc(torch.from_numpy(fx["x"]), force_use_fp32=True).detach().cpu().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "io_tiny.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -346,10 +378,11 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
-         "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants}[w]()
+         "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants,
+         "io_tiny": make_io_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)
