@@ -849,10 +849,23 @@ class TensorCircuit(nn.Module):
         ``use_f64_flows``: update from the FP64 epoch flows (``param_flows_f64``, see
         :meth:`accumulate_param_flows_f64`) instead of the FP32 ``param_flows``.
         """
-        if step_size_rescaling:
-            raise NotImplementedError("step_size_rescaling needs top-down probabilities, which have no CUDA path yet")
         if not (0.0 < step_size <= 1.0):
             raise ValueError("`step_size` should be between 0 and 1.")
+        if step_size_rescaling:
+            # mini-batch EM objective (tensorcircuit.py:566-577): the accumulated flows are scaled
+            # by step / (total root flow) and the walk's own flows are added with weight 1 - step;
+            # the update then uses step 1
+            if use_f64_flows:
+                raise ValueError("step_size_rescaling works on the FP32 parameter flows")
+            cum = self._cum_flow
+            if not cum > 0.0:
+                raise RuntimeError("Please perform a backward pass before calling `mini_batch_em`.")
+            with torch.no_grad():
+                self.init_param_flows(flows_memory=step_size / cum)
+                from .top_down import eval_top_down_probs
+                eval_top_down_probs(self, update_pflow=True, scale=1.0 - step_size, use_cudagraph=use_cudagraph)
+            self._cum_flow_dev.zero_()
+            step_size = 1.0
         if self.param_flows is None and not use_f64_flows:
             raise RuntimeError("run a backward pass before mini_batch_em")
         if use_f64_flows and self.param_flows_f64 is None:

@@ -27,6 +27,8 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``io_tiny.npz``    ``.jpc`` files both ways: the bytes of the reference's file of the tiny
                     circuit, and the reference's parameters and log-likelihoods after loading
                     a file saved by pyjuice_b200;
+* ``tdp_tiny.npz``   flows of the evidence-free pass (all variables missing) on the tiny
+                    circuit: per sample, its top-down probabilities;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -339,6 +341,31 @@ def make_io_variants():
     np.savez_compressed(os.path.join(HERE, "io_tiny.npz"), **out)
 
 
+def make_tdp_variants():
+    """Flows of the evidence-free pass on the tiny circuit: every variable missing, root flow
+    1 per sample (``pc(x, missing_mask=all)``, ``lls.mean().backward()``). Per sample these are
+    the top-down probabilities that ``eval_top_down_probs`` computes; that function itself
+    (and ``mini_batch_em(step_size_rescaling=True)``, which calls it) ends in a
+    segmentation fault under Triton's CPU interpreter, so its own outputs cannot be
+    recorded here."""
+    fx = dict(np.load(os.path.join(HERE, "tiny.npz")))
+    torch.manual_seed(1)
+    pc = juice.compile(build_tiny_dag(juice, dists), max_tied_ns_per_parflow_block=1, verbose=False)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(fx["params0"]))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(fx["in_params0"]))
+    x = torch.from_numpy(fx["x"][:4])
+    out = {}
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, missing_mask=torch.ones(x.shape[1], dtype=torch.bool), force_use_fp32=True)
+    out["lls"] = lls.detach().numpy().copy()
+    lls.mean().backward()
+    out["node_flows"] = pc.node_flows.detach().numpy().copy()
+    out["param_flows"] = pc.param_flows.detach().numpy().copy()
+    out["in_param_flows"] = pc.input_layer_group[0].param_flows.detach().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "tdp_tiny.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -378,11 +405,11 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
          "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants,
-         "io_tiny": make_io_variants}[w]()
+         "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

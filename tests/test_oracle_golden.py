@@ -138,3 +138,29 @@ def test_oracle_queries_match_reference():
     assert np.abs(pf - q["vmask_param_flows"]).max() <= 1e-5 * np.abs(pf).max()
     ref_ipf = q["vmask_in_param_flows"][:ipf.shape[0]]
     assert np.abs(ipf - ref_ipf).max() <= 1e-5 * np.abs(ref_ipf).max()
+
+
+def test_oracle_evidence_free_flows_match_reference():
+    """Flows of the evidence-free pass (every variable missing), whose per-sample node flows
+    are the top-down probabilities, against the reference's own (fixture tdp_tiny.npz)."""
+    fx = load_fixture("tiny")
+    t = load_fixture("tdp_tiny")
+    lay = orc.layout_from_fixture(fx, ncats=4)
+    x = np.zeros([4, 6], dtype=np.int64)
+    miss = np.ones(6, dtype=bool)
+    nm, ems, lls = orc.forward(lay, fx["params0"], fx["in_params0"], x, missing_mask=miss)
+    assert np.abs(lls - t["lls"]).max() <= 1e-5
+    nf, pf, ipf = orc.backward(lay, fx["params0"], x, nm, ems, missing_mask=miss, in_params=fx["in_params0"])
+    # the reference's backward rewrote the node flows of its large sum layers in place as
+    # log f - log m (allow_modify_flows): every row matches in one of the two forms
+    ref = t["node_flows"]
+    with np.errstate(divide="ignore"):
+        rewritten = np.log(nf) - nm
+    ok = np.all(np.abs(nf - ref) <= 1e-5, axis=1) | np.all(np.abs(rewritten - ref) <= 1e-5, axis=1)
+    assert ok.all()
+    n_in0 = lay["input"]["nid_start"]
+    assert np.abs(nf[n_in0:n_in0 + lay["input"]["vids"].shape[0]] -
+                  ref[n_in0:n_in0 + lay["input"]["vids"].shape[0]]).max() <= 1e-5
+    assert np.abs(pf - t["param_flows"]).max() <= 1e-5 * np.abs(pf).max()
+    ref_ipf = t["in_param_flows"][:ipf.shape[0]]
+    assert np.abs(ipf - ref_ipf).max() <= 1e-5 * np.abs(ref_ipf).max()

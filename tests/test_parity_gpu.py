@@ -310,3 +310,41 @@ def test_pflows_tc05_matches_mma_sync(tkc, modified, form, cuda_device):
     ref, got = out
     assert np.isfinite(got).all()
     assert np.abs(got - ref).max() <= (1e-5 if form == 2 else 1e-2) * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_top_down_probs_and_step_size_rescaling(name, cuda_device):
+    """Top-down probabilities (node flows of the evidence-free pass, oracle pinned to the
+    reference's flows) and one mini-batch EM step with step-size rescaling
+    (tensorcircuit.py:566-590) against the oracle."""
+    from pyjuice_b200.model.top_down import eval_top_down_probs
+    fx = load_fixture(name)
+    pc = build_fixture_circuit(name, fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    lay = orc.layout_from_circuit(pc)
+    p0, q0 = fx["params0"], fx["in_params0"]
+    V = pc.num_vars
+    z, miss = np.zeros([1, V], dtype=np.int64), np.ones(V, dtype=bool)
+    nm, ems, _ = orc.forward(lay, p0, q0, z, missing_mask=miss)
+    tdp, tdp_pf, tdp_ipf = orc.backward(lay, p0, z, nm, ems, missing_mask=miss, in_params=q0)
+    pc.init_param_flows(flows_memory=0.0)
+    eval_top_down_probs(pc, update_pflow=True, scale=0.5)
+    assert np.abs(pc._single_node_flows.cpu().numpy() - tdp[:, 0]).max() <= 1e-5
+    assert _rel(pc.param_flows.cpu().numpy(), 0.5 * tdp_pf) <= 1e-4
+    il = pc.input_layer_group[0]
+    assert _rel(il.param_flows.cpu().numpy()[:tdp_ipf.shape[0]], 0.5 * tdp_ipf) <= 1e-4
+    # a batch, then EM with the step rescaled by the batch's root flow
+    B = min(64, fx["x"].shape[0])
+    xb = fx["x"][:B]
+    nmb, emb, _ = orc.forward(lay, p0, q0, xb)
+    _, pf, ipf = orc.backward(lay, p0, xb, nmb, emb)
+    pc.init_param_flows(flows_memory=0.0)
+    pc._cum_flow_dev = None
+    lls = pc(torch.from_numpy(xb).to(cuda_device), force_use_fp32=True)
+    lls.mean().backward()
+    pc.mini_batch_em(step_size=0.3, pseudocount=0.1, step_size_rescaling=True)
+    s = 0.3
+    p1, q1 = orc.em_update(lay, p0, pf * (s / B) + (1 - s) * tdp_pf, q0, ipf * (s / B) + (1 - s) * tdp_ipf, 1.0, 0.1)
+    assert np.abs(pc.params.cpu().numpy() - p1).max() <= 1e-4
+    assert np.abs(il.params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-4
+    assert pc._cum_flow == 0.0
