@@ -29,6 +29,9 @@ the results of one forward / backward / ``mini_batch_em`` step:
                     a file saved by pyjuice_b200;
 * ``tdp_tiny.npz``   flows of the evidence-free pass (all variables missing) on the tiny
                     circuit: per sample, its top-down probabilities;
+* ``structures.npz`` compiled layouts, parameters and log-likelihoods of the reference's PD
+                    (3 x 3 grid) and homogeneous HMM (length 6) generators; flows and one EM
+                    step of the HMM (tied transitions and emissions);
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -366,6 +369,53 @@ def make_tdp_variants():
     np.savez_compressed(os.path.join(HERE, "tdp_tiny.npz"), **out)
 
 
+def make_structures():
+    """Compiled layouts of the reference's PD and HMM generators, with parameters and the
+    FP32 log-likelihoods of seeded data:
+    * PD over a 3 x 3 grid, split interval 1, 32 latents (block size 16), 4 categories, at
+      most 2 product blocks per sum block (so the random block choice is exercised), seed 7;
+    * a homogeneous HMM of length 6, 32 latents, 10 symbols, seeded Dirichlet(1) alpha /
+      beta / gamma (tied transition and emission vectors)."""
+    from pyjuice.structures import PD, HMM
+    out = {}
+    torch.manual_seed(7)
+    root = PD((3, 3), 32, split_intervals=1, max_prod_block_conns=2, input_node_params={"num_cats": 4})
+    torch.manual_seed(8)
+    pc = juice.compile(root, verbose=False)
+    lay = {}
+    collect_layout(pc, lay, full=True)
+    out.update({"pd_" + k: v for k, v in lay.items()})
+    out["pd_params"] = pc.params.detach().numpy().copy()
+    out["pd_in_params"] = pc.input_layer_group[0].params.detach().numpy().copy()
+    x = torch.from_numpy(np.random.default_rng(1).integers(0, 4, size=(16, 9)))
+    out["pd_x"] = x.numpy()
+    out["pd_lls"] = pc(x, force_use_fp32=True).detach().numpy().copy()
+    rng = np.random.default_rng(2)
+    alpha = torch.from_numpy(rng.dirichlet(np.ones(32), size=32).astype(np.float32))
+    beta = torch.from_numpy(rng.dirichlet(np.ones(10), size=32).astype(np.float32))
+    gamma = torch.from_numpy(rng.dirichlet(np.ones(32)).astype(np.float32))
+    out["hmm_alpha"], out["hmm_beta"], out["hmm_gamma"] = alpha.numpy(), beta.numpy(), gamma.numpy()
+    torch.manual_seed(9)
+    pc = juice.compile(HMM(6, 32, 10, homogeneous=True, alpha=alpha, beta=beta, gamma=gamma), verbose=False)
+    lay = {}
+    collect_layout(pc, lay, full=True)
+    out.update({"hmm_" + k: v for k, v in lay.items()})
+    out["hmm_params"] = pc.params.detach().numpy().copy()
+    out["hmm_in_params"] = pc.input_layer_group[0].params.detach().numpy().copy()
+    x = torch.from_numpy(rng.integers(0, 10, size=(16, 6)))
+    out["hmm_x"] = x.numpy()
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    out["hmm_lls"] = lls.detach().numpy().copy()
+    lls.mean().backward()
+    out["hmm_param_flows"] = pc.param_flows.detach().numpy().copy()
+    out["hmm_in_param_flows"] = pc.input_layer_group[0].param_flows.detach().numpy().copy()
+    pc.mini_batch_em(step_size=0.5, pseudocount=0.01)
+    out["hmm_params1"] = pc.params.detach().numpy().copy()
+    out["hmm_in_params1"] = pc.input_layer_group[0].params.detach().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "structures.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -405,11 +455,11 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny", "structures"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
          "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants,
-         "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants}[w]()
+         "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants, "structures": make_structures}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

@@ -348,3 +348,36 @@ def test_top_down_probs_and_step_size_rescaling(name, cuda_device):
     assert np.abs(pc.params.cpu().numpy() - p1).max() <= 1e-4
     assert np.abs(il.params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-4
     assert pc._cum_flow == 0.0
+
+
+def test_pd_and_hmm_match_reference(cuda_device):
+    """The PD and homogeneous-HMM circuits (tied transition and emission vectors) through the
+    device kernels against the reference's own outputs (structures.npz): FP32 log-likelihoods,
+    flows and one EM step of the HMM."""
+    fx = load_fixture("structures")
+    sub = lambda p: {k[len(p):]: v for k, v in fx.items() if k.startswith(p)}
+    pd = sub("pd_")
+    torch.manual_seed(7)
+    pc = juice.compile(juice.structures.PD((3, 3), 32, split_intervals=1, max_prod_block_conns=2,
+                                           input_dist=juice.distributions.Categorical(num_cats=4))).to(cuda_device)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(pd["params"]).to(cuda_device))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(pd["in_params"]).to(cuda_device))
+        lls = pc(torch.from_numpy(pd["x"]).to(cuda_device), force_use_fp32=True).cpu().numpy()
+    assert np.all(np.abs(lls - pd["lls"]) <= 1e-5 * np.abs(pd["lls"]) + 1e-6)
+    hm = sub("hmm_")
+    pc = juice.compile(juice.structures.HMM(6, 32, 10, alpha=torch.from_numpy(hm["alpha"]),
+                                            beta=torch.from_numpy(hm["beta"]),
+                                            gamma=torch.from_numpy(hm["gamma"]))).to(cuda_device)
+    x = torch.from_numpy(hm["x"]).to(cuda_device)
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    assert np.all(np.abs(lls.detach().cpu().numpy() - hm["lls"]) <= 1e-5 * np.abs(hm["lls"]) + 1e-6)
+    lls.mean().backward()
+    assert _rel(pc.param_flows.cpu().numpy(), hm["param_flows"]) <= 1e-4
+    ipf = hm["in_param_flows"]
+    assert _rel(pc.input_layer_group[0].param_flows.cpu().numpy()[:ipf.shape[0]], ipf) <= 1e-4
+    pc.mini_batch_em(step_size=0.5, pseudocount=0.01)
+    assert np.abs(pc.params.cpu().numpy() - hm["params1"]).max() <= 1e-5
+    q1 = hm["in_params1"]
+    assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-5

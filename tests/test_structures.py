@@ -1,0 +1,51 @@
+"""The PD and HMM generators build the same circuits as the reference's (structures.npz):
+the compiled layouts are identical, and the oracle evaluates the reference's parameters on
+our layout to the reference's log-likelihoods (and, for the homogeneous HMM, its flows and
+EM step with tied transition and emission vectors). CPU only."""
+
+import numpy as np
+import torch
+
+from conftest import load_fixture
+from helpers import layout_mismatches
+
+import pyjuice_b200 as juice
+from pyjuice_b200.nodes import distributions as dists
+from oracle import pc_oracle as orc
+
+
+def _sub(fx, prefix):
+    return {k[len(prefix):]: v for k, v in fx.items() if k.startswith(prefix)}
+
+
+def test_pd_matches_reference():
+    fx = _sub(load_fixture("structures"), "pd_")
+    torch.manual_seed(7)
+    root = juice.structures.PD((3, 3), 32, split_intervals=1, max_prod_block_conns=2,
+                               input_dist=dists.Categorical(num_cats=4))
+    pc = juice.compile(root)
+    assert layout_mismatches(pc, fx) == []
+    lay = orc.layout_from_circuit(pc)
+    _, _, lls = orc.forward(lay, fx["params"], fx["in_params"], fx["x"])
+    assert np.allclose(lls, fx["lls"], rtol=1e-6, atol=1e-5)
+
+
+def test_hmm_matches_reference():
+    fx = _sub(load_fixture("structures"), "hmm_")
+    root = juice.structures.HMM(6, 32, 10, homogeneous=True, alpha=torch.from_numpy(fx["alpha"]),
+                                beta=torch.from_numpy(fx["beta"]), gamma=torch.from_numpy(fx["gamma"]))
+    pc = juice.compile(root)
+    assert layout_mismatches(pc, fx) == []
+    assert np.abs(pc.params.numpy() - fx["params"]).max() <= 1e-6
+    assert np.abs(pc.input_layer_group[0].params.numpy()[:fx["in_params"].shape[0]] - fx["in_params"]).max() <= 1e-6
+    lay = orc.layout_from_circuit(pc)
+    nm, ems, lls = orc.forward(lay, fx["params"], fx["in_params"], fx["x"])
+    assert np.allclose(lls, fx["lls"], rtol=1e-6, atol=1e-5)
+    _, pf, ipf = orc.backward(lay, fx["params"], fx["x"], nm, ems)
+    assert np.abs(pf - fx["param_flows"]).max() <= 1e-5 * np.abs(pf).max()
+    ref_ipf = fx["in_param_flows"][:ipf.shape[0]]
+    assert np.abs(ipf - ref_ipf).max() <= 1e-5 * np.abs(ref_ipf).max()
+    p1, q1 = orc.em_update(lay, fx["params"], fx["param_flows"].astype(np.float64), fx["in_params"],
+                           fx["in_param_flows"].astype(np.float64), 0.5, 0.01)
+    assert np.abs(p1 - fx["params1"]).max() <= 1e-6
+    assert np.abs(q1 - fx["in_params1"][:q1.shape[0]]).max() <= 1e-6
