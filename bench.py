@@ -511,9 +511,13 @@ def main():
                   "fp32_dmean_ll_nats": float(abs(l_32.mean() - lls_o.mean())),
                   "mean_ll_nats": float(lls_o.mean()), "samples": int(xs.size(0))}
         hbm, tflops, src = peaks()
+        # the roofline launches read the buffers of a full-batch step: run one (the error
+        # measurements above left buffers of 16 and 64 samples)
+        step(data_dev[:B], {"force_use_bf16": True})
         rf = sum_forward_roofline(pc, data_dev[:B], {"force_use_bf16": True})
         big = rf["largest"]
         achieved = big["bytes"] / big["seconds"] / 1e9
+        step(data_dev[:B], {"force_use_bf16": True})  # node flows of the full batch (rewritten as log f - log m)
         pf = pflows_roofline(pc)
         achieved = pf["bytes"] / pf["seconds"] / 1e9
         roof = {"kernel": "pcb_sum_pflows (sum_pflows_kernel, split-bf16 form, 64-child tiles) of the largest "

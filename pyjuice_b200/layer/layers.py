@@ -597,6 +597,10 @@ class SumLayer(Layer):
         node_flows already hold log f - log m for this layer's nodes)."""
         d = self._desc(node_mars.device)
         B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        for t in (node_flows, element_mars):
+            if t.size(1) != B or t.stride(0) != ld or t.stride(1) != 1:
+                raise ValueError("node flows, node values and element values must share one [rows, B] layout")
         kc = SumLayer.pflow_tile_children
         pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
         prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
