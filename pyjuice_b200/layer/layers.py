@@ -20,6 +20,7 @@ import numpy as np
 import torch
 
 from .. import _native as nat
+from ..autotune import TUNER
 from .compilation import compile_prod_layer, compile_sum_layer
 from .input_layer_compile import compile_input_layer
 
@@ -77,12 +78,45 @@ def _tc05_slices_per_cta(num_tiles: int, B: int, batch_tile: int) -> int:
 
 
 def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream):
-    """One tcgen05 contraction (pcb_lse_contract_tc05) with the batch tile and slices per CTA
-    chosen for the layer's tile count."""
-    bt = _tc05_batch_tile(tiles.size(0), B)
-    nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B, nat.ptr(pack),
-             nat.ptr(tiles), tiles.size(0), nat.ptr(krow), mode, prec, bt, _tc05_slices_per_cta(tiles.size(0), B, bt),
-             stream)
+    """One tcgen05 contraction (pcb_lse_contract_tc05). Samples per CTA (32 or 64) and slices
+    per CTA (1 or 2) come from the autotuner, keyed by mode, precision form, tile count and
+    batch (``SumLayer.tc05_slices_per_cta`` fixes the slices and the static batch tile)."""
+    nt = tiles.size(0)
+
+    def run(c):
+        nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
+                 nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, c[0], c[1], stream)
+
+    bt = _tc05_batch_tile(nt, B)
+    if SumLayer.tc05_slices_per_cta is not None:
+        return run((bt, _tc05_slices_per_cta(nt, B, bt)))
+    cands = [(bt, 1)] + [c for c in ((64, 1), (32, 1), (64, 2), (32, 2)) if c != (bt, 1)]
+    run(TUNER.pick(("tc05", mode, prec, nt, B), cands, run))
+
+
+def _short_tile(key, num_tiles: int, tile_rows: int, B: int, fused: bool, run) -> None:
+    """Launch ``run(batch_tile)`` of a single-stage contraction with the autotuned samples per
+    CTA (16, 32 or 64; at most 32 with a fused product layer); ``SumLayer.short_batch_tile``
+    fixes it, 0 keeps the static rule (_short_batch_tile)."""
+    static = _short_batch_tile(num_tiles, tile_rows, B, fused)
+    fixed = SumLayer.short_batch_tile
+    if fixed is not None:
+        return run(static if fixed == 0 else (min(fixed, 32) if fused else fixed))
+    cands = [static] + [t for t in ((16, 32) if fused else (16, 32, 64)) if t != static]
+    run(TUNER.pick(("short",) + tuple(key) + (num_tiles, tile_rows, B, fused), cands, run))
+
+
+_SCRATCH = {}
+
+
+def _pflow_scratch(like: torch.Tensor) -> torch.Tensor:
+    """A buffer shaped like the parameter flows for timing accumulating candidates."""
+    key = (like.device, like.numel())
+    t = _SCRATCH.get(key)
+    if t is None:
+        t = torch.zeros_like(like)
+        _SCRATCH[key] = t
+    return t
 
 
 def _rows_vec4(tiles: np.ndarray, kw: np.ndarray, rpb: int, w_stride: int) -> bool:
@@ -211,10 +245,13 @@ class SumLayer(Layer):
     pack_short_weights = True
     # Children per parameter-flow tile (32, 64 or 128): with all children of a region in one
     # tile, its node rows are exponentiated once per sample slice instead of once per chunk.
-    pflow_tile_children = 64
-    # BF16 parameter flows on the tcgen05 tensor cores (accumulators in tensor memory);
-    # False: the warp-level mma.sync kernel.
-    pflow_tc05 = True
+    # (None: chosen per layer shape by the autotuner; the static default is 64.)
+    pflow_tile_children = None
+    # BF16 parameter flows on the tcgen05 tensor cores (accumulators in tensor memory) or on
+    # the warp-level mma.sync kernel (False); None: chosen by the autotuner.
+    pflow_tc05 = None
+    # Samples per CTA of the single-stage kernels: None autotuned, 0 the static rule, else fixed.
+    short_batch_tile = None
 
     _tensor_lists = ("partitioned_nids", "partitioned_cids", "partitioned_pids", "partitioned_pfids",
                      "partitioned_chids", "partitioned_parids", "partitioned_parpids")
@@ -478,11 +515,15 @@ class SumLayer(Layer):
         if d["fw_short"] and SumLayer.short_kernels:
             packed = d["fw_pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
             fusion = nat.short_fusion(fuse[0], fuse[1]) if fuse is not None else nat.ptr(None)
-            nat.call("pcb_lse_contract_short", nat.ptr(element_mars if fuse is None else node_mars), nat.ptr(None),
-                     nat.ptr(None), nat.ptr(node_mars), ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"],
-                     self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(packed),
-                     d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B, fuse is not None), fusion,
-                     nat.stream())
+            st = nat.stream()
+
+            def run(bt):
+                nat.call("pcb_lse_contract_short", nat.ptr(element_mars if fuse is None else node_mars),
+                         nat.ptr(None), nat.ptr(None), nat.ptr(node_mars), ld, B, nat.ptr(params), nat.ptr(t),
+                         t.size(0), d["fw_tm"], self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec,
+                         nat.ptr(packed), d["fw_wlayout"], bt, fusion, st)
+
+            _short_tile((0, prec, packed is not None), t.size(0), d["fw_tm"], B, fuse is not None, run)
             return
         if fuse is not None:
             raise RuntimeError("a fused product layer needs the single-stage sum kernel")
@@ -546,12 +587,18 @@ class SumLayer(Layer):
                 fuse = kwargs.get("_fuse_bw")
                 if fuse is not None and allow_modify_flows:
                     raise RuntimeError("a fused product layer needs unmodified node flows")
-                nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(None if allow_modify_flows else node_mars),
-                         nat.ptr(element_mars), nat.ptr(element_flows if fuse is None else node_flows), ld, B,
-                         nat.ptr(params), nat.ptr(et), et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]),
-                         nat.ptr(eg["kw"]), self.block_size, 1 if allow_modify_flows else 2, prec, nat.ptr(packed),
-                         eg["wlayout"], _short_batch_tile(et.size(0), eg["tm"], B, fuse is not None),
-                         nat.short_fusion(out_children=fuse) if fuse is not None else nat.ptr(None), nat.stream())
+                mode = 1 if allow_modify_flows else 2
+                fz = nat.short_fusion(out_children=fuse) if fuse is not None else nat.ptr(None)
+                st = nat.stream()
+
+                def run(bt, eg=eg, et=et, packed=packed, prec=prec, mode=mode, fuse=fuse, fz=fz, st=st):
+                    nat.call("pcb_lse_contract_short", nat.ptr(node_flows),
+                             nat.ptr(None if allow_modify_flows else node_mars), nat.ptr(element_mars),
+                             nat.ptr(element_flows if fuse is None else node_flows), ld, B, nat.ptr(params),
+                             nat.ptr(et), et.size(0), eg["tm"], eg["cbs"], nat.ptr(eg["krow"]), nat.ptr(eg["kw"]),
+                             self.block_size, mode, prec, nat.ptr(packed), eg["wlayout"], bt, fz, st)
+
+                _short_tile((mode, prec, packed is not None), et.size(0), eg["tm"], B, fuse is not None, run)
                 continue
             if kwargs.get("_fuse_bw") is not None:
                 raise RuntimeError("a fused product layer needs the single-stage element-flow kernel")
@@ -601,14 +648,31 @@ class SumLayer(Layer):
         for t in (node_flows, element_mars):
             if t.size(1) != B or t.stride(0) != ld or t.stride(1) != 1:
                 raise ValueError("node flows, node values and element values must share one [rows, B] layout")
-        kc = SumLayer.pflow_tile_children
-        pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
         prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
-        entry = "pcb_sum_pflows_tc05" if (prec > 0 and SumLayer.pflow_tc05 and kc in (64, 128)) else "pcb_sum_pflows"
-        nat.call(entry, nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
-                 node_mars.stride(0), B, nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0),
-                 self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]),
-                 1 if allow_modify_flows else 0, 1 if self._has_tied else 0, kc, prec, nat.stream())
+        st = nat.stream()
+
+        def run(c, target):
+            tc05, kc = c
+            pt = d[{128: "pf_tiles128", 64: "pf_tiles", 32: "pf_tiles32"}[kc]]
+            nat.call("pcb_sum_pflows_tc05" if tc05 else "pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars),
+                     nat.ptr(element_mars), ld, B, nat.ptr(params), nat.ptr(target), nat.ptr(pt), pt.size(0),
+                     self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]),
+                     1 if allow_modify_flows else 0, 1 if self._has_tied else 0, kc, prec, st)
+
+        kc_fixed, tc_fixed = SumLayer.pflow_tile_children, SumLayer.pflow_tc05
+        if prec == 0:
+            cands = [(False, k) for k in ((kc_fixed,) if kc_fixed else (64, 32, 128))]
+        else:
+            kcs = (kc_fixed,) if kc_fixed else (64, 128, 32)
+            tcs = (tc_fixed,) if tc_fixed is not None else (True, False)
+            cands = [(t, k) for t in tcs for k in kcs if not (t and k == 32)]
+        if len(cands) == 1:
+            return run(cands[0], param_flows)
+        # candidates accumulate into a scratch copy while they are timed
+        scratch = _pflow_scratch(param_flows)
+        choice = TUNER.pick(("pflows", prec, bool(allow_modify_flows), self._has_tied, d["pf_tiles"].size(0),
+                             int(d["fw_tm"]), B), cands, lambda c: run(c, scratch))
+        run(choice, param_flows)
 
     def __repr__(self):
         return f"SumLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
