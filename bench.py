@@ -15,11 +15,13 @@ forward -> backward -> ``mini_batch_em(step_size=0.1, pseudocount=0.1)``.
   every step;
 * ``roofline``: the parameter-flow launch of the largest sum layer (the kernel with the
   largest share of the step), timed per launch with CUDA events;
-* ``cpu_baseline``: the FP64 CPU restatement (oracle port) on a bounded sample.
+* ``cpu_baseline``: the FP32 PyTorch CPU restatement of the same step (``oracle/torch_port.py``)
+  at the same batch on all host cores, a few whole steps.
 
-``--impl reference`` times the CPU implementation of the same step instead (the
-reference itself is Python + Triton with no CPU path; its arithmetic is restated by
-``oracle/``), on all host cores, rank 0 only.
+``--impl reference`` times that CPU implementation of the same step instead (the reference
+itself is Python + Triton with no CPU path; its arithmetic is restated by ``oracle/``, whose
+FP64 version is pinned to the reference's own outputs), on all host cores, at the same
+batch, rank 0 only.
 
 Multi-GPU (``torchrun``): data-parallel replicas; each rank runs its own batch and the
 parameter flows are summed with an NCCL all-reduce before every EM update
@@ -246,22 +248,25 @@ def pflows_roofline(pc, reps=10):
             "tiles": d["pf_tiles"].size(0)}
 
 
-def cpu_step_rate(layout, params, in_params, data, budget_s):
-    """FP64 oracle port: forward + backward + EM, batches doubling until ~budget seconds."""
-    from oracle import pc_oracle as orc
-    B, t_used, samples = 8, 0.0, 0
-    while t_used < budget_s:
-        x = data[:B].numpy()
+def cpu_step_rate(layout, params, in_params, data, budget_s, batch=BATCH):
+    """CPU implementation of the same EM step (``oracle/torch_port.py``: the FP32 PyTorch
+    restatement of the reference's arithmetic, batched tensor operations on every host core),
+    at the benchmark's batch: whole steps until about ``budget_s`` seconds have passed (one at
+    least); returns (samples/s, description)."""
+    from oracle import torch_port as tp
+    tl = tp.TorchLayout(layout)
+    p = torch.from_numpy(np.asarray(params, dtype=np.float32))
+    q = torch.from_numpy(np.asarray(in_params, dtype=np.float32))
+    x = data[:batch].long()
+    times = []
+    t_start = time.perf_counter()
+    while not times or time.perf_counter() - t_start < budget_s:
         t0 = time.perf_counter()
-        nm, ems, _ = orc.forward(layout, params, in_params, x)
-        _, pf, ipf = orc.backward(layout, params, x, nm, ems)
-        orc.em_update(layout, params, pf, in_params, ipf, STEP_SIZE, PSEUDOCOUNT)
-        dt = time.perf_counter() - t0
-        t_used += dt
-        samples += B
-        if dt < budget_s / 4 and B < 512:
-            B *= 2
-    return samples / t_used, f"FP64 numpy oracle, batches of 8..{B} samples, {samples} samples in {t_used:.1f} s"
+        tp.em_step(tl, p, q, x, STEP_SIZE, PSEUDOCOUNT)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return batch / med, (f"FP32 PyTorch CPU restatement of the EM step (oracle/torch_port.py), batch {batch}, "
+                         f"median of {len(times)} whole steps ({med:.2f} s each)")
 
 
 def reference_arm(args):
@@ -274,14 +279,15 @@ def reference_arm(args):
     # mutual information is structure building, not the timed path: use a GPU when present
     pc = build_circuit(data, torch.device("cuda") if torch.cuda.is_available() else torch.device("cpu"))
     from oracle import pc_oracle as orc
-    lay = orc.layout_from_circuit(pc)
-    params = pc.params.detach().numpy().astype(np.float64)
-    in_params = pc.input_layer_group[0].params.detach().numpy().astype(np.float64)
-    B = 32
-    x = data[:B].numpy()
-    # A step of this CPU implementation takes seconds (its EM update alone touches all 10.6 M
-    # parameters), so the run is bounded by time: the requested warm-up steps (at most 3),
-    # then timed steps until about two minutes have passed (at least 3, at most --steps).
+    from oracle import torch_port as tp
+    tl = tp.TorchLayout(orc.layout_from_circuit(pc))
+    params = pc.params.detach().cpu().float()
+    in_params = pc.input_layer_group[0].params.detach().cpu().float()
+    B = args.batch
+    x = data[:B].long()
+    # A step of this CPU implementation takes seconds, so the run is bounded by time: the
+    # requested warm-up steps (at most 3), then timed steps until about two minutes have
+    # passed (at least 3, at most --steps).
     warm = max(1, min(args.warmup, 3))
     budget_s = 120.0
     times = []
@@ -289,9 +295,7 @@ def reference_arm(args):
     i = 0
     while True:
         t0 = time.perf_counter()
-        nm, ems, _ = orc.forward(lay, params, in_params, x)
-        _, pf, ipf = orc.backward(lay, params, x, nm, ems)
-        orc.em_update(lay, params, pf, in_params, ipf, STEP_SIZE, PSEUDOCOUNT)
+        params, in_params, _ = tp.em_step(tl, params, in_params, x, STEP_SIZE, PSEUDOCOUNT)
         if i >= warm:
             times.append(time.perf_counter() - t0)
         i += 1
@@ -300,11 +304,12 @@ def reference_arm(args):
         if len(times) >= 3 and time.perf_counter() - t_start > budget_s:
             break
     v = B / statistics.median(times)
-    sample = f"FP64 CPU restatement (oracle port), {B} samples per step, median of {len(times)} steps"
+    sample = (f"FP32 PyTorch CPU restatement of the reference's EM step (oracle/torch_port.py) on {threads} "
+              f"threads, batch {B}, median of {len(times)} steps")
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": args.gpus,
                       "steps": len(times), "warmup": warm, "ms_per_step": 1e3 * statistics.median(times),
-                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                      "data": "synthetic", "config": {"workload": WORKLOAD, "batch": B},
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic", "config": {"workload": WORKLOAD, "batch_per_gpu": B},
                       "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port",
                                        "sample": sample},
                       "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
@@ -537,7 +542,7 @@ def main():
                                            "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm}}
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
-        v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0)
+        v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0, batch=B)
         cpu = {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample}
         result = {
             "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,

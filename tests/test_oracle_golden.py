@@ -164,3 +164,26 @@ def test_oracle_evidence_free_flows_match_reference():
     assert np.abs(pf - t["param_flows"]).max() <= 1e-5 * np.abs(pf).max()
     ref_ipf = t["in_param_flows"][:ipf.shape[0]]
     assert np.abs(ipf - ref_ipf).max() <= 1e-5 * np.abs(ref_ipf).max()
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_torch_port_matches_oracle(name):
+    """The FP32 torch CPU restatement (CPU baseline and reference arm of bench.py) against the
+    FP64 oracle: log-likelihoods, parameter flows and the EM update."""
+    import torch
+    from oracle import torch_port as tp
+    fx = load_fixture(name)
+    lay = orc.layout_from_fixture(fx, ncats=NCATS[name])
+    tl = tp.TorchLayout(lay)
+    p0, q0 = torch.from_numpy(fx["params0"]), torch.from_numpy(fx["in_params0"])
+    x = torch.from_numpy(fx["x"])
+    nm, ems, lls = tp.forward(tl, p0, q0, x)
+    assert np.allclose(lls.numpy(), fx["lls"], rtol=1e-5, atol=1e-5)
+    pf, ipf = tp.backward(tl, p0, x, nm, ems)
+    assert np.abs(pf.numpy() - fx["param_flows"]).max() <= 1e-4 * np.abs(fx["param_flows"]).max()
+    ref_ipf = fx["in_param_flows"]
+    assert np.abs(ipf.numpy()[:ref_ipf.shape[0]] - ref_ipf).max() <= 1e-4 * np.abs(ref_ipf).max()
+    p1, q1 = tp.em_update(tl, p0, torch.from_numpy(fx["param_flows"]), q0, torch.from_numpy(fx["in_param_flows"]),
+                          0.1, 0.1)
+    assert np.abs(p1.numpy() - fx["params1"]).max() <= 1e-6
+    assert np.abs(q1.numpy()[:fx["in_params1"].shape[0]] - fx["in_params1"]).max() <= 1e-6
