@@ -129,7 +129,8 @@ int pcb_input_cat_fwd(const int64_t* data, int64_t data_ld, const float* params,
  * [0, ncats) are skipped. logspace_flows: node flows hold log flows. Where `missing`
  * (may be NULL; same indexing as pcb_input_cat_fwd) marks the variable as missing, the
  * node's flow f goes to every category k as f * params[s_pids[n] + k] (s_pids and params
- * are read only then; categorical.py:102-134).
+ * are read only then; categorical.py:102-134). atomic = 1 when several nodes share flow
+ * slots (tied nodes; the sums are then added with float atomics, as the reference does).
  * Replaces InputLayer._flows_kernel_template + Categorical.bk_flow_fn
  * (src/pyjuice/layer/input_layer.py:1098-1155, categorical.py:94-100), whose atomic
  * scatter this replaces with a per-variable counting sort of the batch.
@@ -139,7 +140,7 @@ int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const float* node_fl
                       const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
                       const int32_t* s_pfids, int32_t node_offset, float* param_flows,
                       int32_t logspace_flows, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
-                      const int32_t* s_pids, const float* params, void* stream);
+                      const int32_t* s_pids, const float* params, int32_t atomic, void* stream);
 
 /*
  * Categorical EM update of the source nodes (in FP64):

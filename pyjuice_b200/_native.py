@@ -95,7 +95,7 @@ _SIGS = {
                            c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
     "pcb_input_cat_bwd": ([c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
                            c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int64,
-                           c_void_p, c_void_p, c_void_p], c_int32),
+                           c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_input_cat_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double,
                           c_int32, c_void_p], c_int32),
     "pcb_pflow_accum": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),

@@ -74,7 +74,8 @@ input_cat_fwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 // up to CB samples; warp-parallel prefix sum of the category counts), then one warp per
 // node copies the node's flow row into shared memory with coalesced loads and sums it per
 // category in sample order, adding the sums to the node's flow slots. Deterministic: no
-// float atomics. Samples whose variable is missing (miss[b * m_sb + v * m_sv] != 0) form
+// float atomics (unless flow slots are shared by tied nodes of different variables:
+// atomic = 1 adds with atomics). Samples whose variable is missing (miss[b * m_sb + v * m_sv] != 0) form
 // their own segment: their flow sum M is spread over the categories as M * params[k]
 // (input_layer.py:537-571, categorical.py:102-134).
 __global__ void __launch_bounds__(256)
@@ -83,7 +84,7 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                      const int* __restrict__ grp_count, const int* __restrict__ grp_ncats,
                      const int* __restrict__ s_pfids, int node_offset, float* __restrict__ pf, bool logspace, int CB,
                      const uint8_t* __restrict__ miss, int64_t m_sb, int64_t m_sv, const int* __restrict__ s_pids,
-                     const float* __restrict__ params) {
+                     const float* __restrict__ params, bool atomic) {
     pcb::pdl_begin();
     extern __shared__ int smem[];
     const int g = blockIdx.x;
@@ -184,7 +185,7 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
 #pragma unroll
                 for (int j = 0; j < kR; ++j) {
                     const int k = k0 + lane + 32 * j;
-                    old[j] = (k < K) ? pf[sf + k] : 0.f;
+                    old[j] = (k < K && !atomic) ? pf[sf + k] : 0.f;
                 }
 #pragma unroll
                 for (int j = 0; j < kR; ++j) {
@@ -198,7 +199,8 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                         const float f = wrow[perm[p]];
                         acc += logspace ? __expf(f) : f;
                     }
-                    pf[sf + k] = old[j] + acc;
+                    if (atomic) atomicAdd(pf + sf + k, acc);  // slot shared by tied nodes
+                    else pf[sf + k] = old[j] + acc;
                 }
             }
             __syncwarp();  // the next node overwrites this warp's row
@@ -232,7 +234,7 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
                                  const int32_t* grp_ncats, int32_t num_groups, int32_t max_ncats,
                                  const int32_t* s_pfids, int32_t node_offset, float* param_flows,
                                  int32_t logspace_flows, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
-                                 const int32_t* s_pids, const float* params, void* stream) {
+                                 const int32_t* s_pids, const float* params, int32_t atomic, void* stream) {
     if (!data || !node_flows || !grp_var || !grp_node0 || !grp_count || !grp_ncats || !s_pfids || !param_flows ||
         B <= 0 || ld < B || data_ld < B || num_groups < 0 || max_ncats <= 0 || (missing && (!s_pids || !params)))
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: bad arguments");
@@ -247,6 +249,7 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
     return pcb::launch_status(pcb::launch_k(input_cat_bwd_kernel, dim3(num_groups), dim3(256), smem,
                                             pcb::as_stream(stream), 1u, data, data_ld, node_flows, ld, B, grp_var,
                                             grp_node0, grp_count, grp_ncats, s_pfids, node_offset, param_flows,
-                                            logspace_flows != 0, CB, missing, miss_sb, miss_sv, s_pids, params),
+                                            logspace_flows != 0, CB, missing, miss_sb, miss_sv, s_pids, params,
+                                            atomic != 0),
                               "pcb_input_cat_bwd");
 }

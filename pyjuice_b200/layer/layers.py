@@ -836,6 +836,7 @@ class InputLayer(Layer, torch.nn.Module):
                     ncats=_i32(ncats), source_nids=_i32(self.source_nids.cpu()),
                     grp_var=_i32(vids[starts]), grp_node0=_i32(starts), grp_count=_i32(counts),
                     grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), max_grp=int(counts.max()),
+                    shared_slots=bool(np.unique(self.s_pfids.cpu().numpy()).size < self.s_pfids.numel()),
                     tied=tied, var_ptr=var_ptr, var_nodes=order.astype(np.int64))
 
     def _init_parameters(self, perturbation: float = 2.0):
@@ -949,7 +950,7 @@ class InputLayer(Layer, torch.nn.Module):
                  nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
                  d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
                  nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.ptr(m), sb, sv, nat.ptr(d["s_pids"]),
-                 nat.ptr(self.params), nat.stream())
+                 nat.ptr(self.params), 1 if d["shared_slots"] else 0, nat.stream())
 
     def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
                       use_f64_flows: bool = False):
