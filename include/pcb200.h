@@ -154,6 +154,32 @@ int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_p
                      double step_size, double pseudocount, int32_t keep_zero_params, void* stream);
 
 /*
+ * Bernoulli (kind 1) and Gaussian (kind 2) input layers; data is FP32 [num_vars, data_ld]
+ * (Bernoulli reads x > 0), missing values indexed as in pcb_input_cat_fwd.
+ * pcb_input_dist_fwd: node_mars = log p (Bernoulli: p = params[s_pid] for x > 0, else 1 - p;
+ *   Gaussian: log N(x; params[s_pid], params[s_pid + 1])), 0 where missing.
+ * pcb_input_dist_bwd: per node, the batch sums of the flow-weighted sufficient statistics
+ *   added to its flow slots: Bernoulli (x > 0, x <= 0) (missing samples add nothing);
+ *   Gaussian (f x, f x^2, f), a missing value contributing (f mu, f (sigma^2 + mu^2), f).
+ *   atomic = 1 when tied nodes share slots. logspace_flows: node flows hold log flows.
+ * pcb_input_dist_em: Bernoulli p' = (1 - s) p + s (f1 + pc / 2) / (f1 + f0 + pc); Gaussian
+ *   moment matching of the step-interpolated expectation parameters, sigma >= min_sigma[n]
+ *   (per node, indexed by the node's layer-local id).
+ * Replace the fw_mar_fn / bk_flow_fn / bk_flow_mask_fn / em_fn kernels of
+ * src/pyjuice/nodes/distributions/bernoulli.py:64-102 and gaussian.py:87-170.
+ */
+int pcb_input_dist_fwd(int32_t kind, const float* data, int64_t data_ld, const float* params, const int32_t* vids,
+                       const int32_t* s_pids, int32_t num_nodes, int32_t node_offset, float* node_mars, int64_t ld,
+                       int32_t B, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv, void* stream);
+int pcb_input_dist_bwd(int32_t kind, const float* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,
+                       const float* params, const int32_t* vids, const int32_t* s_pids, const int32_t* s_pfids,
+                       int32_t num_nodes, int32_t node_offset, float* param_flows, int32_t logspace_flows,
+                       const uint8_t* missing, int64_t miss_sb, int64_t miss_sv, int32_t atomic, void* stream);
+int pcb_input_dist_em(int32_t kind, float* params, const float* param_flows, const int32_t* s_pids,
+                      const int32_t* s_pfids, const float* min_sigma, const int32_t* source_nids,
+                      int32_t num_source_nodes, double step_size, double pseudocount, void* stream);
+
+/*
  * Sum of tied input-node flow slots into the source slot:
  * param_flows[dst + i] = sum_j param_flows[srcs[j] + i], i < n.
  * Replaces InputLayer._pflow_accum_kernel (src/pyjuice/layer/input_layer.py:1254-1272)

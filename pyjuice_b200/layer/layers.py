@@ -770,8 +770,12 @@ class ProdLayer(Layer):
         return f"ProdLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
 
 
+_DIST_KIND = {"Categorical": 0, "Bernoulli": 1, "Gaussian": 2}
+
+
 class InputLayer(Layer, torch.nn.Module):
-    """A layer of Categorical input node vectors."""
+    """A layer of input node vectors of one distribution: Categorical (lookups, counting-sort
+    flows, soft evidence), Bernoulli or Gaussian (``input_dists.cu``)."""
 
     _tensor_lists = ()
 
@@ -781,8 +785,9 @@ class InputLayer(Layer, torch.nn.Module):
         c = compile_input_layer(nodes, cum_nodes, max_tied_ns_per_parflow_block)
         Layer.__init__(self, c["nodes"])
         self.pc_num_vars = pc_num_vars
-        if c["signature"] != "Categorical":
+        if c["signature"] not in _DIST_KIND:
             raise NotImplementedError(f"input distribution {c['signature']} has no CUDA path")
+        self.kind = _DIST_KIND[c["signature"]]
         if c["num_vars_per_node"] != 1:
             raise NotImplementedError("multivariate input nodes have no CUDA path")
         self._output_ind_range = c["nid_range"]
@@ -817,7 +822,12 @@ class InputLayer(Layer, torch.nn.Module):
 
     def _host_desc(self):
         vids = self.vids[:, 0].cpu().numpy()
-        ncats = self.metadata.cpu()[self.s_mids.cpu()].long().numpy()
+        meta = self.metadata.cpu()
+        if self.kind == 0:
+            ncats = meta[self.s_mids.cpu()].long().numpy()
+        else:
+            ncats = np.ones(vids.shape[0], np.int64)
+        min_sigma = (meta[self.s_mids.cpu()].float() if self.kind == 2 else torch.zeros([vids.shape[0]]))
         # runs of consecutive nodes over the same variable
         change = np.ones(vids.shape[0], dtype=bool)
         change[1:] = vids[1:] != vids[:-1]
@@ -837,6 +847,7 @@ class InputLayer(Layer, torch.nn.Module):
                     grp_var=_i32(vids[starts]), grp_node0=_i32(starts), grp_count=_i32(counts),
                     grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), max_grp=int(counts.max()),
                     shared_slots=bool(np.unique(self.s_pfids.cpu().numpy()).size < self.s_pfids.numel()),
+                    min_sigma=min_sigma.contiguous(),
                     tied=tied, var_ptr=var_ptr, var_nodes=order.astype(np.int64))
 
     def _init_parameters(self, perturbation: float = 2.0):
@@ -880,11 +891,19 @@ class InputLayer(Layer, torch.nn.Module):
         if params is not None:
             raise NotImplementedError("external input parameters have no CUDA path")
         d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        m, sb, sv = self._mask_args(missing_mask, B, node_mars.device, _batch_first)
+        if self.kind != 0:
+            xf = data.to(torch.float32)
+            if xf.stride(1) != 1:
+                xf = xf.contiguous()
+            nat.call("pcb_input_dist_fwd", self.kind, nat.ptr(xf), xf.stride(0), nat.ptr(self.params),
+                     nat.ptr(d["vids"]), nat.ptr(d["s_pids"]), self.num_nodes, self._output_ind_range[0],
+                     nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+            return
         data = data.to(torch.long)
         if data.stride(1) != 1:
             data = data.contiguous()
-        B = node_mars.size(1)
-        m, sb, sv = self._mask_args(missing_mask, B, node_mars.device, _batch_first)
         nat.call("pcb_input_cat_fwd", nat.ptr(data), data.stride(0), nat.ptr(self.params), nat.ptr(d["vids"]),
                  nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), self.num_nodes, self._output_ind_range[0],
                  nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
@@ -893,6 +912,8 @@ class InputLayer(Layer, torch.nn.Module):
                      _batch_first: bool = True, **kwargs):
         """Soft evidence ``[B, num_vars, num_cats]`` (FP32, entries in [0, 1]):
         ``node_mars = min(log sum_k E[b, v, k] theta[n, k], 0)`` (conditional.py:25-68, 108-111)."""
+        if self.kind != 0:
+            raise NotImplementedError("soft evidence is defined for Categorical input layers")
         if evidence.dim() != 3 or evidence.dtype != torch.float32:
             raise ValueError("soft evidence must be a float32 [B, num_vars, num_cats] tensor")
         d = self._desc(node_mars.device)
@@ -911,6 +932,8 @@ class InputLayer(Layer, torch.nn.Module):
         """``[B, T, max_ncats]``: per target variable and category, ``sum_n W[n, b] theta[n, k]``
         over the variable's nodes, W = node flows (mode 0) or node flows / exp(node_mars)
         (mode 1, the derivative of the weighted log-likelihood with respect to soft evidence)."""
+        if self.kind != 0:
+            raise NotImplementedError("per-category evidence quantities are defined for Categorical input layers")
         d = self._desc(node_flows.device)
         B = node_flows.size(1)
         nv = d["var_ptr"].shape[0] - 1
@@ -941,11 +964,20 @@ class InputLayer(Layer, torch.nn.Module):
         d = self._desc(node_flows.device)
         if self.param_flows is None:
             self.init_param_flows(0.0)
+        B = node_flows.size(1)
+        m, sb, sv = self._mask_args(missing_mask, B, node_flows.device, _batch_first)
+        if self.kind != 0:
+            xf = data.to(torch.float32)
+            if xf.stride(1) != 1:
+                xf = xf.contiguous()
+            nat.call("pcb_input_dist_bwd", self.kind, nat.ptr(xf), xf.stride(0), nat.ptr(node_flows),
+                     node_flows.stride(0), B, nat.ptr(self.params), nat.ptr(d["vids"]), nat.ptr(d["s_pids"]),
+                     nat.ptr(d["s_pfids"]), self.num_nodes, self._output_ind_range[0], nat.ptr(self.param_flows),
+                     1 if logspace_flows else 0, nat.ptr(m), sb, sv, 1 if d["shared_slots"] else 0, nat.stream())
+            return
         data = data.to(torch.long)
         if data.stride(1) != 1:
             data = data.contiguous()
-        B = node_flows.size(1)
-        m, sb, sv = self._mask_args(missing_mask, B, node_flows.device, _batch_first)
         nat.call("pcb_input_cat_bwd", nat.ptr(data), data.stride(0), nat.ptr(node_flows), node_flows.stride(0), B,
                  nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
                  d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
@@ -961,6 +993,13 @@ class InputLayer(Layer, torch.nn.Module):
         for dst, n, ch in d["tied"]:
             nat.call("pcb_pflow_accum_f64" if use_f64_flows else "pcb_pflow_accum", nat.ptr(pf), dst, n, nat.ptr(ch),
                      ch.size(0), nat.stream())
+        if self.kind != 0:
+            if use_f64_flows:
+                raise NotImplementedError("FP64 epoch flows are kept for Categorical input layers")
+            nat.call("pcb_input_dist_em", self.kind, nat.ptr(self.params), nat.ptr(pf), nat.ptr(d["s_pids"]),
+                     nat.ptr(d["s_pfids"]), nat.ptr(d["min_sigma"]), nat.ptr(d["source_nids"]),
+                     d["source_nids"].size(0), float(step_size), float(pseudocount), nat.stream())
+            return
         nat.call("pcb_input_cat_em_f64flows" if use_f64_flows else "pcb_input_cat_em", nat.ptr(self.params),
                  nat.ptr(pf), nat.ptr(d["s_pids"]), nat.ptr(d["s_pfids"]), nat.ptr(d["ncats"]),
                  nat.ptr(d["source_nids"]), d["source_nids"].size(0), float(step_size), float(pseudocount),

@@ -602,7 +602,7 @@ class TensorCircuit(nn.Module):
             if input_layer_fn is None:
                 if inputs.dim() != 2:
                     raise ValueError("inputs must be [B, num_vars]")
-                data = inputs.permute(1, 0).to(self.device, torch.long).contiguous()
+                data = inputs.permute(1, 0).to(self.device).contiguous()
             nm = self._buffer("node_mars", self.num_nodes, B, 0.0)
             em = self._buffer("element_mars", self.num_elements, B, -float("inf"))
             # dummy rows of every region keep their initial -inf (nothing writes them)
@@ -767,7 +767,7 @@ class TensorCircuit(nn.Module):
             if input_layer_fn is None:
                 if inputs is None or inputs.dim() != 2 or inputs.size(1) != self.num_vars:
                     raise ValueError("inputs must be [B, num_vars]")
-                data = inputs.permute(1, 0).to(self.device, torch.long).contiguous()
+                data = inputs.permute(1, 0).to(self.device).contiguous()
             init = -float("inf") if logspace_flows else 0.0
             nf = self._buffer("node_flows", self.num_nodes, B, init)
             ef = self._buffer("element_flows", self.num_elements, B, init)

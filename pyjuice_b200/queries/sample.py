@@ -56,6 +56,8 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
         raise ValueError("It is ambiguous to sample from multi-head PCs.")
     if pc.device.type != "cuda":
         raise RuntimeError("sampling runs on CUDA only")
+    if any(getattr(layer, "kind", 0) != 0 for layer in pc.input_layer_group):
+        raise NotImplementedError("the device sampler draws Categorical inputs only")
     if seed is None:
         seed = random.randint(0, 2 ** 62)
     dev = pc.device

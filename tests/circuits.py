@@ -83,3 +83,14 @@ def build_layer_test_nodes(juice, dists, block_size: int = 16):
         ns1 = juice.summate(np1, num_node_blocks=2)
         ns2 = juice.summate(np2, num_node_blocks=2)
     return ni, [np0, np1, np2], [ns0, ns1, ns2]
+
+
+def build_dist_dag(juice, dist_factory):
+    """Four variables with input vectors of one distribution (``dist_factory()`` per vector),
+    two sums over pairs and a block-size-1 root: exercises a non-Categorical input layer."""
+    with juice.set_block_size(4):
+        i = [juice.inputs(v, num_node_blocks=2, dist=dist_factory()) for v in range(4)]
+        s01 = juice.summate(juice.multiply(i[0], i[1]), num_node_blocks=2)
+        s23 = juice.summate(juice.multiply(i[2], i[3]), num_node_blocks=2)
+        root = juice.summate(juice.multiply(s01, s23), num_node_blocks=1, block_size=1)
+    return root

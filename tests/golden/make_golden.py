@@ -32,6 +32,8 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``structures.npz`` compiled layouts, parameters and log-likelihoods of the reference's PD
                     (3 x 3 grid) and homogeneous HMM (length 6) generators; flows and one EM
                     step of the HMM (tied transitions and emissions);
+* ``dists.npz``      Bernoulli and Gaussian input layers (four-variable circuit): one FP32
+                    forward / backward / EM step;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -416,6 +418,34 @@ def make_structures():
     np.savez_compressed(os.path.join(HERE, "structures.npz"), **out)
 
 
+def make_dist_variants():
+    """Bernoulli and Gaussian input layers on a four-variable circuit (circuits.build_dist_dag):
+    FP32 forward, backward and mini_batch_em(0.3, 0.1) by the reference, with seeded parameters
+    and data (bool data for Bernoulli, N(0, 1.5) data for Gaussian)."""
+    from circuits import build_dist_dag
+    out = {}
+    rng = np.random.default_rng(21)
+    for name, factory, data in (
+            ("bern", lambda: dists.Bernoulli(), torch.from_numpy(rng.random((32, 4)) < 0.4)),
+            ("gauss", lambda: dists.Gaussian(mu=0.0, sigma=1.0),
+             torch.from_numpy((1.5 * rng.standard_normal((32, 4))).astype(np.float32)))):
+        torch.manual_seed(11)
+        pc = juice.compile(build_dist_dag(juice, factory), verbose=False)
+        out[name + "_params0"] = pc.params.detach().numpy().copy()
+        out[name + "_in_params0"] = pc.input_layer_group[0].params.detach().numpy().copy()
+        out[name + "_x"] = data.numpy()
+        pc.init_param_flows(flows_memory=0.0)
+        lls = pc(data, force_use_fp32=True)
+        out[name + "_lls"] = lls.detach().numpy().copy()
+        lls.mean().backward()
+        out[name + "_param_flows"] = pc.param_flows.detach().numpy().copy()
+        out[name + "_in_param_flows"] = pc.input_layer_group[0].param_flows.detach().numpy().copy()
+        pc.mini_batch_em(step_size=0.3, pseudocount=0.1)
+        out[name + "_params1"] = pc.params.detach().numpy().copy()
+        out[name + "_in_params1"] = pc.input_layer_group[0].params.detach().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "dists.npz"), **out)
+
+
 SAMPLE_SEED = 20261204  # seed of the uniform table (oracle.pc_oracle.uniform_table)
 SAMPLE_S = 256
 
@@ -455,11 +485,12 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny", "structures"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny", "structures", "dists"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
          "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants,
-         "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants, "structures": make_structures}[w]()
+         "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants, "structures": make_structures,
+         "dists": make_dist_variants}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

@@ -381,3 +381,31 @@ def test_pd_and_hmm_match_reference(cuda_device):
     assert np.abs(pc.params.cpu().numpy() - hm["params1"]).max() <= 1e-5
     q1 = hm["in_params1"]
     assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["bern", "gauss"])
+def test_bernoulli_and_gaussian_layers_match_reference(name, cuda_device):
+    """Bernoulli and Gaussian input layers: FP32 forward, flows and one EM step against the
+    reference's own outputs (dists.npz; four-variable circuit, seeded parameters and data)."""
+    from circuits import build_dist_dag
+    fx = load_fixture("dists")
+    g = lambda k: fx[f"{name}_{k}"]
+    factory = (lambda: juice.distributions.Bernoulli()) if name == "bern" else \
+        (lambda: juice.distributions.Gaussian(mu=0.0, sigma=1.0))
+    pc = juice.compile(build_dist_dag(juice, factory)).to(cuda_device)
+    with torch.no_grad():
+        pc.params.copy_(torch.from_numpy(g("params0")).to(cuda_device))
+        pc.input_layer_group[0].params.copy_(torch.from_numpy(g("in_params0")).to(cuda_device))
+    x = torch.from_numpy(g("x")).to(cuda_device)
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(x, force_use_fp32=True)
+    ref = g("lls")
+    assert np.all(np.abs(lls.detach().cpu().numpy() - ref) <= 1e-5 * np.abs(ref) + 1e-5)
+    lls.mean().backward()
+    assert _rel(pc.param_flows.cpu().numpy(), g("param_flows")) <= 1e-4
+    ipf = g("in_param_flows")
+    assert _rel(pc.input_layer_group[0].param_flows.cpu().numpy()[:ipf.shape[0]], ipf) <= 1e-4
+    pc.mini_batch_em(step_size=0.3, pseudocount=0.1)
+    assert np.abs(pc.params.cpu().numpy() - g("params1")).max() <= 1e-5
+    q1 = g("in_params1")
+    assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-4 * max(1.0, np.abs(q1).max())
