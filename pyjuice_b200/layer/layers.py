@@ -19,6 +19,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 import torch
 
+from ctypes import c_void_p
+
 from .. import _native as nat
 from ..autotune import TUNER
 from .compilation import compile_prod_layer, compile_sum_layer
@@ -219,6 +221,52 @@ class Layer:
     def _host_desc(self):
         raise NotImplementedError()
 
+    # ---- partial evaluation (layer.py:38-75): only the node vectors whose scope is one of the
+    # given scopes are evaluated; the other rows keep their values
+    _fw_partial = None
+    _bk_partial = None
+
+    @staticmethod
+    def _ranges(node_vectors, scopes) -> list:
+        """Output-row ranges of the node vectors whose scope is in ``scopes``."""
+        return [ns._output_ind_range for ns in node_vectors if ns.scope in scopes]
+
+    @staticmethod
+    def _keep_rows(first_rows, ranges) -> np.ndarray:
+        first_rows = np.asarray(first_rows, np.int64).reshape(-1)
+        keep = np.zeros(first_rows.shape[0], dtype=bool)
+        for lo, hi in ranges:
+            keep |= (first_rows >= lo) & (first_rows < hi)
+        return keep
+
+    def _partial(self, which: str, device: torch.device):
+        """The device copy of a partial-evaluation table set (``_fw_partial`` / ``_bk_partial``)."""
+        host = self._fw_partial if which == "fw" else self._bk_partial
+        if host is None:
+            return None
+        key = (which, device.type, device.index, id(host))
+        cache = self.__dict__.setdefault("_partial_dev", {})
+        t = cache.get(key)
+        if t is None:
+            def mv(v):
+                if isinstance(v, torch.Tensor):
+                    return v.to(device)
+                if isinstance(v, list):
+                    return [mv(x) for x in v]
+                if isinstance(v, dict):
+                    return {kk: mv(vv) for kk, vv in v.items()}
+                return v
+            t = mv(host)
+            cache.clear()
+            cache[key] = t
+        return t
+
+    def disable_partial_evaluation(self, forward: bool = True, backward: bool = True):
+        if forward:
+            self._fw_partial = None
+        if backward:
+            self._bk_partial = None
+
     def to(self, device):
         device = torch.device(device)
         for name in self._tensor_lists:
@@ -389,6 +437,29 @@ class SumLayer(Layer):
             el_groups=el_groups,
         )
 
+    def enable_partial_evaluation(self, fw_scopes=None, bk_scopes=None):
+        """Tile subsets for the node vectors with the given scopes: forward tiles of those
+        sum vectors; backward element-flow tiles of their product children (rows = elements)
+        and parameter-flow tiles of the sum vectors."""
+        d = self._host_desc()
+        if fw_scopes is not None:
+            rng = self._ranges(self.nodes, set(fw_scopes))
+            t = d["fw_tiles"]
+            self._fw_partial = dict(tiles=t[torch.from_numpy(self._keep_rows(t[:, 0].numpy(), rng))].contiguous())
+        if bk_scopes is not None:
+            scopes = set(bk_scopes)
+            rng = self._ranges(self.nodes, scopes)
+            prods = []
+            for ns in self.nodes:
+                for cs in ns.chs:
+                    if cs not in prods:
+                        prods.append(cs)
+            erng = self._ranges(prods, scopes)
+            el = [eg["tiles"][torch.from_numpy(self._keep_rows(eg["tiles"][:, 0].numpy(), erng))].contiguous()
+                  for eg in d["el_groups"]]
+            pt = d["pf_tiles"]
+            self._bk_partial = dict(el=el, pf=pt[torch.from_numpy(self._keep_rows(pt[:, 0].numpy(), rng))].contiguous())
+
     # ---- forward / backward ----
     def _use_bf16(self, d, B, force_use_bf16, force_use_fp32):
         if force_use_bf16 and force_use_fp32:
@@ -503,6 +574,23 @@ class SumLayer(Layer):
         prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
         t = d["fw_tiles"]
         st = nat.stream()
+        part = self._partial("fw", node_mars.device)
+        if part is not None:
+            # a subset of the tiles: the kernels that read the weights directly (the packed
+            # weights are indexed by the full table's tile numbers)
+            t = part["tiles"]
+            if t.size(0) == 0:
+                return
+            if d["fw_short"] and SumLayer.short_kernels:
+                nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
+                         nat.ptr(node_mars), ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"],
+                         self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(None),
+                         d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B), nat.ptr(None), st)
+            else:
+                nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
+                         ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size,
+                         nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, st)
+            return
         if tc05:
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
@@ -555,6 +643,11 @@ class SumLayer(Layer):
                 raise ValueError("these flow modes read unmodified node flows: pass allow_modify_flows=False")
             self._backward_generic(node_flows, element_flows, node_mars, element_mars, params, param_flows,
                                    propagation_alg, logspace_flows, negate_pflows, accumulate_ch_flows, kwargs)
+            return
+        part = self._partial("bk", node_mars.device)
+        if part is not None:
+            self._backward_partial(part, node_flows, element_flows, node_mars, element_mars, params, param_flows,
+                                   force_use_fp32)
             return
         if allow_modify_flows and not kwargs.get("_flows_modified"):
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
@@ -613,6 +706,34 @@ class SumLayer(Layer):
             with torch.cuda.stream(pflow_stream if ready is not None else torch.cuda.current_stream()):
                 self.param_flows_only(node_flows, node_mars, element_mars, params, param_flows,
                                       allow_modify_flows=allow_modify_flows, force_use_fp32=force_use_fp32)
+
+    def _backward_partial(self, part, node_flows, element_flows, node_mars, element_mars, params, param_flows,
+                          force_use_fp32):
+        """Element flows of the selected elements and parameter flows of the selected nodes,
+        on the kernels that read the weights directly (unmodified node flows)."""
+        d = self._desc(node_mars.device)
+        B = node_mars.size(1)
+        ld = node_mars.stride(0)
+        st = nat.stream()
+        for eg, et in zip(d["el_groups"], part["el"]):
+            if et.size(0) == 0:
+                continue
+            prec = self._el_prec(eg, B, force_use_fp32)
+            if eg["short"] and SumLayer.short_kernels:
+                nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
+                         nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0), eg["tm"], eg["cbs"],
+                         nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size, 2, prec, nat.ptr(None),
+                         eg["wlayout"], _short_batch_tile(et.size(0), eg["tm"], B), nat.ptr(None), st)
+            else:
+                nat.call("pcb_lse_contract", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
+                         nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0), eg["tm"], eg["cbs"],
+                         nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size, 2, prec, st)
+        pt = part["pf"]
+        if param_flows is not None and pt.size(0) > 0:
+            prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
+            nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
+                     nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size,
+                     nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 0, 1 if self._has_tied else 0, 64, prec, st)
 
     def _backward_generic(self, node_flows, element_flows, node_mars, element_mars, params, param_flows,
                           propagation_alg, logspace_flows, negate_pflows, accumulate_ch_flows, kwargs):
@@ -734,8 +855,33 @@ class ProdLayer(Layer):
         return dict(fw_row=fr, fw_off=fo, fw_cnt=fc, fw_chs=fch, bk_row=br, bk_off=bo, bk_cnt=bc, bk_chs=bch,
                     elem2blk=_i32(elem2blk))
 
+    def enable_partial_evaluation(self, fw_scopes=None, bk_scopes=None):
+        """Block subsets: forward blocks of the product vectors with the given scopes, backward
+        blocks writing the child vectors with the given scopes."""
+        d = self._host_desc()
+
+        def subset(prefix, keep):
+            k = torch.from_numpy(keep)
+            rows, offs, cnts = d[prefix + "_row"], d[prefix + "_off"], d[prefix + "_cnt"]
+            return dict(row=rows[k].contiguous(), off=offs[k].contiguous(), cnt=cnts[k].contiguous(),
+                        chs=d[prefix + "_chs"])
+        if fw_scopes is not None:
+            rng = self._ranges(self.nodes, set(fw_scopes))
+            self._fw_partial = subset("fw", self._keep_rows(d["fw_row"].numpy(), rng))
+        if bk_scopes is not None:
+            kids = []
+            for ns in self.nodes:
+                for cs in ns.chs:
+                    if cs not in kids:
+                        kids.append(cs)
+            rng = self._ranges(kids, set(bk_scopes))
+            self._bk_partial = subset("bk", self._keep_rows(d["bk_row"].numpy(), rng))
+
     def forward(self, node_mars: torch.Tensor, element_mars: torch.Tensor, _for_backward: bool = False, **kwargs):
         d = self._desc(node_mars.device)
+        part = self._partial("fw", node_mars.device)
+        if part is not None:
+            d = dict(fw_row=part["row"], fw_off=part["off"], fw_cnt=part["cnt"], fw_chs=part["chs"])
         B = node_mars.size(1)
         ld = node_mars.stride(0)
         if element_mars.stride(0) != ld:
@@ -752,6 +898,15 @@ class ProdLayer(Layer):
         ld = node_flows.stride(0)
         if element_flows.stride(0) != ld:
             raise ValueError("node_flows and element_flows must share a row-major layout")
+        part = self._partial("bk", node_flows.device)
+        if part is not None:
+            if part["row"].size(0) == 0:
+                return
+            # the selected child rows only; accumulate (they may also be written by other layers)
+            nat.call("pcb_prod_gather_sum", nat.ptr(element_flows), nat.ptr(node_flows), ld, B, nat.ptr(part["row"]),
+                     nat.ptr(part["off"]), nat.ptr(part["cnt"]), nat.ptr(part["chs"]), part["row"].size(0),
+                     self.block_size, 1 if self.bk_accumulate else 0, 1 if logspace_flows else 0, nat.stream())
+            return
         # _modify = (node_mars, block flags): the flows of the flagged child blocks are written
         # as log f - log m (what the sum layer below would rewrite them to); overwrite mode only
         mod = kwargs.get("_modify")
@@ -904,9 +1059,13 @@ class InputLayer(Layer, torch.nn.Module):
         data = data.to(torch.long)
         if data.stride(1) != 1:
             data = data.contiguous()
-        nat.call("pcb_input_cat_fwd", nat.ptr(data), data.stride(0), nat.ptr(self.params), nat.ptr(d["vids"]),
-                 nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), self.num_nodes, self._output_ind_range[0],
-                 nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+        part = self._partial("fw", node_mars.device)
+        runs = [(0, self.num_nodes)] if part is None else part["runs"]
+        for n0, cnt in runs:  # the node tables are passed from the run's first node on
+            nat.call("pcb_input_cat_fwd", nat.ptr(data), data.stride(0), nat.ptr(self.params),
+                     c_void_p(d["vids"].data_ptr() + 4 * n0), c_void_p(d["s_pids"].data_ptr() + 4 * n0),
+                     c_void_p(d["ncats"].data_ptr() + 4 * n0), cnt, self._output_ind_range[0] + n0,
+                     nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
 
     def forward_soft(self, evidence: torch.Tensor, node_mars: torch.Tensor, missing_mask=None,
                      _batch_first: bool = True, **kwargs):
@@ -926,6 +1085,28 @@ class InputLayer(Layer, torch.nn.Module):
                  nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
                  d["grp_var"].size(0), d["max_grp"], nat.ptr(d["s_pids"]), self._output_ind_range[0],
                  nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+
+    def enable_partial_evaluation(self, fw_scopes=None, bk_scopes=None):
+        """Node subsets of the input vectors with the given scopes: runs of consecutive nodes
+        (forward) and the variable groups (backward) that hold them."""
+        d = self._host_desc()
+        start = self._output_ind_range[0]
+
+        def node_runs(scopes):
+            runs = []
+            for lo, hi in self._ranges(self.nodes, set(scopes)):
+                runs.append((lo - start, hi - lo))
+            return runs
+        if fw_scopes is not None:
+            self._fw_partial = dict(runs=node_runs(fw_scopes))
+        if bk_scopes is not None:
+            keep = np.zeros(d["grp_var"].numel(), dtype=bool)
+            g0, gc = d["grp_node0"].numpy(), d["grp_count"].numpy()
+            for n0, cnt in node_runs(bk_scopes):
+                keep |= (g0 >= n0) & (g0 < n0 + cnt)
+            k = torch.from_numpy(keep)
+            self._bk_partial = {name: d[name][k].contiguous() for name in ("grp_var", "grp_node0", "grp_count",
+                                                                          "grp_ncats")}
 
     def evidence_backward(self, node_flows: torch.Tensor, node_mars: Optional[torch.Tensor] = None,
                           target_vars=None, mode: int = 0) -> torch.Tensor:
@@ -978,9 +1159,12 @@ class InputLayer(Layer, torch.nn.Module):
         data = data.to(torch.long)
         if data.stride(1) != 1:
             data = data.contiguous()
+        g = self._partial("bk", node_flows.device) or d
+        if g["grp_var"].numel() == 0:
+            return
         nat.call("pcb_input_cat_bwd", nat.ptr(data), data.stride(0), nat.ptr(node_flows), node_flows.stride(0), B,
-                 nat.ptr(d["grp_var"]), nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), nat.ptr(d["grp_ncats"]),
-                 d["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
+                 nat.ptr(g["grp_var"]), nat.ptr(g["grp_node0"]), nat.ptr(g["grp_count"]), nat.ptr(g["grp_ncats"]),
+                 g["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
                  nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.ptr(m), sb, sv, nat.ptr(d["s_pids"]),
                  nat.ptr(self.params), 1 if d["shared_slots"] else 0, nat.stream())
 
@@ -1062,6 +1246,14 @@ class LayerGroup:
     def backward(self, *args, **kwargs):
         for l in self.layers:
             l.backward(*args, **kwargs)
+
+    def enable_partial_evaluation(self, fw_scopes=None, bk_scopes=None):
+        for l in self.layers:
+            l.enable_partial_evaluation(fw_scopes=fw_scopes, bk_scopes=bk_scopes)
+
+    def disable_partial_evaluation(self, forward: bool = True, backward: bool = True):
+        for l in self.layers:
+            l.disable_partial_evaluation(forward=forward, backward=backward)
 
     def callback(self, fn, *args, **kwargs):
         if fn is not None:

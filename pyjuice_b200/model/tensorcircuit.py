@@ -93,6 +93,9 @@ class TensorCircuit(nn.Module):
         self._dev_tables = {}
         self._pack_tables = {}
         self._param_epoch = 0      # bumped by every in-library write of the sum parameters
+        self._fw_partial_eval_enabled = False
+        self._bk_partial_eval_enabled = False
+        self._partial_epoch = 0    # bumped whenever partial evaluation is switched
         self._el_pack_state = None  # parameters and pass settings the element-flow packs were made for
         if device is not None:
             self.to(device)
@@ -563,7 +566,8 @@ class TensorCircuit(nn.Module):
         for gi, group in enumerate(groups):
             alg = propagation_alg if isinstance(propagation_alg, str) else propagation_alg[gi]
             if group.is_prod():
-                fused = (gi + 1 < len(groups) and self._fusion_tables(gi, "fw") is not None and
+                fused = (not self._fw_partial_eval_enabled and gi + 1 < len(groups) and
+                         self._fusion_tables(gi, "fw") is not None and
                          groups[gi + 1][0].runs_single_stage(self.device, B, force_use_bf16, force_use_fp32))
                 if not fused:  # else the next sum layer computes (and writes) these element values
                     group(self.node_mars, self._em_view(gi))
@@ -571,7 +575,7 @@ class TensorCircuit(nn.Module):
                 if gi in fw_groups and fw_ready is not None:
                     main.wait_event(fw_ready)
                     fw_ready = None
-                fz = self._fusion_tables(gi - 1, "fw")
+                fz = None if self._fw_partial_eval_enabled else self._fusion_tables(gi - 1, "fw")
                 if fz is not None and not group[0].runs_single_stage(self.device, B, force_use_bf16, force_use_fp32):
                     fz = None
                 if alg != "LL" and fz is not None:  # the fused kernels run LL only
@@ -623,7 +627,7 @@ class TensorCircuit(nn.Module):
                         if not ret and ret is not None:
                             layer(data, nm, **kwargs)
             sig = (0, id(nm), id(em), id(self._em_resident), id(self.params), B, force_use_bf16, force_use_fp32,
-                   propagation_alg, kwargs.get("alpha"))
+                   propagation_alg, kwargs.get("alpha"), self._partial_epoch)
             run = partial(self._run_inner_forward, force_use_bf16, force_use_fp32, propagation_alg, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
                 self._recorded_cuda_graphs[sig] = self._capture(run)
@@ -687,7 +691,7 @@ class TensorCircuit(nn.Module):
         kwargs = dict(kwargs, _weights_packed=True)
         plain = (propagation_alg == "LL" if isinstance(propagation_alg, str) else
                  all(a == "LL" for a in propagation_alg)) and not negate_pflows and not logspace_flows and \
-            not kwargs.get("allow_neg_flows")
+            not kwargs.get("allow_neg_flows") and not self._bk_partial_eval_enabled
         turn = 0
         def rewrites(g):  # large layers rewrite their node flows as log f - log m
             return allow_modify_flows and any(
@@ -754,7 +758,7 @@ class TensorCircuit(nn.Module):
             raise ValueError("`allow_modify_flows` should be set to `False` when using `logspace_flows`.")
         if not isinstance(propagation_alg, str):
             propagation_alg = tuple(propagation_alg)
-        if propagation_alg != "LL" or negate_pflows or kwargs.get("allow_neg_flows"):
+        if propagation_alg != "LL" or negate_pflows or kwargs.get("allow_neg_flows") or self._bk_partial_eval_enabled:
             # the kernels of these modes read unmodified node flows (the results are the same)
             allow_modify_flows = False
         if sum_layer_pre_backward_callback is not None or sum_layer_post_backward_callback is not None:
@@ -800,7 +804,7 @@ class TensorCircuit(nn.Module):
                 self.init_param_flows(flows_memory=flows_memory)
             sig = (1, id(nf), id(ef), id(self.node_mars), id(self._em_resident), id(self.params),
                    id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows,
-                   propagation_alg, negate_pflows, kwargs.get("alpha"))
+                   propagation_alg, negate_pflows, kwargs.get("alpha"), self._partial_epoch)
             run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,
                           force_use_fp32, propagation_alg=propagation_alg, negate_pflows=negate_pflows, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
@@ -1022,6 +1026,38 @@ class TensorCircuit(nn.Module):
                         param_flows=None, allow_modify_flows=False, force_use_fp32=True)
                     return self.element_flows[nsid:neid, :].detach()
         raise ValueError("node not found in the circuit")
+
+    def enable_partial_evaluation(self, scopes, forward: bool = False, backward: bool = False, overwrite: bool = False):
+        """Evaluate only the node vectors whose scope is one of ``scopes`` (BitSets, or variable
+        ids for single-variable scopes) in later forward and/or backward passes; every other
+        row keeps its value (tensorcircuit.py:815-841). Typical use: after a full pass with
+        ``return_cache=True``, change some variables and re-run with the scopes that contain
+        them (``nodes.get_subsumed_scopes``) and ``cache=``."""
+        from ..nodes.scope import BitSet
+        if not overwrite and ((forward and self._fw_partial_eval_enabled) or
+                              (backward and self._bk_partial_eval_enabled)):
+            raise RuntimeError("Partial evaluation already enabled, consider calling `disable_partial_evaluation` first.")
+        scopes = [BitSet.from_array([v]) if isinstance(v, int) else v for v in scopes]
+        fw = scopes if forward else None
+        bk = scopes if backward else None
+        for layer in self.input_layer_group:
+            layer.enable_partial_evaluation(fw_scopes=fw, bk_scopes=bk)
+        for group in self.inner_layer_groups:
+            group.enable_partial_evaluation(fw_scopes=fw, bk_scopes=bk)
+        self._fw_partial_eval_enabled |= forward
+        self._bk_partial_eval_enabled |= backward
+        self._partial_epoch += 1
+
+    def disable_partial_evaluation(self, forward: bool = True, backward: bool = True):
+        for layer in self.input_layer_group:
+            layer.disable_partial_evaluation(forward=forward, backward=backward)
+        for group in self.inner_layer_groups:
+            group.disable_partial_evaluation(forward=forward, backward=backward)
+        if forward:
+            self._fw_partial_eval_enabled = False
+        if backward:
+            self._bk_partial_eval_enabled = False
+        self._partial_epoch += 1
 
     def layers(self, reverse: bool = False, ret_layer_groups: bool = False, ignore_input_layers: bool = False):
         groups = ([] if ignore_input_layers else [self.input_layer_group]) + list(self.inner_layer_groups)

@@ -5,3 +5,4 @@ from .prod_nodes import ProdNodes
 from .sum_nodes import SumNodes
 from .construction import inputs, multiply, summate, set_block_size
 from . import distributions
+from .methods import get_subsumed_scopes

@@ -117,3 +117,45 @@ def test_circuit_ll_adjoint_vs_central_differences(sign, cuda_device):
         d[b, v, k] = h
         fd = (f(z32, e32 + d) - f(z32, e32 - d)) / (2 * h)
         assert abs(ge[b, v, k] - fd) <= 2e-3 * max(abs(fd), 1e-2), ((b, v, k), ge[b, v, k], fd)
+
+
+@pytest.mark.parametrize("name", ["tiny", "hclt64"])
+def test_partial_evaluation(name, cuda_device):
+    """After a full pass, changing one variable and re-evaluating only the node vectors whose
+    scope contains it (forward, from the cached node values) gives the full pass's
+    log-likelihoods; a partial backward pass over the same scopes gives the full pass's flows
+    of those input nodes."""
+    from pyjuice_b200.nodes import get_subsumed_scopes
+    fx = load_fixture(name)
+    pc = build_fixture_circuit(name, fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(fx["x"][:64]).to(cuda_device)
+    K = 4
+    v = 2
+    with torch.no_grad():
+        _, cache = pc(x, force_use_fp32=True, return_cache=True)
+    x2 = x.clone()
+    x2[:, v] = (x2[:, v] + 1) % K
+    scopes = get_subsumed_scopes(pc, [v])
+    pc.enable_partial_evaluation(scopes, forward=True)
+    with torch.no_grad():
+        part = pc(x2, force_use_fp32=True, cache=cache).clone()
+    pc.disable_partial_evaluation()
+    with torch.no_grad():
+        full = pc(x2, force_use_fp32=True)
+    assert torch.allclose(part, full, rtol=1e-6, atol=1e-5)
+    # backward: full pass, then partial over the same scopes
+    pc.init_param_flows(flows_memory=0.0)
+    pc.backward(inputs=x2, allow_modify_flows=False, force_use_fp32=True)
+    il = pc.input_layer_group[0]
+    lo, hi = il._output_ind_range
+    sel = (il.vids[:, 0] == v).nonzero().view(-1) + lo
+    nf_full = pc.node_flows[sel].clone()
+    ipf_full = il.param_flows.clone()
+    pc.enable_partial_evaluation(scopes, backward=True)
+    pc.init_param_flows(flows_memory=0.0)
+    pc.backward(inputs=x2, force_use_fp32=True)
+    pc.disable_partial_evaluation()
+    assert torch.allclose(pc.node_flows[sel], nf_full, rtol=1e-5, atol=1e-6)
+    slots = torch.cat([il.s_pfids[s - lo] + torch.arange(K, device=cuda_device) for s in sel.tolist()])
+    assert torch.allclose(il.param_flows[slots], ipf_full[slots], rtol=1e-5, atol=1e-6)
