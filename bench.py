@@ -166,6 +166,27 @@ def sum_forward_roofline(pc, x, precision_kw, reps=10):
         pc(x, **precision_kw)
     B = x.size(0)
     per_layer = []
+
+    def timed(fn):
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            fn()
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(reps):
+                fn()
+        graph.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        graph.replay()
+        e1.record()
+        e1.synchronize()
+        del graph
+        return e0.elapsed_time(e1) / 1e3 / reps
+
     with torch.no_grad():
         for gi, g in enumerate(pc.inner_layer_groups):
             if g.is_prod():
@@ -175,35 +196,20 @@ def sum_forward_roofline(pc, x, precision_kw, reps=10):
                 d = layer._desc(x.device)
                 child_rows = int(torch.unique(d["krow"]).numel())
                 nbytes = 4 * B * (child_rows + layer.num_nodes) + 4 * layer.num_edges
-
-                def fwd():
-                    layer(pc.node_mars, pc.element_mars, pc.params, **precision_kw)
-
-                side = torch.cuda.Stream()
-                side.wait_stream(torch.cuda.current_stream())
-                with torch.cuda.stream(side):
-                    fwd()
-                torch.cuda.current_stream().wait_stream(side)
-                graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(graph):
-                    for _ in range(reps):
-                        fwd()
-                graph.replay()
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                graph.replay()
-                e1.record()
-                e1.synchronize()
-                per_layer.append((nbytes, 2 * layer.num_edges * B, e0.elapsed_time(e1) / 1e3 / reps,
-                                  d["fw_tiles"].size(0)))
-                del graph
+                packs = layer.pack_forward_weights(pc.params, B, **precision_kw)
+                # the contraction alone (the weights packed beforehand, as the forward pass
+                # packs all layers' weights on a side stream), then the pack alone
+                t_c = timed(lambda: layer(pc.node_mars, pc.element_mars, pc.params, _weights_packed=packs,
+                                          **precision_kw))
+                t_p = timed(lambda: layer.pack_forward_weights(pc.params, B, **precision_kw)) if packs else 0.0
+                per_layer.append((nbytes, 2 * layer.num_edges * B, t_c, d["fw_tiles"].size(0), t_p))
     tot_b = sum(r[0] for r in per_layer)
     tot_f = sum(r[1] for r in per_layer)
     tot_s = sum(r[2] for r in per_layer)
     big = max(per_layer, key=lambda r: r[0])
     return {"layers": len(per_layer), "bytes": tot_b, "flops": tot_f, "seconds": tot_s,
-            "largest": {"bytes": big[0], "flops": big[1], "seconds": big[2], "tiles": big[3]}}
+            "pack_seconds": sum(r[4] for r in per_layer),
+            "largest": {"bytes": big[0], "flops": big[1], "seconds": big[2], "tiles": big[3], "pack_seconds": big[4]}}
 
 
 def pflows_roofline(pc, reps=10):
@@ -411,6 +417,7 @@ def main():
         return ms, ck
 
     from pyjuice_b200.layer.layers import SumLayer
+    from pyjuice_b200.autotune import TUNER
     use_graph = ws == 1
     SumLayer.bf16_form = 1
     ms_bf16p, _ = timed({"force_use_bf16": True}, use_graph)
@@ -536,10 +543,17 @@ def main():
                 "tensor_tflops_achieved": pf["flops"] / pf["seconds"] / 1e12,
                 "sum_forward_largest_layer": {"us": big["seconds"] * 1e6, "alg_bytes": big["bytes"],
                                               "achieved_gbs": big["bytes"] / big["seconds"] / 1e9,
-                                              "kernels": "pcb_pack_weights + pcb_lse_contract_tc05"},
+                                              "frac": big["bytes"] / big["seconds"] / 1e9 / hbm,
+                                              "tiles": big["tiles"],
+                                              "kernel": "tcgen05 contraction (autotuned: persistent "
+                                                        "warp-specialised or CTA-per-slice), weights packed "
+                                                        "beforehand",
+                                              "pack_us": big["pack_seconds"] * 1e6},
                 "all_sum_layers_forward": {"layers": rf["layers"], "us_total": rf["seconds"] * 1e6,
                                            "achieved_gbs": rf["bytes"] / rf["seconds"] / 1e9,
-                                           "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm}}
+                                           "frac": rf["bytes"] / rf["seconds"] / 1e9 / hbm,
+                                           "pack_us_total": rf["pack_seconds"] * 1e6},
+                "tc05_choices": {k: list(v) for k, v in TUNER.choices.items() if k.startswith("tc05|")}}
         threads = os.cpu_count() or 1
         torch.set_num_threads(threads)
         v, sample = cpu_step_rate(lay, params, in_params, data, budget_s=15.0, batch=B)

@@ -319,6 +319,28 @@ int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux,
                           int32_t mode, int32_t prec, int32_t batch_tile, int32_t slices_per_cta, void* stream);
 
 /*
+ * pcb_lse_contract_tc05 as a persistent, warp-specialised kernel: num_ctas CTAs (0: one
+ * per SM) each own a contiguous run of (tile, batch_tile-sample slice) work units. One warp
+ * stages a unit's source rows in shared memory with 2-D TMA loads (a box of 32 samples x
+ * run_rows rows, 128-byte swizzle) into a ring of stages, eight warps exponentiate into a
+ * double-buffered B operand, one thread issues the MMAs into two tensor-memory
+ * accumulators, and four warps run the epilogue, which writes 32-row x 32-sample blocks of
+ * out through shared memory with TMA stores; loads, conversion, MMAs and stores of
+ * consecutive units overlap, and the packed weights are copied once per tile and CTA.
+ * The caller guarantees that every tile's terms form runs of run_rows (8 or 32) consecutive
+ * source rows: krow[k_off + k] == krow[k_off + (k / run_rows) * run_rows] + k % run_rows
+ * for k < k_cnt. src (and src2) have src_rows rows, out has out_rows rows. Same results and fault reporting as
+ * pcb_lse_contract_tc05; additionally B % 4 == 0, ld % 4 == 0 and 16-byte aligned
+ * src / src2 / aux / out (PCB_E_ARG otherwise).
+ * Replaces the same reference kernels as pcb_lse_contract (sum_layer.py:454-568,
+ * 1572-1730).
+ */
+int pcb_lse_contract_tc05_ws(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
+                             int32_t B, int64_t src_rows, int64_t out_rows, const uint8_t* packed, const PcbLseTile* tiles,
+                             int32_t num_tiles, const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
+                             int32_t run_rows, int32_t num_ctas, void* stream);
+
+/*
  * Sum layers under the MPE / GeneralLL propagation algorithms and the backward pass in
  * log space, with negated parameter flows or accumulated child flows (plain FP32; these
  * serve queries, not the EM step). alg: 0 LL, 1 MPE, 2 GeneralLL (alpha > 0).

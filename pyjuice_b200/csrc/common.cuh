@@ -154,6 +154,23 @@ __device__ __forceinline__ void report_status(int32_t* status, int32_t bits) {
     if (status) atomicOr(status, bits);
 }
 
+// Natural logarithm and exponential on the hardware base-2 approximations (MUFU lg2 / ex2,
+// flush-to-zero forms): ln x = log2(x) ln 2 with subnormal x rescaled by 2^24 first, and
+// e^x = 2^(x log2 e), whose results below the smallest normal float are 0. For the BF16
+// contraction forms, whose operand rounding is far coarser than these approximations.
+__device__ __forceinline__ float fast_log(float x) {
+    const bool sub = x < 1.17549435e-38f;
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(sub ? x * 16777216.f : x));
+    return (r - (sub ? 24.f : 0.f)) * 0.6931471805599453f;
+}
+
+__device__ __forceinline__ float fast_exp(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x * 1.4426950408889634f));
+    return r;
+}
+
 // Vectorised access needs ld % 4 == 0 and a 16-byte aligned base.
 inline bool vec_ok(const void* p, int64_t ld) {
     return (ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);

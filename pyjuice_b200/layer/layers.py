@@ -79,20 +79,59 @@ def _tc05_slices_per_cta(num_tiles: int, B: int, batch_tile: int) -> int:
     return SumLayer.tc05_slices_per_cta or 1
 
 
-def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream):
-    """One tcgen05 contraction (pcb_lse_contract_tc05). Samples per CTA (32 or 64) and slices
-    per CTA (1 or 2) come from the autotuner, keyed by mode, precision form, tile count and
-    batch (``SumLayer.tc05_slices_per_cta`` fixes the slices and the static batch tile)."""
+def _run_rows(tiles_np: np.ndarray, krow_np: np.ndarray) -> int:
+    """32 or 8 when every tile's terms come in runs of that many consecutive source rows
+    (the box height of pcb_lse_contract_tc05_ws), else 0."""
+    for rr in (32, 8):
+        ok = True
+        for off, cnt in {(int(t[2]), int(t[3])) for t in tiles_np}:
+            k = krow_np[off:off + cnt]
+            idx = np.arange(cnt)
+            if not np.array_equal(k, k[(idx // rr) * rr] + idx % rr):
+                ok = False
+                break
+        if ok:
+            return rr
+    return 0
+
+
+def _ws_ok(ld, B, *bufs) -> bool:
+    """Whether pcb_lse_contract_tc05_ws takes these buffers: whole 16-byte chunks per row."""
+    return B % 4 == 0 and ld % 4 == 0 and all(b is None or b.data_ptr() % 16 == 0 for b in bufs)
+
+
+def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream, run_rows=0):
+    """One tcgen05 contraction: the persistent warp-specialised kernel
+    (pcb_lse_contract_tc05_ws, 32- or 64-sample units) or the CTA-per-slice kernel
+    (pcb_lse_contract_tc05, 32 or 64 samples and 1 or 2 slices per CTA), chosen by the
+    autotuner per mode, precision form, tile count and batch. ``SumLayer.tc05_ws`` forces
+    (True) or excludes (False) the persistent kernel; ``SumLayer.tc05_slices_per_cta`` fixes
+    the CTA-per-slice kernel's slices and its static batch tile. ``run_rows``: the tile
+    table's runs of consecutive source rows (``_run_rows``; 0 excludes the persistent kernel)."""
     nt = tiles.size(0)
 
     def run(c):
-        nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
-                 nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, c[0], c[1], stream)
+        if c[0] == "ws":
+            nat.call("pcb_lse_contract_tc05_ws", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
+                     src.size(0), out.size(0), nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, c[1],
+                     run_rows, 0,
+                     stream)
+        else:
+            nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
+                     nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, c[0], c[1], stream)
 
+    ws_ok = SumLayer.tc05_ws is not False and run_rows in (8, 32) and _ws_ok(ld, B, src, src2, aux, out)
+    ws_bt = 32 if mode == 2 or nt * -(-B // 64) < _num_sms() else 64
+    if SumLayer.tc05_ws and ws_ok:
+        return run(("ws", ws_bt))
     bt = _tc05_batch_tile(nt, B)
     if SumLayer.tc05_slices_per_cta is not None:
         return run((bt, _tc05_slices_per_cta(nt, B, bt)))
     cands = [(bt, 1)] + [c for c in ((64, 1), (32, 1), (64, 2), (32, 2)) if c != (bt, 1)]
+    if ws_ok:
+        ws_c = [("ws", ws_bt), ("ws", 96 - ws_bt)]
+        # static default: the persistent kernel once the layer has a unit per SM
+        cands = ws_c + cands if nt * -(-B // ws_bt) >= _num_sms() else cands + ws_c
     run(TUNER.pick(("tc05", mode, prec, nt, B), cands, run))
 
 
@@ -288,6 +327,7 @@ class SumLayer(Layer):
     short_kernels = True  # single-stage kernels for tiles of <= 128 terms
     tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
     tc05_slices_per_cta = None  # sample slices per tcgen05 CTA (None: one)
+    tc05_ws = None        # persistent warp-specialised tcgen05 kernel: None autotuned, True forced, False off
     # The single-stage kernels of small layers read pre-packed weights too (the circuit packs
     # all layers' weights in one launch per pass, so the kernels skip their own conversion).
     pack_short_weights = True
@@ -420,11 +460,12 @@ class SumLayer(Layer):
                 krow=_i32(np.concatenate(klist)), kw=_i32(kw_np),
                 short=int(tiles_np[:, 3].max()) <= _SHORT_K,
                 wlayout=2 if _terms_vec4(tiles_np, kw_np, bs) else 0,
+                run=_run_rows(tiles_np, np.concatenate(klist)),
                 pack=torch.empty([tiles_np.shape[0] * _PACK_BYTES], dtype=torch.uint8)))
 
         fw_np = np.asarray(fw_tiles, np.int64).reshape(-1, 8)
         return dict(
-            fw_tiles=_i32(fw_np), fw_tm=fw_tm,
+            fw_tiles=_i32(fw_np), fw_tm=fw_tm, fw_run=_run_rows(fw_np, krow_c),
             fw_short=bool(fw_np.shape[0]) and int(fw_np[:, 3].max()) <= _SHORT_K,
             fw_wlayout=1 if (fw_np.shape[0] and _rows_vec4(fw_np, kw_c, bs, 1)) else 0,
             fw_pack=torch.empty([fw_np.shape[0] * _PACK_BYTES], dtype=torch.uint8),
@@ -595,7 +636,8 @@ class SumLayer(Layer):
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
                 _weights_packed = True
-            _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st)
+            _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st,
+                       d["fw_run"])
             return
         # _fuse_fw = (term_children, element values out): the product layer below is fused in
         # (the terms are sums of node rows; the element values are written as a side output)
@@ -671,7 +713,7 @@ class SumLayer(Layer):
             if self._el_tc05(eg, prec):
                 st = nat.stream()
                 _tc05_call(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld, B,
-                           eg["pack"], et, eg["krow"], 1 if allow_modify_flows else 2, prec, st)
+                           eg["pack"], et, eg["krow"], 1 if allow_modify_flows else 2, prec, st, eg["run"])
                 continue
             if eg["short"] and SumLayer.short_kernels:
                 packed = eg["pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
@@ -881,6 +923,8 @@ class ProdLayer(Layer):
         d = self._desc(node_mars.device)
         part = self._partial("fw", node_mars.device)
         if part is not None:
+            if part["row"].size(0) == 0:
+                return
             d = dict(fw_row=part["row"], fw_off=part["off"], fw_cnt=part["cnt"], fw_chs=part["chs"])
         B = node_mars.size(1)
         ld = node_mars.stride(0)

@@ -207,6 +207,37 @@ def test_tc05_multi_slice_equals_per_slice(cuda_device):
     assert abs(out[1][0][:16].double().cpu().numpy().mean() - lls_o.mean()) < 1e-3
 
 
+@pytest.mark.parametrize("modify", [True, False])
+def test_tc05_persistent_equals_per_slice(modify, cuda_device):
+    """On HCLT-784 at batch 256, the persistent warp-specialised tcgen05 kernel (TMA-staged
+    child rows, every layer of >= 6 tiles) gives bit-identical node values, node flows and
+    parameter flows to the CTA-per-slice kernel, with modified (mode 1) and unmodified
+    (mode 2) node flows."""
+    from pyjuice_b200.layer.layers import SumLayer
+    fx = load_fixture("hclt784")
+    rng = np.random.default_rng(12)
+    x = torch.from_numpy(rng.integers(0, 256, size=(256, 784))).to(cuda_device)
+    saved = SumLayer.tc05_ws
+    out = []
+    try:
+        for ws in (False, True):
+            SumLayer.tc05_ws = ws
+            pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+            load_fixture_params(pc, fx)
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                lls = pc(x, force_use_bf16=True)
+            pc.backward(inputs=x, allow_modify_flows=modify)
+            torch.cuda.synchronize()
+            out.append((lls.clone(), pc.node_mars.clone(), pc.node_flows.clone(), pc.param_flows.clone()))
+    finally:
+        SumLayer.tc05_ws = saved
+    assert all(l._desc(cuda_device)["fw_run"] == 32 for g in pc.inner_layer_groups if g.is_sum() for l in g.layers
+               if l._desc(cuda_device)["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles)
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("name,B,fw", [("hclt64", 37, dict(force_use_fp32=True)), ("hclt784", 64, dict(force_use_bf16=True)),
                                        ("tiny", 19, dict(force_use_fp32=True))])
 def test_fused_products_equal_unfused(name, B, fw, cuda_device):

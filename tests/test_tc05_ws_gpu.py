@@ -1,0 +1,147 @@
+"""The persistent warp-specialised tcgen05 contraction (pcb_lse_contract_tc05_ws) against the
+CTA-per-slice kernel (pcb_lse_contract_tc05) through the C ABI: both run the same
+arithmetic in the same order (per-sample max, exp, bf16 split, MMAs over 16-term steps,
+FP32 accumulators), so their outputs must be bit-identical, for the sum forward (mode 0) and
+the element flows (modes 1 and 2), in both precision forms, for ragged tiles (fewer rows and
+terms than 128), a partial last sample slice, several tiles per CTA (weights copied again)
+and CTAs owning a single unit. Both are also checked against an FP64 evaluation of the
+contraction. An oversize tile gives NaN rows and the device status bit, as in the other
+kernels."""
+
+import numpy as np
+import pytest
+import torch
+
+from pyjuice_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(B, device, seed, run):
+    """Tiles whose terms come in runs of ``run`` consecutive source rows (random run starts;
+    the last run of a tile may be partial)."""
+    g = torch.Generator().manual_seed(seed)
+    # tiles: (n_rows, k_cnt)
+    shapes = [(128, 128), (96, 100), (40, 17), (128, 128), (128, 64), (33, 128), (128, 1)]
+    T = len(shapes)
+    n_src = 300
+    tiles, krow, kw = [], [], []
+    for t, (nr, kc) in enumerate(shapes):
+        tiles.append([t * 128, nr, len(krow), kc, t * 128 * 128, t * 128, 32, 0])
+        for k0 in range(0, kc, run):
+            start = int(torch.randint(0, n_src - run + 1, (1,), generator=g))
+            krow += [start + j for j in range(min(run, kc - k0))]
+        kw += [k * 128 for k in range(kc)]
+    src = torch.rand([n_src, B], generator=g) * 6 - 8
+    src[7] = -float("inf")                     # a row of -inf terms
+    src[:, 3] = -float("inf")                  # a sample whose terms are all -inf
+    flows = torch.rand([n_src, B], generator=g)
+    flows[11] = 0.0
+    aux = torch.rand([T * 128, B], generator=g) * 4 - 5
+    params = torch.rand([T * 128 * 128], generator=g) + 0.05
+    dev = lambda x: x.to(device)
+    return dict(src=dev(src), flows=dev(flows), aux=dev(aux), params=dev(params),
+                tiles=dev(torch.tensor(tiles, dtype=torch.int32)), krow=dev(torch.tensor(krow, dtype=torch.int32)),
+                kw=dev(torch.tensor(kw, dtype=torch.int32)), shapes=shapes, B=B, T=T, run=run)
+
+
+def _pack(p, device):
+    packed = torch.zeros([p["T"] * 65536], dtype=torch.uint8, device=device)
+    nat.call("pcb_pack_weights", nat.ptr(p["params"]), nat.ptr(p["tiles"]), p["T"], 32, nat.ptr(p["kw"]), 1,
+             nat.ptr(packed), nat.stream())
+    return packed
+
+
+def _run(p, packed, mode, prec, kernel, bt, arg):
+    B, T = p["B"], p["T"]
+    src = p["flows"] if mode == 2 else p["src"]
+    src2 = p["src"] if mode == 2 else None
+    aux = p["aux"] if mode >= 1 else None
+    out = torch.full([T * 128, B], 12345.0, device=p["src"].device)
+    if kernel == "pcb_lse_contract_tc05":
+        nat.call(kernel, nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), B, B, nat.ptr(packed),
+                 nat.ptr(p["tiles"]), T, nat.ptr(p["krow"]), mode, prec, bt, arg, nat.stream())
+    else:
+        nat.call(kernel, nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), B, B, src.size(0), out.size(0),
+                 nat.ptr(packed), nat.ptr(p["tiles"]), T, nat.ptr(p["krow"]), mode, prec, bt, p["run"], arg,
+                 nat.stream())
+    return out
+
+
+def _fp64(p, mode):
+    """The contraction in FP64 with the FP32 weights (mode 0: log-sum; 1/2: element flows)."""
+    B = p["B"]
+    src, flows, aux = p["src"].double().cpu(), p["flows"].double().cpu(), p["aux"].double().cpu()
+    params = p["params"].double().cpu()
+    krow, kw, tiles = p["krow"].cpu(), p["kw"].cpu(), p["tiles"].cpu()
+    out = torch.full([p["T"] * 128, B], 12345.0, dtype=torch.float64)
+    for t in range(p["T"]):
+        o_row, nr, k_off, kc, w_add, a_row, g_str, _ = tiles[t].tolist()
+        rows = krow[k_off:k_off + kc].long()
+        r = torch.arange(nr)
+        wid = kw[k_off:k_off + kc].long()[:, None] + w_add + (r // 32) * g_str + (r % 32)
+        W = params[wid]                                    # [k, r]
+        if mode == 2:
+            v = torch.where(src[rows] == -float("inf"), -float("inf"), torch.log(flows[rows]) - src[rows])
+        else:
+            v = src[rows]
+        m = v.max(dim=0).values
+        m0 = torch.where(torch.isfinite(m), m, torch.zeros_like(m))
+        acc = W.T @ torch.exp(v - m0)                      # [r, B]
+        if mode == 0:
+            res = torch.where(torch.isfinite(m), torch.log(acc) + m0, torch.full_like(acc, -float("inf")))
+        else:
+            res = torch.where(torch.isfinite(m), acc * torch.exp(aux[a_row:a_row + nr] + m0), torch.zeros_like(acc))
+        out[o_row:o_row + nr] = res
+    return out
+
+
+@pytest.mark.parametrize("B,run", [(512, 32), (100, 8), (512, 8)])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("prec", [2, 1])
+def test_ws_bit_identical_to_per_slice_kernel(B, run, mode, prec, cuda_device):
+    p = _problem(B, cuda_device, seed=B + 10 * mode + prec + run, run=run)
+    packed = _pack(p, cuda_device)
+    ref64 = _fp64(p, mode)
+    for bt in (32, 64):
+        base = _run(p, packed, mode, prec, "pcb_lse_contract_tc05", bt, 1)
+        for ctas in (0, 3, 1):  # one per SM (mostly one unit each); 3 and 1: many units and tiles per CTA
+            got = _run(p, packed, mode, prec, "pcb_lse_contract_tc05_ws", bt, ctas)
+            torch.cuda.synchronize()
+            assert nat.device_status(clear=True) == 0
+            assert torch.equal(got, base), (bt, ctas, (got - base).abs().nan_to_num(0).max())
+        # both against FP64 (split form: bf16 hi + lo operands)
+        g = base.double().cpu()
+        fin = torch.isfinite(ref64)
+        assert torch.equal(fin, torch.isfinite(g))
+        tol = 1e-4 if prec == 2 else 2e-2
+        if mode == 0:
+            err = (g[fin] - ref64[fin]).abs().max()
+        else:
+            err = ((g[fin] - ref64[fin]).abs() / ref64[fin].abs().clamp(min=1e-3)).max()
+        assert err <= tol, err
+
+
+def test_ws_oversize_tile_is_reported(cuda_device):
+    B = 64
+    src = torch.zeros([256, B], dtype=torch.float32, device=cuda_device)
+    out = torch.zeros([128, B], dtype=torch.float32, device=cuda_device)
+    krow = torch.zeros([256], dtype=torch.int32, device=cuda_device)
+    tiles = torch.tensor([[0, 128, 0, 129, 0, 0, 0, 0]], dtype=torch.int32, device=cuda_device)
+    packed = torch.zeros([65536], dtype=torch.uint8, device=cuda_device)
+    nat.device_status(clear=True)
+    nat.call("pcb_lse_contract_tc05_ws", nat.ptr(src), nat.ptr(None), nat.ptr(None), nat.ptr(out), B, B, 256, 128,
+             nat.ptr(packed), nat.ptr(tiles), 1, nat.ptr(krow), 0, 2, 64, 32, 0, nat.stream())
+    assert nat.device_status(clear=True) == 2
+    assert torch.isnan(out).all()
+
+
+def test_ws_rejects_unaligned_batch(cuda_device):
+    B = 30
+    src = torch.zeros([8, 32], dtype=torch.float32, device=cuda_device)
+    tiles = torch.tensor([[0, 8, 0, 8, 0, 0, 0, 0]], dtype=torch.int32, device=cuda_device)
+    krow = torch.zeros([8], dtype=torch.int32, device=cuda_device)
+    packed = torch.zeros([65536], dtype=torch.uint8, device=cuda_device)
+    with pytest.raises(RuntimeError, match="B % 4"):
+        nat.call("pcb_lse_contract_tc05_ws", nat.ptr(src), nat.ptr(None), nat.ptr(None), nat.ptr(src), 32, B, 8, 8,
+                 nat.ptr(packed), nat.ptr(tiles), 1, nat.ptr(krow), 0, 2, 64, 8, 0, nat.stream())
