@@ -66,6 +66,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=BATCH)
+    p.add_argument("--workload", default="em", choices=["em", "adjoint"],
+                   help="em: the EM step on HCLT-784 (default); adjoint: the soft-evidence log-likelihood and its "
+                        "gradients on HCLT-3072 (32x32x3 fields, 256 latents, batch 128)")
+    p.add_argument("--fd", action="store_true", help="adjoint workload: also check coordinates of both gradients "
+                                                     "against FP64 central differences of the oracle (minutes)")
     p.add_argument("--profile-step", action="store_true",
                    help="run one warm-up step and one EM step (BF16 form) inside the NVTX range 'em_step', "
                         "for kernel profilers; prints the kernels launched per step")
@@ -322,8 +327,122 @@ def reference_arm(args):
           flush=True)
 
 
+def adjoint_workload(args):
+    """Differentiable HCLT on 3072 vars (three 32x32 quantised random-field channels, 256
+    categories), 256 latents, block 32, batch 128: per step, ``autograd.circuit_ll`` on
+    soft evidence ``E [128, 3072, 256]`` (Dirichlet(1) rows) with sum weights
+    ``softmax(z)``, then ``d mean-LL / d z`` and ``d mean-LL / d E`` (the hand-written
+    adjoint). Timed with CUDA events over ``--steps`` steps after ``--warmup``; evidence and
+    logits resident. ``--fd``: a few coordinates of both gradients at batch 2 against FP64
+    central differences (h = 1e-6) of the oracle."""
+    import pyjuice_b200 as juice
+    from pyjuice_b200 import _native as nat
+    from pyjuice_b200.nodes.distributions import Categorical
+    from pyjuice_b200.structures import hclt_from_tree, chow_liu_tree
+    from pyjuice_b200.structures.hclt import mutual_information_chunked
+    from pyjuice_b200.synthetic import gaussian_field_data
+    ws, rank, local = dist_env()
+    if ws > 1 and rank != 0:
+        return
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    nat.load()
+    side, ch, lat, B, K = 32, 3, 256, 128, NUM_CATS
+    data = gaussian_field_data(8192, side=side, num_cats=K, length_scale=3.0, channels=ch, seed=0)
+    x = data.float().to(device)
+    mi = mutual_information_chunked(x, x, 32, 0.5 / 32, chunk_size=64).cpu().numpy()
+    del x
+    tree = chow_liu_tree(mi)
+    root = tree.center()
+    torch.manual_seed(0)
+    ns = hclt_from_tree(tree.dfs_postorder(root), tree.bfs_children(root), root, lat,
+                        input_dist=Categorical(num_cats=K), block_size=BLOCK)
+    pc = juice.compile(ns).to(device)
+    V = side * side * ch
+    gen = torch.Generator(device=device).manual_seed(5)
+    z = torch.randn([pc.params.numel()], generator=gen, device=device).requires_grad_(True)
+    ev = -torch.log(torch.rand([B, V, K], generator=gen, device=device).clamp_(min=1e-30))
+    ev = (ev / ev.sum(dim=2, keepdim=True)).requires_grad_(True)   # Dirichlet(1) rows
+
+    def step():
+        z.grad = None
+        ev.grad = None
+        lls = juice.autograd.circuit_ll(pc, z, ev)
+        lls.mean().backward()
+        return lls
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        lls = step()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ok = bool(torch.isfinite(lls).all()) and bool(torch.isfinite(z.grad).all()) and bool(torch.isfinite(ev.grad).all())
+    out = {"metric": "adjoint samples/s (soft-evidence LL + d/d sum-logits + d/d evidence) 1xB200",
+           "value": B / (ms / 1e3), "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "HCLT 32x32x3 vars x 256 cats, 256 latents, block 32, soft evidence, batch 128",
+                      "num_nodes": pc.num_nodes, "num_edges": pc.num_edges, "evidence_bytes": ev.numel() * 4},
+           "finite": ok, "mean_ll": float(lls.detach().mean())}
+    if args.fd:
+        out["fd_check"] = adjoint_fd_check(pc, z.detach(), ev.detach()[:2], device)
+    print(json.dumps(out), flush=True)
+
+
+def adjoint_fd_check(pc, z, ev, device, n_coords=2, h=1e-6):
+    """Gradients of sum_b LL_b (b < 2) at the FP32 point against FP64 central differences of
+    the oracle; returns the relative errors."""
+    import pyjuice_b200 as juice
+    from oracle import pc_oracle as orc
+    lay = orc.layout_from_circuit(pc)
+    q0 = pc.input_layer_group[0].params.double().cpu().numpy()
+    pb, nch, bsz = pc._em_pbase.tolist(), pc._em_nch.tolist(), pc._em_bs.tolist()
+
+    def softmax_params(zz):
+        p = np.zeros_like(zz)
+        for b0, k, bs in zip(pb, nch, bsz):
+            blk = zz[b0:b0 + k * bs].reshape(k, bs)
+            e = np.exp(blk - blk.max(axis=0))
+            p[b0:b0 + k * bs] = (e / e.sum(axis=0)).reshape(-1)
+        return p
+
+    z64 = z.double().cpu().numpy()
+    e64 = ev.double().cpu().numpy()
+
+    def f(zz, ee):
+        _, _, lls = orc.forward(lay, softmax_params(zz), q0, evidence=ee)
+        return float(lls[:, 0].sum())
+
+    zt = z.clone().requires_grad_(True)
+    et = ev.clone().requires_grad_(True)
+    juice.autograd.circuit_ll(pc, zt, et).sum().backward()
+    gz, ge = zt.grad.double().cpu().numpy(), et.grad.double().cpu().numpy()
+    rng = np.random.default_rng(3)
+    used = np.concatenate([np.arange(b0, b0 + k * bs) for b0, k, bs in zip(pb, nch, bsz)])
+    errs = {"logits": [], "evidence": []}
+    for i in rng.choice(used, size=n_coords, replace=False):
+        d = np.zeros_like(z64)
+        d[i] = h
+        fd = (f(z64 + d, e64) - f(z64 - d, e64)) / (2 * h)
+        errs["logits"].append(abs(gz[i] - fd) / max(abs(fd), 1e-2))
+    for _ in range(n_coords):
+        b, v, k = rng.integers(ev.size(0)), rng.integers(ev.size(1)), rng.integers(ev.size(2))
+        d = np.zeros_like(e64)
+        d[b, v, k] = h
+        fd = (f(z64, e64 + d) - f(z64, e64 - d)) / (2 * h)
+        errs["evidence"].append(abs(ge[b, v, k] - fd) / max(abs(fd), 1e-2))
+    return {"batch": int(ev.size(0)), "h": h, "coords_each": n_coords,
+            "max_rel_err_logits": max(errs["logits"]), "max_rel_err_evidence": max(errs["evidence"])}
+
+
 def main():
     args = parse()
+    if args.workload == "adjoint":
+        return adjoint_workload(args)
     if args.impl == "reference":
         return reference_arm(args)
     ws, rank, local = dist_env()
