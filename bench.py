@@ -540,12 +540,15 @@ def main():
     use_graph = ws == 1
     SumLayer.bf16_form = 1
     ms_bf16p, _ = timed({"force_use_bf16": True}, use_graph)
+    SumLayer.bf16_form = 3
+    ms_fp8, _ = timed({"force_use_bf16": True}, use_graph)
     SumLayer.bf16_form = 2
     ms_bf16, clocks = timed({"force_use_bf16": True}, use_graph, sample_clocks=True)
     ms_fp32, _ = timed({"force_use_fp32": True}, use_graph)
     value = ws * B * args.steps / (ms_bf16 / 1e3)
     value_fp32 = ws * B * args.steps / (ms_fp32 / 1e3)
     value_bf16p = ws * B * args.steps / (ms_bf16p / 1e3)
+    value_fp8 = ws * B * args.steps / (ms_fp8 / 1e3)
 
     # end to end through the public API, host buffers, LLs read back every step
     host = data[:B * 8].pin_memory()
@@ -614,6 +617,8 @@ def main():
         with torch.no_grad():
             SumLayer.bf16_form = 1
             l_bp = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
+            SumLayer.bf16_form = 3
+            l_f8 = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
             SumLayer.bf16_form = 2
             l_bf = pc(xs.to(device), force_use_bf16=True).double().cpu().numpy()
             l_32 = pc(xs.to(device), force_use_fp32=True).double().cpu().numpy()
@@ -623,7 +628,7 @@ def main():
         _, pf_o, ipf_o = orc.backward(lay, params, xp.numpy(), nm_o, ems_o)
         pf_err = {}
         for name, bform, kw in (("bf16_split", 2, {"force_use_bf16": True}), ("bf16_single", 1, {"force_use_bf16": True}),
-                                ("fp32", 2, {"force_use_fp32": True})):
+                                ("e4m3", 3, {"force_use_bf16": True}), ("fp32", 2, {"force_use_fp32": True})):
             SumLayer.bf16_form = bform
             pc.init_param_flows(flows_memory=0.0)
             with torch.no_grad():
@@ -638,6 +643,8 @@ def main():
                   "bf16_mean_abs_dll_nats": float(np.abs(l_bf - lls_o).mean()),
                   "bf16_single_dmean_ll_nats": float(abs(l_bp.mean() - lls_o.mean())),
                   "bf16_single_mean_abs_dll_nats": float(np.abs(l_bp - lls_o).mean()),
+                  "e4m3_dmean_ll_nats": float(abs(l_f8.mean() - lls_o.mean())),
+                  "e4m3_mean_abs_dll_nats": float(np.abs(l_f8 - lls_o).mean()),
                   "fp32_max_rel_dll": float((np.abs(l_32 - lls_o) / np.abs(lls_o)).max()),
                   "fp32_dmean_ll_nats": float(abs(l_32.mean() - lls_o.mean())),
                   "mean_ll_nats": float(lls_o.mean()), "samples": int(xs.size(0))}
@@ -688,6 +695,9 @@ def main():
             "precision_form": "bf16 tensor cores, operands split into bf16 hi + lo (3 MMAs), FP32 accumulate",
             "fp32_plain": {"value": value_fp32, "unit": "samples/s", "ms_per_step": ms_fp32 / args.steps},
             "bf16_single": {"value": value_bf16p, "unit": "samples/s", "ms_per_step": ms_bf16p / args.steps},
+            "e4m3": {"value": value_fp8, "unit": "samples/s", "ms_per_step": ms_fp8 / args.steps,
+                     "form": "tcgen05 sum contractions (forward, element flows) in e4m3 with per-row weight scales, "
+                             "the rest in split bf16"},
             "ll_error_vs_fp64": ll_err,
             "param_flow_rel_err_vs_fp64": {"samples": 16, "measure": "max |pf - pf_fp64| / max |pf_fp64|", **pf_err},
             "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": B * SIDE * SIDE * 8,

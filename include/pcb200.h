@@ -280,6 +280,18 @@ int pcb_pack_weights(const float* params, const PcbLseTile* tiles, int32_t num_t
                      const int32_t* kw, int32_t w_stride, uint8_t* packed, void* stream);
 
 /*
+ * The same weights packed for the E4M3 form of pcb_lse_contract_tc05 (prec 3): for tile t,
+ * at packed + t * 65536, 16384 bytes of e4m3 values W(k, r) * 448 / max_k W(k, r) in the
+ * K-major no-swizzle layout of a 128 x 128 8-bit operand (core matrices of 8 rows x 16
+ * terms; 128 bytes between core matrices along K, 1024 bytes between 8-row groups),
+ * followed by 128 FP32 factors max_k W(k, r) / 448^2 (per-row scaling; rows and terms
+ * beyond the tile are zero). packed must be 16-byte aligned.
+ * No counterpart in the reference (its sum layers have no 8-bit form).
+ */
+int pcb_pack_weights_fp8(const float* params, const PcbLseTile* tiles, int32_t num_tiles, int32_t rows_per_block,
+                         const int32_t* kw, int32_t w_stride, uint8_t* packed, void* stream);
+
+/*
  * One tile table of a pcb_pack_weights_multi launch: the arguments of one
  * pcb_pack_weights call (rows_per_block as its base-2 logarithm).
  * No counterpart in the reference (see pcb_pack_weights).
@@ -291,13 +303,14 @@ typedef struct {
     int32_t num_tiles;
     int32_t rows_per_block_log2;
     int32_t w_stride;
-    int32_t reserved;
+    int32_t format;              /* 0: bf16 hi + lo (pcb_pack_weights), 1: e4m3 (pcb_pack_weights_fp8) */
 } PcbPackJob;
 
 /*
  * pcb_pack_weights for several tile tables in one launch (device arrays): global tile g
  * (g < total_tiles) is tile tile_index[g] of jobs[tile_job[g]]. The caller guarantees
- * tile_index[g] < that job's num_tiles. Same output as one pcb_pack_weights per job.
+ * tile_index[g] < that job's num_tiles. Same output as one pcb_pack_weights (format 0) or
+ * pcb_pack_weights_fp8 (format 1) per job.
  * No counterpart in the reference (see pcb_pack_weights).
  */
 int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const int32_t* tile_job,
@@ -306,7 +319,9 @@ int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const in
 /*
  * Same contraction and epilogues as pcb_lse_contract (BF16 forms, prec 1 or 2) on the
  * tcgen05 tensor cores with tensor-memory accumulators, for tiles of at most 128 terms,
- * using the weights packed by pcb_pack_weights from the same tile table. One CTA per tile
+ * using the weights packed by pcb_pack_weights from the same tile table; prec 3 is the
+ * E4M3 form (kind::f8f6f4 MMAs, FP32 accumulation) on weights packed by
+ * pcb_pack_weights_fp8, with the exponentials scaled by 448 into e4m3. One CTA per tile
  * and run of slices_per_cta consecutive batch_tile-sample slices (batch_tile 32 or 64):
  * the packed weights are copied once per CTA, and the next slice's source values are
  * loaded while the current slice is processed. A tile with more terms produces NaN rows

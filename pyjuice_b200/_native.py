@@ -116,6 +116,7 @@ _SIGS = {
                                 c_int32, c_int32, c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
                                 c_int32, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_pack_weights": ([c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
+    "pcb_pack_weights_fp8": ([c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p], c_int32),
     "pcb_pack_weights_multi": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_tc05": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                                c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),

@@ -57,6 +57,41 @@ __device__ __forceinline__ constexpr uint32_t make_idesc() {
     return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
+// E4M3 form: a tile's weights as e4m3 bytes in the K-major no-swizzle layout (8 rows x 16
+// terms per core matrix, 128 bytes along K between core matrices, 1024 bytes between 8-row
+// groups), each row scaled by 448 / (its largest weight), followed by 128 FP32 unscale
+// factors (largest weight / 448^2, applied to the accumulator with the B operand's 448).
+constexpr uint32_t kF8Bytes = 128 * KT;
+constexpr uint32_t kF8SBO = (KT / 16) * 128;
+constexpr uint32_t kF8TileBytes = kF8Bytes + 128 * 4;
+
+__device__ __forceinline__ uint64_t make_desc_sbo(uint32_t saddr, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(kLBO >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor of kind::f8f6f4: D f32, A and B e4m3, both K-major, M = 128, N.
+template <int N>
+__device__ __forceinline__ constexpr uint32_t make_idesc_f8() {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f8_ss(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// Two floats as e4m3 (round to nearest, saturating): a in the low byte, b in the high byte.
+__device__ __forceinline__ uint32_t e4m3x2(float a, float b) {
+    uint16_t r;
+    asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(r) : "f"(b), "f"(a));
+    return r;
+}
+
 __device__ __forceinline__ void mma_bf16_ss(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                             uint32_t accumulate) {
     asm volatile(
@@ -170,6 +205,52 @@ __device__ __forceinline__ void pack_tile_part(const float* __restrict__ params,
     }
 }
 
+// E4M3 packing of one tile by a CTA of 256 threads: thread (r, h) takes row r and terms
+// 64 h .. 64 h + 63; the row's largest weight (over both halves) sets its scale.
+__device__ __forceinline__ void pack_tile_fp8(const float* __restrict__ params, const PcbLseTile& t, int rpb_log2,
+                                              const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ dst,
+                                              float (*smax)[128]) {
+    const int rpb_mask = (1 << rpb_log2) - 1;
+    const int nk = min(t.k_cnt, KT);
+    const int r = threadIdx.x & 127, h = threadIdx.x >> 7;
+    const bool row_ok = r < t.n_rows;
+    const int64_t rb = (int64_t)t.w_add + (int64_t)(r >> rpb_log2) * t.g_stride + (int64_t)(r & rpb_mask) * w_stride;
+    float mx = 0.f;
+    for (int j = 0; j < 64; ++j) {
+        const int k = h * 64 + j;
+        if (row_ok && k < nk) mx = fmaxf(mx, __ldg(params + (int64_t)__ldg(kw + t.k_off + k) + rb));
+    }
+    smax[h][r] = mx;
+    __syncthreads();
+    mx = fmaxf(smax[0][r], smax[1][r]);
+    const float sc = mx > 0.f ? 448.f / mx : 0.f;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+        uint32_t wd[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float w[4];
+#pragma unroll
+            for (int z = 0; z < 4; ++z) {
+                const int k = h * 64 + g * 16 + q * 4 + z;
+                w[z] = (row_ok && k < nk) ? __ldg(params + (int64_t)__ldg(kw + t.k_off + k) + rb) * sc : 0.f;
+            }
+            wd[q] = e4m3x2(w[0], w[1]) | (e4m3x2(w[2], w[3]) << 16);
+        }
+        *reinterpret_cast<uint4*>(dst + (uint32_t)(r >> 3) * kF8SBO + (uint32_t)(h * 4 + g) * kLBO +
+                                  (uint32_t)(r & 7) * 16) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    }
+    if (h == 0) reinterpret_cast<float*>(dst + kF8Bytes)[r] = mx / (448.f * 448.f);
+}
+
+__global__ void __launch_bounds__(256)
+pack_weights_fp8_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
+                        const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
+    pcb::pdl_begin();
+    __shared__ float smax[2][128];
+    pack_tile_fp8(params, tiles[blockIdx.x], rpb_log2, kw, w_stride, packed + (size_t)blockIdx.x * kTileBytes, smax);
+}
+
 __global__ void __launch_bounds__(256)
 pack_weights_kernel(const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, int rpb_log2,
                     const int* __restrict__ kw, int w_stride, uint8_t* __restrict__ packed) {
@@ -185,9 +266,16 @@ __global__ void __launch_bounds__(256)
 pack_weights_multi_kernel(const float* __restrict__ params, const PcbPackJob* __restrict__ jobs,
                           const int* __restrict__ tile_job, const int* __restrict__ tile_index) {
     pcb::pdl_begin();
+    __shared__ float smax[2][128];
     const int g = blockIdx.x / kPackSplit;
     const PcbPackJob jb = jobs[tile_job[g]];
     const int ti = tile_index[g];
+    if (jb.format == 1) {  // e4m3: the whole tile in the first of its CTAs (row maxima)
+        if (blockIdx.x % kPackSplit == 0)
+            pack_tile_fp8(params, jb.tiles[ti], jb.rows_per_block_log2, jb.kw, jb.w_stride,
+                          jb.packed + (size_t)ti * kTileBytes, smax);
+        return;
+    }
     pack_tile_part(params, jb.tiles[ti], jb.rows_per_block_log2, jb.kw, jb.w_stride,
                    jb.packed + (size_t)ti * kTileBytes, blockIdx.x % kPackSplit);
 }
@@ -219,7 +307,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // One CTA per tile and run of up to spc consecutive N-sample slices. The packed weights are
 // copied once per CTA; the source values (and epilogue element values) of slice s + 1 are
 // prefetched into L2 while slice s is reduced, exponentiated, contracted and written out.
-template <int N, int MODE, bool SPLIT>
+template <int N, int MODE, int PREC>
 __global__ void __launch_bounds__(tc05_threads<N>(), 2)
 lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const uint8_t* __restrict__ packed,
@@ -228,6 +316,8 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     // tile and term indices (compiled tables) before the wait for the previous kernel
     pcb::pdl_trigger();
     static_assert(N == 32 || N == 64, "sample slice");
+    constexpr bool SPLIT = PREC == 2;
+    constexpr bool FP8 = PREC == 3;
     using S = Tc05Smem<N>;
     constexpr int W = S::W;             // warps
     constexpr int NQ = N / 32;          // groups of 4 x 8 samples
@@ -270,7 +360,7 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t taddr = slot[0];
     if (tid == 0) {
-        const uint32_t wbytes = SPLIT ? kTileBytes : kHalfBytes;
+        const uint32_t wbytes = FP8 ? kF8TileBytes : (SPLIT ? kTileBytes : kHalfBytes);
         mbar_expect_tx(barW, wbytes);
         bulk_copy_g2s(sm + S::oW, packed + (size_t)tile_id * kTileBytes, wbytes, barW);
     }
@@ -391,7 +481,17 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
 #pragma unroll
             for (int j = 0; j < 8; ++j) e[j] = (m[j] == -INFINITY) ? 0.f : pcb::fast_exp(v[it][j] - m[j]);
             const uint32_t off = (uint32_t)n8 * kSBO + (uint32_t)(k >> 3) * kLBO + (uint32_t)(k & 7) * 16;
-            if (SPLIT) {
+            if (FP8) {
+                // K-major e4m3 B operand: sample n's 16 terms k & ~15 .. per 16-byte row;
+                // values scaled by 448 (the largest finite e4m3) before rounding
+                uint8_t* row = eh + (uint32_t)n8 * kF8SBO + (uint32_t)(k >> 4) * kLBO + (uint32_t)(k & 15);
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) {
+                    const uint32_t two = e4m3x2(e[j] * 448.f, e[j + 1] * 448.f);
+                    row[j * 16] = (uint8_t)(two & 0xFF);
+                    row[(j + 1) * 16] = (uint8_t)(two >> 8);
+                }
+            } else if (SPLIT) {
                 uint4 h, l;
                 split8(e, h, l);
                 *reinterpret_cast<uint4*>(eh + off) = h;
@@ -408,7 +508,16 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
         // ---- one thread issues the MMAs ----
         if (tid == 0) {
             if (sl == 0 && !mbar_wait_bounded(barW, 0)) slot[1] = 1;
-            if (slot[1] == 0) {
+            if (slot[1] == 0 && FP8) {
+                constexpr uint32_t idesc = make_idesc_f8<N>();
+                const uint32_t aw = smem_u32(sm + S::oW);
+                const uint32_t ae = smem_u32(eh);
+                for (int s = 0; s < (nk + 31) / 32; ++s) {
+                    const uint32_t o = (uint32_t)s * 2 * kLBO;
+                    mma_f8_ss(taddr, make_desc_sbo(aw + o, kF8SBO), make_desc_sbo(ae + o, kF8SBO), idesc,
+                              s > 0 ? 1u : 0u);
+                }
+            } else if (slot[1] == 0) {
                 constexpr uint32_t idesc = make_idesc<N>();
                 const uint32_t aw = smem_u32(sm + S::oW);
                 const uint32_t ae = smem_u32(eh);
@@ -456,6 +565,11 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
             for (int i = 0; i < 16; ++i) acc[c * 16 + i] = x[i];
         }
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (FP8) {  // undo the row's weight scale and the 448 of the B operand
+            const float us = reinterpret_cast<const float*>(sm + S::oW + kF8Bytes)[r];
+#pragma unroll
+            for (int i = 0; i < CW; ++i) acc[i] *= us;
+        }
         if (r < t.n_rows) {
             float* dst = out + ((int64_t)t.out_row + r) * ld + b0 + cb;
 #pragma unroll
@@ -1043,7 +1157,7 @@ int launch_ws_n(int mode, bool split, int num_tiles, int num_ctas, const CUtenso
 #undef PCB_WS
 }
 
-template <int N, int MODE, bool SPLIT>
+template <int N, int MODE, int PREC>
 int launch(int num_tiles, int spc, const float* src, const float* src2, const float* aux, float* out, int64_t ld,
            int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s, bool vec) {
     constexpr size_t smem = Tc05Smem<N>::bytes();
@@ -1051,14 +1165,14 @@ int launch(int num_tiles, int spc, const float* src, const float* src2, const fl
     static bool configured[64] = {false};
     const int dev = current_device();
     if (!configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(lse_tc05_kernel<N, MODE, SPLIT>,
+        cudaError_t e = cudaFuncSetAttribute(lse_tc05_kernel<N, MODE, PREC>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_contract_tc05: %s", cudaGetErrorString(e));
         configured[dev] = true;
     }
     const int64_t gy = pcb::cdiv(pcb::cdiv(B, N), spc);
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: batch too large");
-    return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, SPLIT>,
+    return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, PREC>,
                                             dim3((unsigned)num_tiles, (unsigned)gy), dim3(tc05_threads<N>()), smem, s,
                                             1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec,
                                             pcb::status_word()),
@@ -1066,12 +1180,13 @@ int launch(int num_tiles, int spc, const float* src, const float* src2, const fl
 }
 
 template <int N>
-int launch_n(int mode, bool split, int num_tiles, int spc, const float* src, const float* src2, const float* aux,
+int launch_n(int mode, int prec, int num_tiles, int spc, const float* src, const float* src2, const float* aux,
              float* out, int64_t ld, int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow,
              cudaStream_t s, bool vec) {
-#define PCB_TC(M, SP) launch<N, M, SP>(num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec)
-    if (split) return mode == 0 ? PCB_TC(0, true) : (mode == 1 ? PCB_TC(1, true) : PCB_TC(2, true));
-    return mode == 0 ? PCB_TC(0, false) : (mode == 1 ? PCB_TC(1, false) : PCB_TC(2, false));
+#define PCB_TC(M, P) launch<N, M, P>(num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec)
+    if (prec == 3) return mode == 0 ? PCB_TC(0, 3) : (mode == 1 ? PCB_TC(1, 3) : PCB_TC(2, 3));
+    if (prec == 2) return mode == 0 ? PCB_TC(0, 2) : (mode == 1 ? PCB_TC(1, 2) : PCB_TC(2, 2));
+    return mode == 0 ? PCB_TC(0, 1) : (mode == 1 ? PCB_TC(1, 1) : PCB_TC(2, 1));
 #undef PCB_TC
 }
 
@@ -1092,6 +1207,20 @@ extern "C" int pcb_pack_weights(const float* params, const PcbLseTile* tiles, in
                                             packed), "pcb_pack_weights");
 }
 
+extern "C" int pcb_pack_weights_fp8(const float* params, const PcbLseTile* tiles, int32_t num_tiles,
+                                    int32_t rows_per_block, const int32_t* kw, int32_t w_stride, uint8_t* packed,
+                                    void* stream) {
+    if (!params || !tiles || !kw || !packed || num_tiles < 0 || rows_per_block <= 0 ||
+        (rows_per_block & (rows_per_block - 1)) || (reinterpret_cast<uintptr_t>(packed) & 15) != 0)
+        return pcb::set_error(PCB_E_ARG, "pcb_pack_weights_fp8: bad arguments");
+    if (num_tiles == 0) return PCB_OK;
+    int rpb_log2 = 0;
+    while ((1 << rpb_log2) < rows_per_block) ++rpb_log2;
+    return pcb::launch_status(pcb::launch_k(pack_weights_fp8_kernel, dim3((unsigned)num_tiles), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, params, tiles, rpb_log2, kw, w_stride, packed),
+                              "pcb_pack_weights_fp8");
+}
+
 extern "C" int pcb_pack_weights_multi(const float* params, const PcbPackJob* jobs, const int32_t* tile_job,
                                       const int32_t* tile_index, int32_t total_tiles, void* stream) {
     if (!params || !jobs || !tile_job || !tile_index || total_tiles < 0)
@@ -1109,18 +1238,17 @@ extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const 
                                      const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
                                      int32_t slices_per_cta, void* stream) {
     if (!src || !out || !packed || !tiles || !krow || B <= 0 || ld < B || num_tiles < 0 || mode < 0 || mode > 2 ||
-        (mode == 2 && !src2) || (mode >= 1 && !aux) || prec < 1 || prec > 2 ||
+        (mode == 2 && !src2) || (mode >= 1 && !aux) || prec < 1 || prec > 3 ||
         (batch_tile != 32 && batch_tile != 64) || slices_per_cta < 1 || (reinterpret_cast<uintptr_t>(packed) & 15) != 0)
         return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: bad arguments");
     if (num_tiles == 0) return PCB_OK;
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!src2 || pcb::vec_ok(src2, ld)) &&
                      (!aux || pcb::vec_ok(aux, ld));
     cudaStream_t s = pcb::as_stream(stream);
-    const bool split = prec == 2;
     const int spc = slices_per_cta;
     if (batch_tile == 32)
-        return launch_n<32>(mode, split, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
-    return launch_n<64>(mode, split, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
+        return launch_n<32>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
+    return launch_n<64>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
 }
 
 extern "C" int pcb_lse_contract_tc05_ws(const float* src, const float* src2, const float* aux, float* out,

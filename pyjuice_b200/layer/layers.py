@@ -95,6 +95,12 @@ def _run_rows(tiles_np: np.ndarray, krow_np: np.ndarray) -> int:
     return 0
 
 
+def _mma(prec: int) -> int:
+    """Precision form for the kernels without an E4M3 form (mma.sync, FP32, parameter flows):
+    form 3 (E4M3 tcgen05 contractions) runs them in split bf16."""
+    return 2 if prec == 3 else prec
+
+
 def _ws_ok(ld, B, *bufs) -> bool:
     """Whether pcb_lse_contract_tc05_ws takes these buffers: whole 16-byte chunks per row."""
     return B % 4 == 0 and ld % 4 == 0 and all(b is None or b.data_ptr() % 16 == 0 for b in bufs)
@@ -120,7 +126,8 @@ def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream
             nat.call("pcb_lse_contract_tc05", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
                      nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, c[0], c[1], stream)
 
-    ws_ok = SumLayer.tc05_ws is not False and run_rows in (8, 32) and _ws_ok(ld, B, src, src2, aux, out)
+    ws_ok = (SumLayer.tc05_ws is not False and prec != 3 and run_rows in (8, 32)
+             and _ws_ok(ld, B, src, src2, aux, out))
     ws_bt = 32 if mode == 2 or nt * -(-B // 64) < _num_sms() else 64
     if SumLayer.tc05_ws and ws_ok:
         return run(("ws", ws_bt))
@@ -317,10 +324,12 @@ class Layer:
 class SumLayer(Layer):
     """A layer of sum node vectors with the same block size.
 
-    Precision forms of the sum contractions: plain FP32 (``force_use_fp32``) or the BF16
+    Precision forms of the sum contractions: plain FP32 (``force_use_fp32``) or the
     tensor-core form. ``SumLayer.bf16_form`` selects the latter's variant: 2 (default)
     splits both operands into bf16 hi + lo parts (three MMAs, FP32-like accuracy), 1 uses
-    single bf16 operands.
+    single bf16 operands, 3 runs the tcgen05 contractions (layers of at least
+    ``tc05_min_tiles`` tiles, forward and element flows) in E4M3 with per-row weight scales
+    and the rest in split bf16.
     """
 
     bf16_form = 2
@@ -539,13 +548,13 @@ class SumLayer(Layer):
 
     def forward_pack_job(self, device: torch.device, B: int, force_use_bf16: bool = False,
                          force_use_fp32: bool = False):
-        """``(tiles, kw, packed, rows_per_block, w_stride)`` of the forward weights this layer
-        reads packed (tcgen05 layers; also the single-stage ones with ``pack_short_weights``),
-        or None."""
+        """``(tiles, kw, packed, rows_per_block, w_stride, format)`` of the forward weights this
+        layer reads packed (tcgen05 layers; also the single-stage ones with
+        ``pack_short_weights``), or None; format 1: E4M3 (precision form 3 on tcgen05)."""
         d = self._desc(device)
         prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
         if tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"]):
-            return (d["fw_tiles"], d["kw"], d["fw_pack"], self.block_size, 1)
+            return (d["fw_tiles"], d["kw"], d["fw_pack"], self.block_size, 1, 1 if (tc05 and prec == 3) else 0)
         return None
 
     def flow_pack_jobs(self, device: torch.device, B: int, force_use_fp32: bool = False):
@@ -554,15 +563,17 @@ class SumLayer(Layer):
         jobs = []
         for eg in d["el_groups"]:
             prec = self._el_prec(eg, B, force_use_fp32)
-            if self._el_tc05(eg, prec) or (SumLayer.pack_short_weights and prec > 0 and eg["short"]):
-                jobs.append((eg["tiles"], eg["kw"], eg["pack"], eg["cbs"], self.block_size))
+            tc05 = self._el_tc05(eg, prec)
+            if tc05 or (SumLayer.pack_short_weights and prec > 0 and eg["short"]):
+                jobs.append((eg["tiles"], eg["kw"], eg["pack"], eg["cbs"], self.block_size,
+                             1 if (tc05 and prec == 3) else 0))
         return jobs
 
     @staticmethod
     def _run_pack_job(params: torch.Tensor, job) -> None:
-        t, kw, packed, rpb, w_stride = job
-        nat.call("pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0), rpb, nat.ptr(kw), w_stride,
-                 nat.ptr(packed), nat.stream())
+        t, kw, packed, rpb, w_stride, fmt = job
+        nat.call("pcb_pack_weights_fp8" if fmt == 1 else "pcb_pack_weights", nat.ptr(params), nat.ptr(t), t.size(0),
+                 rpb, nat.ptr(kw), w_stride, nat.ptr(packed), nat.stream())
 
     def pack_forward_weights(self, params: torch.Tensor, B: int, force_use_bf16: bool = False,
                              force_use_fp32: bool = False) -> bool:
@@ -625,12 +636,12 @@ class SumLayer(Layer):
             if d["fw_short"] and SumLayer.short_kernels:
                 nat.call("pcb_lse_contract_short", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None),
                          nat.ptr(node_mars), ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"],
-                         self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, nat.ptr(None),
+                         self.block_size, nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, _mma(prec), nat.ptr(None),
                          d["fw_wlayout"], _short_batch_tile(t.size(0), d["fw_tm"], B), nat.ptr(None), st)
             else:
                 nat.call("pcb_lse_contract", nat.ptr(element_mars), nat.ptr(None), nat.ptr(None), nat.ptr(node_mars),
                          ld, B, nat.ptr(params), nat.ptr(t), t.size(0), d["fw_tm"], self.block_size,
-                         nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, prec, st)
+                         nat.ptr(d["krow"]), nat.ptr(d["kw"]), 1, 0, _mma(prec), st)
             return
         if tc05:
             if not _weights_packed:
@@ -639,6 +650,7 @@ class SumLayer(Layer):
             _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st,
                        d["fw_run"])
             return
+        prec = _mma(prec)
         # _fuse_fw = (term_children, element values out): the product layer below is fused in
         # (the terms are sums of node rows; the element values are written as a side output)
         fuse = kwargs.get("_fuse_fw")
@@ -715,6 +727,7 @@ class SumLayer(Layer):
                 _tc05_call(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld, B,
                            eg["pack"], et, eg["krow"], 1 if allow_modify_flows else 2, prec, st, eg["run"])
                 continue
+            prec = _mma(prec)
             if eg["short"] and SumLayer.short_kernels:
                 packed = eg["pack"] if (_weights_packed and prec > 0 and SumLayer.pack_short_weights) else None
                 # _fuse_bw = out_children: the product layer below is fused in (each element's
@@ -760,7 +773,7 @@ class SumLayer(Layer):
         for eg, et in zip(d["el_groups"], part["el"]):
             if et.size(0) == 0:
                 continue
-            prec = self._el_prec(eg, B, force_use_fp32)
+            prec = _mma(self._el_prec(eg, B, force_use_fp32))
             if eg["short"] and SumLayer.short_kernels:
                 nat.call("pcb_lse_contract_short", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars),
                          nat.ptr(element_flows), ld, B, nat.ptr(params), nat.ptr(et), et.size(0), eg["tm"], eg["cbs"],
@@ -772,7 +785,7 @@ class SumLayer(Layer):
                          nat.ptr(eg["krow"]), nat.ptr(eg["kw"]), self.block_size, 2, prec, st)
         pt = part["pf"]
         if param_flows is not None and pt.size(0) > 0:
-            prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
+            prec = 0 if force_use_fp32 or B < 16 else _mma(SumLayer.bf16_form)
             nat.call("pcb_sum_pflows", nat.ptr(node_flows), nat.ptr(node_mars), nat.ptr(element_mars), ld, B,
                      nat.ptr(params), nat.ptr(param_flows), nat.ptr(pt), pt.size(0), self.block_size,
                      nat.ptr(d["krow"]), nat.ptr(d["kw"]), nat.ptr(d["kpf"]), 0, 1 if self._has_tied else 0, 64, prec, st)
@@ -811,7 +824,7 @@ class SumLayer(Layer):
         for t in (node_flows, element_mars):
             if t.size(1) != B or t.stride(0) != ld or t.stride(1) != 1:
                 raise ValueError("node flows, node values and element values must share one [rows, B] layout")
-        prec = 0 if force_use_fp32 or B < 16 else SumLayer.bf16_form
+        prec = 0 if force_use_fp32 or B < 16 else _mma(SumLayer.bf16_form)
         st = nat.stream()
 
         def run(c, target):

@@ -46,7 +46,7 @@ def _pc_model_backward_hook(grad, pc, inputs, record_cudagraph, apply_cudagraph,
 
 # One PcbPackJob record (include/pcb200.h): three pointers and four int32 fields.
 _PACK_JOB = np.dtype([("tiles", "<u8"), ("kw", "<u8"), ("packed", "<u8"), ("num_tiles", "<i4"),
-                      ("rpb_log2", "<i4"), ("w_stride", "<i4"), ("reserved", "<i4")])
+                      ("rpb_log2", "<i4"), ("w_stride", "<i4"), ("format", "<i4")])
 
 
 class TensorCircuit(nn.Module):
@@ -513,15 +513,16 @@ class TensorCircuit(nn.Module):
         current stream; returns whether anything was launched."""
         if not jobs:
             return False
-        key = tuple(int(j[2].data_ptr()) for j in jobs)
+        key = tuple((int(j[2].data_ptr()), int(j[5])) for j in jobs)  # packed buffer and format
         tab = self._pack_tables.get(key)
         if tab is None:
             rec = np.zeros(len(jobs), dtype=_PACK_JOB)
             tj, ti = [], []
-            for n, (t, kw, packed, rpb, w_stride) in enumerate(jobs):
+            for n, (t, kw, packed, rpb, w_stride, fmt) in enumerate(jobs):
                 if rpb <= 0 or rpb & (rpb - 1):
                     raise ValueError("rows per block must be a power of two")
-                rec[n] = (t.data_ptr(), kw.data_ptr(), packed.data_ptr(), t.size(0), rpb.bit_length() - 1, w_stride, 0)
+                rec[n] = (t.data_ptr(), kw.data_ptr(), packed.data_ptr(), t.size(0), rpb.bit_length() - 1, w_stride,
+                          fmt)
                 tj.append(np.full(t.size(0), n, np.int32))
                 ti.append(np.arange(t.size(0), dtype=np.int32))
             dev = jobs[0][0].device

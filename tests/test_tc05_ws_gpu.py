@@ -145,3 +145,86 @@ def test_ws_rejects_unaligned_batch(cuda_device):
     with pytest.raises(RuntimeError, match="B % 4"):
         nat.call("pcb_lse_contract_tc05_ws", nat.ptr(src), nat.ptr(None), nat.ptr(None), nat.ptr(src), 32, B, 8, 8,
                  nat.ptr(packed), nat.ptr(tiles), 1, nat.ptr(krow), 0, 2, 64, 8, 0, nat.stream())
+
+
+def _pack_fp8(p, device):
+    packed = torch.zeros([p["T"] * 65536], dtype=torch.uint8, device=device)
+    nat.call("pcb_pack_weights_fp8", nat.ptr(p["params"]), nat.ptr(p["tiles"]), p["T"], 32, nat.ptr(p["kw"]), 1,
+             nat.ptr(packed), nat.stream())
+    return packed
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("bt", [32, 64])
+def test_e4m3_form_vs_fp64(mode, bt, cuda_device):
+    """The E4M3 form of the tcgen05 contraction (per-row weight scales, exponentials scaled by
+    448, FP32 accumulation) against FP64: log-sums within 0.1 nats, element flows within
+    10 % (e4m3 keeps 3 mantissa bits; the errors of 128 positive terms partly average out),
+    the same -inf / zero pattern, and clearly less exact than split bf16."""
+    p = _problem(512, cuda_device, seed=40 + mode, run=32)
+    packed = _pack_fp8(p, cuda_device)
+    got = _run(p, packed, mode, 3, "pcb_lse_contract_tc05", bt, 1).double().cpu()
+    torch.cuda.synchronize()
+    assert nat.device_status(clear=True) == 0
+    ref = _fp64(p, mode)
+    fin = torch.isfinite(ref)
+    assert torch.equal(fin, torch.isfinite(got))
+    if mode == 0:
+        err = (got[fin] - ref[fin]).abs()
+        assert err.max() <= 0.1 and err.mean() <= 0.02, (err.max(), err.mean())
+    else:
+        big = fin & (ref.abs() > 1e-3 * ref[fin].abs().max())
+        rel = ((got[big] - ref[big]).abs() / ref[big].abs())
+        assert rel.max() <= 0.1 and rel.mean() <= 0.02, (rel.max(), rel.mean())
+        assert torch.all(got[fin & (ref == 0)] == 0)
+
+
+def test_e4m3_multi_pack_matches_single(cuda_device):
+    """Format 1 of pcb_pack_weights_multi writes the same bytes as pcb_pack_weights_fp8."""
+    import numpy as np
+    from pyjuice_b200.model.tensorcircuit import _PACK_JOB
+    p = _problem(64, cuda_device, seed=7, run=8)
+    ref = _pack_fp8(p, cuda_device)
+    packed = torch.zeros_like(ref)
+    rec = np.zeros(1, dtype=_PACK_JOB)
+    rec[0] = (p["tiles"].data_ptr(), p["kw"].data_ptr(), packed.data_ptr(), p["T"], 5, 1, 1)
+    jobs = torch.from_numpy(rec.view(np.uint8).copy()).to(cuda_device)
+    tj = torch.zeros([p["T"]], dtype=torch.int32, device=cuda_device)
+    ti = torch.arange(p["T"], dtype=torch.int32, device=cuda_device)
+    nat.call("pcb_pack_weights_multi", nat.ptr(p["params"]), nat.ptr(jobs), nat.ptr(tj), nat.ptr(ti), p["T"],
+             nat.stream())
+    torch.cuda.synchronize()
+    per_tile = 16384 + 512
+    for t in range(p["T"]):
+        assert torch.equal(packed[t * 65536:t * 65536 + per_tile], ref[t * 65536:t * 65536 + per_tile])
+
+
+def test_e4m3_form_on_hclt784_after_bf16(cuda_device):
+    """HCLT-784 at batch 256: a split-bf16 pass, then the E4M3 form on the same circuit (the
+    weight packs switch format), then split bf16 again. The E4M3 log-likelihoods (3 mantissa
+    bits in the 17 tcgen05 levels) stay within 1.5 nats per sample of the split-bf16 ones,
+    0.6 on average (measured: 0.66 and 0.39 at mean LL ~ -2700), and the second split-bf16
+    pass reproduces the first bit for bit."""
+    from conftest import load_fixture
+    from helpers import build_fixture_circuit, load_fixture_params
+    from pyjuice_b200.layer.layers import SumLayer
+    import numpy as np
+    fx = load_fixture("hclt784")
+    pc = build_fixture_circuit("hclt784", fx).to(cuda_device)
+    load_fixture_params(pc, fx)
+    x = torch.from_numpy(np.random.default_rng(21).integers(0, 256, size=(256, 784))).to(cuda_device)
+    saved = SumLayer.bf16_form
+    try:
+        out = []
+        for form in (2, 3, 2):
+            SumLayer.bf16_form = form
+            with torch.no_grad():
+                out.append(pc(x, force_use_bf16=True).clone())
+            pc.init_param_flows(flows_memory=0.0)
+            pc.backward(inputs=x, allow_modify_flows=True)
+            assert torch.isfinite(pc.param_flows).all()
+    finally:
+        SumLayer.bf16_form = saved
+    assert torch.equal(out[0], out[2])
+    d = (out[1] - out[0]).abs()
+    assert torch.isfinite(out[1]).all() and d.max() < 1.5 and d.mean() < 0.6, (d.max(), d.mean())
