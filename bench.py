@@ -66,9 +66,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=BATCH)
-    p.add_argument("--workload", default="em", choices=["em", "adjoint"],
+    p.add_argument("--workload", default="em", choices=["em", "adjoint", "pd"],
                    help="em: the EM step on HCLT-784 (default); adjoint: the soft-evidence log-likelihood and its "
-                        "gradients on HCLT-3072 (32x32x3 fields, 256 latents, batch 128)")
+                        "gradients on HCLT-3072 (32x32x3 fields, 256 latents, batch 128); pd: full-batch EM epochs "
+                        "on a Poon-Domingos circuit over 28x28 (256 latents, block 64, batch 256)")
     p.add_argument("--fd", action="store_true", help="adjoint workload: also check coordinates of both gradients "
                                                      "against FP64 central differences of the oracle (minutes)")
     p.add_argument("--profile-step", action="store_true",
@@ -439,10 +440,97 @@ def adjoint_fd_check(pc, z, ev, device, n_coords=2, h=1e-6):
             "max_rel_err_logits": max(errs["logits"]), "max_rel_err_evidence": max(errs["evidence"])}
 
 
+def pd_workload(args):
+    """Poon-Domingos circuit over 28x28 vars (256 categories), 256 latents, block 64,
+    split_intervals 4, ``torch.manual_seed(0)`` before construction; quantised random-field
+    data. One full-batch EM epoch per precision form (plain FP32, split bf16, E4M3 on the
+    tcgen05 levels): 234 batches of 256 (59,904 samples; the 96-sample remainder of 60,000
+    is dropped), per batch forward + backward + FP64 flow accumulation, then one EM update
+    from the FP64 flows. Epochs timed with CUDA events after one warm-up epoch of the form;
+    the data is resident. LL error of each form against the FP64 oracle on 16 samples at the
+    initial parameters."""
+    import pyjuice_b200 as juice
+    from pyjuice_b200 import _native as nat
+    from pyjuice_b200.layer.layers import SumLayer
+    from pyjuice_b200.nodes.distributions import Categorical
+    from pyjuice_b200.structures import PD
+    ws, rank, local = dist_env()
+    if ws > 1 and rank != 0:
+        return
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    nat.load()
+    B, nb = 256, 234
+    data = make_data(60000)
+    torch.manual_seed(0)
+    ns = PD((SIDE, SIDE), num_latents=256, split_intervals=4, block_size=64, input_dist=Categorical(num_cats=NUM_CATS))
+    pc = juice.compile(ns).to(device)
+    data_dev = data[:B * nb].to(device)
+    forms = (("fp32", 2, {"force_use_fp32": True}), ("bf16_split", 2, {"force_use_bf16": True}),
+             ("e4m3", 3, {"force_use_bf16": True}))
+    # LL error at the initial parameters
+    from oracle import pc_oracle as orc
+    lay = orc.layout_from_circuit(pc)
+    p64 = pc.params.detach().double().cpu().numpy()
+    q64 = pc.input_layer_group[0].params.detach().double().cpu().numpy()
+    xs = data[:16]
+    _, _, lls_o = orc.forward(lay, p64, q64, xs.numpy())
+    ll_err = {}
+    with torch.no_grad():
+        for name, form, kw in forms:
+            SumLayer.bf16_form = form
+            got = pc(xs.to(device), **kw).double().cpu().numpy()
+            ll_err[name] = {"mean_abs_dll_nats": float(np.abs(got - lls_o).mean()),
+                            "max_abs_dll_nats": float(np.abs(got - lls_o).max())}
+    ll_err["mean_ll_nats"] = float(lls_o.mean())
+
+    def epoch(kw):
+        pc.init_param_flows_f64()
+        for i in range(nb):
+            x = data_dev[i * B:(i + 1) * B]
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                pc(x, **kw)
+            pc.backward(inputs=x, allow_modify_flows=True, force_use_fp32="force_use_fp32" in kw)
+            pc.accumulate_param_flows_f64()
+        pc.mini_batch_em(step_size=1.0, pseudocount=PSEUDOCOUNT, use_f64_flows=True)
+
+    res = {}
+    init = pc.params.detach().clone(), pc.input_layer_group[0].params.detach().clone()
+    for name, form, kw in forms:
+        SumLayer.bf16_form = form
+        pc.params.data.copy_(init[0])
+        pc.input_layer_group[0].params.data.copy_(init[1])
+        epoch(kw)  # warm-up (autotuning, buffers)
+        pc.params.data.copy_(init[0])
+        pc.input_layer_group[0].params.data.copy_(init[1])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        epoch(kw)
+        e1.record()
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        res[name] = {"epoch_s": sec, "samples_per_s": B * nb / sec,
+                     "params_finite": bool(torch.isfinite(pc.params).all())}
+    SumLayer.bf16_form = 2
+    out = {"metric": "full-batch EM epoch samples/s (fwd+bwd+FP64 flow accumulation, one EM update) 1xB200",
+           "value": res["bf16_split"]["samples_per_s"], "unit": "samples/s", "n_gpus": 1, "steps": nb,
+           "warmup": 1, "ms_per_step": res["bf16_split"]["epoch_s"] * 1e3 / nb, "higher_is_better": True,
+           "dtype": "bf16", "data": "synthetic",
+           "config": {"workload": "PD 28x28 vars x 256 cats, 256 latents, block 64, split_intervals 4, batch 256, "
+                                  "epoch of 234 batches", "num_nodes": pc.num_nodes, "num_edges": pc.num_edges,
+                      "num_sum_params": pc.num_sum_params},
+           "forms": res, "ll_error_vs_fp64": ll_err}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "adjoint":
         return adjoint_workload(args)
+    if args.workload == "pd":
+        return pd_workload(args)
     if args.impl == "reference":
         return reference_arm(args)
     ws, rank, local = dist_env()

@@ -384,6 +384,43 @@ class TensorCircuit(nn.Module):
             ends = np.concatenate([idx[cuts] + 1, [idx[-1] + 1]])
             ranges = [(int(a), int(b)) for a, b in zip(starts, ends)]
         self._nf_init_ranges = ranges
+        self._ef_init_ranges = self._plan_element_flow_init()
+
+    def _plan_element_flow_init(self):
+        """Per product layer group: the element-flow rows it reads that the sum group right
+        above it does not write.
+
+        As in the reference, the element rows are one buffer that every product layer group
+        reuses: the sum group above a product group writes the flows of that group's
+        elements, which the product layers then read. An element without a parent sum node (a
+        product that no sum block selected, as in PD structures with
+        ``max_prod_block_conns``) is not written there, and its rows would still hold the
+        flows of another group's elements; those rows are zeroed before the product group's
+        backward pass (the reference zeroes the whole buffer, tensorcircuit.py:394-395)."""
+        plan = dict()
+        groups = self.inner_layer_groups
+        for gi, group in enumerate(groups):
+            if not group.is_prod() or gi + 1 >= len(groups):
+                continue
+            read = np.zeros([self.num_elements], dtype=bool)
+            for layer in group:
+                chs = layer._host_desc()["bk_chs"].numpy().astype(np.int64)
+                read[(chs[:, None] + np.arange(layer.block_size)[None, :]).reshape(-1)] = True
+            written = np.zeros([self.num_elements], dtype=bool)
+            for layer in groups[gi + 1]:
+                for eg in layer._host_desc()["el_groups"]:
+                    for t in eg["tiles"].numpy():
+                        written[int(t[0]):int(t[0]) + int(t[1])] = True
+            need = read & ~written
+            need[:self.num_dummy_eles] = False  # filled at the start of the pass
+            idx = np.flatnonzero(need)
+            if not idx.size:
+                continue
+            cuts = np.flatnonzero(np.diff(idx) != 1)
+            starts = np.concatenate([[idx[0]], idx[cuts + 1]])
+            ends = np.concatenate([idx[cuts] + 1, [idx[-1] + 1]])
+            plan[gi] = [(int(a), int(b)) for a, b in zip(starts, ends)]
+        return plan
 
     def _build_em_tables(self):
         """Per sum node block: parameter / flow base, #children, block size (untied vectors only).
@@ -718,6 +755,10 @@ class TensorCircuit(nn.Module):
             if group.is_prod():
                 if layer_id in fused_prod:  # the sum layer above wrote these flows
                     continue
+                # element rows that the sum group above left unwritten (parentless elements)
+                for a, b in self._ef_init_ranges.get(layer_id, ()):
+                    nat.call("pcb_fill_rows", nat.ptr(self.element_flows), B, a, b,
+                             -float("inf") if logspace_flows else 0.0, nat.stream())
                 rf = rw_flags.get(layer_id)
                 group.backward(self.node_flows, self.element_flows, logspace_flows=logspace_flows,
                                _modify=None if rf is None else (self.node_mars, rf))

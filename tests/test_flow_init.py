@@ -80,3 +80,36 @@ def test_shared_children_flows_vs_oracle(cuda_device):
         assert np.abs(nf[real] - nf_o[real]).max() <= 1e-5 * np.abs(nf_o[real]).max()
         pf = pc.param_flows.double().cpu().numpy()
         assert np.abs(pf - pf_o).max() <= 1e-4 * np.abs(pf_o).max()
+
+
+def test_parentless_elements_are_zeroed_each_pass():
+    """A PD structure with max_prod_block_conns = 1 leaves product nodes that no sum block
+    selects. The element rows are one buffer reused by every product group, so per product
+    group the plan zeroes exactly the rows of its elements that have no parent in the sum
+    group above (they would otherwise hold another group's element flows)."""
+    import numpy as np
+    import torch
+    import pyjuice_b200 as juice
+    torch.manual_seed(7)
+    pc = juice.compile(juice.structures.PD((4, 4), 16, split_intervals=1, max_prod_block_conns=1,
+                                           input_dist=juice.distributions.Categorical(num_cats=4)))
+    groups = pc.inner_layer_groups
+    found = 0
+    for gi, group in enumerate(groups):
+        if not group.is_prod() or gi + 1 >= len(groups):
+            continue
+        produced, children = set(), set()
+        for layer in group:
+            for nids in layer.partitioned_nids:
+                for n in nids.tolist():
+                    produced.update(range(n, n + layer.block_size))
+        for layer in groups[gi + 1]:
+            for cids in layer.partitioned_cids:
+                children.update(int(c) for c in cids.reshape(-1).tolist() if c != 0)
+        orphans = produced - children
+        planned = set()
+        for a, b in pc._ef_init_ranges.get(gi, ()):
+            planned.update(range(a, b))
+        assert planned == orphans, gi
+        found += len(orphans)
+    assert found > 0

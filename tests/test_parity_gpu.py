@@ -383,6 +383,35 @@ def test_pd_and_hmm_match_reference(cuda_device):
     assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-5
 
 
+def test_pd_with_parentless_products_flows_vs_oracle(cuda_device):
+    """A PD circuit with products that no sum node selects (max_prod_block_conns = 1): FP32
+    parameter and input flows against the FP64 oracle on two consecutive backward passes
+    (the parentless elements' flow rows must read as zero in every pass), and the second pass
+    equal to the first."""
+    torch.manual_seed(7)
+    pc = juice.compile(juice.structures.PD((4, 4), 16, split_intervals=1, max_prod_block_conns=1,
+                                           input_dist=juice.distributions.Categorical(num_cats=4))).to(cuda_device)
+    assert pc._ef_init_ranges
+    lay = orc.layout_from_circuit(pc)
+    rng = np.random.default_rng(3)
+    x = rng.integers(0, 4, size=(64, 16))
+    p0 = pc.params.double().cpu().numpy()
+    q0 = pc.input_layer_group[0].params.double().cpu().numpy()
+    nm, ems, _ = orc.forward(lay, p0, q0, x)
+    _, pf_o, ipf_o = orc.backward(lay, p0, x, nm, ems)
+    out = []
+    for _ in range(2):
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            pc(torch.from_numpy(x).to(cuda_device), force_use_fp32=True)
+        pc.backward(inputs=torch.from_numpy(x).to(cuda_device), allow_modify_flows=False, force_use_fp32=True)
+        pf = pc.param_flows.double().cpu().numpy()
+        ipf = pc.input_layer_group[0].param_flows.double().cpu().numpy()[:ipf_o.shape[0]]
+        assert _rel(pf, pf_o) <= 1e-4 and _rel(ipf, ipf_o) <= 1e-4
+        out.append((pf, ipf))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("name", ["bern", "gauss"])
 def test_bernoulli_and_gaussian_layers_match_reference(name, cuda_device):
     """Bernoulli and Gaussian input layers: FP32 forward, flows and one EM step against the
