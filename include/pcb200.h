@@ -334,6 +334,21 @@ int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux,
                           int32_t mode, int32_t prec, int32_t batch_tile, int32_t slices_per_cta, void* stream);
 
 /*
+ * pcb_lse_contract_tc05 for a later chunk of the tiles' terms: the tile table holds the
+ * next (at most 128) terms of each tile, and the result is combined with out instead of
+ * overwriting it: log(e^out + e^result) for the sum forward (mode 0), out + result for
+ * the element flows (modes 1/2). A tile of more than 128 terms is contracted exactly by one
+ * pcb_lse_contract_tc05 launch over its first 128 terms and one accumulating launch per
+ * further 128 terms (each chunk with its own per-sample max).
+ * Replaces the same reference kernels as pcb_lse_contract (sum_layer.py:454-568,
+ * 1572-1730) for tiles of any length.
+ */
+int pcb_lse_contract_tc05_accum(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
+                                int32_t B, const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles,
+                                const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
+                                int32_t slices_per_cta, void* stream);
+
+/*
  * pcb_lse_contract_tc05 as a persistent, warp-specialised kernel: num_ctas CTAs (0: one
  * per SM) each own a contiguous run of (tile, batch_tile-sample slice) work units. One warp
  * stages a unit's source rows in shared memory with 2-D TMA loads (a box of 32 samples x

@@ -120,6 +120,8 @@ _SIGS = {
     "pcb_pack_weights_multi": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_tc05": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_int32,
                                c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_lse_contract_tc05_accum": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
+                                     c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_tc05_ws": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int64, c_int64, c_void_p,
                                   c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p],
                                  c_int32),

@@ -304,6 +304,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 
+// log(e^a + e^b) (-inf + -inf = -inf), with the hardware base-2 approximations.
+__device__ __forceinline__ float log_add(float a, float b) {
+    const float hi = fmaxf(a, b), lo = fminf(a, b);
+    return hi == -INFINITY ? -INFINITY : hi + pcb::fast_log(1.f + pcb::fast_exp(lo - hi));
+}
+
 // One CTA per tile and run of up to spc consecutive N-sample slices. The packed weights are
 // copied once per CTA; the source values (and epilogue element values) of slice s + 1 are
 // prefetched into L2 while slice s is reduced, exponentiated, contracted and written out.
@@ -312,7 +318,7 @@ __global__ void __launch_bounds__(tc05_threads<N>(), 2)
 lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
                 float* __restrict__ out, int64_t ld, int B, const uint8_t* __restrict__ packed,
                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, int spc, bool vec,
-                int32_t* __restrict__ status) {
+                bool accum, int32_t* __restrict__ status) {
     // tile and term indices (compiled tables) before the wait for the previous kernel
     pcb::pdl_trigger();
     static_assert(N == 32 || N == 64, "sample slice");
@@ -583,6 +589,18 @@ lse_tc05_kernel(const float* __restrict__ src, const float* __restrict__ src2, c
                     if (fail) o[j] = __int_as_float(0x7fc00000);
                     else if (MODE == 0) o[j] = (mm == -INFINITY) ? -INFINITY : pcb::fast_log(val) + mm;
                     else o[j] = (mm == -INFINITY) ? 0.f : val * pcb::fast_exp(a[c4 * 4 + j] + mm);
+                }
+                if (accum && !fail) {  // a later chunk of the tile's terms: combine with the output
+                    float old[4];
+                    if (vec && b + 3 < B) {
+                        const float4 ov = *reinterpret_cast<const float4*>(dst + c4 * 4);
+                        old[0] = ov.x; old[1] = ov.y; old[2] = ov.z; old[3] = ov.w;
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) old[j] = (b + j < B) ? dst[c4 * 4 + j] : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) o[j] = MODE == 0 ? log_add(old[j], o[j]) : old[j] + o[j];
                 }
                 if (vec && b + 3 < B) {
                     *reinterpret_cast<float4*>(dst + c4 * 4) = make_float4(o[0], o[1], o[2], o[3]);
@@ -1159,7 +1177,7 @@ int launch_ws_n(int mode, bool split, int num_tiles, int num_ctas, const CUtenso
 
 template <int N, int MODE, int PREC>
 int launch(int num_tiles, int spc, const float* src, const float* src2, const float* aux, float* out, int64_t ld,
-           int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s, bool vec) {
+           int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow, cudaStream_t s, bool vec, bool accum) {
     constexpr size_t smem = Tc05Smem<N>::bytes();
     static_assert(smem <= 227 * 1024, "shared memory");
     static bool configured[64] = {false};
@@ -1174,7 +1192,7 @@ int launch(int num_tiles, int spc, const float* src, const float* src2, const fl
     if (gy > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract_tc05: batch too large");
     return pcb::launch_status(pcb::launch_k(lse_tc05_kernel<N, MODE, PREC>,
                                             dim3((unsigned)num_tiles, (unsigned)gy), dim3(tc05_threads<N>()), smem, s,
-                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec,
+                                            1u, src, src2, aux, out, ld, B, packed, tiles, krow, spc, vec, accum,
                                             pcb::status_word()),
                               "pcb_lse_contract_tc05");
 }
@@ -1182,8 +1200,8 @@ int launch(int num_tiles, int spc, const float* src, const float* src2, const fl
 template <int N>
 int launch_n(int mode, int prec, int num_tiles, int spc, const float* src, const float* src2, const float* aux,
              float* out, int64_t ld, int B, const uint8_t* packed, const PcbLseTile* tiles, const int* krow,
-             cudaStream_t s, bool vec) {
-#define PCB_TC(M, P) launch<N, M, P>(num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec)
+             cudaStream_t s, bool vec, bool accum) {
+#define PCB_TC(M, P) launch<N, M, P>(num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec, accum)
     if (prec == 3) return mode == 0 ? PCB_TC(0, 3) : (mode == 1 ? PCB_TC(1, 3) : PCB_TC(2, 3));
     if (prec == 2) return mode == 0 ? PCB_TC(0, 2) : (mode == 1 ? PCB_TC(1, 2) : PCB_TC(2, 2));
     return mode == 0 ? PCB_TC(0, 1) : (mode == 1 ? PCB_TC(1, 1) : PCB_TC(2, 1));
@@ -1233,10 +1251,10 @@ extern "C" int pcb_pack_weights_multi(const float* params, const PcbPackJob* job
                                             tile_index), "pcb_pack_weights_multi");
 }
 
-extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
+static int tc05_entry(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
                                      int32_t B, const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles,
                                      const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
-                                     int32_t slices_per_cta, void* stream) {
+                                     int32_t slices_per_cta, void* stream, bool accum) {
     if (!src || !out || !packed || !tiles || !krow || B <= 0 || ld < B || num_tiles < 0 || mode < 0 || mode > 2 ||
         (mode == 2 && !src2) || (mode >= 1 && !aux) || prec < 1 || prec > 3 ||
         (batch_tile != 32 && batch_tile != 64) || slices_per_cta < 1 || (reinterpret_cast<uintptr_t>(packed) & 15) != 0)
@@ -1247,8 +1265,25 @@ extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const 
     cudaStream_t s = pcb::as_stream(stream);
     const int spc = slices_per_cta;
     if (batch_tile == 32)
-        return launch_n<32>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
-    return launch_n<64>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec);
+        return launch_n<32>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec,
+                            accum);
+    return launch_n<64>(mode, prec, num_tiles, spc, src, src2, aux, out, ld, B, packed, tiles, krow, s, vec, accum);
+}
+
+extern "C" int pcb_lse_contract_tc05(const float* src, const float* src2, const float* aux, float* out, int64_t ld,
+                                     int32_t B, const uint8_t* packed, const PcbLseTile* tiles, int32_t num_tiles,
+                                     const int32_t* krow, int32_t mode, int32_t prec, int32_t batch_tile,
+                                     int32_t slices_per_cta, void* stream) {
+    return tc05_entry(src, src2, aux, out, ld, B, packed, tiles, num_tiles, krow, mode, prec, batch_tile,
+                      slices_per_cta, stream, false);
+}
+
+extern "C" int pcb_lse_contract_tc05_accum(const float* src, const float* src2, const float* aux, float* out,
+                                           int64_t ld, int32_t B, const uint8_t* packed, const PcbLseTile* tiles,
+                                           int32_t num_tiles, const int32_t* krow, int32_t mode, int32_t prec,
+                                           int32_t batch_tile, int32_t slices_per_cta, void* stream) {
+    return tc05_entry(src, src2, aux, out, ld, B, packed, tiles, num_tiles, krow, mode, prec, batch_tile,
+                      slices_per_cta, stream, true);
 }
 
 extern "C" int pcb_lse_contract_tc05_ws(const float* src, const float* src2, const float* aux, float* out,

@@ -95,6 +95,40 @@ def _run_rows(tiles_np: np.ndarray, krow_np: np.ndarray) -> int:
     return 0
 
 
+_MAX_CHUNK_TILES = 16384  # sub-tiles (64 KB of packed weights each) a layer may split its long tiles into
+
+
+def _chunk_table(tiles_np: np.ndarray):
+    """Tiles of more than 128 terms as consecutive chunks of at most 128 terms: chunk j holds
+    terms 128 j .. of every tile that has them (same output rows; ``k_off`` advanced, which
+    also advances the weights). Returns ``(table, [(start, count) per chunk])`` or None when
+    every tile is short (or the split would exceed ``_MAX_CHUNK_TILES``)."""
+    if not tiles_np.shape[0] or int(tiles_np[:, 3].max()) <= _SHORT_K:
+        return None
+    nch = -(-int(tiles_np[:, 3].max()) // _SHORT_K)
+    parts, ranges, start = [], [], 0
+    for j in range(nch):
+        t = tiles_np[tiles_np[:, 3] > _SHORT_K * j].copy()
+        t[:, 2] += _SHORT_K * j
+        t[:, 3] = np.minimum(t[:, 3] - _SHORT_K * j, _SHORT_K)
+        parts.append(t)
+        ranges.append((start, t.shape[0]))
+        start += t.shape[0]
+    if start > _MAX_CHUNK_TILES:
+        return None
+    return np.concatenate(parts), ranges
+
+
+def _tc05_chunks(src, src2, aux, out, ld, B, pack, table, ranges, krow, mode, prec, stream):
+    """A contraction over tiles of any length on the tcgen05 kernels: the first chunk of 128
+    terms overwrites the output, every later chunk combines into it
+    (pcb_lse_contract_tc05_accum: log-add-exp for the forward, sum for element flows)."""
+    for j, (a, n) in enumerate(ranges):
+        t = table[a:a + n]
+        pk = pack[a * _PACK_BYTES:(a + n) * _PACK_BYTES]
+        _tc05_call(src, src2, aux, out, ld, B, pk, t, krow, mode, prec, stream, accum=j > 0)
+
+
 def _mma(prec: int) -> int:
     """Precision form for the kernels without an E4M3 form (mma.sync, FP32, parameter flows):
     form 3 (E4M3 tcgen05 contractions) runs them in split bf16."""
@@ -106,15 +140,21 @@ def _ws_ok(ld, B, *bufs) -> bool:
     return B % 4 == 0 and ld % 4 == 0 and all(b is None or b.data_ptr() % 16 == 0 for b in bufs)
 
 
-def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream, run_rows=0):
+def _tc05_call(src, src2, aux, out, ld, B, pack, tiles, krow, mode, prec, stream, run_rows=0, accum=False):
     """One tcgen05 contraction: the persistent warp-specialised kernel
     (pcb_lse_contract_tc05_ws, 32- or 64-sample units) or the CTA-per-slice kernel
     (pcb_lse_contract_tc05, 32 or 64 samples and 1 or 2 slices per CTA), chosen by the
     autotuner per mode, precision form, tile count and batch. ``SumLayer.tc05_ws`` forces
     (True) or excludes (False) the persistent kernel; ``SumLayer.tc05_slices_per_cta`` fixes
     the CTA-per-slice kernel's slices and its static batch tile. ``run_rows``: the tile
-    table's runs of consecutive source rows (``_run_rows``; 0 excludes the persistent kernel)."""
+    table's runs of consecutive source rows (``_run_rows``; 0 excludes the persistent kernel).
+    ``accum``: combine into the output (a later chunk of long tiles; static launch shape, since
+    timing candidates would accumulate repeatedly)."""
     nt = tiles.size(0)
+    if accum:
+        nat.call("pcb_lse_contract_tc05_accum", nat.ptr(src), nat.ptr(src2), nat.ptr(aux), nat.ptr(out), ld, B,
+                 nat.ptr(pack), nat.ptr(tiles), nt, nat.ptr(krow), mode, prec, _tc05_batch_tile(nt, B), 1, stream)
+        return
 
     def run(c):
         if c[0] == "ws":
@@ -337,6 +377,7 @@ class SumLayer(Layer):
     tc05_min_tiles = 6    # layers with at least this many tiles use the tcgen05 kernels (BF16 forms)
     tc05_slices_per_cta = None  # sample slices per tcgen05 CTA (None: one)
     tc05_ws = None        # persistent warp-specialised tcgen05 kernel: None autotuned, True forced, False off
+    tc05_long = True      # tiles of more than 128 terms as accumulating tcgen05 chunks (BF16 / E4M3 forms)
     # The single-stage kernels of small layers read pre-packed weights too (the circuit packs
     # all layers' weights in one launch per pass, so the kernels skip their own conversion).
     pack_short_weights = True
@@ -464,7 +505,10 @@ class SumLayer(Layer):
                     tiles.append((starts[g] + j0, nr, offs[g], klist[g].shape[0], j0 * bs, starts[g] + j0, gs_w, 0))
             tiles_np = np.asarray(tiles, np.int64).reshape(-1, 8)
             kw_np = np.concatenate(wlist)
+            ech_t = _chunk_table(tiles_np)
             el_groups.append(dict(
+                ch=None if ech_t is None else _i32(ech_t[0]), ch_ranges=None if ech_t is None else ech_t[1],
+                ch_pack=None if ech_t is None else torch.empty([ech_t[0].shape[0] * _PACK_BYTES], dtype=torch.uint8),
                 cbs=cbs, tm=_tile_rows(max(t[1] for t in tiles)), tiles=_i32(tiles_np),
                 krow=_i32(np.concatenate(klist)), kw=_i32(kw_np),
                 short=int(tiles_np[:, 3].max()) <= _SHORT_K,
@@ -473,7 +517,10 @@ class SumLayer(Layer):
                 pack=torch.empty([tiles_np.shape[0] * _PACK_BYTES], dtype=torch.uint8)))
 
         fw_np = np.asarray(fw_tiles, np.int64).reshape(-1, 8)
+        fch = _chunk_table(fw_np)
         return dict(
+            fw_ch=None if fch is None else _i32(fch[0]), fw_ch_ranges=None if fch is None else fch[1],
+            fw_ch_pack=None if fch is None else torch.empty([fch[0].shape[0] * _PACK_BYTES], dtype=torch.uint8),
             fw_tiles=_i32(fw_np), fw_tm=fw_tm, fw_run=_run_rows(fw_np, krow_c),
             fw_short=bool(fw_np.shape[0]) and int(fw_np[:, 3].max()) <= _SHORT_K,
             fw_wlayout=1 if (fw_np.shape[0] and _rows_vec4(fw_np, kw_c, bs, 1)) else 0,
@@ -531,6 +578,15 @@ class SumLayer(Layer):
     def _el_prec(self, eg, B, force_use_fp32):
         return SumLayer.bf16_form if (not force_use_fp32 and eg["tm"] >= 16 and B >= 16) else 0
 
+    def _fw_long(self, d, prec):
+        """Whether the forward runs its tiles of more than 128 terms as tcgen05 chunks."""
+        return (prec > 0 and SumLayer.tc05_long and not d["fw_short"] and d["fw_ch"] is not None
+                and d["fw_ch"].size(0) >= SumLayer.tc05_min_tiles)
+
+    def _el_long(self, eg, prec):
+        return (prec > 0 and SumLayer.tc05_long and not eg["short"] and eg["ch"] is not None
+                and eg["ch"].size(0) >= SumLayer.tc05_min_tiles)
+
     def _el_tc05(self, eg, prec):
         return prec > 0 and eg["short"] and eg["tiles"].size(0) >= SumLayer.tc05_min_tiles
 
@@ -555,6 +611,8 @@ class SumLayer(Layer):
         prec, tc05 = self._fw_tc05(d, B, force_use_bf16, force_use_fp32)
         if tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"]):
             return (d["fw_tiles"], d["kw"], d["fw_pack"], self.block_size, 1, 1 if (tc05 and prec == 3) else 0)
+        if self._fw_long(d, prec):
+            return (d["fw_ch"], d["kw"], d["fw_ch_pack"], self.block_size, 1, 1 if prec == 3 else 0)
         return None
 
     def flow_pack_jobs(self, device: torch.device, B: int, force_use_fp32: bool = False):
@@ -567,6 +625,8 @@ class SumLayer(Layer):
             if tc05 or (SumLayer.pack_short_weights and prec > 0 and eg["short"]):
                 jobs.append((eg["tiles"], eg["kw"], eg["pack"], eg["cbs"], self.block_size,
                              1 if (tc05 and prec == 3) else 0))
+            elif self._el_long(eg, prec):
+                jobs.append((eg["ch"], eg["kw"], eg["ch_pack"], eg["cbs"], self.block_size, 1 if prec == 3 else 0))
         return jobs
 
     @staticmethod
@@ -650,6 +710,12 @@ class SumLayer(Layer):
             _tc05_call(element_mars, None, None, node_mars, ld, B, d["fw_pack"], t, d["krow"], 0, prec, st,
                        d["fw_run"])
             return
+        if self._fw_long(d, prec):
+            if not _weights_packed:
+                self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
+            _tc05_chunks(element_mars, None, None, node_mars, ld, B, d["fw_ch_pack"], d["fw_ch"], d["fw_ch_ranges"],
+                         d["krow"], 0, prec, st)
+            return
         prec = _mma(prec)
         # _fuse_fw = (term_children, element values out): the product layer below is fused in
         # (the terms are sums of node rows; the element values are written as a side output)
@@ -715,8 +781,8 @@ class SumLayer(Layer):
             ready = torch.cuda.Event()
             ready.record()
         # element flows
-        if not _weights_packed and any(self._el_tc05(eg, self._el_prec(eg, B, force_use_fp32))
-                                       for eg in d["el_groups"]):
+        if not _weights_packed and any(self._el_tc05(eg, p) or self._el_long(eg, p)
+                                       for eg in d["el_groups"] for p in (self._el_prec(eg, B, force_use_fp32),)):
             self.pack_flow_weights(params, B, force_use_fp32)
             _weights_packed = True
         for eg in d["el_groups"]:
@@ -726,6 +792,11 @@ class SumLayer(Layer):
                 st = nat.stream()
                 _tc05_call(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld, B,
                            eg["pack"], et, eg["krow"], 1 if allow_modify_flows else 2, prec, st, eg["run"])
+                continue
+            if self._el_long(eg, prec):
+                _tc05_chunks(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld,
+                             B, eg["ch_pack"], eg["ch"], eg["ch_ranges"], eg["krow"], 1 if allow_modify_flows else 2,
+                             prec, nat.stream())
                 continue
             prec = _mma(prec)
             if eg["short"] and SumLayer.short_kernels:

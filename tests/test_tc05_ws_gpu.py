@@ -228,3 +228,97 @@ def test_e4m3_form_on_hclt784_after_bf16(cuda_device):
     assert torch.equal(out[0], out[2])
     d = (out[1] - out[0]).abs()
     assert torch.isfinite(out[1]).all() and d.max() < 1.5 and d.mean() < 0.6, (d.max(), d.mean())
+
+
+def _long_problem(B, device, seed):
+    """Tiles of 1 .. 400 terms (runs of 32 rows), for the chunked tcgen05 path."""
+    g = torch.Generator().manual_seed(seed)
+    shapes = [(128, 400), (96, 300), (40, 129), (128, 128), (128, 17), (33, 257)]
+    T = len(shapes)
+    n_src = 1200
+    tiles, krow, kw = [], [], []
+    for t, (nr, kc) in enumerate(shapes):
+        tiles.append([t * 128, nr, len(krow), kc, t * 128 * 400, t * 128, 32, 0])
+        for k0 in range(0, kc, 32):
+            start = int(torch.randint(0, n_src - 32 + 1, (1,), generator=g))
+            krow += [start + j for j in range(min(32, kc - k0))]
+        kw += [k * 128 for k in range(kc)]
+    src = torch.rand([n_src, B], generator=g) * 30 - 40
+    src[5] = -float("inf")
+    flows = torch.rand([n_src, B], generator=g)
+    aux = torch.rand([T * 128, B], generator=g) * 4 - 5
+    params = torch.rand([T * 128 * 400], generator=g) + 0.05
+    dev = lambda x: x.to(device)
+    return dict(src=dev(src), flows=dev(flows), aux=dev(aux), params=dev(params),
+                tiles=dev(torch.tensor(tiles, dtype=torch.int32)), krow=dev(torch.tensor(krow, dtype=torch.int32)),
+                kw=dev(torch.tensor(kw, dtype=torch.int32)), shapes=shapes, B=B, T=T, run=32)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("prec", [2, 3])
+def test_long_tiles_as_tc05_chunks_vs_fp64(mode, prec, cuda_device):
+    """Tiles of up to 400 terms contracted as accumulating 128-term chunks on the tcgen05
+    kernel (first chunk overwrites, later chunks log-add / add) against FP64: split bf16
+    within 1e-4, E4M3 within the bounds of its single-chunk test."""
+    from pyjuice_b200.layer.layers import _chunk_table, _tc05_chunks
+    p = _long_problem(256, cuda_device, seed=60 + mode + 3 * prec)
+    tab, ranges = _chunk_table(p["tiles"].cpu().numpy().astype("int64"))
+    ct = torch.from_numpy(tab).to(torch.int32).to(cuda_device)
+    pack = torch.zeros([ct.size(0) * 65536], dtype=torch.uint8, device=cuda_device)
+    nat.call("pcb_pack_weights_fp8" if prec == 3 else "pcb_pack_weights", nat.ptr(p["params"]), nat.ptr(ct),
+             ct.size(0), 32, nat.ptr(p["kw"]), 1, nat.ptr(pack), nat.stream())
+    src = p["flows"] if mode == 2 else p["src"]
+    out = torch.full([p["T"] * 128, p["B"]], 12345.0, device=cuda_device)
+    _tc05_chunks(src, p["src"] if mode == 2 else None, p["aux"] if mode else None, out, p["B"], p["B"], pack, ct,
+                 ranges, p["krow"], mode, prec, nat.stream())
+    torch.cuda.synchronize()
+    assert nat.device_status(clear=True) == 0
+    got = out.double().cpu()
+    ref = _fp64(p, mode)
+    rows = torch.zeros([p["T"] * 128], dtype=torch.bool)
+    for t, (nr, _) in enumerate(p["shapes"]):
+        rows[t * 128:t * 128 + nr] = True
+    got, ref = got[rows], ref[rows]
+    fin = torch.isfinite(ref)
+    assert torch.equal(fin, torch.isfinite(got))
+    if mode == 0:
+        err = (got[fin] - ref[fin]).abs()
+        bound = 1e-4 if prec == 2 else 0.1
+    else:
+        big = fin & (ref.abs() > 1e-3 * ref[fin].abs().max())
+        err = (got[big] - ref[big]).abs() / ref[big].abs()
+        bound = 1e-4 if prec == 2 else 0.1
+    assert err.max() <= bound, err.max()
+
+
+def test_pd_long_tiles_on_tc05_vs_oracle(cuda_device):
+    """A PD circuit whose sum layers have tiles of 256 terms (8x8 grid, 64 latents, block 32,
+    four product vectors per sum): the split-bf16 pass runs them as tcgen05 chunks
+    (tc05_min_tiles lowered to 1), and its LLs and parameter flows match the FP64 oracle."""
+    import numpy as np
+    from oracle import pc_oracle as orc
+    import pyjuice_b200 as juice
+    from pyjuice_b200.layer.layers import SumLayer
+    torch.manual_seed(3)
+    pc = juice.compile(juice.structures.PD((8, 8), 64, split_intervals=2, block_size=32, max_prod_block_conns=4,
+                                           input_dist=juice.distributions.Categorical(num_cats=8))).to(cuda_device)
+    saved = SumLayer.tc05_min_tiles
+    try:
+        SumLayer.tc05_min_tiles = 1
+        longs = [l for g in pc.inner_layer_groups if g.is_sum() for l in g if l._desc(cuda_device)["fw_ch"] is not None]
+        assert longs and all(l._fw_long(l._desc(cuda_device), 2) for l in longs)
+        x = np.random.default_rng(5).integers(0, 8, size=(128, 64))
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            lls = pc(torch.from_numpy(x).to(cuda_device), force_use_bf16=True).double().cpu().numpy()
+        pc.backward(inputs=torch.from_numpy(x).to(cuda_device), allow_modify_flows=True)
+        pf = pc.param_flows.double().cpu().numpy()
+    finally:
+        SumLayer.tc05_min_tiles = saved
+    lay = orc.layout_from_circuit(pc)
+    p0 = pc.params.double().cpu().numpy()
+    q0 = pc.input_layer_group[0].params.double().cpu().numpy()
+    nm, ems, lls_o = orc.forward(lay, p0, q0, x)
+    _, pf_o, _ = orc.backward(lay, p0, x, nm, ems)
+    assert np.abs(lls - lls_o).max() <= 1e-3
+    assert np.abs(pf - pf_o).max() <= 1e-3 * np.abs(pf_o).max()
