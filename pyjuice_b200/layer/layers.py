@@ -95,7 +95,7 @@ def _run_rows(tiles_np: np.ndarray, krow_np: np.ndarray) -> int:
     return 0
 
 
-_MAX_CHUNK_TILES = 16384  # sub-tiles (64 KB of packed weights each) a layer may split its long tiles into
+_MAX_CHUNK_TILES = 4096  # sub-tiles (64 KB of packed weights each, 256 MB) a layer may split its long tiles into
 
 
 def _chunk_table(tiles_np: np.ndarray):
@@ -117,6 +117,15 @@ def _chunk_table(tiles_np: np.ndarray):
     if start > _MAX_CHUNK_TILES:
         return None
     return np.concatenate(parts), ranges
+
+
+def _ch_pack(holder: dict, key: str) -> torch.Tensor:
+    """The packed-weight buffer of a long-tile chunk table, allocated on the device at first
+    use (``holder[key + '_bytes']`` bytes)."""
+    if holder[key] is None:
+        holder[key] = torch.empty([holder[key + "_bytes"]], dtype=torch.uint8, device=holder["fw_ch" if key ==
+                                  "fw_ch_pack" else "ch"].device)
+    return holder[key]
 
 
 def _tc05_chunks(src, src2, aux, out, ld, B, pack, table, ranges, krow, mode, prec, stream):
@@ -508,7 +517,7 @@ class SumLayer(Layer):
             ech_t = _chunk_table(tiles_np)
             el_groups.append(dict(
                 ch=None if ech_t is None else _i32(ech_t[0]), ch_ranges=None if ech_t is None else ech_t[1],
-                ch_pack=None if ech_t is None else torch.empty([ech_t[0].shape[0] * _PACK_BYTES], dtype=torch.uint8),
+                ch_pack=None, ch_pack_bytes=0 if ech_t is None else ech_t[0].shape[0] * _PACK_BYTES,
                 cbs=cbs, tm=_tile_rows(max(t[1] for t in tiles)), tiles=_i32(tiles_np),
                 krow=_i32(np.concatenate(klist)), kw=_i32(kw_np),
                 short=int(tiles_np[:, 3].max()) <= _SHORT_K,
@@ -520,7 +529,7 @@ class SumLayer(Layer):
         fch = _chunk_table(fw_np)
         return dict(
             fw_ch=None if fch is None else _i32(fch[0]), fw_ch_ranges=None if fch is None else fch[1],
-            fw_ch_pack=None if fch is None else torch.empty([fch[0].shape[0] * _PACK_BYTES], dtype=torch.uint8),
+            fw_ch_pack=None, fw_ch_pack_bytes=0 if fch is None else fch[0].shape[0] * _PACK_BYTES,
             fw_tiles=_i32(fw_np), fw_tm=fw_tm, fw_run=_run_rows(fw_np, krow_c),
             fw_short=bool(fw_np.shape[0]) and int(fw_np[:, 3].max()) <= _SHORT_K,
             fw_wlayout=1 if (fw_np.shape[0] and _rows_vec4(fw_np, kw_c, bs, 1)) else 0,
@@ -612,7 +621,7 @@ class SumLayer(Layer):
         if tc05 or (SumLayer.pack_short_weights and prec > 0 and d["fw_short"]):
             return (d["fw_tiles"], d["kw"], d["fw_pack"], self.block_size, 1, 1 if (tc05 and prec == 3) else 0)
         if self._fw_long(d, prec):
-            return (d["fw_ch"], d["kw"], d["fw_ch_pack"], self.block_size, 1, 1 if prec == 3 else 0)
+            return (d["fw_ch"], d["kw"], _ch_pack(d, "fw_ch_pack"), self.block_size, 1, 1 if prec == 3 else 0)
         return None
 
     def flow_pack_jobs(self, device: torch.device, B: int, force_use_fp32: bool = False):
@@ -626,7 +635,7 @@ class SumLayer(Layer):
                 jobs.append((eg["tiles"], eg["kw"], eg["pack"], eg["cbs"], self.block_size,
                              1 if (tc05 and prec == 3) else 0))
             elif self._el_long(eg, prec):
-                jobs.append((eg["ch"], eg["kw"], eg["ch_pack"], eg["cbs"], self.block_size, 1 if prec == 3 else 0))
+                jobs.append((eg["ch"], eg["kw"], _ch_pack(eg, "ch_pack"), eg["cbs"], self.block_size, 1 if prec == 3 else 0))
         return jobs
 
     @staticmethod
@@ -713,7 +722,7 @@ class SumLayer(Layer):
         if self._fw_long(d, prec):
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
-            _tc05_chunks(element_mars, None, None, node_mars, ld, B, d["fw_ch_pack"], d["fw_ch"], d["fw_ch_ranges"],
+            _tc05_chunks(element_mars, None, None, node_mars, ld, B, _ch_pack(d, "fw_ch_pack"), d["fw_ch"], d["fw_ch_ranges"],
                          d["krow"], 0, prec, st)
             return
         prec = _mma(prec)
@@ -795,7 +804,7 @@ class SumLayer(Layer):
                 continue
             if self._el_long(eg, prec):
                 _tc05_chunks(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld,
-                             B, eg["ch_pack"], eg["ch"], eg["ch_ranges"], eg["krow"], 1 if allow_modify_flows else 2,
+                             B, _ch_pack(eg, "ch_pack"), eg["ch"], eg["ch_ranges"], eg["krow"], 1 if allow_modify_flows else 2,
                              prec, nat.stream())
                 continue
             prec = _mma(prec)
