@@ -580,6 +580,15 @@ def hmm_workload(args):
         pc.backward(inputs=x, allow_modify_flows=True)
         pc.mini_batch_em(step_size=STEP_SIZE, pseudocount=PSEUDOCOUNT)
 
+    if args.profile_step:  # one warm-up step, then one step in the NVTX range "em_step"
+        step()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("em_step")
+        step()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile_step": "hmm", "ok": bool(torch.isfinite(pc.params).all())}), flush=True)
+        return
     init = pc.params.detach().clone(), pc.input_layer_group[0].params.detach().clone()
     res = {}
     for name, long_tc05 in (("tc05_chunks", True), ("mma_sync", False)):
