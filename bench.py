@@ -384,12 +384,32 @@ def adjoint_workload(args):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     ok = bool(torch.isfinite(lls).all()) and bool(torch.isfinite(z.grad).all()) and bool(torch.isfinite(ev.grad).all())
+    peak_resident = torch.cuda.max_memory_allocated(device)
+    # the same steps with the element values recomputed per layer group instead of resident
+    pc.recompute_element_values = True
+    pc.__dict__.pop("_em_resident", None)
+    torch.cuda.empty_cache()
+    torch.cuda.reset_peak_memory_stats(device)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for _ in range(args.steps):
+        step()
+    e3.record()
+    e3.synchronize()
+    ms_rc = e2.elapsed_time(e3) / args.steps
+    peak_recompute = torch.cuda.max_memory_allocated(device)
+    pc.recompute_element_values = False
     out = {"metric": "adjoint samples/s (soft-evidence LL + d/d sum-logits + d/d evidence) 1xB200",
            "value": B / (ms / 1e3), "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "HCLT 32x32x3 vars x 256 cats, 256 latents, block 32, soft evidence, batch 128",
                       "num_nodes": pc.num_nodes, "num_edges": pc.num_edges, "evidence_bytes": ev.numel() * 4},
-           "finite": ok, "mean_ll": float(lls.detach().mean())}
+           "finite": ok, "mean_ll": float(lls.detach().mean()),
+           "element_values": {"resident": {"ms_per_step": ms, "peak_bytes": peak_resident},
+                              "recomputed_per_layer_group": {"ms_per_step": ms_rc, "peak_bytes": peak_recompute}}}
     if args.fd:
         out["fd_check"] = adjoint_fd_check(pc, z.detach(), ev.detach()[:2], device)
     print(json.dumps(out), flush=True)

@@ -90,6 +90,12 @@ class TensorCircuit(nn.Module):
         self._run_params = dict()
         self._cum_flow_dev = None
         self._side_streams = dict()
+        # False (default): every product layer group keeps its element values resident for
+        # the backward pass. True: they share element_mars (as in the reference) and the
+        # backward pass recomputes each group's element values from the kept node values
+        # right before the sum group above it, saving the resident buffer
+        # (num_elements of all groups x batch x 4 bytes).
+        self.recompute_element_values = False
         self._dev_tables = {}
         self._pack_tables = {}
         self._param_epoch = 0      # bumped by every in-library write of the sum parameters
@@ -535,6 +541,8 @@ class TensorCircuit(nn.Module):
 
     def _em_view(self, group_id: int) -> torch.Tensor:
         """Element values of product layer group ``group_id`` (rows indexed like ``element_mars``)."""
+        if self.recompute_element_values:
+            return self.element_mars
         off, rows = self._em_region[group_id]
         return self._em_resident[off:off + rows]
 
@@ -648,7 +656,8 @@ class TensorCircuit(nn.Module):
             nm = self._buffer("node_mars", self.num_nodes, B, 0.0)
             em = self._buffer("element_mars", self.num_elements, B, -float("inf"))
             # dummy rows of every region keep their initial -inf (nothing writes them)
-            self._buffer("_em_resident", self._em_rows, B, -float("inf"))
+            if not self.recompute_element_values:
+                self._buffer("_em_resident", self._em_rows, B, -float("inf"))
             if not _no_buffer_reset:
                 nat.call("pcb_fill_rows", nat.ptr(nm), B, 0, self.num_dummy_nodes, 0.0, nat.stream())
                 nat.call("pcb_fill_rows", nat.ptr(em), B, 0, self.num_dummy_eles, -float("inf"), nat.stream())
@@ -664,7 +673,8 @@ class TensorCircuit(nn.Module):
                         ret = input_layer_fn(layer, inputs, nm, **kwargs)
                         if not ret and ret is not None:
                             layer(data, nm, **kwargs)
-            sig = (0, id(nm), id(em), id(self._em_resident), id(self.params), B, force_use_bf16, force_use_fp32,
+            sig = (0, id(nm), id(em), id(self.__dict__.get("_em_resident")), id(self.params), B, force_use_bf16,
+                   force_use_fp32,
                    propagation_alg, kwargs.get("alpha"), self._partial_epoch)
             run = partial(self._run_inner_forward, force_use_bf16, force_use_fp32, propagation_alg, **kwargs)
             if record_cudagraph and sig not in self._recorded_cuda_graphs:
@@ -773,11 +783,18 @@ class TensorCircuit(nn.Module):
                     el_ready = None
                 fz = fuse_bw.get(layer_id)
                 alg = propagation_alg if isinstance(propagation_alg, str) else propagation_alg[layer_id]
+                pstream = sides[turn % len(sides)]
+                if self.recompute_element_values:
+                    # the element values of the product group below, recomputed into the shared
+                    # buffer; the parameter flows then stay on this stream (the next recompute
+                    # overwrites the buffer)
+                    self.inner_layer_groups[layer_id - 1](self.node_mars, self.element_mars)
+                    pstream = None
                 group.backward(self.node_flows, self.element_flows, self.node_mars, self._em_view(layer_id - 1),
                                self.params,
                                param_flows=self.param_flows if compute_param_flows else None,
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
-                               force_use_fp32=force_use_fp32, _pflow_stream=sides[turn % len(sides)], _fuse_bw=fz,
+                               force_use_fp32=force_use_fp32, _pflow_stream=pstream, _fuse_bw=fz,
                                _flows_modified=layer_id in rewritten, propagation_alg=alg,
                                negate_pflows=negate_pflows, **kwargs)
                 turn += 1
@@ -844,7 +861,7 @@ class TensorCircuit(nn.Module):
                 nf.copy_(cache["node_flows"])
             if compute_param_flows:
                 self.init_param_flows(flows_memory=flows_memory)
-            sig = (1, id(nf), id(ef), id(self.node_mars), id(self._em_resident), id(self.params),
+            sig = (1, id(nf), id(ef), id(self.node_mars), id(self.__dict__.get("_em_resident")), id(self.params),
                    id(self.param_flows), B, allow_modify_flows, logspace_flows, force_use_fp32, compute_param_flows,
                    propagation_alg, negate_pflows, kwargs.get("alpha"), self._partial_epoch)
             run = partial(self._run_inner_backward, compute_param_flows, allow_modify_flows, logspace_flows,

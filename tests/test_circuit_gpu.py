@@ -207,6 +207,35 @@ def test_tc05_multi_slice_equals_per_slice(cuda_device):
     assert abs(out[1][0][:16].double().cpu().numpy().mean() - lls_o.mean()) < 1e-3
 
 
+@pytest.mark.parametrize("name,B,kw", [("hclt64", 64, dict(force_use_fp32=True)),
+                                       ("hclt784", 128, dict(force_use_bf16=True))])
+def test_recomputed_element_values_equal_resident(name, B, kw, cuda_device):
+    """``recompute_element_values``: the element values share element_mars and the backward
+    pass recomputes each product group's values before the sum group above it (no resident
+    buffer is allocated); LLs, node flows and parameter flows are bit-identical to the
+    resident default, and one EM step gives the same parameters."""
+    fx = load_fixture(name)
+    rng = np.random.default_rng(4)
+    ncat = 4 if name == "hclt64" else 256
+    nvar = 64 if name == "hclt64" else 784
+    x = torch.from_numpy(rng.integers(0, ncat, size=(B, nvar))).to(cuda_device)
+    out = []
+    for recompute in (False, True):
+        pc = build_fixture_circuit(name, fx).to(cuda_device)
+        load_fixture_params(pc, fx)
+        pc.recompute_element_values = recompute
+        pc.init_param_flows(flows_memory=0.0)
+        with torch.no_grad():
+            lls = pc(x, **kw)
+        pc.backward(inputs=x, allow_modify_flows=True, force_use_fp32="force_use_fp32" in kw)
+        pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+        torch.cuda.synchronize()
+        assert ("_em_resident" in pc.__dict__) != recompute
+        out.append((lls.clone(), pc.node_flows.clone(), pc.param_flows.clone(), pc.params.clone()))
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("modify", [True, False])
 def test_tc05_persistent_equals_per_slice(modify, cuda_device):
     """On HCLT-784 at batch 256, the persistent warp-specialised tcgen05 kernel (TMA-staged

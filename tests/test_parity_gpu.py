@@ -383,6 +383,44 @@ def test_pd_and_hmm_match_reference(cuda_device):
     assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-5
 
 
+def test_batched_hmms_forest_vs_oracle(cuda_device):
+    """Four HMMs of different lengths and hidden sizes in one circuit (batched_hmms): the
+    log-likelihood equals the sum of the four HMMs' own (FP64 oracle, each HMM compiled
+    alone), and the forest's parameter and input flows match the oracle on the forest."""
+    rng = np.random.default_rng(0)
+    specs = [(5, 16), (3, 32), (7, 16), (4, 64)]
+    V = 12
+    params = []
+    for T, L in specs:
+        params.append(tuple(torch.from_numpy(rng.dirichlet(np.full(n, 0.5), size=m) if m else
+                                             rng.dirichlet(np.full(n, 0.5))).float()
+                            for m, n in ((L, L), (L, V), (0, L))))
+    pc = juice.compile(juice.structures.batched_hmms(specs, V, params=params)).to(cuda_device)
+    x = rng.integers(0, V, size=(64, sum(T for T, _ in specs)))
+    pc.init_param_flows(flows_memory=0.0)
+    lls = pc(torch.from_numpy(x).to(cuda_device), force_use_fp32=True)
+    lls.mean().backward()
+    lay = orc.layout_from_circuit(pc)
+    p0 = pc.params.double().cpu().numpy()
+    q0 = pc.input_layer_group[0].params.double().cpu().numpy()
+    nm, ems, lls_o = orc.forward(lay, p0, q0, x)
+    _, pf_o, ipf_o = orc.backward(lay, p0, x, nm, ems)
+    got = lls.detach().double().cpu().numpy()
+    assert np.abs(got - lls_o).max() <= 1e-5 * np.abs(lls_o).max()
+    assert _rel(pc.param_flows.cpu().numpy(), pf_o) <= 1e-4  # mean-LL gradient: unit root flows
+    ipf = pc.input_layer_group[0].param_flows.cpu().numpy()[:ipf_o.shape[0]]
+    assert _rel(ipf, ipf_o) <= 1e-4
+    ref, off = np.zeros(64), 0
+    for (T, L), (a, b, g) in zip(specs, params):
+        h = juice.compile(juice.structures.HMM(T, L, V, alpha=a, beta=b, gamma=g, block_size=16))
+        hl = orc.layout_from_circuit(h)
+        _, _, l1 = orc.forward(hl, h.params.double().numpy(), h.input_layer_group[0].params.double().numpy(),
+                               x[:, off:off + T])
+        ref += l1[:, 0]
+        off += T
+    assert np.abs(lls_o[:, 0] - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
 def test_pd_with_parentless_products_flows_vs_oracle(cuda_device):
     """A PD circuit with products that no sum node selects (max_prod_block_conns = 1): FP32
     parameter and input flows against the FP64 oracle on two consecutive backward passes
