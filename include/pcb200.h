@@ -267,6 +267,45 @@ int pcb_lse_contract_short(const float* src, const float* src2, const float* aux
                            const PcbShortFusion* fusion, void* stream);
 
 /*
+ * One level of a pcb_lse_levels_short launch: a sum layer with the product layer below it
+ * fused (the forward form of PcbShortFusion), its tiles being tiles[tile0 ..
+ * tile0 + num_tiles) of the launch's concatenated tables.
+ */
+typedef struct {
+    const uint8_t* packed;   /* reserved, NULL: each item converts its FP32 weights itself */
+    float* element_out;      /* the product layer's element values (written as a side output) */
+    int32_t tile0;
+    int32_t num_tiles;
+    int32_t rpb_log2;        /* rows per block of the level's tiles, base-2 logarithm */
+    int32_t w_stride;
+    int32_t row_splits;      /* 64-row items per tile: (tile rows + 63) / 64 */
+    int32_t need;            /* items per sample slice of all earlier levels */
+    int32_t wvec;            /* the weight layout of pcb_lse_contract_short's wlayout 1 */
+    int32_t item0;           /* first work item of the level */
+} PcbShortLevel;
+
+/*
+ * The forward of a run of consecutive small levels (each a product layer fused into the sum
+ * layer above it, as pcb_lse_contract_short with PcbShortFusion.term_children) in one
+ * persistent launch over node_mars. Work items (level, sample slice of batch_tile, tile,
+ * 64-row split) are numbered level by level (item0 and need as in PcbShortLevel); num_ctas
+ * CTAs take items from a counter in that order, and an item first waits (bounded) until
+ * its sample slice has finished every item of the earlier levels: no grid-wide
+ * synchronisation, since samples are independent. Same results as one
+ * pcb_lse_contract_short launch per level (prec 0 FP32, 1 bf16, 2 split bf16). krow, kw and
+ * term_children are the levels' tables concatenated (tile k_off indexing all three).
+ * counters: a caller-owned int32 workspace of 1 + num_slices entries (zeroed here). A wait
+ * that runs out reports PCB_STATUS_WAIT_TIMEOUT.
+ * Replaces the reference's per-layer launches of the product and sum forward kernels
+ * (prod_layer.py:160-204, sum_layer.py:454-568) for those levels.
+ */
+int pcb_lse_levels_short(float* node_mars, int64_t ld, int32_t B, const float* params, const PcbLseTile* tiles,
+                         const int32_t* krow, const int32_t* kw, const int32_t* term_children,
+                         const PcbShortLevel* levels, int32_t num_levels, int32_t total_items, int32_t num_slices,
+                         int32_t* counters, int32_t prec, int32_t batch_tile, int32_t wk, int32_t num_ctas,
+                         void* stream);
+
+/*
  * Weights of LSE-contraction tiles (at most 128 rows x 128 terms each, same tile table,
  * kw, rows_per_block and w_stride as pcb_lse_contract) packed for
  * pcb_lse_contract_tc05: for tile t, 65536 bytes at packed + t * 65536 hold W(k, r)

@@ -122,6 +122,9 @@ _SIGS = {
                                c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
     "pcb_lse_contract_tc05_accum": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p,
                                      c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p], c_int32),
+    "pcb_lse_levels_short": ([c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_int32, c_int32, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p],
+                             c_int32),
     "pcb_lse_contract_tc05_ws": ([c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_int64, c_int64, c_void_p,
                                   c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p],
                                  c_int32),

@@ -31,6 +31,12 @@
 namespace {
 
 constexpr int kThreads = 128;
+
+int current_device_ls() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d < 0 ? 0 : (d > 63 ? 63 : d);
+}
 constexpr int KMAX = 128;
 constexpr int kFuse = 4;  // children per element of a fused product layer (table stride)
 
@@ -76,16 +82,18 @@ struct Smem {
     static constexpr size_t bytes() { return 4ull * (oIdx + (2 + kFuse) * KMAX); }
 };
 
+// One work item of the single-stage contraction: rows r0 .. r0 + RM - 1 of tile t (number
+// tile_index of its table, for the packed weights) for samples b0 .. b0 + TB - 1. With pdl,
+// the source rows are read after the programmatic-launch wait.
 template <int RM, int TB, int MODE, int PREC, bool WK, bool FUSE>
-__global__ void __launch_bounds__(kThreads)
-lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
-                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
-                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
-                 int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
-                 const uint8_t* __restrict__ packed, PcbShortFusion fu, int32_t* __restrict__ status) {
-    // The term indices and the weights (compiled tables and parameters) are read before the
-    // wait for the previous kernel; only the source rows and the packed weights after it.
-    pcb::pdl_trigger();
+__device__ __forceinline__ void short_item(const float* __restrict__ src, const float* __restrict__ src2,
+                                           const float* __restrict__ aux, float* __restrict__ out, int64_t ld, int B,
+                                           const float* __restrict__ params, const PcbLseTile t, int tile_index, int r0,
+                                           int b0, const int* __restrict__ krow, const int* __restrict__ kw,
+                                           int w_stride, int rpb_log2, bool vec, bool wvec,
+                                           const uint8_t* __restrict__ packed, const PcbShortFusion& fu,
+                                           int32_t* __restrict__ status, bool pdl, const int* wait_ctr = nullptr,
+                                           int wait_need = 0) {
     using S = Smem<RM, TB, MODE, PREC, WK, FUSE>;
     constexpr int ES = S::ES, WS = S::WS, WROW = S::WROW;
     constexpr int PARTS = kThreads / TB;  // threads per sample column in the max / exp passes
@@ -102,9 +110,6 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     int* sRow = reinterpret_cast<int*>(sm + S::oIdx);
     int* sKw = sRow + KMAX;
 
-    const PcbLseTile t = tiles[blockIdx.x / row_splits];
-    const int r0 = (blockIdx.x % row_splits) * RM;
-    const int b0 = blockIdx.y * TB;
     const int tid = threadIdx.x;
     const int nrows = min(RM, t.n_rows - r0);
     if (nrows <= 0) return;
@@ -191,7 +196,19 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
         }
     }
 
-    pcb::pdl_wait();
+    if (pdl) pcb::pdl_wait();
+    if (wait_ctr != nullptr && wait_need > 0) {
+        // the node rows this item reads are written by earlier items (persistent launch)
+        if (tid == 0) {
+            const volatile int* done = wait_ctr;
+            int i = 0;
+            while (*done < wait_need && ++i < (1 << 20)) {
+            }
+            if (*done < wait_need) pcb::report_status(status, PCB_STATUS_WAIT_TIMEOUT);
+            __threadfence();
+        }
+        __syncthreads();
+    }
     {
         constexpr int NX = TB / 4;
         constexpr int IT = KMAX * NX / kThreads;
@@ -230,7 +247,7 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     // packed bf16 weights (hi, then lo): rows r0 .. r0 + RM - 1 are RM / 8 core-matrix row
     // groups of 2048 bytes in each half of the tile's 64 KB block
     if (pk) {
-        const uint8_t* srcp = packed + (size_t)(blockIdx.x / row_splits) * 65536 + (size_t)(r0 / 8) * 2048;
+        const uint8_t* srcp = packed + (size_t)tile_index * 65536 + (size_t)(r0 / 8) * 2048;
         uint8_t* dstp = reinterpret_cast<uint8_t*>(pW);
         constexpr int CH = kPackHalf / 16;
         constexpr int IT = (PREC == 2 ? 2 : 1) * CH / kThreads;
@@ -487,6 +504,89 @@ lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, 
     }
 }
 
+template <int RM, int TB, int MODE, int PREC, bool WK, bool FUSE>
+__global__ void __launch_bounds__(kThreads)
+lse_short_kernel(const float* __restrict__ src, const float* __restrict__ src2, const float* __restrict__ aux,
+                 float* __restrict__ out, int64_t ld, int B, const float* __restrict__ params,
+                 const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
+                 int w_stride, int rpb_log2, int row_splits, bool vec, bool wvec,
+                 const uint8_t* __restrict__ packed, PcbShortFusion fu, int32_t* __restrict__ status) {
+    // The term indices and the weights (compiled tables and parameters) are read before the
+    // wait for the previous kernel; only the source rows and the packed weights after it.
+    pcb::pdl_trigger();
+    const int ti = blockIdx.x / row_splits;
+    short_item<RM, TB, MODE, PREC, WK, FUSE>(src, src2, aux, out, ld, B, params, tiles[ti], ti,
+                                             (blockIdx.x % row_splits) * RM, blockIdx.y * TB, krow, kw, w_stride,
+                                             rpb_log2, vec, wvec, packed, fu, status, true);
+}
+
+// ---------------------------------------------------------------------------------------
+// A run of small levels (fused product + sum forward) in one persistent launch. Work items
+// (level, slice, tile, row split) are numbered level by level; every CTA takes the next
+// item from a global counter, waits until its sample slice has finished all items of the
+// earlier levels (a per-slice completion counter), runs the item and counts it done.
+// Samples are independent, so no other synchronisation is needed. Items are handed out in
+// level order to running CTAs only, so an item waits only for items that running CTAs
+// hold: the wait always ends (and is bounded in any case).
+template <int RM, int TB, int PREC, bool WK>
+__global__ void __launch_bounds__(kThreads)
+short_levels_kernel(float* __restrict__ nm, int64_t ld, int B, const float* __restrict__ params,
+                    const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow, const int* __restrict__ kw,
+                    const int* __restrict__ term_children, const PcbShortLevel* __restrict__ levels, int num_levels,
+                    int total_items, int* __restrict__ counters, bool vec, int32_t* __restrict__ status) {
+    pcb::pdl_trigger();
+    pcb::pdl_wait();
+    __shared__ int s_item;
+    int lv = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counters, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total_items) break;
+        while (lv + 1 < num_levels && levels[lv + 1].item0 <= item) ++lv;
+        const PcbShortLevel L = levels[lv];
+        const int local = item - L.item0;
+        const int split = local % L.row_splits;
+        const int ts = local / L.row_splits;
+        const int tile = ts % L.num_tiles;
+        const int slice = ts / L.num_tiles;
+        PcbShortFusion fu;
+        fu.term_children = term_children;
+        fu.element_out = L.element_out;
+        fu.out_children = nullptr;
+        short_item<RM, TB, 0, PREC, WK, true>(nm, nullptr, nullptr, nm, ld, B, params, tiles[L.tile0 + tile], tile,
+                                              split * RM, slice * TB, krow, kw, L.w_stride, L.rpb_log2, vec,
+                                              L.wvec != 0, nullptr, fu, status, false, counters + 1 + slice, L.need);
+        __syncthreads();  // the item's stores, then the next item reuses the shared memory
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(counters + 1 + slice, 1);
+        }
+    }
+}
+
+template <int TB, int PREC, bool WK>
+int launch_levels(float* nm, int64_t ld, int B, const float* params, const PcbLseTile* tiles, const int* krow,
+                  const int* kw, const int* term_children, const PcbShortLevel* levels, int num_levels,
+                  int total_items, int* counters, int num_ctas, cudaStream_t s, bool vec) {
+    constexpr int RM = 64;
+    constexpr size_t smem = Smem<RM, TB, 0, PREC, WK, true>::bytes();
+    static_assert(smem <= 227 * 1024, "shared memory");
+    static bool configured[64] = {false};
+    const int dev = current_device_ls();
+    if (!configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(short_levels_kernel<RM, TB, PREC, WK>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_levels_short: %s", cudaGetErrorString(e));
+        configured[dev] = true;
+    }
+    return pcb::launch_status(pcb::launch_k(short_levels_kernel<RM, TB, PREC, WK>, dim3((unsigned)num_ctas),
+                                            dim3(kThreads), smem, s, 1u, nm, ld, B, params, tiles, krow, kw,
+                                            term_children, levels, num_levels, total_items, counters, vec,
+                                            pcb::status_word()),
+                              "pcb_lse_levels_short");
+}
+
 int current_device() {
     int d = 0;
     cudaGetDevice(&d);
@@ -598,4 +698,32 @@ extern "C" int pcb_lse_contract_short(const float* src, const float* src2, const
     if (batch_tile == 32) return PCB_SH(64, 32);
     return PCB_SH(64, 64);
 #undef PCB_SH
+}
+
+extern "C" int pcb_lse_levels_short(float* node_mars, int64_t ld, int32_t B, const float* params,
+                                    const PcbLseTile* tiles, const int32_t* krow, const int32_t* kw,
+                                    const int32_t* term_children, const PcbShortLevel* levels, int32_t num_levels,
+                                    int32_t total_items, int32_t num_slices, int32_t* counters, int32_t prec,
+                                    int32_t batch_tile, int32_t wk, int32_t num_ctas, void* stream) {
+    if (!node_mars || !params || !tiles || !krow || !kw || !term_children || !levels || !counters || B <= 0 ||
+        ld < B || num_levels <= 0 || total_items < 0 || num_slices <= 0 || prec < 0 || prec > 2 ||
+        (batch_tile != 16 && batch_tile != 32) || num_ctas <= 0 || (int64_t)num_slices * batch_tile < B)
+        return pcb::set_error(PCB_E_ARG, "pcb_lse_levels_short: bad arguments");
+    cudaStream_t s = pcb::as_stream(stream);
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(int32_t) * (size_t)(1 + num_slices), s);
+    if (e != cudaSuccess) return pcb::set_error(PCB_E_CUDA, "pcb_lse_levels_short: %s", cudaGetErrorString(e));
+    if (total_items == 0) return PCB_OK;
+    const bool vec = pcb::vec_ok(node_mars, ld);
+    const int ctas = num_ctas < total_items ? num_ctas : total_items;
+#define PCB_LV(TBV, P, W) \
+    launch_levels<TBV, P, W>(node_mars, ld, B, params, tiles, krow, kw, term_children, levels, num_levels, total_items, counters, ctas, s, vec)
+    if (batch_tile == 16) {
+        if (prec == 0) return wk ? PCB_LV(16, 0, true) : PCB_LV(16, 0, false);
+        if (prec == 1) return wk ? PCB_LV(16, 1, true) : PCB_LV(16, 1, false);
+        return wk ? PCB_LV(16, 2, true) : PCB_LV(16, 2, false);
+    }
+    if (prec == 0) return wk ? PCB_LV(32, 0, true) : PCB_LV(32, 0, false);
+    if (prec == 1) return wk ? PCB_LV(32, 1, true) : PCB_LV(32, 1, false);
+    return wk ? PCB_LV(32, 2, true) : PCB_LV(32, 2, false);
+#undef PCB_LV
 }

@@ -26,7 +26,7 @@ import torch
 import torch.nn as nn
 
 from .. import _native as nat
-from ..layer.layers import InputLayer, LayerGroup, ProdLayer, SumLayer
+from ..layer.layers import InputLayer, LayerGroup, ProdLayer, SumLayer, _mma, _num_sms
 from ..nodes import CircuitNodes, multiply, summate
 
 
@@ -43,6 +43,11 @@ def _pc_model_backward_hook(grad, pc, inputs, record_cudagraph, apply_cudagraph,
                 apply_cudagraph=apply_cudagraph, propagation_alg=propagation_alg, **kwargs)
     return None
 
+
+# One PcbShortLevel record (include/pcb200.h): two pointers and eight int32 fields.
+_SHORT_LEVEL = np.dtype([("packed", "<u8"), ("element_out", "<u8"), ("tile0", "<i4"), ("num_tiles", "<i4"),
+                         ("rpb_log2", "<i4"), ("w_stride", "<i4"), ("row_splits", "<i4"), ("need", "<i4"),
+                         ("wvec", "<i4"), ("item0", "<i4")])
 
 # One PcbPackJob record (include/pcb200.h): three pointers and four int32 fields.
 _PACK_JOB = np.dtype([("tiles", "<u8"), ("kw", "<u8"), ("packed", "<u8"), ("num_tiles", "<i4"),
@@ -96,6 +101,7 @@ class TensorCircuit(nn.Module):
         # right before the sum group above it, saving the resident buffer
         # (num_elements of all groups x batch x 4 bytes).
         self.recompute_element_values = False
+        self._level_runs = dict()
         self._dev_tables = {}
         self._pack_tables = {}
         self._param_epoch = 0      # bumped by every in-library write of the sum parameters
@@ -584,6 +590,82 @@ class TensorCircuit(nn.Module):
         return (self.params.data_ptr(), self.params._version, self._param_epoch, B, bool(force_use_fp32),
                 SumLayer.bf16_form, SumLayer.pack_short_weights, SumLayer.tc05_min_tiles)
 
+    # The forward of the run of small levels next to the root (product layer fused into the
+    # single-stage sum kernel above it) in one persistent launch (pcb_lse_levels_short)
+    # instead of one launch per level. Off by default: on HCLT-784 (batch 512, BF16) the
+    # EM step took 2.65 ms with it against 2.42 ms with the per-level launches, whose
+    # programmatic dependent launches already hide most of the launch gaps.
+    fuse_levels_forward = False
+
+    def _level_run(self, B, force_use_bf16, force_use_fp32):
+        """Sum group indices of the longest run of consecutive small levels that the
+        persistent launch can take (each: one product layer with a forward fusion table below
+        one single-stage sum layer), or []."""
+        groups = self.inner_layer_groups
+        ok = []
+        for g in range(1, len(groups), 2):
+            if not (groups[g].is_sum() and groups[g - 1].is_prod() and len(groups[g]) == 1 and len(groups[g - 1]) == 1):
+                ok.append(False)
+                continue
+            h = self._fusion_host.get(g - 1)
+            layer = groups[g][0]
+            ok.append(h is not None and h["fw"] is not None and TensorCircuit.fuse_products and
+                      SumLayer.short_kernels and
+                      layer.runs_single_stage(self.device, B, force_use_bf16, force_use_fp32))
+        best, cur = [], []
+        for i, o in enumerate(ok):
+            cur = cur + [2 * i + 1] if o else []
+            if len(cur) > len(best):
+                best = cur
+        return best if len(best) >= 2 else []
+
+    def _level_tables(self, run, B, force_use_bf16, force_use_fp32):
+        """Concatenated tables and level records of a pcb_lse_levels_short launch (cached)."""
+        first = self.inner_layer_groups[run[0]][0]
+        prec = _mma(first._fw_tc05(first._desc(self.device), B, force_use_bf16, force_use_fp32)[0])
+        key = (tuple(run), B, prec, SumLayer.pack_short_weights, id(self.__dict__.get("_em_resident")),
+               id(self.element_mars), self.recompute_element_values)
+        t = self._level_runs.get(key)
+        if t is not None:
+            return t
+        tb = 32
+        nsl = -(-B // tb)
+        tiles, krow, kw, tch, recs = [], [], [], [], []
+        koff = tile0 = need = item0 = 0
+        for g in run:
+            layer = self.inner_layer_groups[g][0]
+            d = layer._host_desc()
+            dd = layer._desc(self.device)
+            tt = d["fw_tiles"].numpy().astype(np.int64).copy()
+            tt[:, 2] += koff
+            tiles.append(tt)
+            krow.append(d["krow"].numpy())
+            kw.append(d["kw"].numpy())
+            tch.append(self._fusion_host[g - 1]["fw"].reshape(-1))
+            splits = -(-int(d["fw_tm"]) // 64)
+            # the items convert the weights themselves, before their dependency wait
+            packed = 0
+            per_slice = tt.shape[0] * splits
+            recs.append((packed, self._em_view(g - 1).data_ptr(), tile0, tt.shape[0], layer.block_size.bit_length() - 1,
+                         1, splits, need, 1 if d["fw_wlayout"] == 1 else 0, item0))
+            koff += d["krow"].numel()
+            tile0 += tt.shape[0]
+            need += per_slice
+            item0 += per_slice * nsl
+        dev = self.device
+        rec = np.zeros(len(recs), dtype=_SHORT_LEVEL)
+        for i, r in enumerate(recs):
+            rec[i] = r
+        t = dict(tiles=torch.from_numpy(np.concatenate(tiles).astype(np.int32)).to(dev),
+                 krow=torch.from_numpy(np.concatenate(krow).astype(np.int32)).to(dev),
+                 kw=torch.from_numpy(np.concatenate(kw).astype(np.int32)).to(dev),
+                 tch=torch.from_numpy(np.concatenate(tch).astype(np.int32)).to(dev),
+                 levels=torch.from_numpy(rec.view(np.uint8).copy()).to(dev), num_levels=len(run),
+                 items=item0, slices=nsl, tb=tb, prec=prec,
+                 counters=torch.zeros([1 + nsl], dtype=torch.int32, device=dev))
+        self._level_runs[key] = t
+        return t
+
     def _run_inner_forward(self, force_use_bf16, force_use_fp32, propagation_alg, **kwargs):
         # The weights that the sum kernels read packed are packed on a side stream in two
         # launches: the forward's (waited for before the first layer that reads them) and the
@@ -592,11 +674,14 @@ class TensorCircuit(nn.Module):
         side = self._side_stream(main)
         side.wait_stream(main)
         B = self.node_mars.size(1)
+        plain = propagation_alg == "LL" if isinstance(propagation_alg, str) else all(a == "LL" for a in propagation_alg)
+        run = (self._level_run(B, force_use_bf16, force_use_fp32)
+               if (TensorCircuit.fuse_levels_forward and plain and not self._fw_partial_eval_enabled) else [])
         fw_jobs, el_jobs, fw_groups = [], [], set()
         for gi, group in enumerate(self.inner_layer_groups):
             if group.is_sum():
                 for layer in group:
-                    job = layer.forward_pack_job(self.device, B, force_use_bf16, force_use_fp32)
+                    job = None if gi in run else layer.forward_pack_job(self.device, B, force_use_bf16, force_use_fp32)
                     if job is not None:
                         fw_jobs.append(job)
                         fw_groups.add(gi)
@@ -609,8 +694,20 @@ class TensorCircuit(nn.Module):
             self._multi_pack(el_jobs)
         self._el_pack_state = self._pack_state_key(B, force_use_fp32)
         groups = self.inner_layer_groups
+        in_run = set(run) | set(g - 1 for g in run)
         for gi, group in enumerate(groups):
             alg = propagation_alg if isinstance(propagation_alg, str) else propagation_alg[gi]
+            if gi in in_run:
+                if gi == run[0] - 1:  # the whole run in one launch
+                    if fw_ready is not None:
+                        main.wait_event(fw_ready)
+                        fw_ready = None
+                    lt = self._level_tables(run, B, force_use_bf16, force_use_fp32)
+                    nat.call("pcb_lse_levels_short", nat.ptr(self.node_mars), self.node_mars.stride(0), B,
+                             nat.ptr(self.params), nat.ptr(lt["tiles"]), nat.ptr(lt["krow"]), nat.ptr(lt["kw"]),
+                             nat.ptr(lt["tch"]), nat.ptr(lt["levels"]), lt["num_levels"], lt["items"], lt["slices"],
+                             nat.ptr(lt["counters"]), lt["prec"], lt["tb"], 0, 4 * _num_sms(), nat.stream())
+                continue
             if group.is_prod():
                 fused = (not self._fw_partial_eval_enabled and gi + 1 < len(groups) and
                          self._fusion_tables(gi, "fw") is not None and

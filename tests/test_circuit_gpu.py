@@ -12,6 +12,7 @@ from helpers import build_fixture_circuit, fixture_params, load_fixture_params
 from oracle import pc_oracle as orc
 
 import pyjuice_b200 as juice
+from pyjuice_b200 import _native as nat
 
 pytestmark = pytest.mark.gpu
 
@@ -205,6 +206,44 @@ def test_tc05_multi_slice_equals_per_slice(cuda_device):
     p0, q0 = fixture_params(pc, fx)
     _, _, lls_o = orc.forward(orc.layout_from_circuit(pc), p0, q0, xn[:16])
     assert abs(out[1][0][:16].double().cpu().numpy().mean() - lls_o.mean()) < 1e-3
+
+
+@pytest.mark.parametrize("name,B,kw", [("hclt64", 100, dict(force_use_fp32=True)),
+                                       ("hclt784", 256, dict(force_use_bf16=True))])
+def test_persistent_small_levels_forward_equals_per_level(name, B, kw, cuda_device):
+    """The forward of the run of small levels in one persistent launch (pcb_lse_levels_short:
+    per-slice completion counters instead of one product and one sum launch per level)
+    gives bit-identical log-likelihoods, node values, element values, flows and EM
+    parameters, with a clean device status word (no wait ran out)."""
+    from pyjuice_b200.model.tensorcircuit import TensorCircuit
+    fx = load_fixture(name)
+    rng = np.random.default_rng(8)
+    ncat = 4 if name == "hclt64" else 256
+    nvar = 64 if name == "hclt64" else 784
+    x = torch.from_numpy(rng.integers(0, ncat, size=(B, nvar))).to(cuda_device)
+    saved = TensorCircuit.fuse_levels_forward
+    out = []
+    try:
+        for on in (False, True):
+            TensorCircuit.fuse_levels_forward = on
+            pc = build_fixture_circuit(name, fx).to(cuda_device)
+            load_fixture_params(pc, fx)
+            if on:
+                assert len(pc._level_run(B, kw.get("force_use_bf16", False), kw.get("force_use_fp32", False))) >= 2
+            nat.device_status(clear=True)
+            pc.init_param_flows(flows_memory=0.0)
+            with torch.no_grad():
+                lls = pc(x, **kw)
+            pc.backward(inputs=x, allow_modify_flows=True, force_use_fp32="force_use_fp32" in kw)
+            pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+            torch.cuda.synchronize()
+            assert nat.device_status(clear=True) == 0
+            out.append((lls.clone(), pc.node_mars.clone(), pc._em_resident.clone(), pc.node_flows.clone(),
+                        pc.param_flows.clone(), pc.params.clone()))
+    finally:
+        TensorCircuit.fuse_levels_forward = saved
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)
 
 
 @pytest.mark.parametrize("name,B,kw", [("hclt64", 64, dict(force_use_fp32=True)),
