@@ -154,30 +154,73 @@ int pcb_input_cat_em(float* params, const float* param_flows, const int32_t* s_p
                      double step_size, double pseudocount, int32_t keep_zero_params, void* stream);
 
 /*
- * Bernoulli (kind 1) and Gaussian (kind 2) input layers; data is FP32 [num_vars, data_ld]
- * (Bernoulli reads x > 0), missing values indexed as in pcb_input_cat_fwd.
+ * Bernoulli (kind 1), Gaussian (kind 2) and DiscreteLogistic (kind 3) input layers; data is
+ * FP32 [num_vars, data_ld] (Bernoulli reads x > 0; DiscreteLogistic reads bin indices),
+ * missing values indexed as in pcb_input_cat_fwd. meta: per-node metadata indexed by the
+ * node's layer-local id, Gaussian min_sigma[n] (EM only), DiscreteLogistic
+ * (lo, hi, num_cats, min_std) at meta[4 n .. 4 n + 3] (all three calls); NULL otherwise.
  * pcb_input_dist_fwd: node_mars = log p (Bernoulli: p = params[s_pid] for x > 0, else 1 - p;
- *   Gaussian: log N(x; params[s_pid], params[s_pid + 1])), 0 where missing.
+ *   Gaussian: log N(x; params[s_pid], params[s_pid + 1]); DiscreteLogistic with
+ *   (mu, s) = params[s_pid ..] and w = (hi - lo) / num_cats: log(F(lo + (x + 1) w) - F(lo + x w)),
+ *   F(v) = 1 / (1 + exp((mu - v) / s)), F = 1 above the last bin and 0 below the first,
+ *   clamped at -1000), 0 where missing.
  * pcb_input_dist_bwd: per node, the batch sums of the flow-weighted sufficient statistics
  *   added to its flow slots: Bernoulli (x > 0, x <= 0) (missing samples add nothing);
- *   Gaussian (f x, f x^2, f), a missing value contributing (f mu, f (sigma^2 + mu^2), f).
+ *   Gaussian (f x, f x^2, f), a missing value contributing (f mu, f (sigma^2 + mu^2), f);
+ *   DiscreteLogistic the same with the bin midpoint m = lo + (x + 1/2) w for x and the
+ *   variance s^2 pi^2 / 3 for sigma^2.
  *   atomic = 1 when tied nodes share slots. logspace_flows: node flows hold log flows.
  * pcb_input_dist_em: Bernoulli p' = (1 - s) p + s (f1 + pc / 2) / (f1 + f0 + pc); Gaussian
- *   moment matching of the step-interpolated expectation parameters, sigma >= min_sigma[n]
- *   (per node, indexed by the node's layer-local id).
+ *   moment matching of the step-interpolated expectation parameters, sigma >= min_sigma[n];
+ *   DiscreteLogistic the same on the standard deviation s pi / sqrt(3) >= min_std.
  * Replace the fw_mar_fn / bk_flow_fn / bk_flow_mask_fn / em_fn kernels of
- * src/pyjuice/nodes/distributions/bernoulli.py:64-102 and gaussian.py:87-170.
+ * src/pyjuice/nodes/distributions/bernoulli.py:64-102, gaussian.py:87-170 and
+ * discrete_logistic.py:81-202.
  */
 int pcb_input_dist_fwd(int32_t kind, const float* data, int64_t data_ld, const float* params, const int32_t* vids,
-                       const int32_t* s_pids, int32_t num_nodes, int32_t node_offset, float* node_mars, int64_t ld,
-                       int32_t B, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv, void* stream);
+                       const int32_t* s_pids, const float* meta, int32_t num_nodes, int32_t node_offset,
+                       float* node_mars, int64_t ld, int32_t B, const uint8_t* missing, int64_t miss_sb,
+                       int64_t miss_sv, void* stream);
 int pcb_input_dist_bwd(int32_t kind, const float* data, int64_t data_ld, const float* node_flows, int64_t ld, int32_t B,
                        const float* params, const int32_t* vids, const int32_t* s_pids, const int32_t* s_pfids,
-                       int32_t num_nodes, int32_t node_offset, float* param_flows, int32_t logspace_flows,
-                       const uint8_t* missing, int64_t miss_sb, int64_t miss_sv, int32_t atomic, void* stream);
+                       const float* meta, int32_t num_nodes, int32_t node_offset, float* param_flows,
+                       int32_t logspace_flows, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
+                       int32_t atomic, void* stream);
 int pcb_input_dist_em(int32_t kind, float* params, const float* param_flows, const int32_t* s_pids,
-                      const int32_t* s_pfids, const float* min_sigma, const int32_t* source_nids,
+                      const int32_t* s_pfids, const float* meta, const int32_t* source_nids,
                       int32_t num_source_nodes, double step_size, double pseudocount, void* stream);
+
+/*
+ * SoftEvidenceCategorical input layers (categorical nodes times per-sample evidence over the
+ * categories). Evidence: log-weights L[b, u, j] at evidence_logp + b e_sb + u e_su + j, j < K,
+ * u = grp_lvid[g] for the group's variable; dense (cat_ids NULL: j is the category, K <= every
+ * node's num_cats) or sparse (cat_ids at the same offsets give the category of entry j).
+ * Groups: runs of consecutive nodes over one variable (grp_var, grp_node0 layer-local,
+ * grp_count); node_grp: the group of each node (sparse forward only).
+ * pcb_input_poe_fwd: node_mars[n, b] = log theta[n, x] + L[b, u, x] - log Z[n, b],
+ *   Z = sum_j theta[n, cat_j] exp(L[b, u, j]), with x = data[v, b]; 0 where missing; a
+ *   category outside the node's or the evidence's range gives -inf (sparse: no entry) or NaN
+ *   (dense).
+ * pcb_input_poe_evidence_bwd: evidence_grad[b, u, j] += sum_n f[n, b] ([cat_j == x] -
+ *   theta[n, cat_j] exp(L[b, u, j]) / Z[n, b]) over the variable's nodes, f the node flows
+ *   (logspace_flows: node_flows hold log f); Z recovered from node_mars of the forward.
+ * Replace fw_kernel, bk_softevi_kernel (softevi_categorical.py:310-462, 502-681); the
+ * parameter flows (bk_params_kernel, 464-500) are pcb_input_cat_bwd's.
+ */
+int pcb_input_poe_fwd(const int64_t* data, int64_t data_ld, const float* evidence_logp, const int64_t* cat_ids,
+                      int64_t e_sb, int64_t e_su, int32_t K, const float* params, const int32_t* grp_var,
+                      const int32_t* grp_lvid, const int32_t* grp_node0, const int32_t* grp_count,
+                      int32_t num_groups, int32_t max_group_nodes, const int32_t* node_grp, int32_t num_nodes,
+                      const int32_t* s_pids, const int32_t* ncats, int32_t node_offset, float* node_mars,
+                      int64_t ld, int32_t B, const uint8_t* missing, int64_t miss_sb, int64_t miss_sv,
+                      void* stream);
+int pcb_input_poe_evidence_bwd(const int64_t* data, int64_t data_ld, const float* node_flows, const float* node_mars,
+                               int64_t ld, int32_t B, int32_t logspace_flows, const float* evidence_logp,
+                               const int64_t* cat_ids, int64_t e_sb, int64_t e_su, int32_t K, float* evidence_grad,
+                               int64_t g_sb, int64_t g_su, const float* params, const int32_t* grp_var,
+                               const int32_t* grp_lvid, const int32_t* grp_node0, const int32_t* grp_count,
+                               int32_t num_groups, int32_t max_group_nodes, const int32_t* s_pids,
+                               const int32_t* ncats, int32_t node_offset, void* stream);
 
 /*
  * Sum of tied input-node flow slots into the source slot:
@@ -621,6 +664,17 @@ int pcb_sample_prod(int32_t* nlist, int32_t* ncnt, int32_t* elist, int32_t* ecnt
 int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
                      const int32_t* vids, const int32_t* s_pids, const int32_t* ncats, const float* params,
                      int64_t* samples, int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream);
+/*
+ * pcb_sample_input for a SoftEvidenceCategorical layer: node n of sample s draws category k
+ * with probability theta[n, k] exp(L[s, u, k]) / sum_k' (...) over k < K, L the evidence
+ * log-weights at evidence_logp + s e_sb + u e_su + k and u = node_lvid[n] (layer-local n);
+ * the first k whose cumulative probability exceeds the uniform (the last category if rounding
+ * leaves none). Replaces sample_kernel (softevi_categorical.py:683-761).
+ */
+int pcb_sample_input_poe(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
+                         const int32_t* vids, const int32_t* s_pids, const int32_t* node_lvid, const float* params,
+                         const float* evidence_logp, int64_t e_sb, int64_t e_su, int32_t K, int64_t* samples,
+                         int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream);
 
 /*
  * Whole-circuit sampling that allocates nothing. No counterpart in the reference: the

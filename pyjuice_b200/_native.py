@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(_HERE, "libpcb200.so")
 CSRC = os.path.join(_HERE, "csrc")
 SOURCES = ["capi_common.cu", "lse_contract.cu", "lse_contract_tc.cu", "lse_short.cu", "lse_tc05.cu", "prod_kernels.cu", "sum_pflows.cu",
            "sum_pflows_tc05.cu", "sum_generic.cu", "em_kernels.cu", "input_kernels.cu", "sample_kernels.cu", "sample_noalloc.cu",
-           "input_soft.cu", "input_dists.cu"]
+           "input_soft.cu", "input_dists.cu", "input_poe.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-shared",
               "-Xcompiler", "-fPIC"]
 
@@ -98,13 +98,20 @@ _SIGS = {
                            c_void_p, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_input_cat_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double,
                           c_int32, c_void_p], c_int32),
-    "pcb_input_dist_fwd": ([c_int32, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p,
-                            c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
+    "pcb_input_dist_fwd": ([c_int32, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32,
+                            c_void_p, c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
     "pcb_input_dist_bwd": ([c_int32, c_void_p, c_int64, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p,
-                            c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int64, c_int32,
-                            c_void_p], c_int32),
+                            c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int64,
+                            c_int32, c_void_p], c_int32),
     "pcb_input_dist_em": ([c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
                            c_double, c_void_p], c_int32),
+    "pcb_input_poe_fwd": ([c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int64, c_int32, c_void_p, c_void_p,
+                           c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p,
+                           c_int32, c_void_p, c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p], c_int32),
+    "pcb_input_poe_evidence_bwd": ([c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_int32, c_int32, c_void_p,
+                                    c_void_p, c_int64, c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p,
+                                    c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p,
+                                    c_int32, c_void_p], c_int32),
     "pcb_pflow_accum": ([c_void_p, c_int64, c_int64, c_void_p, c_int32, c_void_p], c_int32),
     "pcb_prod_gather_sum": ([c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_int32, c_int32, c_void_p], c_int32),
@@ -168,6 +175,9 @@ _SIGS = {
                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int32),
     "pcb_sample_input": ([c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
+    "pcb_sample_input_poe": ([c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_int64, c_int64, c_int32, c_void_p, c_int64, c_void_p, c_int64,
+                              c_uint64, c_void_p], c_int32),
     "pcb_sample_circuit_noalloc": ([c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p, c_int64, c_uint64,
                                     c_void_p, c_void_p], c_int32),
 }

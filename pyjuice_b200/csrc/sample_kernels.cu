@@ -124,6 +124,40 @@ __global__ void sample_input_kernel(const int* __restrict__ nlist, const int* __
     samples[(int64_t)s * sld + vids[n]] = pick;
 }
 
+// SoftEvidenceCategorical inputs: category k with probability theta[n, k] exp(L[s, u, k]) / Z
+// over k < K (the evidence of sample s for the node's variable u), the first category whose
+// cumulative probability exceeds the uniform (softevi_categorical.py:683-761); the last
+// category when rounding leaves the uniform above the total.
+__global__ void sample_input_poe_kernel(const int* __restrict__ nlist, const int* __restrict__ ncnt, int S, int cap_n,
+                                        int lo, int hi, const int* __restrict__ vids, const int* __restrict__ s_pids,
+                                        const int* __restrict__ node_lvid, const float* __restrict__ params,
+                                        const float* __restrict__ logp, int64_t e_sb, int64_t e_su, int K,
+                                        int64_t* __restrict__ samples, int64_t sld, const float* __restrict__ uniforms,
+                                        int64_t u_ld, uint64_t seed) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)S * cap_n) return;
+    const int s = (int)(idx / cap_n);
+    const int j = (int)(idx % cap_n);
+    if (j >= ncnt[s]) return;
+    const int id = nlist[idx];
+    if (id < lo || id >= hi) return;
+    const int n = id - lo;
+    const int64_t sp = s_pids[n];
+    const float* L = logp + (int64_t)s * e_sb + (int64_t)node_lvid[n] * e_su;
+    float m = -INFINITY;
+    for (int k = 0; k < K; ++k) m = fmaxf(m, L[k]);
+    float z = 0.f;
+    for (int k = 0; k < K; ++k) z += params[sp + k] * expf(L[k] - m);
+    const float u = (uniforms ? uniforms[(int64_t)id * u_ld + s] : uniform(seed, (uint32_t)id, (uint32_t)s)) * z;
+    float cum = 0.f;
+    int pick = K - 1;
+    for (int k = 0; k < K; ++k) {
+        cum += params[sp + k] * expf(L[k] - m);
+        if (cum > u) { pick = k; break; }
+    }
+    samples[(int64_t)s * sld + vids[n]] = pick;
+}
+
 }  // namespace
 
 extern "C" {
@@ -166,6 +200,21 @@ int pcb_sample_input(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32
     sample_input_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
         nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, ncats, params, samples, sld, uniforms, u_ld, seed);
     return pcb::check_launch("pcb_sample_input");
+}
+
+int pcb_sample_input_poe(const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo, int32_t hi,
+                         const int32_t* vids, const int32_t* s_pids, const int32_t* node_lvid, const float* params,
+                         const float* evidence_logp, int64_t e_sb, int64_t e_su, int32_t K, int64_t* samples,
+                         int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream) {
+    if (!nlist || !ncnt || !vids || !s_pids || !node_lvid || !params || !evidence_logp || K <= 0 || !samples ||
+        S < 0 || cap_n <= 0 || hi < lo || (uniforms && u_ld < S))
+        return pcb::set_error(PCB_E_ARG, "pcb_sample_input_poe: bad arguments");
+    if (S == 0) return PCB_OK;
+    const int64_t total = (int64_t)S * cap_n;
+    sample_input_poe_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
+        nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, node_lvid, params, evidence_logp, e_sb, e_su, K, samples, sld,
+        uniforms, u_ld, seed);
+    return pcb::check_launch("pcb_sample_input_poe");
 }
 
 }  // extern "C"

@@ -1062,12 +1062,15 @@ class ProdLayer(Layer):
         return f"ProdLayer(nid_range={self._layer_nid_range}, num_nodes={self.num_nodes}, num_edges={self.num_edges})"
 
 
-_DIST_KIND = {"Categorical": 0, "Bernoulli": 1, "Gaussian": 2}
+_DIST_KIND = {"Categorical": 0, "Bernoulli": 1, "Gaussian": 2, "DiscreteLogistic": 3,
+              "ExternSoftEvidenceCategorical": 4}
+_CATEGORICAL_KINDS = (0, 4)  # parameter layout, flow histogram and EM of the Categorical
 
 
 class InputLayer(Layer, torch.nn.Module):
     """A layer of input node vectors of one distribution: Categorical (lookups, counting-sort
-    flows, soft evidence), Bernoulli or Gaussian (``input_dists.cu``)."""
+    flows, soft evidence), Bernoulli, Gaussian or DiscreteLogistic (``input_dists.cu``), or
+    SoftEvidenceCategorical (``input_poe.cu``: categorical nodes times per-sample evidence)."""
 
     _tensor_lists = ()
 
@@ -1115,11 +1118,18 @@ class InputLayer(Layer, torch.nn.Module):
     def _host_desc(self):
         vids = self.vids[:, 0].cpu().numpy()
         meta = self.metadata.cpu()
-        if self.kind == 0:
+        if self.kind in _CATEGORICAL_KINDS:
             ncats = meta[self.s_mids.cpu()].long().numpy()
         else:
             ncats = np.ones(vids.shape[0], np.int64)
-        min_sigma = (meta[self.s_mids.cpu()].float() if self.kind == 2 else torch.zeros([vids.shape[0]]))
+        # per-node metadata of input_dists.cu: Gaussian min_sigma; DiscreteLogistic
+        # (lo, hi, num_cats, min_std)
+        width = {2: 1, 3: 4}.get(self.kind, 1)
+        if self.kind in (2, 3):
+            sm = self.s_mids.cpu().long()
+            node_meta = torch.stack([meta[sm + j].float() for j in range(width)], dim=1).reshape(-1)
+        else:
+            node_meta = torch.zeros([vids.shape[0]])
         # runs of consecutive nodes over the same variable
         change = np.ones(vids.shape[0], dtype=bool)
         change[1:] = vids[1:] != vids[:-1]
@@ -1130,6 +1140,11 @@ class InputLayer(Layer, torch.nn.Module):
             tied.append((int(dst), int(n), ch.clone().long()))
         # nodes of every variable (CSR over the variable ids 0 .. max vid), for the evidence
         # backward contractions
+        # the index of each group's variable among the layer's variables (the evidence row of
+        # a SoftEvidenceCategorical layer), and the group of each node
+        layer_vars = np.unique(vids)
+        grp_lvid = np.searchsorted(layer_vars, vids[starts])
+        node_grp = np.repeat(np.arange(starts.shape[0]), counts)
         order = np.argsort(vids, kind="stable")
         var_ptr = np.zeros(int(vids.max()) + 2, np.int64)
         np.add.at(var_ptr, vids + 1, 1)
@@ -1137,9 +1152,11 @@ class InputLayer(Layer, torch.nn.Module):
         return dict(vids=_i32(vids), s_pids=_i32(self.s_pids.cpu()), s_pfids=_i32(self.s_pfids.cpu()),
                     ncats=_i32(ncats), source_nids=_i32(self.source_nids.cpu()),
                     grp_var=_i32(vids[starts]), grp_node0=_i32(starts), grp_count=_i32(counts),
-                    grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), max_grp=int(counts.max()),
+                    grp_ncats=_i32(ncats[starts]), max_ncats=int(ncats.max()), min_ncats=int(ncats.min()), max_grp=int(counts.max()),
                     shared_slots=bool(np.unique(self.s_pfids.cpu().numpy()).size < self.s_pfids.numel()),
-                    min_sigma=min_sigma.contiguous(),
+                    node_meta=node_meta.contiguous(), grp_lvid=_i32(grp_lvid), node_grp=_i32(node_grp),
+                    node_lvid=_i32(grp_lvid[node_grp]),
+                    num_layer_vars=int(layer_vars.shape[0]),
                     tied=tied, var_ptr=var_ptr, var_nodes=order.astype(np.int64))
 
     def _init_parameters(self, perturbation: float = 2.0):
@@ -1185,12 +1202,16 @@ class InputLayer(Layer, torch.nn.Module):
         d = self._desc(node_mars.device)
         B = node_mars.size(1)
         m, sb, sv = self._mask_args(missing_mask, B, node_mars.device, _batch_first)
+        if self.kind == 4:
+            self._forward_poe(data, node_mars, d, B, (m, sb, sv), kwargs)
+            return
         if self.kind != 0:
             xf = data.to(torch.float32)
             if xf.stride(1) != 1:
                 xf = xf.contiguous()
             nat.call("pcb_input_dist_fwd", self.kind, nat.ptr(xf), xf.stride(0), nat.ptr(self.params),
-                     nat.ptr(d["vids"]), nat.ptr(d["s_pids"]), self.num_nodes, self._output_ind_range[0],
+                     nat.ptr(d["vids"]), nat.ptr(d["s_pids"]), nat.ptr(d["node_meta"]), self.num_nodes,
+                     self._output_ind_range[0],
                      nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
             return
         data = data.to(torch.long)
@@ -1203,6 +1224,61 @@ class InputLayer(Layer, torch.nn.Module):
                      c_void_p(d["vids"].data_ptr() + 4 * n0), c_void_p(d["s_pids"].data_ptr() + 4 * n0),
                      c_void_p(d["ncats"].data_ptr() + 4 * n0), cnt, self._output_ind_range[0] + n0,
                      nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv, nat.stream())
+
+    def _poe_evidence(self, d, B: int, device, kwargs):
+        """(log-weights, category ids or None) of a SoftEvidenceCategorical layer's evidence,
+        ``categorical_evidence_logp`` [B, num_layer_vars, K] (FP32) and optionally
+        ``soft_evidence_cat_ids`` (int64, same shape) (softevi_categorical.py:25-84)."""
+        ev = kwargs.get("categorical_evidence_logp")
+        if ev is None:
+            raise ValueError("a SoftEvidenceCategorical input layer needs `categorical_evidence_logp`")
+        if ev.dim() != 3 or ev.dtype != torch.float32 or ev.device != device:
+            raise ValueError("`categorical_evidence_logp` must be a float32 [B, num_vars, num_cats] tensor "
+                             "on the circuit's device")
+        if ev.size(0) != B or ev.size(1) < d["num_layer_vars"]:
+            raise ValueError(f"`categorical_evidence_logp` must be [{B}, >= {d['num_layer_vars']}, K]")
+        ids = kwargs.get("soft_evidence_cat_ids")
+        if ids is None and ev.size(2) > d["min_ncats"]:
+            raise ValueError("`categorical_evidence_logp` has more categories than the nodes")
+        if ev.stride(2) != 1:
+            ev = ev.contiguous()
+        if ids is not None:
+            if ids.shape != ev.shape or ids.device != device:
+                raise ValueError("`soft_evidence_cat_ids` must have the shape of `categorical_evidence_logp`")
+            ids = ids.to(torch.long)
+            if ids.stride() != ev.stride():
+                ids = ids.contiguous()
+                ev = ev.contiguous()
+        return ev, ids
+
+    def _forward_poe(self, data, node_mars, d, B, mask, kwargs):
+        ev, ids = self._poe_evidence(d, B, node_mars.device, kwargs)
+        data = data.to(torch.long)
+        if data.stride(1) != 1:
+            data = data.contiguous()
+        m, sb, sv = mask
+        nat.call("pcb_input_poe_fwd", nat.ptr(data), data.stride(0), nat.ptr(ev), nat.ptr(ids), ev.stride(0),
+                 ev.stride(1), ev.size(2), nat.ptr(self.params), nat.ptr(d["grp_var"]), nat.ptr(d["grp_lvid"]),
+                 nat.ptr(d["grp_node0"]), nat.ptr(d["grp_count"]), d["grp_var"].size(0), d["max_grp"],
+                 nat.ptr(d["node_grp"]), self.num_nodes, nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]),
+                 self._output_ind_range[0], nat.ptr(node_mars), node_mars.stride(0), B, nat.ptr(m), sb, sv,
+                 nat.stream())
+
+    def _backward_poe_evidence(self, data, node_flows, node_mars, d, B, logspace_flows, kwargs):
+        """``categorical_evidence_logp_grad`` += the gradient of the flow-weighted node values
+        with respect to the evidence log-weights (softevi_categorical.py:502-661)."""
+        ev, ids = self._poe_evidence(d, B, node_flows.device, kwargs)
+        grad = kwargs["categorical_evidence_logp_grad"]
+        if grad.shape != ev.shape or grad.dtype != torch.float32 or grad.device != node_flows.device or \
+                grad.stride(2) != 1:
+            raise ValueError("`categorical_evidence_logp_grad` must be a float32 tensor shaped like the evidence, "
+                             "contiguous over categories")
+        nat.call("pcb_input_poe_evidence_bwd", nat.ptr(data), data.stride(0), nat.ptr(node_flows),
+                 nat.ptr(node_mars), node_flows.stride(0), B, 1 if logspace_flows else 0, nat.ptr(ev), nat.ptr(ids),
+                 ev.stride(0), ev.stride(1), ev.size(2), nat.ptr(grad), grad.stride(0), grad.stride(1),
+                 nat.ptr(self.params), nat.ptr(d["grp_var"]), nat.ptr(d["grp_lvid"]), nat.ptr(d["grp_node0"]),
+                 nat.ptr(d["grp_count"]), d["grp_var"].size(0), d["max_grp"], nat.ptr(d["s_pids"]),
+                 nat.ptr(d["ncats"]), self._output_ind_range[0], nat.stream())
 
     def forward_soft(self, evidence: torch.Tensor, node_mars: torch.Tensor, missing_mask=None,
                      _batch_first: bool = True, **kwargs):
@@ -1284,13 +1360,20 @@ class InputLayer(Layer, torch.nn.Module):
             self.init_param_flows(0.0)
         B = node_flows.size(1)
         m, sb, sv = self._mask_args(missing_mask, B, node_flows.device, _batch_first)
-        if self.kind != 0:
+        if self.kind == 4:
+            # parameter flows: the categorical histogram of the observed categories, missing or
+            # not; then the evidence gradient when asked for (softevi_categorical.py:87-123, 464-500)
+            if "categorical_evidence_logp" not in kwargs:
+                return
+            m, sb, sv = None, 0, 0
+        if self.kind not in _CATEGORICAL_KINDS:
             xf = data.to(torch.float32)
             if xf.stride(1) != 1:
                 xf = xf.contiguous()
             nat.call("pcb_input_dist_bwd", self.kind, nat.ptr(xf), xf.stride(0), nat.ptr(node_flows),
                      node_flows.stride(0), B, nat.ptr(self.params), nat.ptr(d["vids"]), nat.ptr(d["s_pids"]),
-                     nat.ptr(d["s_pfids"]), self.num_nodes, self._output_ind_range[0], nat.ptr(self.param_flows),
+                     nat.ptr(d["s_pfids"]), nat.ptr(d["node_meta"]), self.num_nodes, self._output_ind_range[0],
+                     nat.ptr(self.param_flows),
                      1 if logspace_flows else 0, nat.ptr(m), sb, sv, 1 if d["shared_slots"] else 0, nat.stream())
             return
         data = data.to(torch.long)
@@ -1304,6 +1387,8 @@ class InputLayer(Layer, torch.nn.Module):
                  g["grp_var"].size(0), d["max_ncats"], nat.ptr(d["s_pfids"]), self._output_ind_range[0],
                  nat.ptr(self.param_flows), 1 if logspace_flows else 0, nat.ptr(m), sb, sv, nat.ptr(d["s_pids"]),
                  nat.ptr(self.params), 1 if d["shared_slots"] else 0, nat.stream())
+        if self.kind == 4 and "categorical_evidence_logp_grad" in kwargs:
+            self._backward_poe_evidence(data, node_flows, node_mars, d, B, logspace_flows, kwargs)
 
     def mini_batch_em(self, step_size: float, pseudocount: float = 0.0, keep_zero_params: bool = False,
                       use_f64_flows: bool = False):
@@ -1314,11 +1399,11 @@ class InputLayer(Layer, torch.nn.Module):
         for dst, n, ch in d["tied"]:
             nat.call("pcb_pflow_accum_f64" if use_f64_flows else "pcb_pflow_accum", nat.ptr(pf), dst, n, nat.ptr(ch),
                      ch.size(0), nat.stream())
-        if self.kind != 0:
+        if self.kind not in _CATEGORICAL_KINDS:
             if use_f64_flows:
                 raise NotImplementedError("FP64 epoch flows are kept for Categorical input layers")
             nat.call("pcb_input_dist_em", self.kind, nat.ptr(self.params), nat.ptr(pf), nat.ptr(d["s_pids"]),
-                     nat.ptr(d["s_pfids"]), nat.ptr(d["min_sigma"]), nat.ptr(d["source_nids"]),
+                     nat.ptr(d["s_pfids"]), nat.ptr(d["node_meta"]), nat.ptr(d["source_nids"]),
                      d["source_nids"].size(0), float(step_size), float(pseudocount), nat.stream())
             return
         nat.call("pcb_input_cat_em_f64flows" if use_f64_flows else "pcb_input_cat_em", nat.ptr(self.params),

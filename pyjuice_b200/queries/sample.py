@@ -47,6 +47,10 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
     device; node ``n`` of sample ``s`` then draws with ``uniforms[n, s]`` instead of the
     seeded hash. With the draws the reference's ``tl.rand`` made for each (node, sample),
     the samples equal the reference's bit for bit.
+
+    SoftEvidenceCategorical input layers draw from their categorical distribution times the
+    evidence ``categorical_evidence_logp`` ``[num_samples, num_vars, K]`` (log-weights, dense),
+    which such circuits need (softevi_categorical.py:196-222, 683-761).
     """
     if conditional:
         raise NotImplementedError("conditional sampling has no CUDA path yet")
@@ -56,8 +60,20 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
         raise ValueError("It is ambiguous to sample from multi-head PCs.")
     if pc.device.type != "cuda":
         raise RuntimeError("sampling runs on CUDA only")
-    if any(getattr(layer, "kind", 0) != 0 for layer in pc.input_layer_group):
-        raise NotImplementedError("the device sampler draws Categorical inputs only")
+    evidence = kwargs.get("categorical_evidence_logp")
+    for layer in pc.input_layer_group:
+        kind = getattr(layer, "kind", 0)
+        if kind == 4:
+            if evidence is None:
+                raise ValueError("sampling a SoftEvidenceCategorical layer needs `categorical_evidence_logp`")
+            if (evidence.dtype != torch.float32 or evidence.dim() != 3 or evidence.size(0) != num_samples or
+                    evidence.device != pc.device or evidence.stride(2) != 1 or
+                    evidence.size(1) < layer._desc(pc.device)["num_layer_vars"] or
+                    evidence.size(2) > layer._desc(pc.device)["min_ncats"]):
+                raise ValueError("`categorical_evidence_logp` must be a float32 [num_samples, num_vars, K <= num_cats] "
+                                 "tensor on the circuit's device, contiguous over categories")
+        elif kind != 0:
+            raise NotImplementedError("the device sampler draws Categorical and SoftEvidenceCategorical inputs only")
     if seed is None:
         seed = random.randint(0, 2 ** 62)
     dev = pc.device
@@ -70,10 +86,10 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
                              f"the circuit's device {dev}")
         u_ld = uniforms.stride(0)
     with torch.cuda.device(dev):
-        return _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns)
+        return _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns, evidence)
 
 
-def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns):
+def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns, evidence=None):
     dev = pc.device
     cap_n, cap_e = _scope_bounds(pc)
     cap_n = max(cap_n, 1)
@@ -106,6 +122,12 @@ def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns):
     for layer in pc.input_layer_group:
         d = layer._desc(dev)
         lo, hi = layer._output_ind_range
+        if getattr(layer, "kind", 0) == 4:
+            nat.call("pcb_sample_input_poe", nat.ptr(nlist), nat.ptr(ncnt), S, cap_n, lo, hi, nat.ptr(d["vids"]),
+                     nat.ptr(d["s_pids"]), nat.ptr(d["node_lvid"]), nat.ptr(layer.params), nat.ptr(evidence),
+                     evidence.stride(0), evidence.stride(1), evidence.size(2), nat.ptr(samples), pc.num_vars,
+                     nat.ptr(uniforms), u_ld, seed, st)
+            continue
         nat.call("pcb_sample_input", nat.ptr(nlist), nat.ptr(ncnt), S, cap_n, lo, hi, nat.ptr(d["vids"]),
                  nat.ptr(d["s_pids"]), nat.ptr(d["ncats"]), nat.ptr(layer.params), nat.ptr(samples), pc.num_vars,
                  nat.ptr(uniforms), u_ld, seed, st)
@@ -137,6 +159,8 @@ def noalloc_sample_plan(pc):
         raise ValueError("It is ambiguous to sample from multi-head PCs.")
     if pc.device.type != "cuda":
         raise RuntimeError("sampling runs on CUDA only")
+    if any(getattr(layer, "kind", 0) != 0 for layer in pc.input_layer_group):
+        raise NotImplementedError("the allocation-free sampler draws Categorical inputs only")
     dev = pc.device
     key = (str(dev), pc.params.data_ptr(), tuple(layer.params.data_ptr() for layer in pc.input_layer_group))
     cached = getattr(pc, "_noalloc_sample_plan", None)

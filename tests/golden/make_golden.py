@@ -32,8 +32,8 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``structures.npz`` compiled layouts, parameters and log-likelihoods of the reference's PD
                     (3 x 3 grid) and homogeneous HMM (length 6) generators; flows and one EM
                     step of the HMM (tied transitions and emissions);
-* ``dists.npz``      Bernoulli and Gaussian input layers (four-variable circuit): one FP32
-                    forward / backward / EM step;
+* ``dists.npz``      Bernoulli, Gaussian and DiscreteLogistic input layers (four-variable
+                    circuit): one FP32 forward / backward / EM step;
 * ``samples_{tiny,hclt64}.npz``  256 samples the reference's ``queries.sample`` drew on the
                     circuits and parameters of ``tiny.npz`` / ``hclt64.npz`` with every
                     ``tl.rand`` draw replaced by a table lookup by (node, sample)
@@ -419,16 +419,19 @@ def make_structures():
 
 
 def make_dist_variants():
-    """Bernoulli and Gaussian input layers on a four-variable circuit (circuits.build_dist_dag):
-    FP32 forward, backward and mini_batch_em(0.3, 0.1) by the reference, with seeded parameters
-    and data (bool data for Bernoulli, N(0, 1.5) data for Gaussian)."""
+    """Bernoulli, Gaussian and DiscreteLogistic input layers on a four-variable circuit
+    (circuits.build_dist_dag): FP32 forward, backward and mini_batch_em(0.3, 0.1) by the
+    reference, with seeded parameters and data (bool data for Bernoulli, N(0, 1.5) data for
+    Gaussian, bin indices 0..7 for DiscreteLogistic over 8 bins of [-2, 2])."""
     from circuits import build_dist_dag
     out = {}
     rng = np.random.default_rng(21)
     for name, factory, data in (
             ("bern", lambda: dists.Bernoulli(), torch.from_numpy(rng.random((32, 4)) < 0.4)),
             ("gauss", lambda: dists.Gaussian(mu=0.0, sigma=1.0),
-             torch.from_numpy((1.5 * rng.standard_normal((32, 4))).astype(np.float32)))):
+             torch.from_numpy((1.5 * rng.standard_normal((32, 4))).astype(np.float32))),
+            ("dlog", lambda: dists.DiscreteLogistic(val_range=(-2.0, 2.0), num_cats=8),
+             torch.from_numpy(rng.integers(0, 8, size=(32, 4)).astype(np.float32)))):
         torch.manual_seed(11)
         pc = juice.compile(build_dist_dag(juice, factory), verbose=False)
         out[name + "_params0"] = pc.params.detach().numpy().copy()

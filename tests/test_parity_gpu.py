@@ -450,15 +450,17 @@ def test_pd_with_parentless_products_flows_vs_oracle(cuda_device):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("name", ["bern", "gauss"])
+@pytest.mark.parametrize("name", ["bern", "gauss", "dlog"])
 def test_bernoulli_and_gaussian_layers_match_reference(name, cuda_device):
-    """Bernoulli and Gaussian input layers: FP32 forward, flows and one EM step against the
-    reference's own outputs (dists.npz; four-variable circuit, seeded parameters and data)."""
+    """Bernoulli, Gaussian and DiscreteLogistic input layers: FP32 forward, flows and one EM
+    step against the reference's own outputs (dists.npz; four-variable circuit, seeded
+    parameters and data)."""
     from circuits import build_dist_dag
     fx = load_fixture("dists")
     g = lambda k: fx[f"{name}_{k}"]
-    factory = (lambda: juice.distributions.Bernoulli()) if name == "bern" else \
-        (lambda: juice.distributions.Gaussian(mu=0.0, sigma=1.0))
+    factory = {"bern": lambda: juice.distributions.Bernoulli(),
+               "gauss": lambda: juice.distributions.Gaussian(mu=0.0, sigma=1.0),
+               "dlog": lambda: juice.distributions.DiscreteLogistic(val_range=(-2.0, 2.0), num_cats=8)}[name]
     pc = juice.compile(build_dist_dag(juice, factory)).to(cuda_device)
     with torch.no_grad():
         pc.params.copy_(torch.from_numpy(g("params0")).to(cuda_device))

@@ -49,3 +49,22 @@ def test_hmm_matches_reference():
                            fx["in_param_flows"].astype(np.float64), 0.5, 0.01)
     assert np.abs(p1 - fx["params1"]).max() <= 1e-6
     assert np.abs(q1 - fx["in_params1"][:q1.shape[0]]).max() <= 1e-6
+
+
+def test_discrete_logistic_layer_matches_reference_layout():
+    """A DiscreteLogistic input layer compiles to the reference's sizes (two parameters and
+    three flow slots per node, dists.npz), with seeded initial parameters equal to the
+    reference's (same torch draws), and the per-node metadata the kernels read is
+    (lo, hi, num_cats, min_std) of each node. CPU only."""
+    from circuits import build_dist_dag
+    fx = load_fixture("dists")
+    torch.manual_seed(11)
+    pc = juice.compile(build_dist_dag(juice, lambda: dists.DiscreteLogistic(val_range=(-2.0, 2.0), num_cats=8)))
+    layer = pc.input_layer_group[0]
+    assert layer.num_parameters == fx["dlog_in_params0"].shape[0]
+    assert layer.num_param_flows == fx["dlog_in_param_flows"].shape[0]
+    assert np.abs(layer.params.detach().numpy()[:layer.num_parameters] - fx["dlog_in_params0"]).max() <= 1e-6
+    assert pc.params.numel() == fx["dlog_params0"].shape[0]
+    meta = layer._host_desc()["node_meta"].numpy().reshape(-1, 4)
+    assert meta.shape[0] == layer.num_nodes
+    assert np.allclose(meta, np.array([-2.0, 2.0, 8.0, 0.01], np.float32))
