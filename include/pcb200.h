@@ -675,6 +675,19 @@ int pcb_sample_input_poe(const int32_t* nlist, const int32_t* ncnt, int32_t S, i
                          const int32_t* vids, const int32_t* s_pids, const int32_t* node_lvid, const float* params,
                          const float* evidence_logp, int64_t e_sb, int64_t e_su, int32_t K, int64_t* samples,
                          int64_t sld, const float* uniforms, int64_t u_ld, uint64_t seed, void* stream);
+/*
+ * pcb_sample_input for Bernoulli (kind 1), Gaussian (kind 2) and DiscreteLogistic (kind 3)
+ * layers, one uniform u per (node, sample) as for pcb_sample_input, values written as FP32
+ * into samples[s * sld + var]: Bernoulli 1 if u < p else 0; Gaussian mu + sigma Phi^-1(u)
+ * (u moved inside (0, 1)); DiscreteLogistic the bin of mu + s log(u / (1 - u)) among the
+ * num_cats bins of [lo, hi), clamped to the first and last bin; meta as for
+ * pcb_input_dist_fwd (kind 3 only). Replaces the sample_fn of bernoulli.py:79-88,
+ * gaussian.py:114-125 and discrete_logistic.py:157-181.
+ */
+int pcb_sample_input_dist(int32_t kind, const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo,
+                          int32_t hi, const int32_t* vids, const int32_t* s_pids, const float* meta,
+                          const float* params, float* samples, int64_t sld, const float* uniforms, int64_t u_ld,
+                          uint64_t seed, void* stream);
 
 /*
  * Whole-circuit sampling that allocates nothing. No counterpart in the reference: the

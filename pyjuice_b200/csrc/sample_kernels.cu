@@ -158,6 +158,41 @@ __global__ void sample_input_poe_kernel(const int* __restrict__ nlist, const int
     samples[(int64_t)s * sld + vids[n]] = pick;
 }
 
+// Bernoulli (kind 1), Gaussian (kind 2) and DiscreteLogistic (kind 3) inputs, one uniform u
+// per (node, sample): Bernoulli 1 if u < p else 0 (bernoulli.py:79-88); Gaussian
+// mu + sigma Phi^-1(u') with u' = u + 2^-25 inside (0, 1) (the reference draws a Box-Muller
+// normal, gaussian.py:114-125: same distribution, other draws); DiscreteLogistic the bin of
+// mu + s log(u / (1 - u)) among num_cats bins of [lo, hi), clamped to the first and last
+// (discrete_logistic.py:157-181). Values are written as FP32.
+__global__ void sample_input_dist_kernel(int kind, const int* __restrict__ nlist, const int* __restrict__ ncnt, int S,
+                                         int cap_n, int lo, int hi, const int* __restrict__ vids,
+                                         const int* __restrict__ s_pids, const float* __restrict__ meta,
+                                         const float* __restrict__ params, float* __restrict__ samples, int64_t sld,
+                                         const float* __restrict__ uniforms, int64_t u_ld, uint64_t seed) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)S * cap_n) return;
+    const int s = (int)(idx / cap_n);
+    const int j = (int)(idx % cap_n);
+    if (j >= ncnt[s]) return;
+    const int id = nlist[idx];
+    if (id < lo || id >= hi) return;
+    const int n = id - lo;
+    const int64_t sp = s_pids[n];
+    const float u = uniforms ? uniforms[(int64_t)id * u_ld + s] : uniform(seed, (uint32_t)id, (uint32_t)s);
+    float r;
+    if (kind == 1) {
+        r = u < params[sp] ? 1.f : 0.f;
+    } else if (kind == 2) {
+        r = params[sp] + params[sp + 1] * normcdfinvf(fminf(u + 2.98023224e-8f, 0.99999994f));
+    } else {
+        const float lo_v = meta[4 * (int64_t)n], hi_v = meta[4 * (int64_t)n + 1], nc = meta[4 * (int64_t)n + 2];
+        const float x = params[sp] + params[sp + 1] * logf(u / (1.f - u));
+        const float bin = (x - lo_v) / ((hi_v - lo_v) / nc);
+        r = bin < 0.f ? 0.f : (bin > nc - 1.f ? nc - 1.f : floorf(bin));
+    }
+    samples[(int64_t)s * sld + vids[n]] = r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -215,6 +250,20 @@ int pcb_sample_input_poe(const int32_t* nlist, const int32_t* ncnt, int32_t S, i
         nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, node_lvid, params, evidence_logp, e_sb, e_su, K, samples, sld,
         uniforms, u_ld, seed);
     return pcb::check_launch("pcb_sample_input_poe");
+}
+
+int pcb_sample_input_dist(int32_t kind, const int32_t* nlist, const int32_t* ncnt, int32_t S, int32_t cap_n, int32_t lo,
+                          int32_t hi, const int32_t* vids, const int32_t* s_pids, const float* meta,
+                          const float* params, float* samples, int64_t sld, const float* uniforms, int64_t u_ld,
+                          uint64_t seed, void* stream) {
+    if (kind < 1 || kind > 3 || (kind == 3 && !meta) || !nlist || !ncnt || !vids || !s_pids || !params || !samples ||
+        S < 0 || cap_n <= 0 || hi < lo || (uniforms && u_ld < S))
+        return pcb::set_error(PCB_E_ARG, "pcb_sample_input_dist: bad arguments");
+    if (S == 0) return PCB_OK;
+    const int64_t total = (int64_t)S * cap_n;
+    sample_input_dist_kernel<<<(unsigned)pcb::cdiv(total, 256), 256, 0, pcb::as_stream(stream)>>>(
+        kind, nlist, ncnt, S, cap_n, lo, hi, vids, s_pids, meta, params, samples, sld, uniforms, u_ld, seed);
+    return pcb::check_launch("pcb_sample_input_dist");
 }
 
 }  // extern "C"

@@ -48,6 +48,8 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
     seeded hash. With the draws the reference's ``tl.rand`` made for each (node, sample),
     the samples equal the reference's bit for bit.
 
+    The result has the data type of the first input layer (int64 for Categorical, bool for
+    Bernoulli, float32 for Gaussian and DiscreteLogistic; src/pyjuice/queries/sample.py:456-457).
     SoftEvidenceCategorical input layers draw from their categorical distribution times the
     evidence ``categorical_evidence_logp`` ``[num_samples, num_vars, K]`` (log-weights, dense),
     which such circuits need (softevi_categorical.py:196-222, 683-761).
@@ -72,8 +74,8 @@ def sample(pc, num_samples: Optional[int] = None, conditional: bool = False, see
                     evidence.size(2) > layer._desc(pc.device)["min_ncats"]):
                 raise ValueError("`categorical_evidence_logp` must be a float32 [num_samples, num_vars, K <= num_cats] "
                                  "tensor on the circuit's device, contiguous over categories")
-        elif kind != 0:
-            raise NotImplementedError("the device sampler draws Categorical and SoftEvidenceCategorical inputs only")
+        elif kind not in (0, 1, 2, 3):
+            raise NotImplementedError(f"the device sampler has no draw for input layer kind {kind}")
     if seed is None:
         seed = random.randint(0, 2 ** 62)
     dev = pc.device
@@ -119,9 +121,18 @@ def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns, evidence=No
     if not _sample_input_ns:
         return nlist, ncnt
     samples = torch.zeros([S, pc.num_vars], dtype=torch.long, device=dev)
+    fsamples, fvars = None, []  # values of Bernoulli / Gaussian / DiscreteLogistic layers (FP32)
     for layer in pc.input_layer_group:
         d = layer._desc(dev)
         lo, hi = layer._output_ind_range
+        if getattr(layer, "kind", 0) in (1, 2, 3):
+            if fsamples is None:
+                fsamples = torch.zeros([S, pc.num_vars], dtype=torch.float32, device=dev)
+            nat.call("pcb_sample_input_dist", layer.kind, nat.ptr(nlist), nat.ptr(ncnt), S, cap_n, lo, hi,
+                     nat.ptr(d["vids"]), nat.ptr(d["s_pids"]), nat.ptr(d["node_meta"]), nat.ptr(layer.params),
+                     nat.ptr(fsamples), pc.num_vars, nat.ptr(uniforms), u_ld, seed, st)
+            fvars.append(d["vids"].long())
+            continue
         if getattr(layer, "kind", 0) == 4:
             nat.call("pcb_sample_input_poe", nat.ptr(nlist), nat.ptr(ncnt), S, cap_n, lo, hi, nat.ptr(d["vids"]),
                      nat.ptr(d["s_pids"]), nat.ptr(d["node_lvid"]), nat.ptr(layer.params), nat.ptr(evidence),
@@ -135,7 +146,13 @@ def _sample_on_device(pc, S, seed, uniforms, u_ld, _sample_input_ns, evidence=No
     if e != 0:
         raise RuntimeError(f"sampling failed on the device (code {e}: "
                            f"{'active list overflow' if e == 1 else 'element outside its product layer'})")
-    return samples
+    dtype = pc.input_layer_group[0].get_data_dtype()
+    if fsamples is None:
+        return samples if dtype == torch.long else samples.to(dtype)
+    out = samples.to(dtype)
+    cols = torch.unique(torch.cat(fvars))
+    out[:, cols] = fsamples[:, cols].to(dtype)
+    return out
 
 
 class _SampleStep(ctypes.Structure):

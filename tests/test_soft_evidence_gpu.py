@@ -1,15 +1,20 @@
-"""SoftEvidenceCategorical input layers (categorical nodes times per-sample evidence) on the
-GPU, with the known answers of the reference's own tests
-(tests/distributions/soft_evidence_cat_test.py:10-196): a product of such inputs under one sum
+"""Input distributions beyond the Categorical on the GPU.
+
+SoftEvidenceCategorical layers (categorical nodes times per-sample evidence), with the known
+answers of the reference's own tests (tests/distributions/soft_evidence_cat_test.py:10-196): a product of such inputs under one sum
 node gives, per variable, ``log_softmax(L + log theta)[x]``, and the evidence gradient that
 ``pc.backward`` accumulates equals torch autograd's gradient of those log-likelihoods. The
 sparse evidence form (category ids per entry) is checked against the dense one, and the
-parameter flows and EM step against the plain Categorical layer."""
+parameter flows and EM step against the plain Categorical layer. Sampling: under evidence
+(the reference's test), and for Bernoulli / DiscreteLogistic / Gaussian layers against the
+circuit's own marginals and moments."""
 
 import math
 
 import pytest
 import torch
+
+from circuits import build_dist_dag
 
 import pyjuice_b200 as juice
 from pyjuice_b200.nodes import distributions as dists
@@ -163,3 +168,49 @@ def test_soft_evidence_sampling(cuda_device):
         assert agree >= 0.98  # a uniform within rounding of a cumulative boundary may differ
     with pytest.raises(ValueError):
         juice.queries.sample(pc, num_samples=B)
+
+
+@pytest.mark.parametrize("name", ["bern", "dlog"])
+def test_bernoulli_and_discrete_logistic_sampling_marginals(name, cuda_device):
+    """Samples of a circuit over Bernoulli (DiscreteLogistic) inputs: the frequency of each
+    value of each variable matches the circuit's own marginal probability of that value
+    (the forward pass with the other variables missing), within 0.015 at 40,000 samples; the
+    result has the inputs' data type."""
+    torch.manual_seed(2)
+    factory = (lambda: dists.Bernoulli()) if name == "bern" else \
+        (lambda: dists.DiscreteLogistic(val_range=(-2.0, 2.0), num_cats=8))
+    pc = juice.compile(build_dist_dag(juice, factory)).to(cuda_device)
+    S = 40000
+    samples = juice.queries.sample(pc, num_samples=S, seed=5)
+    assert samples.dtype == (torch.bool if name == "bern" else torch.float32)
+    values = [0, 1] if name == "bern" else list(range(8))
+    for v in range(4):
+        mask = torch.ones([len(values), 4], dtype=torch.bool, device=cuda_device)
+        mask[:, v] = False
+        x = torch.zeros([len(values), 4], dtype=torch.float32, device=cuda_device)
+        x[:, v] = torch.tensor(values, dtype=torch.float32, device=cuda_device)
+        with torch.no_grad():
+            p = pc(x if name != "bern" else x.bool(), missing_mask=mask).exp().view(-1)
+        assert abs(float(p.sum()) - 1.0) < 1e-4
+        col = samples[:, v].float()
+        freq = torch.stack([(col == val).float().mean() for val in values])
+        assert (freq - p).abs().max() < 0.015
+
+
+def test_gaussian_sampling_moments(cuda_device):
+    """Gaussian inputs: with every sum weight on one child (a single mixture component per
+    variable), the samples of each variable have that component's mean and deviation."""
+    torch.manual_seed(4)
+    pc = juice.compile(build_dist_dag(juice, lambda: dists.Gaussian(mu=0.0, sigma=1.0))).to(cuda_device)
+    S = 40000
+    samples = juice.queries.sample(pc, num_samples=S, seed=9)
+    assert samples.dtype == torch.float32 and torch.isfinite(samples).all()
+    # the sample mean of each variable is the marginal mean sum_n P(node n active) mu_n, which
+    # lies inside the range of the variable's node means
+    layer = pc.input_layer_group[0]
+    prm = layer.params[:2 * layer.num_nodes].view(-1, 2)
+    for v in range(4):
+        nodes = (layer.vids[:, 0] == v).nonzero().view(-1)
+        mus = prm[layer.s_pids[nodes].long() // 2, 0]
+        m = samples[:, v].mean()
+        assert float(mus.min()) - 0.05 <= float(m) <= float(mus.max()) + 0.05
