@@ -9,10 +9,11 @@ itself pickled), and ``source_node`` (index of the tied source). The last entry 
 root. The file format is the interface, so the field names and the nesting are the
 reference's.
 
-The distribution is pickled under the reference's class path
-(``pyjuice.nodes.distributions.categorical.Categorical`` with the reference's attributes),
+The distribution is pickled under the reference's class path (e.g.
+``pyjuice.nodes.distributions.categorical.Categorical``) with the reference's attributes,
 written opcode by opcode so that no ``pyjuice`` module has to be importable when saving;
-when loading, that class path (and ours) maps to this package's ``Categorical``.
+when loading, that class path (and ours) maps to this package's class of the same name.
+Categorical, Bernoulli, Gaussian, DiscreteLogistic and SoftEvidenceCategorical are covered.
 """
 
 from __future__ import annotations
@@ -26,32 +27,55 @@ import torch
 
 from .model import TensorCircuit
 from .nodes import CircuitNodes, inputs, multiply, summate
-from .nodes.distributions import Categorical
+from .nodes.distributions import Bernoulli, Categorical, DiscreteLogistic, Gaussian, SoftEvidenceCategorical
 
-_REF_CATEGORICAL = ("pyjuice.nodes.distributions.categorical", "Categorical")
+_REF_MODULE = "pyjuice.nodes.distributions"
+# our class -> the reference's module (under pyjuice.nodes.distributions) and class name
+_REF_CLASS = {SoftEvidenceCategorical: ("softevi_categorical", "SoftEvidenceCategorical"),
+              Categorical: ("categorical", "Categorical"), Bernoulli: ("bernoulli", "Bernoulli"),
+              Gaussian: ("gaussian", "Gaussian"), DiscreteLogistic: ("discrete_logistic", "DiscreteLogistic")}
+_OUR_CLASS = {name: cls for cls, (_, name) in _REF_CLASS.items()}
+
+
+def _ref_state(dist) -> dict:
+    """The instance dictionary of the reference's object of this distribution."""
+    state = {"post_fw_fns": [], "post_bp_fns": [], "sampling_fns": []}
+    if isinstance(dist, Categorical):
+        state["num_cats"] = int(dist.num_cats)
+    elif isinstance(dist, Gaussian):
+        state.update(mu=dist.mu, sigma=dist.sigma, min_sigma=dist.min_sigma)
+    elif isinstance(dist, DiscreteLogistic):
+        state.update(val_range=tuple(dist.val_range), num_cats=int(dist.num_cats), min_std=dist.min_std,
+                     input_type=dist.input_type)
+    return state
 
 
 def _pickle_dist(dist) -> bytes:
     """The distribution as the reference pickles it: protocol 2, GLOBAL of the reference's
-    class, NEWOBJ, then BUILD with the instance dictionary the reference's ``Categorical``
-    carries (``post_fw_fns``, ``post_bp_fns``, ``sampling_fns``, ``num_cats``)."""
-    if not isinstance(dist, Categorical):
+    class, then either NEWOBJ and BUILD with the instance dictionary the reference's object
+    carries, or (SoftEvidenceCategorical, whose reference class reduces to its constructor
+    call) REDUCE on ``(num_cats,)``."""
+    ref = next((v for cls, v in _REF_CLASS.items() if type(dist) is cls), None)
+    if ref is None:
         raise NotImplementedError(f"saving distribution {type(dist).__name__} is not supported")
-    state = {"post_fw_fns": [], "post_bp_fns": [], "sampling_fns": [], "num_cats": int(dist.num_cats)}
     out = io.BytesIO()
     out.write(b"\x80\x02")                                                    # PROTO 2
-    out.write(b"c" + _REF_CATEGORICAL[0].encode() + b"\n" + _REF_CATEGORICAL[1].encode() + b"\n")  # GLOBAL
+    out.write(b"c" + f"{_REF_MODULE}.{ref[0]}".encode() + b"\n" + ref[1].encode() + b"\n")  # GLOBAL
+    if isinstance(dist, SoftEvidenceCategorical):
+        out.write(pickle.dumps((int(dist.num_cats),), protocol=2)[2:-1])      # the argument tuple
+        out.write(b"R.")                                                      # REDUCE, STOP
+        return out.getvalue()
     out.write(b")\x81")                                                       # EMPTY_TUPLE, NEWOBJ
-    out.write(pickle.dumps(state, protocol=2)[2:-1])                          # the dict (no PROTO / STOP)
+    out.write(pickle.dumps(_ref_state(dist), protocol=2)[2:-1])               # the dict (no PROTO / STOP)
     out.write(b"b.")                                                          # BUILD, STOP
     return out.getvalue()
 
 
 class _DistUnpickler(pickle.Unpickler):
     def find_class(self, module, name):
-        if name == "Categorical" and (module.startswith("pyjuice.nodes.distributions") or
-                                      module.startswith("pyjuice_b200.nodes.distributions")):
-            return Categorical
+        if name in _OUR_CLASS and (module.startswith(_REF_MODULE) or
+                                   module.startswith("pyjuice_b200.nodes.distributions")):
+            return _OUR_CLASS[name]
         raise pickle.UnpicklingError(f"distribution class {module}.{name} is not supported")
 
 
@@ -59,7 +83,10 @@ def _unpickle_dist(blob: bytes):
     dist = _DistUnpickler(io.BytesIO(blob)).load()
     for attr in ("post_fw_fns", "post_bp_fns", "sampling_fns"):
         dist.__dict__.pop(attr, None)
-    dist.num_cats = int(dist.num_cats)
+    if hasattr(dist, "num_cats"):
+        dist.num_cats = int(dist.num_cats)
+    if isinstance(dist, DiscreteLogistic):
+        dist.val_range = (float(dist.val_range[0]), float(dist.val_range[1]))
     return dist
 
 

@@ -27,6 +27,9 @@ the results of one forward / backward / ``mini_batch_em`` step:
 * ``io_tiny.npz``    ``.jpc`` files both ways: the bytes of the reference's file of the tiny
                     circuit, and the reference's parameters and log-likelihoods after loading
                     a file saved by pyjuice_b200;
+* ``io_dists.npz``  ``.jpc`` files both ways for the four-variable circuit over Bernoulli,
+                    Gaussian, DiscreteLogistic and SoftEvidenceCategorical inputs: the bytes of
+                    the reference's files, and what the reference loads from ours;
 * ``tdp_tiny.npz``   flows of the evidence-free pass (all variables missing) on the tiny
                     circuit: per sample, its top-down probabilities;
 * ``structures.npz`` compiled layouts, parameters and log-likelihoods of the reference's PD
@@ -346,6 +349,49 @@ def make_io_variants():
     np.savez_compressed(os.path.join(HERE, "io_tiny.npz"), **out)
 
 
+def make_io_dists():
+    """.jpc files both ways for circuits.build_dist_dag over each non-Categorical input
+    distribution: the reference saves its circuit (input parameters of dists.npz where it has
+    them; file bytes stored), and the reference loads the file pyjuice_b200 saved from the
+    same circuit and parameters (its parameters stored, and its FP32 log-likelihoods of the
+    dists.npz data for the three distributions that need no evidence)."""
+    import tempfile
+    from circuits import build_dist_dag
+    import pyjuice_b200 as mine
+    from pyjuice_b200.nodes import distributions as mdists
+    dfx = dict(np.load(os.path.join(HERE, "dists.npz")))
+    kinds = (("bern", "Bernoulli", {}), ("gauss", "Gaussian", {"mu": 0.0, "sigma": 1.0}),
+             ("dlog", "DiscreteLogistic", {"val_range": (-2.0, 2.0), "num_cats": 8}),
+             ("poe", "SoftEvidenceCategorical", {"num_cats": 6}))
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, cls, kw in kinds:
+            torch.manual_seed(11)
+            pc = juice.compile(build_dist_dag(juice, lambda: getattr(dists, cls)(**kw)), verbose=False)
+            if name + "_in_params0" in dfx:
+                with torch.no_grad():
+                    pc.params.copy_(torch.from_numpy(dfx[name + "_params0"]))
+                    pc.input_layer_group[0].params.copy_(torch.from_numpy(dfx[name + "_in_params0"]))
+            out[name + "_params"] = pc.params.detach().numpy().copy()
+            out[name + "_in_params"] = pc.input_layer_group[0].params.detach().numpy().copy()
+            juice.save(os.path.join(d, name + "_ref.jpc"), pc)
+            with open(os.path.join(d, name + "_ref.jpc"), "rb") as f:
+                out[name + "_ref_jpc"] = np.frombuffer(f.read(), dtype=np.uint8).copy()
+            torch.manual_seed(11)
+            mpc = mine.compile(build_dist_dag(mine, lambda: getattr(mdists, cls)(**kw)))
+            with torch.no_grad():
+                mpc.params.copy_(torch.from_numpy(out[name + "_params"]))
+                mpc.input_layer_group[0].params.copy_(torch.from_numpy(out[name + "_in_params"]))
+            mine.save(os.path.join(d, name + "_ours.jpc"), mpc)
+            rpc = juice.compile(juice.load(os.path.join(d, name + "_ours.jpc")), verbose=False)
+            out[name + "_ref_loads_ours_params"] = rpc.params.detach().numpy().copy()
+            out[name + "_ref_loads_ours_in_params"] = rpc.input_layer_group[0].params.detach().numpy().copy()
+            if name != "poe":
+                x = torch.from_numpy(dfx[name + "_x"])
+                out[name + "_ref_loads_ours_lls"] = rpc(x, force_use_fp32=True).detach().numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "io_dists.npz"), **out)
+
+
 def make_tdp_variants():
     """Flows of the evidence-free pass on the tiny circuit: every variable missing, root flow
     1 per sample (``pc(x, missing_mask=all)``, ``lls.mean().backward()``). Per sample these are
@@ -488,12 +534,12 @@ def make_samples(name: str):
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny", "structures", "dists"]
+    which = sys.argv[1:] or ["tiny", "hclt64", "hclt784", "samples_tiny", "samples_hclt64", "em_tiny", "alg_tiny", "query_tiny", "io_tiny", "tdp_tiny", "structures", "dists", "io_dists"]
     for w in which:
         t = time.time()
         {"tiny": make_tiny, "hclt64": make_hclt64, "hclt784": make_hclt784,
          "samples_tiny": lambda: make_samples("tiny"), "samples_hclt64": lambda: make_samples("hclt64"),
          "em_tiny": make_em_variants, "alg_tiny": make_alg_variants, "query_tiny": make_query_variants,
          "io_tiny": make_io_variants, "tdp_tiny": make_tdp_variants, "structures": make_structures,
-         "dists": make_dist_variants}[w]()
+         "dists": make_dist_variants, "io_dists": make_io_dists}[w]()
         print(w, "done in", round(time.time() - t, 1), "s", flush=True)

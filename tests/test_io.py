@@ -7,6 +7,7 @@ import os
 import tempfile
 
 import numpy as np
+import pytest
 import torch
 
 from conftest import load_fixture
@@ -58,3 +59,37 @@ def test_save_load_round_trip():
     juice.TensorCircuit._normalize_host(pc, ref)
     assert torch.allclose(pc2.params, ref, atol=1e-6)
     assert pc2.num_nodes == pc.num_nodes and pc2.num_edges == pc.num_edges
+
+
+@pytest.mark.parametrize("name,cls", [("bern", "Bernoulli"), ("gauss", "Gaussian"), ("dlog", "DiscreteLogistic"),
+                                      ("poe", "SoftEvidenceCategorical")])
+def test_distribution_files_both_ways(name, cls):
+    """.jpc files of circuits over Bernoulli, Gaussian, DiscreteLogistic and
+    SoftEvidenceCategorical inputs (io_dists.npz): the reference's file loads here with its
+    distribution class, attributes and parameters; the reference loaded the file saved here to
+    the same parameters and (dists.npz data) the log-likelihoods it computes for its own
+    circuit."""
+    io_fx = load_fixture("io_dists")
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "ref.jpc")
+        with open(path, "wb") as f:
+            f.write(io_fx[name + "_ref_jpc"].tobytes())
+        pc = juice.compile(juice.load(path))
+    layer = pc.input_layer_group[0]
+    dist = layer.nodes[0].dist
+    assert type(dist).__name__ == cls
+    if cls == "DiscreteLogistic":
+        assert dist.val_range == (-2.0, 2.0) and dist.num_cats == 8 and dist.min_std == 0.01
+    if cls == "Gaussian":
+        assert dist.mu == 0.0 and dist.sigma == 1.0 and dist.min_sigma == 0.01
+    if cls == "SoftEvidenceCategorical":
+        assert dist.num_cats == 6
+    ref_in = io_fx[name + "_in_params"]
+    assert np.array_equal(layer.params.numpy()[:ref_in.shape[0]], ref_in)
+    assert np.abs(pc.params.numpy() - io_fx[name + "_params"]).max() <= 1e-6
+    # the reference's view of our file
+    assert np.abs(io_fx[name + "_ref_loads_ours_params"] - io_fx[name + "_params"]).max() <= 1e-6
+    assert np.array_equal(io_fx[name + "_ref_loads_ours_in_params"], ref_in)
+    if name != "poe":
+        lls = load_fixture("dists")[name + "_lls"]
+        assert np.allclose(io_fx[name + "_ref_loads_ours_lls"], lls, rtol=1e-6, atol=1e-6)
