@@ -18,6 +18,7 @@ Differences that are deliberate:
 
 from __future__ import annotations
 
+import hashlib
 from functools import partial
 from typing import Callable, Optional, Sequence, Union
 
@@ -26,7 +27,7 @@ import torch
 import torch.nn as nn
 
 from .. import _native as nat
-from ..layer.layers import InputLayer, LayerGroup, ProdLayer, SumLayer, _mma, _num_sms
+from ..layer.layers import InputLayer, LayerGroup, ProdLayer, SumLayer, _ch_pack, _mma, _num_sms
 from ..nodes import CircuitNodes, multiply, summate
 
 
@@ -559,11 +560,77 @@ class TensorCircuit(nn.Module):
             pool.append(torch.cuda.Stream(device=main.device))
         return pool[i]
 
+    # Sum layers whose packed weights would be byte-identical (tied layers: the time steps of
+    # a homogeneous HMM) share one packed buffer, packed once per pass.
+    share_tied_packs = True
+
+    def _share_tied_packs(self):
+        """Point the packed-weight buffers of sum layers with identical packing inputs at one
+        buffer (once per device).
+
+        A packed tile is a function of the parameter values and of (rows, terms, the terms'
+        weight offsets kw[k_off ..], w_add, g_stride) and the layout (rows per block, weight
+        stride, format): two buffers whose tables agree in all of these hold the same bytes
+        whenever both are packed from the same parameters. Tables are compared per role
+        (forward tiles, forward 128-term chunks, element-flow tiles and chunks), so the layers
+        sharing a buffer also make the same kernel choices; the pack jobs then name the
+        buffer once (``_multi_pack`` drops repeated buffers)."""
+        key = (self.device.type, self.device.index)
+        done = self.__dict__.setdefault("_shared_packs_done", set())
+        if key in done or not TensorCircuit.share_tied_packs:
+            return
+        done.add(key)
+        canon = dict()
+
+        def content(tiles, kw):
+            t = tiles.cpu().numpy().astype(np.int64)
+            kwn = kw.cpu().numpy()
+            if t.shape[0] == 0:
+                return None
+            cnt = t[:, 3]
+            idx = np.arange(int(cnt.sum())) + np.repeat(t[:, 2] - (np.cumsum(cnt) - cnt), cnt)
+            h = hashlib.sha1(np.ascontiguousarray(t[:, [1, 3, 4, 6]]).tobytes())
+            h.update(kwn[idx].astype(np.int64).tobytes())
+            return (t.shape[0], h.hexdigest())
+
+        def share(role, holder, tab_key, pack_key, rpb, w_stride, kw, lazy):
+            tab = holder.get(tab_key)
+            if tab is None:
+                return
+            c = content(tab, kw)
+            if c is None:
+                return
+            k = (role, rpb, w_stride) + c
+            first = canon.get(k)
+            if first is None:
+                canon[k] = (holder, pack_key, lazy)
+                return
+            fh, fk, flazy = first
+            holder[pack_key] = _ch_pack(fh, fk) if flazy else fh[fk]
+
+        for group in self.inner_layer_groups:
+            if not group.is_sum():
+                continue
+            for layer in group:
+                d = layer._desc(self.device)
+                share("fw", d, "fw_tiles", "fw_pack", layer.block_size, 1, d["kw"], False)
+                share("fwch", d, "fw_ch", "fw_ch_pack", layer.block_size, 1, d["kw"], True)
+                for eg in d["el_groups"]:
+                    share("el", eg, "tiles", "pack", eg["cbs"], layer.block_size, eg["kw"], False)
+                    share("elch", eg, "ch", "ch_pack", eg["cbs"], layer.block_size, eg["kw"], True)
+
     def _multi_pack(self, jobs) -> bool:
         """All given weight packs (``SumLayer.forward_pack_job`` tuples) in one launch on the
-        current stream; returns whether anything was launched."""
+        current stream; returns whether anything was launched. A buffer named by several jobs
+        (shared by tied layers) is packed once."""
         if not jobs:
             return False
+        seen, uniq = set(), []
+        for j in jobs:
+            if (int(j[2].data_ptr()), int(j[5])) not in seen:
+                seen.add((int(j[2].data_ptr()), int(j[5])))
+                uniq.append(j)
+        jobs = uniq
         key = tuple((int(j[2].data_ptr()), int(j[5])) for j in jobs)  # packed buffer and format
         tab = self._pack_tables.get(key)
         if tab is None:
@@ -673,6 +740,7 @@ class TensorCircuit(nn.Module):
         main = torch.cuda.current_stream()
         side = self._side_stream(main)
         side.wait_stream(main)
+        self._share_tied_packs()
         B = self.node_mars.size(1)
         plain = propagation_alg == "LL" if isinstance(propagation_alg, str) else all(a == "LL" for a in propagation_alg)
         run = (self._level_run(B, force_use_bf16, force_use_fp32)
@@ -822,6 +890,7 @@ class TensorCircuit(nn.Module):
         for side in sides:
             side.wait_stream(main)
         B = self.node_mars.size(1)
+        self._share_tied_packs()
         # Element-flow weights: packed by the forward pass when the parameters have not changed
         # since (the state is set by the forward only, so that every run of a captured backward
         # makes the same choice); otherwise packed here in one launch.

@@ -492,3 +492,37 @@ def test_sampling_matches_reference_draws(name, cuda_device):
     wide = torch.zeros([pc.num_nodes, S + 13], dtype=torch.float32, device=cuda_device)
     wide[:, :S] = table
     assert np.array_equal(juice.queries.sample(pc, S, uniforms=wide).cpu().numpy(), sf["samples"])
+
+
+@pytest.mark.parametrize("H", [64, 256, 512])
+def test_shared_tied_packs_equal_separate(H, cuda_device):
+    """The time steps of a homogeneous HMM (tied transitions) share one packed-weight buffer
+    (short packed tiles at 64 hidden states, tcgen05 chunks of long tiles at 256 and 512),
+    packed once per pass: log-likelihoods, parameter flows and the EM update of two
+    split-bf16 steps are bit-identical to separate buffers packed per layer."""
+    from pyjuice_b200.model.tensorcircuit import TensorCircuit
+    saved = TensorCircuit.share_tied_packs
+    out = []
+    try:
+        for share in (False, True):
+            TensorCircuit.share_tied_packs = share
+            torch.manual_seed(0)
+            pc = juice.compile(juice.structures.HMM(8, H, 50, homogeneous=True)).to(cuda_device)
+            x = torch.randint(0, 50, (128, 8), generator=torch.Generator().manual_seed(1)).to(cuda_device)
+            res = []
+            for _ in range(2):
+                pc.init_param_flows(flows_memory=0.0)
+                lls = pc(x, force_use_bf16=True)
+                lls.mean().backward()
+                res += [lls.detach().clone(), pc.param_flows.clone()]
+                pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
+                res.append(pc.params.clone())
+            if share:
+                ptrs = [l._desc(pc.device)["fw_pack"].data_ptr() for g in pc.inner_layer_groups if g.is_sum()
+                        for l in g]
+                assert len(set(ptrs)) < len(ptrs)
+            out.append(res)
+    finally:
+        TensorCircuit.share_tied_packs = saved
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a, b)

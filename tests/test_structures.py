@@ -68,3 +68,20 @@ def test_discrete_logistic_layer_matches_reference_layout():
     meta = layer._host_desc()["node_meta"].numpy().reshape(-1, 4)
     assert meta.shape[0] == layer.num_nodes
     assert np.allclose(meta, np.array([-2.0, 2.0, 8.0, 0.01], np.float32))
+
+
+def test_tied_hmm_layers_share_packed_weights():
+    """Packed-weight buffers: the tied time steps of a homogeneous HMM share one (forward and
+    element-flow tables alike); an HMM without tied transitions shares none. CPU only (the
+    buffers are planned, not filled)."""
+    pc = juice.compile(juice.structures.HMM(6, 32, 10, homogeneous=True))
+    pc._share_tied_packs()
+    layers = [l for g in pc.inner_layer_groups if g.is_sum() for l in g]
+    fw = [l._desc(pc.device)["fw_pack"].data_ptr() for l in layers]
+    el = [l._desc(pc.device)["el_groups"][0]["pack"].data_ptr() for l in layers]
+    assert len(set(fw[:-1])) == 1 and len(set(el[:-1])) == 1  # the transitions; the last layer is the root
+    assert fw[-1] != fw[0]
+    pc = juice.compile(juice.structures.HMM(6, 32, 10, homogeneous=False))
+    pc._share_tied_packs()
+    fw = [l._desc(pc.device)["fw_pack"].data_ptr() for g in pc.inner_layer_groups if g.is_sum() for l in g]
+    assert len(set(fw)) == len(fw)
