@@ -498,11 +498,14 @@ def test_sampling_matches_reference_draws(name, cuda_device):
 def test_shared_tied_packs_equal_separate(H, cuda_device):
     """The time steps of a homogeneous HMM (tied transitions) share one packed-weight buffer
     (short packed tiles at 64 hidden states, tcgen05 chunks of long tiles at 256 and 512),
-    packed once per pass: log-likelihoods, parameter flows and the EM update of two
-    split-bf16 steps are bit-identical to separate buffers packed per layer."""
+    packed once per pass: log-likelihoods, sum-parameter flows and the sum EM update of two
+    split-bf16 steps are bit-identical to separate buffers packed per layer. (The tied
+    emission table's flows are summed with atomics, in no fixed order, so the emission
+    parameters after the first step are made equal before the second.)"""
     from pyjuice_b200.model.tensorcircuit import TensorCircuit
     saved = TensorCircuit.share_tied_packs
     out = []
+    q1 = None
     try:
         for share in (False, True):
             TensorCircuit.share_tied_packs = share
@@ -510,13 +513,20 @@ def test_shared_tied_packs_equal_separate(H, cuda_device):
             pc = juice.compile(juice.structures.HMM(8, H, 50, homogeneous=True)).to(cuda_device)
             x = torch.randint(0, 50, (128, 8), generator=torch.Generator().manual_seed(1)).to(cuda_device)
             res = []
-            for _ in range(2):
+            for step in range(2):
                 pc.init_param_flows(flows_memory=0.0)
                 lls = pc(x, force_use_bf16=True)
                 lls.mean().backward()
                 res += [lls.detach().clone(), pc.param_flows.clone()]
                 pc.mini_batch_em(step_size=0.1, pseudocount=0.1)
                 res.append(pc.params.clone())
+                if step == 0:
+                    q = pc.input_layer_group[0].params
+                    if q1 is None:
+                        q1 = q.clone()
+                    else:
+                        with torch.no_grad():
+                            q.copy_(q1)
             if share:
                 ptrs = [l._desc(pc.device)["fw_pack"].data_ptr() for g in pc.inner_layer_groups if g.is_sum()
                         for l in g]
