@@ -125,6 +125,52 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
     }
 }
 
+// Forward of tiles of one row (sum layers of block size 1, e.g. a root over thousands of
+// children): out[row, b] = log sum_k w_k exp(src[krow[k], b]). Lane = sample (32 consecutive
+// samples per CTA, coalesced rows), warp = every 8th term; each thread keeps an online
+// (max, scaled sum) over its terms, and the 8 warps' pairs are combined through shared
+// memory. Weight of term k: params[kw[k_off + k] + w_add].
+constexpr int kRowWarps = 8;
+
+__global__ void __launch_bounds__(32 * kRowWarps)
+lse_row_kernel(const float* __restrict__ src, float* __restrict__ out, int64_t ld, int B,
+               const float* __restrict__ params, const PcbLseTile* __restrict__ tiles, const int* __restrict__ krow,
+               const int* __restrict__ kw) {
+    pcb::pdl_begin();
+    __shared__ float sM[kRowWarps][32], sS[kRowWarps][32];
+    const PcbLseTile t = tiles[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = blockIdx.y * 32 + lane;
+    float m = -INFINITY, sum = 0.f;
+    if (b < B) {
+#pragma unroll 4
+        for (int k = warp; k < t.k_cnt; k += kRowWarps) {
+            const float e = __ldg(src + (int64_t)__ldg(krow + t.k_off + k) * ld + b);
+            const float w = __ldg(params + (int64_t)__ldg(kw + t.k_off + k) + t.w_add);
+            if (e == -INFINITY) continue;
+            if (e > m) {
+                sum = sum * expf(m - e) + w;
+                m = e;
+            } else {
+                sum = fmaf(w, expf(e - m), sum);
+            }
+        }
+    }
+    sM[warp][lane] = m;
+    sS[warp][lane] = sum;
+    __syncthreads();
+    if (warp == 0 && b < B && t.n_rows > 0) {
+        float mm = -INFINITY;
+#pragma unroll
+        for (int w = 0; w < kRowWarps; ++w) mm = fmaxf(mm, sM[w][lane]);
+        float ss = 0.f;
+#pragma unroll
+        for (int w = 0; w < kRowWarps; ++w)
+            if (sM[w][lane] != -INFINITY) ss = fmaf(sS[w][lane], expf(sM[w][lane] - mm), ss);
+        out[(int64_t)t.out_row * ld + b] = mm == -INFINITY ? -INFINITY : logf(ss) + mm;
+    }
+}
+
 template <int TM, int TB, int RN, int MODE>
 int launch_mode(dim3 grid, const float* src, const float* src2, const float* aux, float* out, int64_t ld, int B,
                 const float* params, const PcbLseTile* tiles, const int* krow, const int* kw, int w_stride,
@@ -187,6 +233,12 @@ extern "C" int pcb_lse_contract(const float* src, const float* src2, const float
                                      w_stride, mode, prec == 2, s);
     }
     if (prec != 0) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: prec must be 0, 1 or 2");
+    if (tile_rows == 1 && mode == 0) {
+        const dim3 grid((unsigned)num_tiles, (unsigned)pcb::cdiv(B, 32));
+        if (grid.y > 65535) return pcb::set_error(PCB_E_ARG, "pcb_lse_contract: batch too large");
+        return pcb::launch_status(pcb::launch_k(lse_row_kernel, grid, dim3(32 * kRowWarps), 0, s, 1u, src, out, ld,
+                                                B, params, tiles, krow, kw), "pcb_lse_contract");
+    }
     const bool vec = pcb::vec_ok(src, ld) && pcb::vec_ok(out, ld) && (!aux || pcb::vec_ok(aux, ld)) &&
                      (!src2 || pcb::vec_ok(src2, ld));
 #define PCB_LSE(TM, TB, RN) launch_cfg<TM, TB, RN>(src, src2, aux, out, ld, B, params, tiles, num_tiles, krow, kw, w_stride, rpb_log2, mode, s, vec)

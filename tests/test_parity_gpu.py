@@ -478,3 +478,25 @@ def test_bernoulli_and_gaussian_layers_match_reference(name, cuda_device):
     assert np.abs(pc.params.cpu().numpy() - g("params1")).max() <= 1e-5
     q1 = g("in_params1")
     assert np.abs(pc.input_layer_group[0].params.cpu().numpy()[:q1.shape[0]] - q1).max() <= 1e-4 * max(1.0, np.abs(q1).max())
+
+
+@pytest.mark.parametrize("K,B", [(4096, 64), (4096, 200), (37, 70)])
+def test_one_row_sum_forward_vs_oracle(K, B, cuda_device):
+    """A block-size-1 sum node over K product children (the one-row FP32 forward kernel: lanes
+    over samples, warps over terms, online log-sum-exp): log-likelihoods against the FP64
+    oracle, ragged batch, children with -inf values (zero input probabilities) included."""
+    torch.manual_seed(5)
+    n0 = juice.inputs(0, num_nodes=K, dist=juice.distributions.Categorical(num_cats=4))
+    n1 = juice.inputs(1, num_nodes=K, dist=juice.distributions.Categorical(num_cats=4))
+    root = juice.summate(juice.multiply(n0, n1), num_nodes=1)
+    pc = juice.compile(root)
+    with torch.no_grad():
+        q = pc.input_layer_group[0].params
+        q[: 4 * K: 7] = 0.0  # some categories impossible for some nodes
+    pc = pc.to(cuda_device)
+    x = np.random.default_rng(2).integers(0, 4, size=(B, 2))
+    lls = pc(torch.from_numpy(x).to(cuda_device), force_use_fp32=True).detach().double().cpu().numpy()
+    lay = orc.layout_from_circuit(pc)
+    _, _, ref = orc.forward(lay, pc.params.double().cpu().numpy(),
+                            pc.input_layer_group[0].params.double().cpu().numpy(), x)
+    assert np.all(np.abs(lls - ref) <= 1e-5 * np.abs(ref) + 1e-5)
