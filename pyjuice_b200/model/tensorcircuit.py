@@ -663,6 +663,9 @@ class TensorCircuit(nn.Module):
     # EM step took 2.65 ms with it against 2.42 ms with the per-level launches, whose
     # programmatic dependent launches already hide most of the launch gaps.
     fuse_levels_forward = False
+    # CTAs of that launch (0: four per SM). The run's levels hold a few dozen work items each,
+    # so fewer CTAs leave SMs to the side-stream weight packs that overlap it.
+    levels_forward_ctas = 0
 
     def _level_run(self, B, force_use_bf16, force_use_fp32):
         """Sum group indices of the longest run of consecutive small levels that the
@@ -774,7 +777,8 @@ class TensorCircuit(nn.Module):
                     nat.call("pcb_lse_levels_short", nat.ptr(self.node_mars), self.node_mars.stride(0), B,
                              nat.ptr(self.params), nat.ptr(lt["tiles"]), nat.ptr(lt["krow"]), nat.ptr(lt["kw"]),
                              nat.ptr(lt["tch"]), nat.ptr(lt["levels"]), lt["num_levels"], lt["items"], lt["slices"],
-                             nat.ptr(lt["counters"]), lt["prec"], lt["tb"], 0, 4 * _num_sms(), nat.stream())
+                             nat.ptr(lt["counters"]), lt["prec"], lt["tb"], 0,
+                             TensorCircuit.levels_forward_ctas or 4 * _num_sms(), nat.stream())
                 continue
             if group.is_prod():
                 fused = (not self._fw_partial_eval_enabled and gi + 1 < len(groups) and
