@@ -434,6 +434,16 @@ int pcb_lse_contract_tc05_accum(const float* src, const float* src2, const float
                                 int32_t slices_per_cta, void* stream);
 
 /*
+ * Combine of long tiles contracted as chunks in one launch: every 128-term chunk j of the
+ * tile holding output row dst_rows[r] wrote its partial result to row j * num_rows + r of
+ * partials (pcb_lse_contract_tc05 on a table whose out_row fields point there);
+ * out[dst_rows[r], b] = log sum_j exp(partial) (mode 0) or sum_j partial (modes 1/2), over
+ * j < chunks_per_row[r], in that order.
+ */
+int pcb_chunk_combine(const float* partials, int64_t ld, int32_t B, int32_t num_rows, const int32_t* dst_rows,
+                      const int32_t* chunks_per_row, float* out, int32_t mode, void* stream);
+
+/*
  * pcb_lse_contract_tc05 as a persistent, warp-specialised kernel: num_ctas CTAs (0: one
  * per SM) each own a contiguous run of (tile, batch_tile-sample slice) work units. One warp
  * stages a unit's source rows in shared memory with 2-D TMA loads (a box of 32 samples x

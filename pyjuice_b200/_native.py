@@ -180,6 +180,8 @@ _SIGS = {
                               c_uint64, c_void_p], c_int32),
     "pcb_sample_input_dist": ([c_int32, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p,
                                c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_void_p], c_int32),
+    "pcb_chunk_combine": ([c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_void_p],
+                          c_int32),
     "pcb_sample_circuit_noalloc": ([c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p, c_int64, c_uint64,
                                     c_void_p, c_void_p], c_int32),
 }

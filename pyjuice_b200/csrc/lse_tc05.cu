@@ -1286,6 +1286,51 @@ extern "C" int pcb_lse_contract_tc05_accum(const float* src, const float* src2, 
                       slices_per_cta, stream, true);
 }
 
+namespace {
+
+// Long tiles as 128-term chunks contracted in one launch into partial rows, then combined:
+// out[dst_rows[r], b] = log sum_j exp(part[j S + r, b]) (mode 0) or sum_j part[j S + r, b]
+// (modes 1/2), j < nch[r], in a fixed order. One thread per (row, sample), samples fastest.
+__global__ void __launch_bounds__(256)
+chunk_combine_kernel(const float* __restrict__ part, int64_t ld, int B, int S, const int* __restrict__ dst_rows,
+                     const int* __restrict__ nch, float* __restrict__ out, int mode) {
+    pcb::pdl_begin();
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)S * B) return;
+    const int r = (int)(i / B), b = (int)(i % B);
+    const int n = nch[r];
+    const float* p = part + (int64_t)r * ld + b;
+    const int64_t js = (int64_t)S * ld;
+    float res;
+    if (mode == 0) {
+        float m = -INFINITY;
+        for (int j = 0; j < n; ++j) m = fmaxf(m, p[j * js]);
+        float sum = 0.f;
+        if (m != -INFINITY)
+            for (int j = 0; j < n; ++j) sum += expf(p[j * js] - m);
+        res = m == -INFINITY ? -INFINITY : m + logf(sum);
+    } else {
+        res = 0.f;
+        for (int j = 0; j < n; ++j) res += p[j * js];
+    }
+    out[(int64_t)dst_rows[r] * ld + b] = res;
+}
+
+}  // namespace
+
+extern "C" int pcb_chunk_combine(const float* partials, int64_t ld, int32_t B, int32_t num_rows,
+                                 const int32_t* dst_rows, const int32_t* chunks_per_row, float* out, int32_t mode,
+                                 void* stream) {
+    if (!partials || !dst_rows || !chunks_per_row || !out || B <= 0 || ld < B || num_rows < 0 || mode < 0 || mode > 2)
+        return pcb::set_error(PCB_E_ARG, "pcb_chunk_combine: bad arguments");
+    if (num_rows == 0) return PCB_OK;
+    const int64_t total = (int64_t)num_rows * B;
+    return pcb::launch_status(pcb::launch_k(chunk_combine_kernel, dim3((unsigned)pcb::cdiv(total, 256)), dim3(256), 0,
+                                            pcb::as_stream(stream), 1u, partials, ld, (int)B, (int)num_rows, dst_rows,
+                                            chunks_per_row, out, (int)mode),
+                              "pcb_chunk_combine");
+}
+
 extern "C" int pcb_lse_contract_tc05_ws(const float* src, const float* src2, const float* aux, float* out,
                                         int64_t ld, int32_t B, int64_t src_rows, int64_t out_rows, const uint8_t* packed,
                                         const PcbLseTile* tiles, int32_t num_tiles, const int32_t* krow, int32_t mode,

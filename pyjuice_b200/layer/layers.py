@@ -128,10 +128,59 @@ def _ch_pack(holder: dict, key: str) -> torch.Tensor:
     return holder[key]
 
 
-def _tc05_chunks(src, src2, aux, out, ld, B, pack, table, ranges, krow, mode, prec, stream):
-    """A contraction over tiles of any length on the tcgen05 kernels: the first chunk of 128
-    terms overwrites the output, every later chunk combines into it
-    (pcb_lse_contract_tc05_accum: log-add-exp for the forward, sum for element flows)."""
+def _chunk_plan(table: torch.Tensor, ranges):
+    """The chunk table with each tile's output rows moved into a partials buffer (chunk j's
+    rows at j * S + the row's index among the S output rows), the output row and the number
+    of chunks of each of those S rows (for pcb_chunk_combine)."""
+    t = table.cpu().numpy().astype(np.int64).copy()
+    n = t[:, 1]
+    rows_all = np.arange(int(n.sum())) + np.repeat(t[:, 0] - (np.cumsum(n) - n), n)
+    rows = np.unique(rows_all)
+    S = rows.shape[0]
+    nch = np.zeros(S, np.int64)
+    for j, (a, c) in enumerate(ranges):
+        first = np.searchsorted(rows, t[a:a + c, 0])
+        cover = np.arange(int(n[a:a + c].sum())) + np.repeat(first - (np.cumsum(n[a:a + c]) - n[a:a + c]), n[a:a + c])
+        nch[cover] = j + 1
+        t[a:a + c, 0] = j * S + first
+    dev = table.device
+    return dict(table=_i32(t).to(dev), dst=_i32(rows).to(dev), nch=_i32(nch).to(dev), S=S, nchunks=len(ranges))
+
+
+_CHUNK_SCRATCH = dict()  # device -> FP32 partials buffer shared by the long-tile contractions
+
+
+def _chunk_scratch(device, rows: int, ld: int) -> torch.Tensor:
+    """A [rows, ld] view of the device's partials buffer (grown when too small). The
+    contractions that use it run one after another on the pass's stream."""
+    key = (device.type, device.index)
+    buf = _CHUNK_SCRATCH.get(key)
+    if buf is None or buf.numel() < rows * ld:
+        buf = torch.empty([rows * ld], dtype=torch.float32, device=device)
+        _CHUNK_SCRATCH[key] = buf
+    return buf[:rows * ld].view(rows, ld)
+
+
+def _tc05_chunks(src, src2, aux, out, ld, B, pack, table, ranges, krow, mode, prec, stream, holder=None,
+                 plan_key=None):
+    """A contraction over tiles of any length on the tcgen05 kernels, in 128-term chunks.
+
+    With ``SumLayer.chunk_partials`` (and a ``holder`` dict to cache the plan in): every chunk
+    of every tile in one launch, each writing its partial result to its own rows of a shared
+    buffer, then pcb_chunk_combine (log-sum-exp for the forward, sum for element flows) into
+    the output; a layer of long tiles thus fills the GPU with all its chunks at once.
+    Otherwise: one launch per chunk index, the first overwriting the output and every later
+    one combining into it (pcb_lse_contract_tc05_accum)."""
+    if SumLayer.chunk_partials and holder is not None:
+        plan = holder.get(plan_key)
+        if plan is None:
+            plan = _chunk_plan(table, ranges)
+            holder[plan_key] = plan
+        part = _chunk_scratch(out.device, plan["S"] * plan["nchunks"], ld)
+        _tc05_call(src, src2, aux, part, ld, B, pack, plan["table"], krow, mode, prec, stream)
+        nat.call("pcb_chunk_combine", nat.ptr(part), ld, B, plan["S"], nat.ptr(plan["dst"]), nat.ptr(plan["nch"]),
+                 nat.ptr(out), mode, stream)
+        return
     for j, (a, n) in enumerate(ranges):
         t = table[a:a + n]
         pk = pack[a * _PACK_BYTES:(a + n) * _PACK_BYTES]
@@ -387,6 +436,7 @@ class SumLayer(Layer):
     tc05_slices_per_cta = None  # sample slices per tcgen05 CTA (None: one)
     tc05_ws = None        # persistent warp-specialised tcgen05 kernel: None autotuned, True forced, False off
     tc05_long = True      # tiles of more than 128 terms as accumulating tcgen05 chunks (BF16 / E4M3 forms)
+    chunk_partials = True  # all chunks of a layer in one launch into partial rows, then pcb_chunk_combine
     # The single-stage kernels of small layers read pre-packed weights too (the circuit packs
     # all layers' weights in one launch per pass, so the kernels skip their own conversion).
     pack_short_weights = True
@@ -723,7 +773,7 @@ class SumLayer(Layer):
             if not _weights_packed:
                 self.pack_forward_weights(params, B, force_use_bf16, force_use_fp32)
             _tc05_chunks(element_mars, None, None, node_mars, ld, B, _ch_pack(d, "fw_ch_pack"), d["fw_ch"], d["fw_ch_ranges"],
-                         d["krow"], 0, prec, st)
+                         d["krow"], 0, prec, st, holder=d, plan_key="fw_ch_plan")
             return
         prec = _mma(prec)
         # _fuse_fw = (term_children, element values out): the product layer below is fused in
@@ -805,7 +855,7 @@ class SumLayer(Layer):
             if self._el_long(eg, prec):
                 _tc05_chunks(node_flows, None if allow_modify_flows else node_mars, element_mars, element_flows, ld,
                              B, _ch_pack(eg, "ch_pack"), eg["ch"], eg["ch_ranges"], eg["krow"], 1 if allow_modify_flows else 2,
-                             prec, nat.stream())
+                             prec, nat.stream(), holder=eg, plan_key="ch_plan")
                 continue
             prec = _mma(prec)
             if eg["short"] and SumLayer.short_kernels:

@@ -256,9 +256,11 @@ def _long_problem(B, device, seed):
 
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("prec", [2, 3])
-def test_long_tiles_as_tc05_chunks_vs_fp64(mode, prec, cuda_device):
-    """Tiles of up to 400 terms contracted as accumulating 128-term chunks on the tcgen05
-    kernel (first chunk overwrites, later chunks log-add / add) against FP64: split bf16
+@pytest.mark.parametrize("partials", [False, True])
+def test_long_tiles_as_tc05_chunks_vs_fp64(mode, prec, partials, cuda_device):
+    """Tiles of up to 400 terms contracted as 128-term chunks on the tcgen05 kernel against
+    FP64: one launch per chunk index (first chunk overwrites, later chunks log-add / add), or
+    every chunk in one launch into partial rows combined by pcb_chunk_combine. Split bf16
     within 1e-4, E4M3 within the bounds of its single-chunk test."""
     from pyjuice_b200.layer.layers import _chunk_table, _tc05_chunks
     p = _long_problem(256, cuda_device, seed=60 + mode + 3 * prec)
@@ -270,7 +272,7 @@ def test_long_tiles_as_tc05_chunks_vs_fp64(mode, prec, cuda_device):
     src = p["flows"] if mode == 2 else p["src"]
     out = torch.full([p["T"] * 128, p["B"]], 12345.0, device=cuda_device)
     _tc05_chunks(src, p["src"] if mode == 2 else None, p["aux"] if mode else None, out, p["B"], p["B"], pack, ct,
-                 ranges, p["krow"], mode, prec, nat.stream())
+                 ranges, p["krow"], mode, prec, nat.stream(), holder=dict() if partials else None, plan_key="plan")
     torch.cuda.synchronize()
     assert nat.device_status(clear=True) == 0
     got = out.double().cpu()
