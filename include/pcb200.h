@@ -264,7 +264,7 @@ int pcb_prod_gather_sum_modify(const float* in, float* out, int64_t ld, int32_t 
  * mode 1 (element flows):  out[out_row + r, b] = acc * exp(aux[aux_row + r, b] + m_b)
  * mode 2 (element flows, unmodified node flows): as mode 1 with src = log(src) - src2.
  * FP32 forward of one-row tiles (tile_rows 1, mode 0: sum layers of block size 1): lanes over
- * 32 samples, 8 warps over the terms, online log-sum-exp, for roots over thousands of
+ * 32 samples, 32 warps over the terms, online log-sum-exp, for roots over thousands of
  * children.
  * Replaces SumLayer._fw_triton_block_sparse_*_kernel, _fw_triton_sparse_kernel,
  * _fw_triton_large_sparse_kernel (src/pyjuice/layer/sum_layer.py:454-1104) and

@@ -96,6 +96,8 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
     int* perm = keys + CB;         // [CB]
     float* rows = reinterpret_cast<float*>(perm + CB);  // [warps][CB]
     int* seg = perm + CB + (blockDim.x >> 5) * CB;      // [K + 3]: categories, dropped, missing
+    int* ucat = seg + K + 3;                            // [CB]: the categories present in the chunk
+    __shared__ int sU;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -152,7 +154,24 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
             }
         }
         __syncthreads();
-        // seg[k] now holds the end of category k; its start is the end of category k-1.
+        // seg[k] now holds the end of category k; its start is the end of category k-1. The
+        // categories that occur in this chunk, in order (at most one per sample): without
+        // missing values only their slots change, so the nodes' loops run over them instead
+        // of all K categories (a vocabulary of thousands against a batch of tens).
+        if (warp == 0) {
+            int nu = 0;
+            for (int base = 0; base < K; base += 32) {
+                const int k = base + lane;
+                const bool present = k < K && seg[k] > (k == 0 ? 0 : seg[k - 1]);
+                const unsigned bal = __ballot_sync(0xffffffffu, present);
+                if (present) ucat[nu + __popc(bal & ((1u << lane) - 1u))] = k;
+                nu += __popc(bal);
+            }
+            if (lane == 0) sU = nu;
+        }
+        __syncthreads();
+        const bool dense = seg[K + 1] > seg[K];  // missing samples: every category gets flow
+        const int L = dense ? K : sU;
         float* wrow = rows + warp * CB;
         const bool vec4 = ((ld & 3) == 0) && ((c0 & 3) == 0) && ((reinterpret_cast<uintptr_t>(nf) & 15) == 0);
         for (int n = warp; n < cnt; n += (blockDim.x >> 5)) {
@@ -177,20 +196,22 @@ input_cat_bwd_kernel(const int64_t* __restrict__ data, int64_t data_ld, const fl
                 for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
             }
             const int64_t sp = miss ? s_pids[node0 + n] : 0;
-            // categories lane, lane + 32, ...: the slots' old values are loaded for a batch of
-            // kR categories at once (one round trip), then summed and stored
+            // list entries lane, lane + 32, ... (all categories, or the present ones): the
+            // slots' old values are loaded for a batch of kR entries at once (one round trip),
+            // then summed and stored
             constexpr int kR = 8;
-            for (int k0 = 0; k0 < K; k0 += 32 * kR) {
+            for (int k0 = 0; k0 < L; k0 += 32 * kR) {
                 float old[kR];
 #pragma unroll
                 for (int j = 0; j < kR; ++j) {
-                    const int k = k0 + lane + 32 * j;
-                    old[j] = (k < K && !atomic) ? pf[sf + k] : 0.f;
+                    const int idx = k0 + lane + 32 * j;
+                    old[j] = (idx < L && !atomic) ? pf[sf + (dense ? idx : ucat[idx])] : 0.f;
                 }
 #pragma unroll
                 for (int j = 0; j < kR; ++j) {
-                    const int k = k0 + lane + 32 * j;
-                    if (k >= K) continue;
+                    const int idx = k0 + lane + 32 * j;
+                    if (idx >= L) continue;
+                    const int k = dense ? idx : ucat[idx];
                     const int s = (k == 0) ? 0 : seg[k - 1];
                     const int e = seg[k];
                     if (e == s && msum == 0.f) continue;
@@ -240,7 +261,7 @@ extern "C" int pcb_input_cat_bwd(const int64_t* data, int64_t data_ld, const flo
         return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: bad arguments");
     if (num_groups == 0) return PCB_OK;
     const int CB = B < 1024 ? B : 1024;
-    const size_t smem = (size_t)(2 * CB + 8 * CB + max_ncats + 3) * sizeof(int);
+    const size_t smem = (size_t)(2 * CB + 8 * CB + max_ncats + 3 + CB) * sizeof(int);
     if (smem > 200 * 1024) return pcb::set_error(PCB_E_ARG, "pcb_input_cat_bwd: too many categories (%d)", max_ncats);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(input_cat_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -127,10 +127,10 @@ lse_f32_kernel(const float* __restrict__ src, const float* __restrict__ src2, co
 
 // Forward of tiles of one row (sum layers of block size 1, e.g. a root over thousands of
 // children): out[row, b] = log sum_k w_k exp(src[krow[k], b]). Lane = sample (32 consecutive
-// samples per CTA, coalesced rows), warp = every 8th term; each thread keeps an online
-// (max, scaled sum) over its terms, and the 8 warps' pairs are combined through shared
+// samples per CTA, coalesced rows), warp = every 32nd term; each thread keeps an online
+// (max, scaled sum) over its terms, and the 32 warps' pairs are combined through shared
 // memory. Weight of term k: params[kw[k_off + k] + w_add].
-constexpr int kRowWarps = 8;
+constexpr int kRowWarps = 32;
 
 __global__ void __launch_bounds__(32 * kRowWarps)
 lse_row_kernel(const float* __restrict__ src, float* __restrict__ out, int64_t ld, int B,
