@@ -151,12 +151,19 @@ _CHUNK_SCRATCH = dict()  # device -> FP32 partials buffer shared by the long-til
 _CHUNK_SCRATCH_MAX_BYTES = 1 << 30
 
 
+_CHUNK_SCRATCH_RETIRED = []  # smaller buffers replaced by a larger one: CUDA graphs captured earlier still write them
+
+
 def _chunk_scratch(device, rows: int, ld: int) -> torch.Tensor:
-    """A [rows, ld] view of the device's partials buffer (grown when too small). The
-    contractions that use it run one after another on the pass's stream."""
+    """A [rows, ld] view of the device's partials buffer (grown when too small; a replaced
+    buffer is kept alive, since a CUDA graph captured with it still uses its address). The
+    contractions that use it run one after another on the pass's stream; passes of
+    different circuits on concurrent streams would share it."""
     key = (device.type, device.index)
     buf = _CHUNK_SCRATCH.get(key)
     if buf is None or buf.numel() < rows * ld:
+        if buf is not None:
+            _CHUNK_SCRATCH_RETIRED.append(buf)
         buf = torch.empty([rows * ld], dtype=torch.float32, device=device)
         _CHUNK_SCRATCH[key] = buf
     return buf[:rows * ld].view(rows, ld)
