@@ -42,3 +42,30 @@ def test_hclt64_layers_have_block_runs():
             d = layer._host_desc()
             if layer.block_size >= 8 and d["fw_tiles"].size(0) >= SumLayer.tc05_min_tiles:
                 assert d["fw_run"] in (8, 32)
+
+
+def test_chunk_plan_remaps_rows_into_partials():
+    """The plan of the one-launch long-tile contraction: chunk j of a tile writes its rows at
+    j * S + (the rows' index among the S output rows); every output row has as many chunks as
+    its tile (at most 128 terms each), all of them written. CPU only."""
+    import torch
+    from pyjuice_b200.layer.layers import _chunk_plan, _chunk_table
+    tiles = np.array([[0, 128, 0, 300, 0, 0, 32, 0], [128, 64, 300, 129, 0, 128, 32, 0],
+                      [300, 5, 429, 40, 0, 300, 32, 0]], np.int64)
+    tab, ranges = _chunk_table(tiles)
+    plan = _chunk_plan(torch.from_numpy(tab).int(), ranges)
+    S = plan["S"]
+    assert S == 128 + 64 + 5 and plan["nchunks"] == 3
+    dst = plan["dst"].numpy()
+    assert np.array_equal(dst, np.concatenate([np.arange(0, 192), np.arange(300, 305)]))
+    nch = plan["nch"].numpy()
+    assert np.array_equal(nch, np.concatenate([np.full(128, 3), np.full(64, 2), np.full(5, 1)]))
+    t = plan["table"].numpy()
+    written = set()
+    for j, (a, n) in enumerate(ranges):
+        for row in t[a:a + n]:
+            for r in range(int(row[0]), int(row[0]) + int(row[1])):
+                assert r // S == j
+                written.add(r)
+    expect = {j * S + r for r in range(S) for j in range(int(nch[r]))}
+    assert written == expect
