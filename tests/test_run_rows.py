@@ -1,6 +1,7 @@
-"""Host-side run detection for the TMA-staged tcgen05 contraction: a tile table qualifies
-for boxes of r rows when every tile's terms come in runs of r consecutive source rows
-(the last run of a tile may be shorter)."""
+"""Host-side tile planning for the tcgen05 contractions: run detection for the TMA-staged
+kernel (a tile table qualifies for boxes of r rows when every tile's terms come in runs of r
+consecutive source rows; the last run of a tile may be shorter), and the partial-row plan of
+the one-launch long-tile contraction."""
 
 import numpy as np
 
