@@ -543,6 +543,19 @@ int pcb_sum_pflows_tc05(const float* node_flows, const float* node_mars, const f
                         void* stream);
 
 /*
+ * pcb_sum_pflows_tc05 over a tied set of sum layers (the time steps of a homogeneous HMM):
+ * layers that share the tiles' parameters and flow slots, layer i's node rows and child
+ * rows being the tiles' (tiles[].nid, cids[]) shifted by row_deltas[2 i] and
+ * row_deltas[2 i + 1]. All num_layers layers' samples accumulate into one tensor-memory
+ * tile per CTA and the flow slots are updated once, instead of once per layer.
+ */
+int pcb_sum_pflows_tc05_tied(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld,
+                             int32_t B, const float* params, float* param_flows, const PcbPflowTile* tiles,
+                             int32_t num_tiles, int32_t rows_per_block, const int32_t* cids, const int32_t* pids,
+                             const int32_t* pfids, int32_t modified, int32_t atomic, int32_t tile_children,
+                             int32_t prec, const int32_t* row_deltas, int32_t num_layers, void* stream);
+
+/*
  * Sum-parameter EM update, per node block (FP64 normalisation):
  *   for node i < bs, child k < nch:   p = params[pbase + k * bs + i], f = pflows[pfbase + k * bs + i]
  *   theta' = (1 - s) * p + s * (f + pc / nch) / (sum_k f + pc)

@@ -148,6 +148,9 @@ _SIGS = {
     "pcb_sum_pflows_tc05": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                              c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_void_p],
                             c_int32),
+    "pcb_sum_pflows_tc05_tied": ([c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p,
+                                  c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
+                                  c_void_p, c_int32, c_void_p], c_int32),
     "pcb_sum_em": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double, c_double, c_int32,
                     c_void_p], c_int32),
     "pcb_sum_em_f64flows": ([c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,

@@ -74,7 +74,7 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
                        int64_t ld, int B, const float* __restrict__ params, float* __restrict__ pf,
                        const PcbPflowTile* __restrict__ tiles, int rpb_log2, const int* __restrict__ cids,
                        const int* __restrict__ pids, const int* __restrict__ pfids, int slice, bool vec,
-                       int32_t* __restrict__ status) {
+                       const int* __restrict__ deltas, int nlay, int32_t* __restrict__ status) {
     pcb::pdl_trigger();
     using P = Plan<TKC, MODIFIED>;
     static_assert(TKC == 64 || TKC == 128, "children per tile");
@@ -120,9 +120,17 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
 
     const int bs0 = crank * slice;
     const int bs1 = min(B, bs0 + slice);
-    const int nch = bs1 > bs0 ? (bs1 - bs0 + KB - 1) / KB : 0;
+    // chunks of this CTA's batch slice, for each of the nlay layers that share the tile's
+    // parameters and flow slots (a tied set; layer i's node rows and child rows are the
+    // tile's shifted by deltas[2 i] and deltas[2 i + 1]): all accumulate into D
+    const int nchl = bs1 > bs0 ? (bs1 - bs0 + KB - 1) / KB : 0;
+    const int nch = nchl * nlay;
 
-    auto issue = [&](int b0, int st) {
+    auto issue = [&](int cidx, int st) {
+        const int li = nchl > 0 ? cidx / nchl : 0;
+        const int b0 = bs0 + (cidx - li * nchl) * KB;
+        const int dn = deltas ? __ldg(deltas + 2 * li) : 0;
+        const int de = deltas ? __ldg(deltas + 2 * li + 1) : 0;
         float* stage = dsm + st * P::kStage;
         constexpr int NX = KB / 4;
 #pragma unroll
@@ -135,7 +143,7 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
             for (int h = 0; h < (MODIFIED ? 1 : 2); ++h) {
                 float* d = stage + (h == 0 ? P::sA : P::sA2) + r * RS + c4;
                 if (r < t.n_rows) {
-                    const float* g = (h == 0 ? nf : nm) + ((int64_t)t.nid + r) * ld + b;
+                    const float* g = (h == 0 ? nf : nm) + ((int64_t)t.nid + dn + r) * ld + b;
                     if (vec && b + 3 < bs1) {
                         pcb::cp_async16(d, g);
                     } else {
@@ -160,7 +168,7 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
             float* d = stage + P::sC + k * RS + c4;
             const int row = sCid[k];
             if (row >= 0) {
-                const float* g = em + (int64_t)row * ld + b;
+                const float* g = em + (int64_t)(row + de) * ld + b;
                 if (vec && b + 3 < bs1) {
                     pcb::cp_async16(d, g);
                 } else {
@@ -195,11 +203,11 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
     };
 
     bool fail = false;
-    if (nch > 0) issue(bs0, 0);
+    if (nch > 0) issue(0, 0);
     for (int c = 0; c < nch; ++c) {
         const int st = c & 1;
         if (c + 1 < nch) {
-            issue(bs0 + (c + 1) * KB, st ^ 1);
+            issue(c + 1, st ^ 1);
             pcb::cp_async_wait<1>();
         } else {
             pcb::cp_async_wait<0>();
@@ -343,7 +351,7 @@ sum_pflows_tc05_kernel(const float* __restrict__ nf, const float* __restrict__ n
 template <int TKC, bool MODIFIED, bool ATOMIC, bool SPLIT>
 int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld, int B, const float* params,
            float* pf, const PcbPflowTile* tiles, int num_tiles, int rpb_log2, const int* cids, const int* pids,
-           const int* pfids, cudaStream_t s, bool vec) {
+           const int* pfids, cudaStream_t s, bool vec, const int* deltas, int nlay) {
     const int slice = (int)pcb::cdiv(pcb::cdiv(B, cs), KB) * KB;
     using P = Plan<TKC, MODIFIED>;
     constexpr size_t smem = P::bytes();
@@ -361,16 +369,18 @@ int launch(int cs, const float* nf, const float* nm, const float* em, int64_t ld
     return pcb::launch_status(
         pcb::launch_k(sum_pflows_tc05_kernel<TKC, MODIFIED, ATOMIC, SPLIT>, dim3((unsigned)num_tiles * cs),
                       dim3(kThreads), smem, s, (unsigned)cs, nf, nm, em, ld, B, params, pf, tiles, rpb_log2, cids,
-                      pids, pfids, slice, vec, pcb::status_word()),
+                      pids, pfids, slice, vec, deltas, nlay, pcb::status_word()),
         "pcb_sum_pflows_tc05");
 }
 
 template <int TKC, bool SPLIT>
 int launch_flags(int cs, bool modified, bool atomic, const float* nf, const float* nm, const float* em, int64_t ld,
                  int B, const float* params, float* pf, const PcbPflowTile* tiles, int num_tiles, int rpb_log2,
-                 const int* cids, const int* pids, const int* pfids, cudaStream_t s, bool vec) {
+                 const int* cids, const int* pids, const int* pfids, cudaStream_t s, bool vec, const int* deltas,
+                 int nlay) {
 #define PCB_PF(M, A) \
-    launch<TKC, M, A, SPLIT>(cs, nf, nm, em, ld, B, params, pf, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec)
+    launch<TKC, M, A, SPLIT>(cs, nf, nm, em, ld, B, params, pf, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec, \
+                             deltas, nlay)
     if (modified) return atomic ? PCB_PF(true, true) : PCB_PF(true, false);
     return atomic ? PCB_PF(false, true) : PCB_PF(false, false);
 #undef PCB_PF
@@ -378,14 +388,16 @@ int launch_flags(int cs, bool modified, bool atomic, const float* nf, const floa
 
 }  // namespace
 
-extern "C" int pcb_sum_pflows_tc05(const float* node_flows, const float* node_mars, const float* element_mars,
-                                   int64_t ld, int32_t B, const float* params, float* param_flows,
-                                   const PcbPflowTile* tiles, int32_t num_tiles, int32_t rows_per_block,
-                                   const int32_t* cids, const int32_t* pids, const int32_t* pfids, int32_t modified,
-                                   int32_t atomic, int32_t tile_children, int32_t prec, void* stream) {
+namespace {
+
+int pflows_tc05_impl(const float* node_flows, const float* node_mars, const float* element_mars, int64_t ld, int32_t B,
+                     const float* params, float* param_flows, const PcbPflowTile* tiles, int32_t num_tiles,
+                     int32_t rows_per_block, const int32_t* cids, const int32_t* pids, const int32_t* pfids,
+                     int32_t modified, int32_t atomic, int32_t tile_children, int32_t prec, const int32_t* deltas,
+                     int32_t nlay, void* stream) {
     if (!node_flows || !node_mars || !element_mars || !params || !param_flows || !tiles || !cids || !pids || !pfids ||
         B <= 0 || ld < B || num_tiles < 0 || rows_per_block <= 0 || (rows_per_block & (rows_per_block - 1)) ||
-        (tile_children != 64 && tile_children != 128) || prec < 1 || prec > 2)
+        (tile_children != 64 && tile_children != 128) || prec < 1 || prec > 2 || nlay < 1 || (nlay > 1 && !deltas))
         return pcb::set_error(PCB_E_ARG, "pcb_sum_pflows_tc05: bad arguments");
     if (num_tiles == 0) return PCB_OK;
     int rpb_log2 = 0;
@@ -404,8 +416,31 @@ extern "C" int pcb_sum_pflows_tc05(const float* node_flows, const float* node_ma
     cudaStream_t s = pcb::as_stream(stream);
     const bool mod = modified != 0, at = atomic != 0, split = prec == 2;
 #define PCB_PK(T, S) \
-    launch_flags<T, S>(cs, mod, at, node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec)
+    launch_flags<T, S>(cs, mod, at, node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles, rpb_log2, cids, pids, pfids, s, vec, deltas, nlay)
     if (tile_children == 64) return split ? PCB_PK(64, true) : PCB_PK(64, false);
     return split ? PCB_PK(128, true) : PCB_PK(128, false);
 #undef PCB_PK
+}
+
+}  // namespace
+
+extern "C" int pcb_sum_pflows_tc05(const float* node_flows, const float* node_mars, const float* element_mars,
+                                   int64_t ld, int32_t B, const float* params, float* param_flows,
+                                   const PcbPflowTile* tiles, int32_t num_tiles, int32_t rows_per_block,
+                                   const int32_t* cids, const int32_t* pids, const int32_t* pfids, int32_t modified,
+                                   int32_t atomic, int32_t tile_children, int32_t prec, void* stream) {
+    return pflows_tc05_impl(node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles,
+                            rows_per_block, cids, pids, pfids, modified, atomic, tile_children, prec, nullptr, 1,
+                            stream);
+}
+
+extern "C" int pcb_sum_pflows_tc05_tied(const float* node_flows, const float* node_mars, const float* element_mars,
+                                        int64_t ld, int32_t B, const float* params, float* param_flows,
+                                        const PcbPflowTile* tiles, int32_t num_tiles, int32_t rows_per_block,
+                                        const int32_t* cids, const int32_t* pids, const int32_t* pfids,
+                                        int32_t modified, int32_t atomic, int32_t tile_children, int32_t prec,
+                                        const int32_t* row_deltas, int32_t num_layers, void* stream) {
+    return pflows_tc05_impl(node_flows, node_mars, element_mars, ld, B, params, param_flows, tiles, num_tiles,
+                            rows_per_block, cids, pids, pfids, modified, atomic, tile_children, prec, row_deltas,
+                            num_layers, stream);
 }

@@ -847,6 +847,9 @@ class SumLayer(Layer):
         if allow_modify_flows and not kwargs.get("_flows_modified"):
             nat.call("pcb_modify_flows", nat.ptr(node_flows), nat.ptr(node_mars), ld, B, self._layer_nid_range[0],
                      self._layer_nid_range[1], nat.stream())
+        skip = kwargs.get("_pflow_skip")
+        if skip and id(self) in skip:  # the circuit launches them once for this layer's tied set
+            param_flows = None
         # The parameter flows only read this layer's node flows / mars and its children's element
         # values, so with a side stream they run concurrently with the element flows (and with
         # everything the caller issues next on the current stream).

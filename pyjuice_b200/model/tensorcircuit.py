@@ -241,6 +241,16 @@ class TensorCircuit(nn.Module):
         self.num_root_nodes = self.root_ns.num_nodes
         self._root_node_range = (self.num_nodes - self.num_root_nodes, self.num_nodes)
         self._node2tiednodes = node2tiednodes
+        # The source of a tied set shares its parameter-flow slots with up to
+        # max_tied_ns_per_parflow_block - 1 tied vectors in other layers, whose parameter
+        # flows may run at the same time on other streams: its layer adds with atomics too.
+        sources = {id(ns.get_source_ns()) for group in self.inner_layer_groups if group.is_sum()
+                   for layer in group for ns in layer.nodes if ns.is_tied()}
+        for group in self.inner_layer_groups:
+            if group.is_sum():
+                for layer in group:
+                    if any(id(ns) in sources for ns in layer.nodes):
+                        layer._has_tied = True
         self._build_em_tables()
         self._plan_node_flow_init()
         self._plan_product_fusion()
@@ -619,6 +629,56 @@ class TensorCircuit(nn.Module):
                     share("el", eg, "tiles", "pack", eg["cbs"], layer.block_size, eg["kw"], False)
                     share("elch", eg, "ch", "ch_pack", eg["cbs"], layer.block_size, eg["kw"], True)
 
+    # Parameter flows of a tied set of sum layers (the time steps of a homogeneous HMM) in one
+    # launch (pcb_sum_pflows_tc05_tied) once the last of them has its node flows, instead of
+    # one launch per layer that re-reads and re-writes the shared flow slots.
+    tied_pflows = True
+
+    def _tied_pflow_sets(self, modify_of: dict):
+        """Tied sets of sum layers for pcb_sum_pflows_tc05_tied (cached per flow-rewrite
+        pattern): layers whose parameter-flow tables (64-child tiles) agree except for a
+        constant shift of their node rows and of their children's element rows, with the same
+        parameters and flow slots, block size and rewrite mode. Each set: its members, the
+        group of the member that the backward pass reaches last (smallest group index; its
+        tables are the reference), and per member (node row, element row) shifts relative to
+        it, the element shift including the distance between the members' element-value
+        regions."""
+        key = (self.device.type, self.device.index, tuple(sorted(modify_of.items())))
+        cache = self.__dict__.setdefault("_tied_pflow_cache", dict())
+        if key in cache:
+            return cache[key]
+        by_key = dict()
+        for gi, group in enumerate(self.inner_layer_groups):
+            if not group.is_sum():
+                continue
+            for layer in group:
+                if not layer._has_tied:
+                    continue
+                d = layer._desc(self.device)
+                pt = d["pf_tiles"].cpu().numpy().astype(np.int64)
+                if pt.shape[0] == 0:
+                    continue
+                krow = d["krow"].cpu().numpy().astype(np.int64)
+                h = hashlib.sha1(np.ascontiguousarray(pt[:, 1:]).tobytes())
+                h.update((pt[:, 0] - pt[0, 0]).tobytes())
+                h.update((krow - krow[0]).tobytes())
+                h.update(d["kw"].cpu().numpy().astype(np.int64).tobytes())
+                h.update(d["kpf"].cpu().numpy().astype(np.int64).tobytes())
+                k = (layer.block_size, bool(modify_of.get(gi)), pt.shape[0], h.hexdigest())
+                by_key.setdefault(k, []).append((gi, layer, int(pt[0, 0]), int(krow[0])))
+        sets = []
+        for members in by_key.values():
+            if len(members) < 2:
+                continue
+            members.sort(key=lambda m: m[0])
+            rgi, _, rn, rk = members[0]
+            roff = self._em_region[rgi - 1][0]
+            deltas = [(n - rn, (self._em_region[gi - 1][0] - roff) + (k - rk)) for gi, _, n, k in members]
+            sets.append(dict(last_gi=rgi, ref=members[0][1], layers=[m[1] for m in members],
+                             deltas=torch.tensor(deltas, dtype=torch.int32).reshape(-1).to(self.device)))
+        cache[key] = sets
+        return sets
+
     def _multi_pack(self, jobs) -> bool:
         """All given weight packs (``SumLayer.forward_pack_job`` tuples) in one launch on the
         current stream; returns whether anything was launched. A buffer named by several jobs
@@ -926,6 +986,15 @@ class TensorCircuit(nn.Module):
                                                              backward=True):
                 fuse_bw[g] = fz
         fused_prod = set(g - 1 for g in fuse_bw)
+        # parameter flows of tied sets in one launch each (tcgen05 form, resident element values)
+        pprec = 0 if force_use_fp32 or B < 16 else _mma(SumLayer.bf16_form)
+        tied_sets = []
+        if (TensorCircuit.tied_pflows and compute_param_flows and plain and pprec > 0 and
+                not self.recompute_element_values and SumLayer.pflow_tc05 is not False and
+                SumLayer.pflow_tile_children in (None, 0, 64)):
+            tied_sets = self._tied_pflow_sets({g: rewrites(g) for g, grp in enumerate(self.inner_layer_groups)
+                                               if grp.is_sum()})
+        pflow_skip = {id(l) for ts in tied_sets for l in ts["layers"]}
         rw_flags, rewritten = (self._rewrite_plan(fused_prod) if (TensorCircuit.fuse_flow_rewrite and
                                                                   allow_modify_flows and not logspace_flows)
                                else (dict(), set()))
@@ -966,8 +1035,27 @@ class TensorCircuit(nn.Module):
                                allow_modify_flows=modify, logspace_flows=logspace_flows,
                                force_use_fp32=force_use_fp32, _pflow_stream=pstream, _fuse_bw=fz,
                                _flows_modified=layer_id in rewritten, propagation_alg=alg,
-                               negate_pflows=negate_pflows, **kwargs)
+                               negate_pflows=negate_pflows, _pflow_skip=pflow_skip, **kwargs)
                 turn += 1
+                for ts in tied_sets:
+                    if ts["last_gi"] != layer_id:
+                        continue
+                    # every member has its (rewritten) node flows now
+                    ev = torch.cuda.Event()
+                    ev.record(main)
+                    side = sides[turn % len(sides)]
+                    side.wait_event(ev)
+                    ref = ts["ref"]
+                    rd = ref._desc(self.device)
+                    pt = rd["pf_tiles"]
+                    with torch.cuda.stream(side):
+                        nat.call("pcb_sum_pflows_tc05_tied", nat.ptr(self.node_flows), nat.ptr(self.node_mars),
+                                 nat.ptr(self._em_view(layer_id - 1)), self.node_mars.stride(0), B,
+                                 nat.ptr(self.params), nat.ptr(self.param_flows), nat.ptr(pt), pt.size(0),
+                                 ref.block_size, nat.ptr(rd["krow"]), nat.ptr(rd["kw"]), nat.ptr(rd["kpf"]),
+                                 1 if modify else 0, 1, 64, pprec, nat.ptr(ts["deltas"]), len(ts["layers"]),
+                                 nat.stream())
+                    turn += 1
         for side in sides:
             main.wait_stream(side)
 

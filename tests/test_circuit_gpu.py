@@ -536,3 +536,39 @@ def test_shared_tied_packs_equal_separate(H, cuda_device):
         TensorCircuit.share_tied_packs = saved
     for a, b in zip(out[0], out[1]):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("H,homogeneous", [(64, True), (256, True), (512, True), (256, False)])
+def test_tied_set_parameter_flows(H, homogeneous, cuda_device):
+    """Parameter flows of a tied set (the time steps of a homogeneous HMM, source included)
+    in one launch (pcb_sum_pflows_tc05_tied) against one launch per layer: the same flows up
+    to the order of the FP32 sums (split bf16, two backward passes accumulated), and against
+    the FP64 oracle within the split-bf16 bound. Without tied transitions nothing changes."""
+    from pyjuice_b200.model.tensorcircuit import TensorCircuit
+    saved = TensorCircuit.tied_pflows
+    out = []
+    try:
+        for on in (False, True):
+            TensorCircuit.tied_pflows = on
+            torch.manual_seed(0)
+            pc = juice.compile(juice.structures.HMM(8, H, 50, homogeneous=homogeneous)).to(cuda_device)
+            x = torch.randint(0, 50, (128, 8), generator=torch.Generator().manual_seed(1)).to(cuda_device)
+            pc.init_param_flows(flows_memory=0.0)
+            for _ in range(2):
+                lls = pc(x, force_use_bf16=True)
+                lls.mean().backward()
+            if on:
+                sets = pc.__dict__.get("_tied_pflow_cache", {})
+                assert bool(sum(len(v) for v in sets.values())) == homogeneous
+            out.append((pc, x, pc.param_flows.double().clone()))
+    finally:
+        TensorCircuit.tied_pflows = saved
+    a, b = out[0][2], out[1][2]
+    assert (a - b).abs().max() <= 1e-5 * a.abs().max()
+    pc, x = out[1][0], out[1][1].cpu().numpy()
+    lay = orc.layout_from_circuit(pc)
+    p0 = pc.params.double().cpu().numpy()
+    q0 = pc.input_layer_group[0].params.double().cpu().numpy()
+    nm, ems, _ = orc.forward(lay, p0, q0, x)
+    _, pf_o, _ = orc.backward(lay, p0, x, nm, ems)
+    assert np.abs(b.cpu().numpy() - 2 * pf_o).max() <= 2e-3 * np.abs(2 * pf_o).max()
