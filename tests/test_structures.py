@@ -1,7 +1,9 @@
 """The PD and HMM generators build the same circuits as the reference's (structures.npz):
 the compiled layouts are identical, and the oracle evaluates the reference's parameters on
 our layout to the reference's log-likelihoods (and, for the homogeneous HMM, its flows and
-EM step with tied transition and emission vectors). CPU only."""
+EM step with tied transition and emission vectors). Also the host plans that tied layers
+enable (shared packed weights, one parameter-flow launch per tied set) and the
+DiscreteLogistic layer's layout. CPU only."""
 
 import numpy as np
 import torch
@@ -85,3 +87,25 @@ def test_tied_hmm_layers_share_packed_weights():
     pc._share_tied_packs()
     fw = [l._desc(pc.device)["fw_pack"].data_ptr() for g in pc.inner_layer_groups if g.is_sum() for l in g]
     assert len(set(fw)) == len(fw)
+
+
+def test_tied_hmm_layers_form_one_parameter_flow_set():
+    """The tied-set plan of the parameter flows: a homogeneous HMM's transition layers (the
+    tied time steps and their source) form one set whose node / element row shifts follow the
+    layers' positions; the source layer adds with atomics like its tied layers; an HMM
+    without tied transitions has no set. CPU only (planning, no launch)."""
+    pc = juice.compile(juice.structures.HMM(8, 64, 10, homogeneous=True))
+    sums = [(gi, l) for gi, g in enumerate(pc.inner_layer_groups) if g.is_sum() for l in g]
+    assert all(l._has_tied for _, l in sums[:-1]) and not sums[-1][1]._has_tied  # the root is untied
+    sets = pc._tied_pflow_sets({gi: False for gi, _ in sums})
+    assert len(sets) == 1
+    ts = sets[0]
+    assert len(ts["layers"]) == len(sums) - 1 and ts["last_gi"] == sums[0][0]
+    deltas = ts["deltas"].view(-1, 2).numpy()
+    ref = ts["ref"]
+    for (dn, de), layer in zip(deltas, ts["layers"]):
+        assert dn == layer._layer_nid_range[0] - ref._layer_nid_range[0]
+        assert de % 128 == 0  # element-value regions of 2 x 64 rows per time step
+    pc = juice.compile(juice.structures.HMM(8, 64, 10, homogeneous=False))
+    sums = [(gi, l) for gi, g in enumerate(pc.inner_layer_groups) if g.is_sum() for l in g]
+    assert pc._tied_pflow_sets({gi: False for gi, _ in sums}) == []
